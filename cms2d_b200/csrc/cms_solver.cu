@@ -1,0 +1,690 @@
+// libcmsgpu: B200 (sm_100a) drop-in for CMS-Flow's solve() boundary.
+//
+// Host driver of the device kernels in cms_krylov.cuh.  One handle owns a CUDA
+// stream, the device-order sparsity pattern and every work buffer; the
+// per-call path allocates nothing once the handle has seen a call of the same
+// precision.  Scalars of the Krylov recurrences stay on the device; the host
+// only enqueues kernels and polls the device `done` flag between chunks of
+// iterations, so a converged solve stops at exactly the iteration the
+// reference's stopping test selects (later kernels see `done` and return).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "cms_common.cuh"
+#include "cms_krylov.cuh"
+#include "cms_order.h"
+#include "cmsgpu.h"
+
+static char g_last_error[512] = "";
+
+namespace cms {
+
+#define CMS_CUDA(call)                                                                   \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess) {                                                             \
+      std::snprintf(g_last_error, sizeof(g_last_error), "%s:%d %s: %s", __FILE__, __LINE__, #call, \
+                    cudaGetErrorString(e_));                                             \
+      return CMS_DEVICE_ERROR;                                                           \
+    }                                                                                    \
+  } while (0)
+
+
+template <typename T>
+struct Mat {
+  T* aoff = nullptr;
+  T* diag = nullptr;
+  T* luoff = nullptr;
+  T* invd = nullptr;
+};
+
+template <typename T>
+struct Work {
+  T *b = nullptr, *x = nullptr, *r = nullptr, *r0 = nullptr, *p = nullptr, *u = nullptr, *v = nullptr, *z = nullptr;
+  T* vv[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+};
+
+template <typename T>
+struct Staging {  // natural-order copies for the host-pointer entry points
+  T *acoef = nullptr, *ss = nullptr, *sp = nullptr, *res = nullptr, *phi = nullptr;
+};
+
+}  // namespace cms
+
+struct cms_solver {
+  cms::HostPattern hp;
+  cms_solver_opts opts{};
+  cudaStream_t stream = nullptr;
+  int dev = 0;
+  // pattern
+  int *d_perm = nullptr, *d_iperm = nullptr, *d_c2c = nullptr, *d_ncface = nullptr, *d_iwet = nullptr,
+      *d_col = nullptr;
+  signed char *d_fslot = nullptr, *d_nup = nullptr;
+  int K = 0;
+  cms::GroupTab tab{};           // all-row launches
+  std::vector<int> gblocks; // blocks per group
+  // numeric buffers
+  cms::Mat<double> A64;
+  cms::Mat<float> A32;
+  cms::Work<double> W64;
+  cms::Work<float> W32;
+  double* ir_r64 = nullptr;  // refinement: FP64 residual scratch (unused when null)
+  cms::DevState* d_st = nullptr;
+  cms::DevState* h_st = nullptr;  // pinned mirror
+  double* d_part = nullptr;
+  int max_blocks = 0;
+  cms::Staging<double> S64;
+  cms::Staging<float> S32;
+  size_t bytes = 0;
+  long long launches = 0;
+  std::vector<void*> allocs;
+
+  template <typename P>
+  int alloc(P** p, size_t count) {
+    size_t nb = std::max<size_t>(count, 1) * sizeof(P);
+    CMS_CUDA(cudaMalloc((void**)p, nb));
+    CMS_CUDA(cudaMemsetAsync(*p, 0, nb, stream));
+    allocs.push_back((void*)*p);
+    bytes += nb;
+    return CMS_OK;
+  }
+};
+
+namespace cms {
+
+using Solver = ::cms_solver;
+
+static inline int nblk(int rows) { return (rows + TPB - 1) / TPB; }
+
+#define CHK(...)                     \
+  do {                               \
+    int rc_ = (__VA_ARGS__);         \
+    if (rc_ != CMS_OK) return rc_;   \
+  } while (0)
+
+#define LAUNCH_CHECK(S)                          \
+  do {                                           \
+    (S)->launches++;                             \
+    cudaError_t e_ = cudaGetLastError();         \
+    if (e_ != cudaSuccess) {                     \
+      std::snprintf(g_last_error, sizeof(g_last_error), "launch: %s", cudaGetErrorString(e_)); \
+      return CMS_DEVICE_ERROR;                   \
+    }                                            \
+  } while (0)
+
+template <typename T>
+static int alloc_precision(Solver* S, Mat<T>& A, Work<T>& W) {
+  const size_t n = S->hp.n, K = std::max(S->K, 1);
+  CHK(S->alloc(&A.aoff, K * n));
+  CHK(S->alloc(&A.diag, n));
+  CHK(S->alloc(&A.luoff, K * n));
+  CHK(S->alloc(&A.invd, n));
+  CHK(S->alloc(&W.b, n));
+  CHK(S->alloc(&W.x, n));
+  CHK(S->alloc(&W.r, n));
+  CHK(S->alloc(&W.r0, n));
+  CHK(S->alloc(&W.p, n));
+  CHK(S->alloc(&W.u, n));
+  CHK(S->alloc(&W.v, n));
+  CHK(S->alloc(&W.z, n));
+  for (int j = 1; j <= 4; ++j) CHK(S->alloc(&W.vv[j], n));
+  return CMS_OK;
+}
+
+template <typename T>
+static int alloc_staging(Solver* S, Staging<T>& st) {
+  if (st.acoef) return CMS_OK;
+  const size_t nD = S->hp.nD, nmf = S->hp.nmf;
+  CHK(S->alloc(&st.acoef, nD * nmf));
+  CHK(S->alloc(&st.ss, nD));
+  CHK(S->alloc(&st.sp, nD));
+  CHK(S->alloc(&st.res, nD));
+  CHK(S->alloc(&st.phi, nD));
+  return CMS_OK;
+}
+
+static int create(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, const int* ncface, const int* iwet,
+                  const cms_solver_opts* opts, Solver** out) {
+  if (!out || !cell2cell || !ncface || ncells <= 0 || ncellsD < ncells || nmaxfaces <= 0 || nmaxfaces > KMAX)
+    return CMS_BAD_ARGUMENT;
+  auto* S = new cms_solver();
+  if (opts) S->opts = *opts; else cms_solver_default_opts(&S->opts);
+  std::string err = build_pattern(ncells, ncellsD, nmaxfaces, cell2cell, ncface, S->opts.ordering, S->hp);
+  if (!err.empty()) {
+    std::snprintf(g_last_error, sizeof(g_last_error), "%s", err.c_str());
+    delete S;
+    return CMS_BAD_ARGUMENT;
+  }
+  HostPattern& P = S->hp;
+  if (P.KL > KMAX || P.KU > KMAX) {
+    std::snprintf(g_last_error, sizeof(g_last_error), "more than %d lower/upper couplings in a row", KMAX);
+    delete S;
+    return CMS_UNSUPPORTED;
+  }
+  S->K = P.KL + P.KU;
+  int rc = CMS_OK;
+  auto fail = [&](int code) { cms_solver_destroy(S); return code; };
+  if (cudaGetDevice(&S->dev) != cudaSuccess) return fail(CMS_DEVICE_ERROR);
+  if (cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(CMS_DEVICE_ERROR);
+  const size_t n = P.n, nD = P.nD, nmf = P.nmf, K = std::max(S->K, 1);
+  if ((rc = S->alloc(&S->d_perm, n)) || (rc = S->alloc(&S->d_iperm, n)) || (rc = S->alloc(&S->d_c2c, nD * nmf)) ||
+      (rc = S->alloc(&S->d_ncface, nD)) || (rc = S->alloc(&S->d_iwet, nD)) || (rc = S->alloc(&S->d_col, K * n)) ||
+      (rc = S->alloc(&S->d_fslot, n * nmf)) || (rc = S->alloc(&S->d_nup, n)))
+    return fail(rc);
+  cudaStream_t s = S->stream;
+  if (cudaMemcpyAsync(S->d_perm, P.perm.data(), n * sizeof(int), cudaMemcpyHostToDevice, s) ||
+      cudaMemcpyAsync(S->d_iperm, P.iperm.data(), n * sizeof(int), cudaMemcpyHostToDevice, s) ||
+      cudaMemcpyAsync(S->d_c2c, cell2cell, nD * nmf * sizeof(int), cudaMemcpyHostToDevice, s) ||
+      cudaMemcpyAsync(S->d_ncface, ncface, nD * sizeof(int), cudaMemcpyHostToDevice, s) ||
+      cudaMemcpyAsync(S->d_col, P.col.data(), P.col.size() * sizeof(int), cudaMemcpyHostToDevice, s) ||
+      cudaMemcpyAsync(S->d_fslot, P.fslot.data(), n * nmf, cudaMemcpyHostToDevice, s) ||
+      cudaMemcpyAsync(S->d_nup, P.nup.data(), n, cudaMemcpyHostToDevice, s))
+    return fail(CMS_DEVICE_ERROR);
+  {
+    std::vector<int> w(nD, 1);
+    if (iwet) std::memcpy(w.data(), iwet, nD * sizeof(int));
+    if (cudaMemcpyAsync(S->d_iwet, w.data(), nD * sizeof(int), cudaMemcpyHostToDevice, s) ||
+        cudaStreamSynchronize(s))
+      return fail(CMS_DEVICE_ERROR);
+  }
+  // group tables
+  S->gblocks.resize(P.G);
+  int tot = 0;
+  for (int g = 0; g < P.G; ++g) {
+    S->gblocks[g] = nblk(P.gstart[g + 1] - P.gstart[g]);
+    tot += S->gblocks[g];
+  }
+  GroupTab& t = S->tab;
+  std::memset(&t, 0, sizeof(t));
+  if (P.G <= MAXG) {
+    t.ng = P.G;
+    int b = 0;
+    for (int g = 0; g < P.G; ++g) {
+      t.start[g] = P.gstart[g];
+      t.blk[g] = b;
+      t.kl[g] = P.gkl[g];
+      t.ku[g] = P.gku[g];
+      b += S->gblocks[g];
+    }
+    t.start[P.G] = P.gstart[P.G];
+    t.blk[P.G] = b;
+  } else {  // level schedule: one merged group with the global slot bounds
+    t.ng = 1;
+    t.start[0] = 0;
+    t.start[1] = P.n;
+    t.blk[0] = 0;
+    t.blk[1] = nblk(P.n);
+    t.kl[0] = P.KL;
+    t.ku[0] = P.KU;
+  }
+  S->max_blocks = std::max(tot, std::max(t.blk[t.ng], nblk(P.n))) + 1;
+  if ((rc = S->alloc(&S->d_part, (size_t)3 * S->max_blocks)) || (rc = S->alloc(&S->d_st, 1))) return fail(rc);
+  if (cudaMallocHost((void**)&S->h_st, sizeof(DevState)) != cudaSuccess) return fail(CMS_DEVICE_ERROR);
+  if ((rc = alloc_precision(S, S->A64, S->W64)) || (rc = alloc_precision(S, S->A32, S->W32))) return fail(rc);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return fail(CMS_DEVICE_ERROR);
+  *out = S;
+  return CMS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Launch helpers
+
+template <typename T>
+static int factor(Solver* S, Mat<T>& A) {
+  const HostPattern& P = S->hp;
+  for (int g = 0; g < P.G; ++g) {
+    const int r0 = P.gstart[g], r1 = P.gstart[g + 1];
+    if (r1 <= r0) continue;
+    k_ilu0<T><<<nblk(r1 - r0), TPB, 0, S->stream>>>(P.n, r0, r1, P.KL, P.gkl[g], P.gku[g], S->d_col, S->d_nup,
+                                                     A.aoff, A.diag, A.luoff, A.invd);
+    LAUNCH_CHECK(S);
+  }
+  return CMS_OK;
+}
+
+template <typename T, int MODE>
+static int sweep_fwd(Solver* S, Mat<T>& A, Work<T>& W, int step, const T* yin, T* p, T* r, const T* u, T* x) {
+  const HostPattern& P = S->hp;
+  GmVecs gv;
+  for (int j = 0; j < 5; ++j) gv.v[j] = W.vv[j];
+  for (int g = 0; g < P.G; ++g) {
+    const int r0 = P.gstart[g], r1 = P.gstart[g + 1];
+    if (r1 <= r0) continue;
+    k_fwd<T, MODE><<<nblk(r1 - r0), TPB, 0, S->stream>>>(P.n, r0, r1, P.gkl[g], step, S->d_col, A.luoff, W.z, yin, p,
+                                                         r, u, x, gv, S->d_st);
+    LAUNCH_CHECK(S);
+  }
+  return CMS_OK;
+}
+
+template <typename T, bool FINAL>
+static int sweep_bwd(Solver* S, Mat<T>& A, Work<T>& W, T* x, int need_active) {
+  const HostPattern& P = S->hp;
+  for (int g = P.G - 1; g >= 0; --g) {
+    const int r0 = P.gstart[g], r1 = P.gstart[g + 1];
+    if (r1 <= r0) continue;
+    k_bwd<T, FINAL><<<nblk(r1 - r0), TPB, 0, S->stream>>>(P.n, r0, r1, P.KL, P.gku[g], S->d_col, A.luoff, A.invd, W.z,
+                                                          x, need_active, S->d_st);
+    LAUNCH_CHECK(S);
+  }
+  return CMS_OK;
+}
+
+static int poll_done(Solver* S, bool& done) {
+  CMS_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, S->stream));
+  CMS_CUDA(cudaStreamSynchronize(S->stream));
+  done = S->h_st->done != 0;
+  return CMS_OK;
+}
+
+// One BiCGStab iteration (pbicgstab.f90:41-96) = 4G + 3 launches.
+template <typename T>
+static int bicg_iter(Solver* S, Mat<T>& A, Work<T>& W) {
+  const HostPattern& P = S->hp;
+  const int nb_all = S->tab.blk[S->tab.ng];
+  CHK((sweep_fwd<T, FWD_BICG_P>(S, A, W, 0, nullptr, W.p, W.r, W.u, W.x)));
+  CHK((sweep_bwd<T, false>(S, A, W, nullptr, 0)));
+  k_spmv<T, SPMV_BICG_U><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, 0, S->d_col, A.aoff, A.diag, W.z, W.u,
+                                                        W.r0, S->d_part, S->d_st);
+  LAUNCH_CHECK(S);
+  CHK((sweep_fwd<T, FWD_BICG_R>(S, A, W, 0, nullptr, W.p, W.r, W.u, W.x)));
+  CHK((sweep_bwd<T, false>(S, A, W, nullptr, 0)));
+  k_spmv<T, SPMV_BICG_V><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, 0, S->d_col, A.aoff, A.diag, W.z, W.v,
+                                                        W.r, S->d_part, S->d_st);
+  LAUNCH_CHECK(S);
+  k_bicg_update<T><<<nblk(P.n), TPB, 0, S->stream>>>(P.n, W.z, W.v, W.x, W.r, W.r0, S->d_part, S->d_st);
+  LAUNCH_CHECK(S);
+  return CMS_OK;
+}
+
+// BiCGStab from x (or 0) on b, ending when the device stopping test fires.
+template <typename T>
+static int run_bicgstab(Solver* S, Mat<T>& A, Work<T>& W, int maxit, int norm, double tol, int xzero) {
+  const HostPattern& P = S->hp;
+  const int nb_all = S->tab.blk[S->tab.ng];
+  CHK(factor<T>(S, A));
+  k_bicg_init<T><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, xzero, maxit, norm, tol, S->d_col, A.aoff, A.diag,
+                                                W.b, W.x, W.r, W.r0, W.p, W.u, W.v, S->d_part, S->d_st);
+  LAUNCH_CHECK(S);
+  int issued = 0, chunk = 2;
+  while (issued < maxit) {
+    const int c = std::min(chunk, maxit - issued);
+    for (int q = 0; q < c; ++q) CHK(bicg_iter<T>(S, A, W));
+    issued += c;
+    bool done = false;
+    CHK(poll_done(S, done));
+    if (done) break;
+    chunk = std::min(chunk * 2, 16);
+  }
+  return CMS_OK;
+}
+
+// GMRES(3) restarts (pgmres.f90:129-241).
+template <typename T>
+static int run_gmres(Solver* S, Mat<T>& A, Work<T>& W, int maxit, double tol) {
+  const HostPattern& P = S->hp;
+  const int nb_all = S->tab.blk[S->tab.ng];
+  CHK(factor<T>(S, A));
+  k_gm_start<<<1, 1, 0, S->stream>>>(S->d_st, maxit, tol);
+  LAUNCH_CHECK(S);
+  GmVecs gv;
+  for (int j = 0; j < 5; ++j) gv.v[j] = W.vv[j];
+  for (int cyc = 0; cyc < maxit; ++cyc) {
+    k_gm_resid<T><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, S->d_col, A.aoff, A.diag, W.b, W.x, W.vv[1],
+                                                 S->d_part, S->d_st);
+    LAUNCH_CHECK(S);
+    for (int i = 1; i <= 3; ++i) {
+      CHK((sweep_fwd<T, FWD_GM_SCALE>(S, A, W, i, nullptr, nullptr, nullptr, nullptr, nullptr)));
+      CHK((sweep_bwd<T, false>(S, A, W, nullptr, 1)));
+      k_spmv<T, SPMV_GM><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, i, S->d_col, A.aoff, A.diag, W.z,
+                                                        W.vv[i + 1], W.vv[1], S->d_part, S->d_st);
+      LAUNCH_CHECK(S);
+      for (int j = 1; j <= i; ++j) {
+        k_mgs<T><<<nblk(P.n), TPB, 0, S->stream>>>(P.n, j, i, gv, S->d_part, S->d_st);
+        LAUNCH_CHECK(S);
+      }
+    }
+    CHK((sweep_fwd<T, FWD_GM_COMB>(S, A, W, 0, nullptr, nullptr, nullptr, nullptr, nullptr)));
+    CHK((sweep_bwd<T, true>(S, A, W, W.x, 0)));
+    k_gm_cycle_end<<<1, 1, 0, S->stream>>>(S->d_st);
+    LAUNCH_CHECK(S);
+    if ((cyc & 1) || cyc + 1 == maxit) {
+      bool done = false;
+      CHK(poll_done(S, done));
+      if (done) break;
+    }
+  }
+  return CMS_OK;
+}
+
+template <typename T>
+static int run_krylov(Solver* S, Mat<T>& A, Work<T>& W, int nsolv, int maxit, int norm, double tol, int xzero) {
+  if (nsolv == 3) return run_bicgstab<T>(S, A, W, maxit, norm, tol, xzero);
+  if (nsolv == 4) {
+    if (xzero) {
+      CMS_CUDA(cudaMemsetAsync(W.x, 0, sizeof(T) * S->hp.n, S->stream));
+    }
+    return run_gmres<T>(S, A, W, maxit, tol);
+  }
+  return CMS_UNSUPPORTED;
+}
+
+// FP64 residual norm^2 of the device-order system into slot (A in TA, x in TX).
+template <typename TA, typename TX>
+static int resid64(Solver* S, Mat<TA>& A, const double* b, const TX* x, double* rout, float* rout32, int slot) {
+  const HostPattern& P = S->hp;
+  k_resid64<TA, TX><<<S->tab.blk[S->tab.ng], TPB, 0, S->stream>>>(P.n, P.KL, S->tab, S->d_col, A.aoff, A.diag, b, x,
+                                                                  rout, rout32, slot, S->d_part, S->d_st);
+  LAUNCH_CHECK(S);
+  return CMS_OK;
+}
+
+// Iterative refinement: FP64 residual/correction, FP32 matrix + factor + Krylov.
+static int run_refine(Solver* S, int nsolv, int maxit, double tol, cms_solve_info* info) {
+  const HostPattern& P = S->hp;
+  const int n = P.n;
+  // A32 was written by the prologue; b64/x64 live in W64.b / W64.x.
+  CHK(factor<float>(S, S->A32));
+  int steps = 0, inner_total = 0;
+  double nrm0 = -1.0, rel = 1.0;
+  const double itol = S->opts.inner_tol > 0 ? S->opts.inner_tol : 1e-2;
+  const int imax = S->opts.inner_max > 0 ? S->opts.inner_max : 50;
+  const int rmax = S->opts.max_refine > 0 ? S->opts.max_refine : 30;
+  for (;;) {
+    CHK(resid64<double, double>(S, S->A64, S->W64.b, S->W64.x, nullptr, S->W32.b, S_NRM2));
+    CMS_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, S->stream));
+    CMS_CUDA(cudaStreamSynchronize(S->stream));
+    const double nrm = std::sqrt(S->h_st->s[S_NRM2]);
+    if (nrm0 < 0) nrm0 = nrm;
+    rel = nrm0 > 0 ? nrm / nrm0 : 0.0;
+    if (!std::isfinite(rel)) {
+      info->status = CMS_NONFINITE;
+      break;
+    }
+    if (rel <= tol || steps >= rmax || inner_total >= maxit) break;
+    // inner FP32 solve A32 d = r32 from d = 0 (factor already built)
+    if (nsolv == 3) {
+      const int nb_all = S->tab.blk[S->tab.ng];
+      k_bicg_init<float><<<nb_all, TPB, 0, S->stream>>>(n, P.KL, S->tab, 1, imax, 2, itol, S->d_col, S->A32.aoff,
+                                                        S->A32.diag, S->W32.b, S->W32.x, S->W32.r, S->W32.r0,
+                                                        S->W32.p, S->W32.u, S->W32.v, S->d_part, S->d_st);
+      LAUNCH_CHECK(S);
+      int issued = 0, chunk = 2;
+      while (issued < imax) {
+        const int c = std::min(chunk, imax - issued);
+        for (int q = 0; q < c; ++q) CHK(bicg_iter<float>(S, S->A32, S->W32));
+        issued += c;
+        bool done = false;
+        CHK(poll_done(S, done));
+        if (done) break;
+        chunk = std::min(chunk * 2, 16);
+      }
+    } else {
+      CMS_CUDA(cudaMemsetAsync(S->W32.x, 0, sizeof(float) * n, S->stream));
+      CHK(run_gmres<float>(S, S->A32, S->W32, imax, itol));
+    }
+    CMS_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, S->stream));
+    CMS_CUDA(cudaStreamSynchronize(S->stream));
+    inner_total += (nsolv == 3) ? S->h_st->iter : S->h_st->inner;
+    k_ir_correct<<<nblk(n), TPB, 0, S->stream>>>(n, S->W32.x, S->W64.x);
+    LAUNCH_CHECK(S);
+    ++steps;
+  }
+  info->iters = inner_total;
+  info->inner = inner_total;
+  info->refine_steps = steps;
+  info->relres = rel;
+  if (info->status == CMS_OK && rel > tol) info->status = CMS_NOT_CONVERGED;
+  return CMS_OK;
+}
+
+// The whole solve() on device-resident natural-order arrays.
+template <typename T>
+static int solve_dev(Solver* S, const T* acoef, T* ss, const T* sp, T* res, T* phi, T relax, int nswp, int nsolv,
+                     cms_solve_info* info) {
+  const HostPattern& P = S->hp;
+  cms_solve_info loc{};
+  if (!info) info = &loc;
+  std::memset(info, 0, sizeof(*info));
+  info->ncolors = P.G;
+  info->true_relres = -1.0;
+  if (nsolv != 3 && nsolv != 4) return info->status = CMS_UNSUPPORTED;
+  const int maxit = S->opts.max_iters > 0 ? S->opts.max_iters : nswp;
+  const double tol = S->opts.tol > 0 ? S->opts.tol : 1e-3;
+  const int norm = S->opts.norm == 2 ? 2 : 1;
+  int prec = S->opts.precision;
+  if (sizeof(T) == 4) prec = CMS_PREC_FP32;
+  const bool is64 = sizeof(T) == 8;
+  Mat<T>& A = *reinterpret_cast<Mat<T>*>(is64 ? (void*)&S->A64 : (void*)&S->A32);
+  Work<T>& W = *reinterpret_cast<Work<T>*>(is64 ? (void*)&S->W64 : (void*)&S->W32);
+  // prologue: ap, ss, res, rmom + device-order system (and FP32 copy)
+  float* a2 = (is64 && prec == CMS_PREC_FP32_REFINE) ? S->A32.aoff : nullptr;
+  float* d2 = (is64 && prec == CMS_PREC_FP32_REFINE) ? S->A32.diag : nullptr;
+  k_prologue<T, float><<<nblk(P.n), TPB, 0, S->stream>>>(P.n, P.nmf, acoef, ss, sp, res, phi, S->d_c2c, S->d_ncface,
+                                                         S->d_iwet, S->d_fslot, S->d_iperm, relax, A.aoff, A.diag,
+                                                         W.b, W.x, a2, d2, S->d_part, S->d_st);
+  LAUNCH_CHECK(S);
+  if (S->opts.verify) {
+    if (is64) CHK((resid64<double, double>(S, S->A64, S->W64.b, S->W64.x, nullptr, nullptr, S_TRUE0)));
+    else {
+      k_convert<double, float><<<nblk(P.n), TPB, 0, S->stream>>>(P.n, S->W32.b, S->W64.r);
+      LAUNCH_CHECK(S);
+      CHK((resid64<float, float>(S, S->A32, S->W64.r, S->W32.x, nullptr, nullptr, S_TRUE0)));
+    }
+  }
+  if (is64 && prec == CMS_PREC_FP32_REFINE) {
+    CHK(run_refine(S, nsolv, maxit, tol, info));
+  } else {
+    CHK(run_krylov<T>(S, A, W, nsolv, maxit, norm, tol, 0));
+  }
+  if (S->opts.verify) {
+    if (is64) CHK((resid64<double, double>(S, S->A64, S->W64.b, S->W64.x, nullptr, nullptr, S_TRUE1)));
+    else CHK((resid64<float, float>(S, S->A32, S->W64.r, S->W32.x, nullptr, nullptr, S_TRUE1)));
+  }
+  k_scatter<T, T><<<nblk(P.n), TPB, 0, S->stream>>>(P.n, S->d_perm, W.x, phi);
+  LAUNCH_CHECK(S);
+  CMS_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, S->stream));
+  CMS_CUDA(cudaStreamSynchronize(S->stream));
+  const DevState& h = *S->h_st;
+  info->rmom = h.s[S_RMOM];
+  if (!(is64 && prec == CMS_PREC_FP32_REFINE)) {
+    info->iters = h.iter;
+    info->inner = (nsolv == 4) ? h.inner : h.iter;
+    info->relres = h.s[S_RELRES];
+    if (h.nonfinite) info->status = CMS_NONFINITE;
+    else if (!h.converged) info->status = CMS_NOT_CONVERGED;
+  }
+  if (S->opts.verify) {
+    const double t0 = std::sqrt(h.s[S_TRUE0]), t1 = std::sqrt(h.s[S_TRUE1]);
+    info->true_relres = t0 > 0 ? t1 / t0 : 0.0;
+    if (!std::isfinite(t1)) info->status = CMS_NONFINITE;
+  }
+  return info->status;
+}
+
+template <typename T>
+static int solve_host(Solver* S, const T* acoef, T* ss, const T* sp, T* res, T* phi, T relax, int nswp, int nsolv,
+                      cms_solve_info* info) {
+  const bool is64 = sizeof(T) == 8;
+  Staging<T>& st = *reinterpret_cast<Staging<T>*>(is64 ? (void*)&S->S64 : (void*)&S->S32);
+  CHK(alloc_staging<T>(S, st));
+  const size_t nD = S->hp.nD, nmf = S->hp.nmf;
+  cudaStream_t s = S->stream;
+  CMS_CUDA(cudaMemcpyAsync(st.acoef, acoef, nD * nmf * sizeof(T), cudaMemcpyHostToDevice, s));
+  CMS_CUDA(cudaMemcpyAsync(st.ss, ss, nD * sizeof(T), cudaMemcpyHostToDevice, s));
+  CMS_CUDA(cudaMemcpyAsync(st.sp, sp, nD * sizeof(T), cudaMemcpyHostToDevice, s));
+  CMS_CUDA(cudaMemcpyAsync(st.phi, phi, nD * sizeof(T), cudaMemcpyHostToDevice, s));
+  const int rc = solve_dev<T>(S, st.acoef, st.ss, st.sp, st.res, st.phi, relax, nswp, nsolv, info);
+  if (rc == CMS_DEVICE_ERROR || rc == CMS_BAD_ARGUMENT || rc == CMS_UNSUPPORTED) return rc;
+  const size_t n = S->hp.n;
+  CMS_CUDA(cudaMemcpyAsync(ss, st.ss, n * sizeof(T), cudaMemcpyDeviceToHost, s));
+  CMS_CUDA(cudaMemcpyAsync(res, st.res, n * sizeof(T), cudaMemcpyDeviceToHost, s));
+  CMS_CUDA(cudaMemcpyAsync(phi, st.phi, n * sizeof(T), cudaMemcpyDeviceToHost, s));
+  CMS_CUDA(cudaStreamSynchronize(s));
+  return rc;
+}
+
+}  // namespace cms
+
+using cms::Solver;
+
+extern "C" {
+
+void cms_solver_default_opts(cms_solver_opts* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->ordering = CMS_ORDER_MULTICOLOR;
+  o->precision = CMS_PREC_FP64;
+  o->norm = 1;
+  o->tol = 1.0e-3;
+  o->max_iters = 0;
+  o->inner_tol = 1.0e-2;
+  o->inner_max = 50;
+  o->max_refine = 30;
+  o->verify = 1;
+}
+
+int cms_solver_create(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, const int* ncface,
+                      const int* iwet, const cms_solver_opts* opts, cms_solver** out) {
+  if (!out) return CMS_BAD_ARGUMENT;
+  return cms::create(ncells, ncellsD, nmaxfaces, cell2cell, ncface, iwet, opts, out);
+}
+
+int cms_solver_update_wet(cms_solver* s, const int* iwet) {
+  if (!s || !iwet) return CMS_BAD_ARGUMENT;
+  if (cudaMemcpyAsync(s->d_iwet, iwet, s->hp.nD * sizeof(int), cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
+      cudaStreamSynchronize(s->stream) != cudaSuccess)
+    return CMS_DEVICE_ERROR;
+  return CMS_OK;
+}
+
+int cms_solver_set_opts(cms_solver* s, const cms_solver_opts* o) {
+  if (!s || !o) return CMS_BAD_ARGUMENT;
+  if (o->ordering != s->opts.ordering) return CMS_BAD_ARGUMENT;  // the ordering is fixed at creation
+  s->opts = *o;
+  return CMS_OK;
+}
+
+int cms_solver_solve_d(cms_solver* s, const double* acoef, double* ss, const double* sp, double* res, double* phi,
+                       double relax, int nswp, int nsolv, cms_solve_info* info) {
+  if (!s || !acoef || !ss || !sp || !res || !phi) return CMS_BAD_ARGUMENT;
+  return cms::solve_host<double>(s, acoef, ss, sp, res, phi, relax, nswp, nsolv, info);
+}
+int cms_solver_solve_f(cms_solver* s, const float* acoef, float* ss, const float* sp, float* res, float* phi,
+                       float relax, int nswp, int nsolv, cms_solve_info* info) {
+  if (!s || !acoef || !ss || !sp || !res || !phi) return CMS_BAD_ARGUMENT;
+  return cms::solve_host<float>(s, acoef, ss, sp, res, phi, relax, nswp, nsolv, info);
+}
+int cms_solver_solve_dev_d(cms_solver* s, const double* acoef, double* ss, const double* sp, double* res,
+                           double* phi, double relax, int nswp, int nsolv, cms_solve_info* info) {
+  if (!s || !acoef || !ss || !sp || !res || !phi) return CMS_BAD_ARGUMENT;
+  return cms::solve_dev<double>(s, acoef, ss, sp, res, phi, relax, nswp, nsolv, info);
+}
+int cms_solver_solve_dev_f(cms_solver* s, const float* acoef, float* ss, const float* sp, float* res, float* phi,
+                           float relax, int nswp, int nsolv, cms_solve_info* info) {
+  if (!s || !acoef || !ss || !sp || !res || !phi) return CMS_BAD_ARGUMENT;
+  return cms::solve_dev<float>(s, acoef, ss, sp, res, phi, relax, nswp, nsolv, info);
+}
+
+int cms_solver_ncolors(const cms_solver* s) { return s ? s->hp.G : -1; }
+size_t cms_solver_device_bytes(const cms_solver* s) { return s ? s->bytes : 0; }
+int cms_solver_get_perm(const cms_solver* s, int* perm) {
+  if (!s || !perm) return CMS_BAD_ARGUMENT;
+  std::memcpy(perm, s->hp.perm.data(), s->hp.perm.size() * sizeof(int));
+  return CMS_OK;
+}
+long long cms_solver_launches(const cms_solver* s) { return s ? s->launches : 0; }
+void* cms_solver_stream(cms_solver* s) { return s ? (void*)s->stream : nullptr; }
+
+void cms_solver_destroy(cms_solver* s) {
+  if (!s) return;
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  for (void* p : s->allocs) cudaFree(p);
+  if (s->h_st) cudaFreeHost(s->h_st);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+}
+
+// ---- reference-shaped global API ----
+static cms_solver* g_solver = nullptr;
+static cms_solver_opts g_opts;
+static bool g_opts_set = false;
+static cms_solve_info g_info;
+static std::mutex g_mu;
+
+int cms_gpu_init(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, const int* ncface, const int* iwet) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (g_solver) { cms_solver_destroy(g_solver); g_solver = nullptr; }
+  if (!g_opts_set) cms_solver_default_opts(&g_opts);
+  return cms_solver_create(ncells, ncellsD, nmaxfaces, cell2cell, ncface, iwet, &g_opts, &g_solver);
+}
+int cms_gpu_set_opts(const cms_solver_opts* o) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!o) return CMS_BAD_ARGUMENT;
+  if (g_solver && o->ordering != g_opts.ordering) return CMS_BAD_ARGUMENT;
+  g_opts = *o;
+  g_opts_set = true;
+  if (g_solver) return cms_solver_set_opts(g_solver, o);
+  return CMS_OK;
+}
+int cms_gpu_update_wet(const int* iwet) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  return g_solver ? cms_solver_update_wet(g_solver, iwet) : CMS_BAD_ARGUMENT;
+}
+int cms_gpu_solve_d(int n, const double* acoef, double* ss, const double* sp, double* res, double* phi, double relax,
+                    int nswp, int nsolv, double* rmom) {
+  (void)n;  // the variable index selects relax/nswp on the caller's side
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!g_solver) return CMS_BAD_ARGUMENT;
+  int rc = cms_solver_solve_d(g_solver, acoef, ss, sp, res, phi, relax, nswp, nsolv, &g_info);
+  if (rmom) *rmom = g_info.rmom;
+  return rc;
+}
+int cms_gpu_solve_f(int n, const float* acoef, float* ss, const float* sp, float* res, float* phi, float relax,
+                    int nswp, int nsolv, float* rmom) {
+  (void)n;
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!g_solver) return CMS_BAD_ARGUMENT;
+  int rc = cms_solver_solve_f(g_solver, acoef, ss, sp, res, phi, relax, nswp, nsolv, &g_info);
+  if (rmom) *rmom = (float)g_info.rmom;
+  return rc;
+}
+int cms_gpu_last_info(cms_solve_info* info) {
+  if (!info) return CMS_BAD_ARGUMENT;
+  *info = g_info;
+  return CMS_OK;
+}
+int cms_gpu_finalize(void) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (g_solver) { cms_solver_destroy(g_solver); g_solver = nullptr; }
+  return CMS_OK;
+}
+
+int cms_order_build(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, const int* ncface, int ordering,
+                    int* perm, int* gstart, int* kl_ku) {
+  if (!cell2cell || !ncface || !perm || !gstart || !kl_ku) return -CMS_BAD_ARGUMENT;
+  cms::HostPattern P;
+  std::string err = cms::build_pattern(ncells, ncellsD, nmaxfaces, cell2cell, ncface, ordering, P);
+  if (!err.empty()) {
+    std::snprintf(g_last_error, sizeof(g_last_error), "%s", err.c_str());
+    return -CMS_BAD_ARGUMENT;
+  }
+  std::memcpy(perm, P.perm.data(), sizeof(int) * P.n);
+  std::memcpy(gstart, P.gstart.data(), sizeof(int) * (P.G + 1));
+  kl_ku[0] = P.KL;
+  kl_ku[1] = P.KU;
+  return P.G;
+}
+
+const char* cms_gpu_version(void) { return "cmsgpu 0.1 (sm_100a)"; }
+
+const char* cms_gpu_last_error(void) { return g_last_error; }
+
+}  // extern "C"

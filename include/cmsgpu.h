@@ -1,0 +1,159 @@
+/* cmsgpu.h -- C-ABI of the B200 (sm_100a) implicit-flow solver library libcmsgpu.so.
+ *
+ * The library replaces the linear-solver boundary of CMS-Flow's implicit
+ * SIMPLEC step.  All arrays follow the reference's in-memory layout:
+ *   - cells 1..ncells are active, ncells+1..ncellsD are dummy (ghost) cells;
+ *   - cell2cell(k,i), acoef(k,i) are Fortran column-major [nmaxfaces][ncellsD]
+ *     arrays: element (k,i) sits at offset (i-1)*nmaxfaces + (k-1);
+ *   - neighbour indices are 1-based; ncface(i) faces are used per cell.
+ * Every entry point returns a status: CMS_OK (0), CMS_NOT_CONVERGED (1),
+ * CMS_NONFINITE (2), CMS_DEVICE_ERROR (3), CMS_BAD_ARGUMENT (4),
+ * CMS_UNSUPPORTED (5).  The library never aborts the caller; the reference's
+ * `iconv` global (source/solvers/solv_def.f90:8) is set by the caller from
+ * the status (iconv = 0 for CMS_NONFINITE, 1 otherwise).
+ *
+ * Two calling styles are offered:
+ *   - a handle API (cms_solver_*), reentrant per handle, one CUDA stream per
+ *     handle;
+ *   - the reference-shaped global API (cms_gpu_*) that mirrors the module
+ *     state of solv_def: one implicit handle created by cms_gpu_init.
+ */
+#ifndef CMSGPU_H
+#define CMSGPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  CMS_OK = 0,
+  CMS_NOT_CONVERGED = 1,
+  CMS_NONFINITE = 2,
+  CMS_DEVICE_ERROR = 3,
+  CMS_BAD_ARGUMENT = 4,
+  CMS_UNSUPPORTED = 5
+};
+
+/* Unknown ordering used by the ILU(0) factor and its sweeps. */
+enum {
+  CMS_ORDER_MULTICOLOR = 0, /* greedy multicolour ordering: 2 colours on a Cartesian grid */
+  CMS_ORDER_NATURAL = 1     /* the reference's natural order, level-scheduled sweeps */
+};
+
+/* Arithmetic of the Krylov solve. */
+enum {
+  CMS_PREC_FP64 = 0,        /* plain FP64 drop-in (ikind=8 build) */
+  CMS_PREC_FP32_REFINE = 1, /* FP32 matrix/factor/SpMV/sweeps inside FP64 iterative refinement */
+  CMS_PREC_FP32 = 2         /* FP32 throughout (ikind=4 build); dots accumulate in FP64 */
+};
+
+typedef struct cms_solver_opts {
+  int ordering;      /* CMS_ORDER_*                                                    */
+  int precision;     /* CMS_PREC_* (used by the *_d entry points; *_f is FP32)         */
+  int norm;          /* BiCGStab stopping norm: 1 = L1 of the recursive residual
+                        (pbicgstab.f90:95), 2 = L2                                     */
+  double tol;        /* relative tolerance; the reference hard-codes 1e-3
+                        (pbicgstab.f90:95, pgmres.f90:19)                              */
+  int max_iters;     /* > 0 overrides the nswp argument                                */
+  double inner_tol;  /* refinement: relative L2 reduction asked of each FP32 solve     */
+  int inner_max;     /* refinement: iteration cap of each FP32 solve                   */
+  int max_refine;    /* refinement: cap on FP64 residual/correction steps              */
+  int verify;        /* 1: compute the FP64 true residual after the solve (one extra
+                        pass); 0: skip it (true_relres = -1)                           */
+} cms_solver_opts;
+
+typedef struct cms_solve_info {
+  int status;        /* CMS_*                                                          */
+  int iters;         /* BiCGStab iterations or GMRES restarts (refinement: all inner)  */
+  int inner;         /* GMRES Arnoldi steps (BiCGStab: iterations)                     */
+  int refine_steps;  /* FP64 refinement steps (0 outside CMS_PREC_FP32_REFINE)         */
+  double relres;     /* the ratio the stopping test last saw                           */
+  double true_relres;/* ||b - A x||_2 / ||b - A x0||_2 in FP64 after the solve         */
+  double rmom;       /* RMS of the normalised residual before the solve (solvers.f90:240) */
+  int ncolors;       /* number of groups the sweeps run (colours or levels)            */
+} cms_solve_info;
+
+typedef struct cms_solver cms_solver;
+
+/* Fills opts with the reference defaults: multicolour, FP64, L1, tol 1e-3. */
+void cms_solver_default_opts(cms_solver_opts* opts);
+
+/* solv_init (source/solvers/solvers.f90:93-202) + indexm (sparse.f90:2-70):
+ * copies the connectivity, builds the unknown ordering, the ELL sparsity
+ * pattern and the sweep schedule, and allocates all device buffers.
+ * iwet may be NULL (all wet). */
+int cms_solver_create(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, const int* ncface,
+                      const int* iwet, const cms_solver_opts* opts, cms_solver** out);
+
+/* Replaces iwet (flow_wetdry output); the pattern is unchanged. */
+int cms_solver_update_wet(cms_solver* s, const int* iwet);
+
+int cms_solver_set_opts(cms_solver* s, const cms_solver_opts* opts);
+
+/* solve(acoef,ss,sp,res,phi,n) (source/solvers/solvers.f90:205-304) with HOST
+ * arrays: ap=(sum acoef - sp)/relax; ss += (1-relax)*phi*ap; res = normalised
+ * residual; rmom = RMS(res); then BiCGStab (nsolv=3, pbicgstab.f90) or
+ * GMRES(3) (nsolv=4, pgmres.f90) preconditioned by ILU(0) of the same matrix.
+ * ss, res and phi are updated in place; nswp caps iterations (restarts). */
+int cms_solver_solve_d(cms_solver* s, const double* acoef, double* ss, const double* sp, double* res, double* phi,
+                       double relax, int nswp, int nsolv, cms_solve_info* info);
+int cms_solver_solve_f(cms_solver* s, const float* acoef, float* ss, const float* sp, float* res, float* phi,
+                       float relax, int nswp, int nsolv, cms_solve_info* info);
+
+/* Same contract with DEVICE pointers (arrays already resident in HBM, same
+ * layout).  The call is ordered on the handle's stream and returns after the
+ * solve has finished. */
+int cms_solver_solve_dev_d(cms_solver* s, const double* acoef, double* ss, const double* sp, double* res, double* phi,
+                           double relax, int nswp, int nsolv, cms_solve_info* info);
+int cms_solver_solve_dev_f(cms_solver* s, const float* acoef, float* ss, const float* sp, float* res, float* phi,
+                           float relax, int nswp, int nsolv, cms_solve_info* info);
+
+/* Number of groups the sweeps run and device bytes held by the handle. */
+int cms_solver_ncolors(const cms_solver* s);
+size_t cms_solver_device_bytes(const cms_solver* s);
+/* Device-order permutation: perm[r] = natural 0-based cell of device row r. */
+int cms_solver_get_perm(const cms_solver* s, int* perm);
+/* Kernel launches issued by the handle since creation (counted on the host). */
+long long cms_solver_launches(const cms_solver* s);
+/* The stream the handle runs on (a cudaStream_t). */
+void* cms_solver_stream(cms_solver* s);
+
+void cms_solver_destroy(cms_solver* s);
+
+/* Host-only (no device calls): the unknown ordering a handle would use.
+ * perm[r] = natural 0-based cell of device row r (ncells entries);
+ * gstart[0..G] = device-row range of each sweep group (ncells+1 entries
+ * available); kl_ku[0..1] = max lower / upper couplings per row.  Returns the
+ * number of groups G (> 0) or -CMS_BAD_ARGUMENT. */
+int cms_order_build(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, const int* ncface, int ordering,
+                    int* perm, int* gstart, int* kl_ku);
+
+/* ---- reference-shaped global API (one implicit handle, like solv_def) ---- */
+
+/* solv_init: source/solvers/solvers.f90:93-202. */
+int cms_gpu_init(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, const int* ncface, const int* iwet);
+int cms_gpu_set_opts(const cms_solver_opts* opts);
+int cms_gpu_update_wet(const int* iwet);
+/* solve(acoef,ss,sp,res,phi,n): source/solvers/solvers.f90:205.  relax, nswp
+ * and nsolv are the comvarbl values relax(n), nswp(n), nsolv; rmom receives
+ * rmom(n).  Double for the ikind=8 build, float for ikind=4. */
+int cms_gpu_solve_d(int n, const double* acoef, double* ss, const double* sp, double* res, double* phi, double relax,
+                    int nswp, int nsolv, double* rmom);
+int cms_gpu_solve_f(int n, const float* acoef, float* ss, const float* sp, float* res, float* phi, float relax,
+                    int nswp, int nsolv, float* rmom);
+/* The cms_solve_info of the last cms_gpu_solve_* call. */
+int cms_gpu_last_info(cms_solve_info* info);
+int cms_gpu_finalize(void);
+
+/* Library version string. */
+const char* cms_gpu_version(void);
+/* Text of the last error a call reported (device or argument errors). */
+const char* cms_gpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CMSGPU_H */

@@ -1,0 +1,113 @@
+"""ctypes binding of the CPU oracle (oracle/liboracle.so) -- test infrastructure.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module; the product (cms2d_b200) never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+PC_ILUTP = 0
+PC_ILU0 = 1
+
+
+def build(force: bool = False) -> str:
+    so = os.path.join(_HERE, "liboracle.so")
+    srcs = [os.path.join(_HERE, f) for f in ("cms_oracle.cpp", "cms_flow_oracle.cpp", "Makefile")]
+    if force or not os.path.exists(so) or any(os.path.getmtime(s) > os.path.getmtime(so) for s in srcs):
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return so
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        so = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(so):
+            build()
+        L = C.CDLL(so)
+        P = C.c_void_p
+        i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+        f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+        f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+        L.orc_create.restype = P
+        L.orc_create.argtypes = [C.c_int, C.c_int, C.c_int, i32p, i32p, i32p, C.c_int]
+        L.orc_destroy.argtypes = [P]
+        L.orc_nnz.argtypes = [P]
+        L.orc_nnz.restype = C.c_int
+        L.orc_pattern.argtypes = [P, i32p, i32p]
+        L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_set_threads.restype = C.c_int
+        ip = C.POINTER(C.c_int)
+        dp = C.POINTER(C.c_double)
+        L.orc_solve_d.argtypes = [P, f64p, f64p, f64p, f64p, f64p, C.c_double, C.c_int, C.c_int, C.c_int, C.c_double,
+                                  C.c_int, C.c_double, C.c_double, dp, ip, ip, dp]
+        L.orc_solve_d.restype = C.c_int
+        fp = C.POINTER(C.c_float)
+        L.orc_solve_f.argtypes = [P, f32p, f32p, f32p, f32p, f32p, C.c_float, C.c_int, C.c_int, C.c_int, C.c_float,
+                                  C.c_int, C.c_float, C.c_float, fp, ip, ip, dp]
+        L.orc_solve_f.restype = C.c_int
+        L.orc_lusol_d.argtypes = [P, f64p, f64p]
+        _LIB = L
+    return _LIB
+
+
+def set_threads(n: int) -> int:
+    return lib().orc_set_threads(int(n))
+
+
+class OracleSolver:
+    """CPU restatement of solv_init + solve (source/solvers/solvers.f90:93-304)."""
+
+    def __init__(self, grid, iwet=None, fix_last_cell: bool = True):
+        self.g = grid
+        L = lib()
+        iw = np.ones(grid.ncellsD, np.int32) if iwet is None else np.ascontiguousarray(iwet, np.int32)
+        self._h = L.orc_create(grid.ncells, grid.ncellsD, grid.nmaxfaces,
+                               np.ascontiguousarray(grid.cell2cell, np.int32),
+                               np.ascontiguousarray(grid.ncface, np.int32), iw, int(fix_last_cell))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().orc_destroy(h)
+            self._h = None
+
+    def pattern(self):
+        L = lib()
+        nnz = L.orc_nnz(self._h)
+        ia = np.zeros(self.g.ncells + 1, np.int32)
+        ja = np.zeros(nnz, np.int32)
+        L.orc_pattern(self._h, ia, ja)
+        return ia, ja
+
+    def solve(self, acoef, ss, sp, res, phi, relax=1.0, nswp=15, nsolv=3, precond=PC_ILU0, tol=1e-3, lfil=None,
+              droptol=1e-3, permtol=0.5):
+        """Arguments mirror solve(acoef,ss,sp,res,phi,n): ss, res and phi are updated in place.
+
+        Returns dict(status, rmom, iters, inner, relres).
+        """
+        L = lib()
+        if lfil is None:
+            lfil = 8 if nsolv == 4 else 35  # solvers.f90:195-199
+        dt = acoef.dtype
+        rm = (C.c_double if dt == np.float64 else C.c_float)()
+        it = C.c_int(); inner = C.c_int(); rr = C.c_double()
+        fn = L.orc_solve_d if dt == np.float64 else L.orc_solve_f
+        for a in (acoef, ss, sp, res, phi):
+            assert a.dtype == dt and a.flags.c_contiguous
+        st = fn(self._h, acoef, ss, sp, res, phi, relax, int(nswp), int(nsolv), int(precond), tol, int(lfil), droptol,
+                permtol, C.byref(rm), C.byref(it), C.byref(inner), C.byref(rr))
+        return dict(status=st, rmom=rm.value, iters=it.value, inner=inner.value, relres=rr.value)
+
+    def lusol(self, y):
+        x = np.zeros_like(y)
+        lib().orc_lusol_d(self._h, np.ascontiguousarray(y, np.float64), x)
+        return x
