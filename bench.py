@@ -1,0 +1,315 @@
+"""Benchmark of the B200 implicit hot path (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload solve] [--cells 1000000] [--precision fp32_refine|fp64]
+
+Workload "solve": the pressure-correction system of the solver sweep at 1M
+unknowns (telescoping 5-point stencil with up to two extra neighbours per face
+at refinement interfaces, seeded off-diagonals in [-1,-0.1], diagonal 1.02 x
+the off-diagonal sum, N(0,1) right-hand side), solved by ILU(0)-BiCGStab to a
+1e-6 relative FP64 residual.  One step = one solve from phi = 0.
+
+Multi-GPU: the path does not shard (the ILU(0) sweeps are global
+recurrences), so N ranks run N independent replicas and `value` counts the
+solves of all ranks over the max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "timesteps/s at 1M cells, FP32+refine vs plain FP64 GPU @1e-6 resid; HBM GB/s"
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1])); mx = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def build_solve_case(cells: int, seed: int):
+    from cms2d_b200 import grid as G
+    g = G.solver_test_grid(cells)
+    acoef, ss, sp, phi = G.random_system(g, seed=seed)
+    return g, acoef, ss, sp, phi
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from cms2d_b200 import solver as S
+
+    world, rank, local = dist_setup()
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    g, acoef, ss, sp, phi = build_solve_case(args.cells, seed=17 + rank)
+    N = g.ncells
+    solver = S.Solver(g, precision=args.precision, tol=1e-6, norm=2, verify=False, inner_tol=args.inner_tol,
+                      inner_max=args.inner_max, nsolv=3)
+    nswp = 5000
+    # device-resident inputs
+    t_acoef = torch.from_numpy(acoef).to(dev)
+    t_sp = torch.from_numpy(sp).to(dev)
+    t_ss0 = torch.from_numpy(ss).to(dev)
+    t_phi0 = torch.from_numpy(phi).to(dev)
+    t_ss = t_ss0.clone(); t_phi = t_phi0.clone(); t_res = torch.zeros_like(t_ss)
+    sstream = torch.cuda.ExternalStream(solver.stream_handle, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
+
+    def step():
+        t_ss.copy_(t_ss0); t_phi.copy_(t_phi0)
+        torch.cuda.synchronize(dev)
+        return solver.solve(t_acoef, t_ss, t_sp, t_res, t_phi, relax=1.0, nswp=nswp, nsolv=3)
+
+    for _ in range(args.warmup):
+        info = step()
+    # timed: K steps, per-step CUDA events on the solver stream, L2 flushed between steps
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    launches0 = solver.launches
+    ms_total = 0.0
+    infos = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            t_ss.copy_(t_ss0); t_phi.copy_(t_phi0)
+            flush.fill_(1.0)
+            torch.cuda.synchronize(dev)
+            e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(sstream)
+            infos.append(solver.solve(t_acoef, t_ss, t_sp, t_res, t_phi, relax=1.0, nswp=nswp, nsolv=3))
+            e1.record(sstream)
+            e1.synchronize()
+            ms_total += e0.elapsed_time(e1)
+    torch.cuda.synchronize(dev)
+    launches = solver.launches - launches0
+    if world > 1:
+        t = torch.tensor([ms_total], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+        dist.barrier()
+    ms_step = ms_total / args.steps
+    value = world * args.steps / (ms_total / 1e3)  # solves/s over all ranks
+    if args.ncu:  # profiler pass: the timed steps only
+        if world > 1:
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps({"ncu_pass": True, "ms_per_step": ms_step, "iters": infos[-1]["iters"]}), flush=True)
+        return
+
+    # true residual of the last solve (device-resident inputs unchanged)
+    solver.set_options(verify=True)
+    chk = step()
+    solver.set_options(verify=False)
+
+    # e2e: host (pinned) buffers through the C-ABI host entry point, copies included
+    h_acoef = torch.from_numpy(acoef).pin_memory().numpy()
+    h_sp = torch.from_numpy(sp).pin_memory().numpy()
+    h_ss = torch.from_numpy(ss).pin_memory().numpy()
+    h_phi = torch.from_numpy(phi).pin_memory().numpy()
+    h_res = torch.zeros(g.ncellsD, dtype=torch.float64).pin_memory().numpy()
+    e2e_ms = 0.0
+    ne2e = max(1, min(args.steps, 5))
+    for q in range(ne2e + 1):
+        h_ss[:] = ss; h_phi[:] = phi
+        flush.fill_(1.0); torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        solver.solve(h_acoef, h_ss, h_sp, h_res, h_phi, relax=1.0, nswp=nswp, nsolv=3)
+        t1 = time.perf_counter()
+        if q > 0:
+            e2e_ms += (t1 - t0) * 1e3
+    e2e_ms /= ne2e
+    h2d = acoef.nbytes + ss.nbytes + sp.nbytes + phi.nbytes
+    d2h = 3 * N * 8
+
+    # roofline: per-kernel-class events on the solver stream over K profiled steps
+    solver.profile(True)
+    solver.profile_read(reset=True)
+    for _ in range(args.steps):
+        t_ss.copy_(t_ss0); t_phi.copy_(t_phi0); flush.fill_(1.0); torch.cuda.synchronize(dev)
+        solver.solve(t_acoef, t_ss, t_sp, t_res, t_phi, relax=1.0, nswp=nswp, nsolv=3)
+    prof = solver.profile_read(reset=True)
+    solver.profile(False)
+    top = max(prof, key=lambda k: prof[k]["ms"])
+    peak, peak_kind = _peaks()
+    tot_ms = sum(v["ms"] for v in prof.values())
+    ach = prof[top]["bytes"] / (prof[top]["ms"] / 1e3) / 1e9 if prof[top]["ms"] > 0 else 0.0
+    kernels = {k: {"share": round(v["ms"] / tot_ms, 4) if tot_ms else 0, "launches": v["launches"],
+                   "avg_us": round(1e3 * v["ms"] / v["launches"], 2) if v["launches"] else 0,
+                   "GBps": round(v["bytes"] / (v["ms"] / 1e3) / 1e9, 1) if v["ms"] > 0 else 0}
+               for k, v in prof.items() if v["launches"]}
+
+    out = {
+        "metric": METRIC,
+        "value": round(value, 4),
+        "unit": "solves/s (1M-unknown pressure-correction system to 1e-6)",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms_step, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64 refine" if args.precision == "fp32_refine" else args.precision.replace("fp", "f"),
+        "data": "synthetic (seeded solver-sweep system)",
+        "config": {"workload": f"pp-system solve, {N} unknowns, telescoping 5-point+interfaces, "
+                               f"ILU0-BiCGStab to ||r||2/||r0||2<=1e-6 ({args.precision})",
+                   "cells": N, "precision": args.precision, "ordering": "multicolor",
+                   "colours": solver.ncolors, "parallelism": f"replicas x{world}",
+                   "l2": "flushed between steps (256 MB write)"},
+        "iters_per_step": infos[-1]["iters"], "refine_steps": infos[-1].get("refine_steps", 0),
+        "true_relres": chk["true_relres"],
+        "e2e": {"value": round(world * 1e3 / e2e_ms, 4), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_ms, 3)},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": top, "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(ach / peak, 4), "peak_kind": peak_kind, "traffic": None},
+        "kernels": kernels,
+    }
+    out["clocks"] = clk.summary()
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        out["cpu_baseline"] = cpu_baseline(args, g, acoef, ss, sp, phi)
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def cpu_baseline(args, g, acoef, ss, sp, phi, threads=None):
+    """The oracle port (the reference's algorithm restated) on host cores."""
+    from oracle import oracle as O
+    threads = threads or os.cpu_count()
+    O.set_threads(threads)
+    o = O.OracleSolver(g)
+    a, b, c, p = [x.copy() for x in (acoef, ss, sp, phi)]
+    r = np.zeros_like(b)
+    t0 = time.perf_counter()
+    out = o.solve(a, b, c, r, p, relax=1.0, nswp=5000, nsolv=3, precond=O.PC_ILU0, tol=1e-6, norm=2)
+    dt = time.perf_counter() - t0
+    return {"value": round(1.0 / dt, 4), "unit": "solves/s", "cores": threads, "kind": "port",
+            "sample": f"1 full solve of the same {g.ncells}-unknown system, natural-order ILU0-BiCGStab "
+                      f"(serial factor/sweeps as in the reference), {out['iters']} iterations",
+            "iters": out["iters"]}
+
+
+def run_reference(args):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return
+    g, acoef, ss, sp, phi = build_solve_case(args.cells, seed=17)
+    for _ in range(args.warmup):
+        cpu_baseline(args, g, acoef, ss, sp, phi)
+    times = []
+    for _ in range(args.steps):
+        cb = cpu_baseline(args, g, acoef, ss, sp, phi)
+        times.append(1.0 / cb["value"])
+    v = args.steps / sum(times)
+    out = {"impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": "solves/s",
+           "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": round(1e3 * sum(times) / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded solver-sweep system)",
+           "config": {"workload": f"pp-system solve, {g.ncells} unknowns, CPU oracle port", "cells": g.ncells},
+           "cpu_baseline": {"value": round(v, 4), "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
+                            "sample": "full solves of the same system"},
+           "e2e": {"value": round(v, 4), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="solve", choices=["solve"])
+    ap.add_argument("--cells", type=int, default=1_000_000)
+    ap.add_argument("--precision", default="fp32_refine", choices=["fp32_refine", "fp64"])
+    ap.add_argument("--inner-tol", type=float, default=1e-2)
+    ap.add_argument("--inner-max", type=int, default=100)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ncu", action="store_true", help="warm-up and timed steps only (profiler runs)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

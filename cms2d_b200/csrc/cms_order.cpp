@@ -89,6 +89,8 @@ std::string build_pattern(int n, int nD, int nmf, const int* cell2cell, const in
   P.nup.assign(n, 0);
   P.gkl.assign(G, 0);
   P.gku.assign(G, 0);
+  P.glo.assign(G, 0);
+  P.gup.assign(G, 0);
   int KL = 0, KU = 0;
   long long nnz = 0;
   for (int r = 0; r < n; ++r) {
@@ -108,6 +110,8 @@ std::string build_pattern(int n, int nD, int nmf, const int* cell2cell, const in
     P.nlo[r] = (signed char)nl;
     P.nup[r] = (signed char)nu;
     int g = grp[i];
+    P.glo[g] += nl;
+    P.gup[g] += nu;
     P.gkl[g] = std::max(P.gkl[g], nl);
     P.gku[g] = std::max(P.gku[g], nu);
     KL = std::max(KL, nl);

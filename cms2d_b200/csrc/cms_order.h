@@ -22,6 +22,7 @@ struct HostPattern {
   std::vector<signed char> fslot;  // [n * nmf] ELL slot of face k of natural cell i; -1 dummy/none
   std::vector<signed char> nlo, nup;  // [n] lower / upper entry counts per device row
   long long nnz_off = 0;     // stored off-diagonal couplings between active cells
+  std::vector<long long> glo, gup;  // [G] lower / upper entries stored in each group
 };
 
 // ordering: 0 = greedy multicolour over the natural order, 1 = natural order

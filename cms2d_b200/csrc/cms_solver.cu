@@ -85,6 +85,15 @@ struct cms_solver {
   size_t bytes = 0;
   long long launches = 0;
   std::vector<void*> allocs;
+  // optional per-kernel-class timing (CUDA events on the handle's stream)
+  int prof_on = 0;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  struct ProfRec { int cat; size_t ev; double bytes; };
+  std::vector<ProfRec> prof_recs;
+  double prof_ms[16] = {0};
+  double prof_bytes[16] = {0};
+  long long prof_count[16] = {0};
 
   template <typename P>
   int alloc(P** p, size_t count) {
@@ -117,6 +126,41 @@ static inline int nblk(int rows) { return (rows + TPB - 1) / TPB; }
       std::snprintf(g_last_error, sizeof(g_last_error), "launch: %s", cudaGetErrorString(e_)); \
       return CMS_DEVICE_ERROR;                   \
     }                                            \
+  } while (0)
+
+// Kernel classes timed by the profiler (cms_solver_profile_*).
+enum ProfCat : int {
+  P_PROLOGUE = 0, P_ILU0 = 1, P_FWD = 2, P_BWD = 3, P_SPMV = 4, P_VEC = 5, P_RESID64 = 6, P_SCALAR = 7,
+  P_NCAT = 8
+};
+
+static void prof_begin(Solver* S) {
+  if (!S->prof_on) return;
+  if (S->ev_used + 2 > S->ev_pool.size()) {
+    for (int q = 0; q < 256; ++q) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) { S->prof_on = 0; return; }
+      S->ev_pool.push_back(e);
+    }
+  }
+  cudaEventRecord(S->ev_pool[S->ev_used], S->stream);
+}
+
+static void prof_end(Solver* S, int cat, double bytes) {
+  if (!S->prof_on) return;
+  cudaEventRecord(S->ev_pool[S->ev_used + 1], S->stream);
+  S->prof_recs.push_back({cat, S->ev_used, bytes});
+  S->ev_used += 2;
+}
+
+// Launch with error check, launch count and optional timing; BYTES are the
+// algorithmic bytes of the launch (each array the kernel touches counted once).
+#define KLAUNCH(S, CAT, BYTES, ...)   \
+  do {                                \
+    prof_begin(S);                    \
+    __VA_ARGS__;                      \
+    LAUNCH_CHECK(S);                  \
+    prof_end(S, CAT, (double)(BYTES)); \
   } while (0)
 
 template <typename T>
@@ -239,12 +283,14 @@ static int create(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, 
 template <typename T>
 static int factor(Solver* S, Mat<T>& A) {
   const HostPattern& P = S->hp;
+  const double s = sizeof(T);
   for (int g = 0; g < P.G; ++g) {
     const int r0 = P.gstart[g], r1 = P.gstart[g + 1];
     if (r1 <= r0) continue;
-    k_ilu0<T><<<nblk(r1 - r0), TPB, 0, S->stream>>>(P.n, r0, r1, P.KL, P.gkl[g], P.gku[g], S->d_col, S->d_nup,
-                                                     A.aoff, A.diag, A.luoff, A.invd);
-    LAUNCH_CHECK(S);
+    const double R = r1 - r0, E = (double)(P.glo[g] + P.gup[g]);
+    KLAUNCH(S, P_ILU0, R * (3 * s + 1) + E * (2 * s + 4),
+            (k_ilu0<T><<<nblk(r1 - r0), TPB, 0, S->stream>>>(P.n, r0, r1, P.KL, P.gkl[g], P.gku[g], S->d_col,
+                                                              S->d_nup, A.aoff, A.diag, A.luoff, A.invd)));
   }
   return CMS_OK;
 }
@@ -252,14 +298,18 @@ static int factor(Solver* S, Mat<T>& A) {
 template <typename T, int MODE>
 static int sweep_fwd(Solver* S, Mat<T>& A, Work<T>& W, int step, const T* yin, T* p, T* r, const T* u, T* x) {
   const HostPattern& P = S->hp;
+  const double s = sizeof(T);
+  // vectors streamed per row by each mode (reads + writes)
+  const double vec = MODE == FWD_PLAIN ? 2 : MODE == FWD_BICG_P ? 5 : MODE == FWD_BICG_R ? 7 : MODE == FWD_GM_SCALE ? 3 : 4;
   GmVecs gv;
   for (int j = 0; j < 5; ++j) gv.v[j] = W.vv[j];
   for (int g = 0; g < P.G; ++g) {
     const int r0 = P.gstart[g], r1 = P.gstart[g + 1];
     if (r1 <= r0) continue;
-    k_fwd<T, MODE><<<nblk(r1 - r0), TPB, 0, S->stream>>>(P.n, r0, r1, P.gkl[g], step, S->d_col, A.luoff, W.z, yin, p,
-                                                         r, u, x, gv, S->d_st);
-    LAUNCH_CHECK(S);
+    const double R = r1 - r0, E = (double)P.glo[g];
+    KLAUNCH(S, P_FWD, R * s * vec + E * (s + 4) + (E > 0 ? R * s : 0.0),
+            (k_fwd<T, MODE><<<nblk(r1 - r0), TPB, 0, S->stream>>>(P.n, r0, r1, P.gkl[g], step, S->d_col, A.luoff,
+                                                                   W.z, yin, p, r, u, x, gv, S->d_st)));
   }
   return CMS_OK;
 }
@@ -267,12 +317,14 @@ static int sweep_fwd(Solver* S, Mat<T>& A, Work<T>& W, int step, const T* yin, T
 template <typename T, bool FINAL>
 static int sweep_bwd(Solver* S, Mat<T>& A, Work<T>& W, T* x, int need_active) {
   const HostPattern& P = S->hp;
+  const double s = sizeof(T);
   for (int g = P.G - 1; g >= 0; --g) {
     const int r0 = P.gstart[g], r1 = P.gstart[g + 1];
     if (r1 <= r0) continue;
-    k_bwd<T, FINAL><<<nblk(r1 - r0), TPB, 0, S->stream>>>(P.n, r0, r1, P.KL, P.gku[g], S->d_col, A.luoff, A.invd, W.z,
-                                                          x, need_active, S->d_st);
-    LAUNCH_CHECK(S);
+    const double R = r1 - r0, E = (double)P.gup[g];
+    KLAUNCH(S, P_BWD, R * s * (FINAL ? 5 : 3) + E * (s + 4) + (E > 0 ? R * s : 0.0),
+            (k_bwd<T, FINAL><<<nblk(r1 - r0), TPB, 0, S->stream>>>(P.n, r0, r1, P.KL, P.gku[g], S->d_col, A.luoff,
+                                                                    A.invd, W.z, x, need_active, S->d_st)));
   }
   return CMS_OK;
 }
@@ -284,6 +336,12 @@ static int poll_done(Solver* S, bool& done) {
   return CMS_OK;
 }
 
+// algorithmic bytes of one all-row matrix pass: diag + ELL values/indices + nvec vectors
+template <typename T>
+static double spmv_bytes(const Solver* S, double nvec) {
+  return (double)S->hp.n * sizeof(T) * (1 + nvec) + (double)S->hp.nnz_off * (sizeof(T) + 4);
+}
+
 // One BiCGStab iteration (pbicgstab.f90:41-96) = 4G + 3 launches.
 template <typename T>
 static int bicg_iter(Solver* S, Mat<T>& A, Work<T>& W) {
@@ -291,29 +349,31 @@ static int bicg_iter(Solver* S, Mat<T>& A, Work<T>& W) {
   const int nb_all = S->tab.blk[S->tab.ng];
   CHK((sweep_fwd<T, FWD_BICG_P>(S, A, W, 0, nullptr, W.p, W.r, W.u, W.x)));
   CHK((sweep_bwd<T, false>(S, A, W, nullptr, 0)));
-  k_spmv<T, SPMV_BICG_U><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, 0, S->d_col, A.aoff, A.diag, W.z, W.u,
-                                                        W.r0, S->d_part, S->d_st);
-  LAUNCH_CHECK(S);
+  KLAUNCH(S, P_SPMV, spmv_bytes<T>(S, 3),
+          (k_spmv<T, SPMV_BICG_U><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, 0, S->d_col, A.aoff, A.diag, W.z,
+                                                                  W.u, W.r0, S->d_part, S->d_st)));
   CHK((sweep_fwd<T, FWD_BICG_R>(S, A, W, 0, nullptr, W.p, W.r, W.u, W.x)));
   CHK((sweep_bwd<T, false>(S, A, W, nullptr, 0)));
-  k_spmv<T, SPMV_BICG_V><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, 0, S->d_col, A.aoff, A.diag, W.z, W.v,
-                                                        W.r, S->d_part, S->d_st);
-  LAUNCH_CHECK(S);
-  k_bicg_update<T><<<nblk(P.n), TPB, 0, S->stream>>>(P.n, W.z, W.v, W.x, W.r, W.r0, S->d_part, S->d_st);
-  LAUNCH_CHECK(S);
+  KLAUNCH(S, P_SPMV, spmv_bytes<T>(S, 3),
+          (k_spmv<T, SPMV_BICG_V><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, 0, S->d_col, A.aoff, A.diag, W.z,
+                                                                  W.v, W.r, S->d_part, S->d_st)));
+  KLAUNCH(S, P_VEC, (double)P.n * sizeof(T) * 7,
+          (k_bicg_update<T><<<nblk(P.n), TPB, 0, S->stream>>>(P.n, W.z, W.v, W.x, W.r, W.r0, S->d_part, S->d_st)));
   return CMS_OK;
 }
 
 // BiCGStab from x (or 0) on b, ending when the device stopping test fires.
 template <typename T>
-static int run_bicgstab(Solver* S, Mat<T>& A, Work<T>& W, int maxit, int norm, double tol, int xzero) {
+static int run_bicgstab(Solver* S, Mat<T>& A, Work<T>& W, int maxit, int norm, double tol, int xzero,
+                        bool do_factor = true) {
   const HostPattern& P = S->hp;
   const int nb_all = S->tab.blk[S->tab.ng];
-  CHK(factor<T>(S, A));
-  k_bicg_init<T><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, xzero, maxit, norm, tol, S->d_col, A.aoff, A.diag,
-                                                W.b, W.x, W.r, W.r0, W.p, W.u, W.v, S->d_part, S->d_st);
-  LAUNCH_CHECK(S);
-  int issued = 0, chunk = 2;
+  if (do_factor) CHK(factor<T>(S, A));
+  KLAUNCH(S, P_VEC, xzero ? (double)P.n * sizeof(T) * 7 : spmv_bytes<T>(S, 7),
+          (k_bicg_init<T><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, xzero, maxit, norm, tol, S->d_col, A.aoff,
+                                                          A.diag, W.b, W.x, W.r, W.r0, W.p, W.u, W.v, S->d_part,
+                                                          S->d_st)));
+  int issued = 0, chunk = S->prof_on ? 1 : 2;
   while (issued < maxit) {
     const int c = std::min(chunk, maxit - issued);
     for (int q = 0; q < c; ++q) CHK(bicg_iter<T>(S, A, W));
@@ -321,41 +381,39 @@ static int run_bicgstab(Solver* S, Mat<T>& A, Work<T>& W, int maxit, int norm, d
     bool done = false;
     CHK(poll_done(S, done));
     if (done) break;
-    chunk = std::min(chunk * 2, 16);
+    if (!S->prof_on) chunk = std::min(chunk * 2, 16);
   }
   return CMS_OK;
 }
 
 // GMRES(3) restarts (pgmres.f90:129-241).
 template <typename T>
-static int run_gmres(Solver* S, Mat<T>& A, Work<T>& W, int maxit, double tol) {
+static int run_gmres(Solver* S, Mat<T>& A, Work<T>& W, int maxit, double tol, bool do_factor = true) {
   const HostPattern& P = S->hp;
   const int nb_all = S->tab.blk[S->tab.ng];
-  CHK(factor<T>(S, A));
-  k_gm_start<<<1, 1, 0, S->stream>>>(S->d_st, maxit, tol);
-  LAUNCH_CHECK(S);
+  const double vb = (double)P.n * sizeof(T);
+  if (do_factor) CHK(factor<T>(S, A));
+  KLAUNCH(S, P_SCALAR, 0, (k_gm_start<<<1, 1, 0, S->stream>>>(S->d_st, maxit, tol)));
   GmVecs gv;
   for (int j = 0; j < 5; ++j) gv.v[j] = W.vv[j];
   for (int cyc = 0; cyc < maxit; ++cyc) {
-    k_gm_resid<T><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, S->d_col, A.aoff, A.diag, W.b, W.x, W.vv[1],
-                                                 S->d_part, S->d_st);
-    LAUNCH_CHECK(S);
+    KLAUNCH(S, P_VEC, spmv_bytes<T>(S, 3),
+            (k_gm_resid<T><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, S->d_col, A.aoff, A.diag, W.b, W.x,
+                                                           W.vv[1], S->d_part, S->d_st)));
     for (int i = 1; i <= 3; ++i) {
       CHK((sweep_fwd<T, FWD_GM_SCALE>(S, A, W, i, nullptr, nullptr, nullptr, nullptr, nullptr)));
       CHK((sweep_bwd<T, false>(S, A, W, nullptr, 1)));
-      k_spmv<T, SPMV_GM><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, i, S->d_col, A.aoff, A.diag, W.z,
-                                                        W.vv[i + 1], W.vv[1], S->d_part, S->d_st);
-      LAUNCH_CHECK(S);
+      KLAUNCH(S, P_SPMV, spmv_bytes<T>(S, 3),
+              (k_spmv<T, SPMV_GM><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, i, S->d_col, A.aoff, A.diag, W.z,
+                                                                  W.vv[i + 1], W.vv[1], S->d_part, S->d_st)));
       for (int j = 1; j <= i; ++j) {
-        k_mgs<T><<<nblk(P.n), TPB, 0, S->stream>>>(P.n, j, i, gv, S->d_part, S->d_st);
-        LAUNCH_CHECK(S);
+        KLAUNCH(S, P_VEC, vb * 4, (k_mgs<T><<<nblk(P.n), TPB, 0, S->stream>>>(P.n, j, i, gv, S->d_part, S->d_st)));
       }
     }
     CHK((sweep_fwd<T, FWD_GM_COMB>(S, A, W, 0, nullptr, nullptr, nullptr, nullptr, nullptr)));
     CHK((sweep_bwd<T, true>(S, A, W, W.x, 0)));
-    k_gm_cycle_end<<<1, 1, 0, S->stream>>>(S->d_st);
-    LAUNCH_CHECK(S);
-    if ((cyc & 1) || cyc + 1 == maxit) {
+    KLAUNCH(S, P_SCALAR, 0, (k_gm_cycle_end<<<1, 1, 0, S->stream>>>(S->d_st)));
+    if (S->prof_on || (cyc & 1) || cyc + 1 == maxit) {
       bool done = false;
       CHK(poll_done(S, done));
       if (done) break;
@@ -380,9 +438,12 @@ static int run_krylov(Solver* S, Mat<T>& A, Work<T>& W, int nsolv, int maxit, in
 template <typename TA, typename TX>
 static int resid64(Solver* S, Mat<TA>& A, const double* b, const TX* x, double* rout, float* rout32, int slot) {
   const HostPattern& P = S->hp;
-  k_resid64<TA, TX><<<S->tab.blk[S->tab.ng], TPB, 0, S->stream>>>(P.n, P.KL, S->tab, S->d_col, A.aoff, A.diag, b, x,
-                                                                  rout, rout32, slot, S->d_part, S->d_st);
-  LAUNCH_CHECK(S);
+  const double bytes = (double)P.n * (sizeof(TA) + 8 + sizeof(TX) + (rout ? 8 : 0) + (rout32 ? 4 : 0)) +
+                       (double)P.nnz_off * (sizeof(TA) + 4);
+  KLAUNCH(S, P_RESID64, bytes,
+          (k_resid64<TA, TX><<<S->tab.blk[S->tab.ng], TPB, 0, S->stream>>>(P.n, P.KL, S->tab, S->d_col, A.aoff, A.diag,
+                                                                            b, x, rout, rout32, slot, S->d_part,
+                                                                            S->d_st)));
   return CMS_OK;
 }
 
@@ -411,30 +472,15 @@ static int run_refine(Solver* S, int nsolv, int maxit, double tol, cms_solve_inf
     if (rel <= tol || steps >= rmax || inner_total >= maxit) break;
     // inner FP32 solve A32 d = r32 from d = 0 (factor already built)
     if (nsolv == 3) {
-      const int nb_all = S->tab.blk[S->tab.ng];
-      k_bicg_init<float><<<nb_all, TPB, 0, S->stream>>>(n, P.KL, S->tab, 1, imax, 2, itol, S->d_col, S->A32.aoff,
-                                                        S->A32.diag, S->W32.b, S->W32.x, S->W32.r, S->W32.r0,
-                                                        S->W32.p, S->W32.u, S->W32.v, S->d_part, S->d_st);
-      LAUNCH_CHECK(S);
-      int issued = 0, chunk = 2;
-      while (issued < imax) {
-        const int c = std::min(chunk, imax - issued);
-        for (int q = 0; q < c; ++q) CHK(bicg_iter<float>(S, S->A32, S->W32));
-        issued += c;
-        bool done = false;
-        CHK(poll_done(S, done));
-        if (done) break;
-        chunk = std::min(chunk * 2, 16);
-      }
+      CHK(run_bicgstab<float>(S, S->A32, S->W32, imax, 2, itol, 1, false));
     } else {
       CMS_CUDA(cudaMemsetAsync(S->W32.x, 0, sizeof(float) * n, S->stream));
-      CHK(run_gmres<float>(S, S->A32, S->W32, imax, itol));
+      CHK(run_gmres<float>(S, S->A32, S->W32, imax, itol, false));
     }
     CMS_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, S->stream));
     CMS_CUDA(cudaStreamSynchronize(S->stream));
     inner_total += (nsolv == 3) ? S->h_st->iter : S->h_st->inner;
-    k_ir_correct<<<nblk(n), TPB, 0, S->stream>>>(n, S->W32.x, S->W64.x);
-    LAUNCH_CHECK(S);
+    KLAUNCH(S, P_VEC, (double)n * 20, (k_ir_correct<<<nblk(n), TPB, 0, S->stream>>>(n, S->W32.x, S->W64.x)));
     ++steps;
   }
   info->iters = inner_total;
@@ -467,15 +513,20 @@ static int solve_dev(Solver* S, const T* acoef, T* ss, const T* sp, T* res, T* p
   // prologue: ap, ss, res, rmom + device-order system (and FP32 copy)
   float* a2 = (is64 && prec == CMS_PREC_FP32_REFINE) ? S->A32.aoff : nullptr;
   float* d2 = (is64 && prec == CMS_PREC_FP32_REFINE) ? S->A32.diag : nullptr;
-  k_prologue<T, float><<<nblk(P.n), TPB, 0, S->stream>>>(P.n, P.nmf, acoef, ss, sp, res, phi, S->d_c2c, S->d_ncface,
-                                                         S->d_iwet, S->d_fslot, S->d_iperm, relax, A.aoff, A.diag,
-                                                         W.b, W.x, a2, d2, S->d_part, S->d_st);
-  LAUNCH_CHECK(S);
+  {
+    const double sz = sizeof(T);
+    const double per = P.nmf * (sz + 4 + 1) + 4 + 4 + 4 + sz * 7 + (a2 ? 4 : 0);
+    KLAUNCH(S, P_PROLOGUE, (double)P.n * per + (double)P.nnz_off * (sz + (a2 ? 4 : 0)),
+            (k_prologue<T, float><<<nblk(P.n), TPB, 0, S->stream>>>(P.n, P.nmf, acoef, ss, sp, res, phi, S->d_c2c,
+                                                                     S->d_ncface, S->d_iwet, S->d_fslot, S->d_iperm,
+                                                                     relax, A.aoff, A.diag, W.b, W.x, a2, d2,
+                                                                     S->d_part, S->d_st)));
+  }
   if (S->opts.verify) {
     if (is64) CHK((resid64<double, double>(S, S->A64, S->W64.b, S->W64.x, nullptr, nullptr, S_TRUE0)));
     else {
-      k_convert<double, float><<<nblk(P.n), TPB, 0, S->stream>>>(P.n, S->W32.b, S->W64.r);
-      LAUNCH_CHECK(S);
+      KLAUNCH(S, P_VEC, (double)P.n * 12,
+              (k_convert<double, float><<<nblk(P.n), TPB, 0, S->stream>>>(P.n, S->W32.b, S->W64.r)));
       CHK((resid64<float, float>(S, S->A32, S->W64.r, S->W32.x, nullptr, nullptr, S_TRUE0)));
     }
   }
@@ -488,8 +539,8 @@ static int solve_dev(Solver* S, const T* acoef, T* ss, const T* sp, T* res, T* p
     if (is64) CHK((resid64<double, double>(S, S->A64, S->W64.b, S->W64.x, nullptr, nullptr, S_TRUE1)));
     else CHK((resid64<float, float>(S, S->A32, S->W64.r, S->W32.x, nullptr, nullptr, S_TRUE1)));
   }
-  k_scatter<T, T><<<nblk(P.n), TPB, 0, S->stream>>>(P.n, S->d_perm, W.x, phi);
-  LAUNCH_CHECK(S);
+  KLAUNCH(S, P_VEC, (double)P.n * (4 + 2 * sizeof(T)),
+          (k_scatter<T, T><<<nblk(P.n), TPB, 0, S->stream>>>(P.n, S->d_perm, W.x, phi)));
   CMS_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, S->stream));
   CMS_CUDA(cudaStreamSynchronize(S->stream));
   const DevState& h = *S->h_st;
@@ -593,6 +644,33 @@ int cms_solver_solve_dev_f(cms_solver* s, const float* acoef, float* ss, const f
   return cms::solve_dev<float>(s, acoef, ss, sp, res, phi, relax, nswp, nsolv, info);
 }
 
+int cms_solver_profile(cms_solver* s, int enable) {
+  if (!s) return CMS_BAD_ARGUMENT;
+  s->prof_on = enable ? 1 : 0;
+  return CMS_OK;
+}
+
+int cms_solver_profile_read(cms_solver* s, int reset, double* ms, double* bytes, long long* count) {
+  if (!s) return CMS_BAD_ARGUMENT;
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess) return CMS_DEVICE_ERROR;
+  for (const auto& r : s->prof_recs) {
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, s->ev_pool[r.ev], s->ev_pool[r.ev + 1]) != cudaSuccess) return CMS_DEVICE_ERROR;
+    s->prof_ms[r.cat] += t;
+    s->prof_bytes[r.cat] += r.bytes;
+    s->prof_count[r.cat] += 1;
+  }
+  s->prof_recs.clear();
+  s->ev_used = 0;
+  for (int c = 0; c < cms::P_NCAT; ++c) {
+    if (ms) ms[c] = s->prof_ms[c];
+    if (bytes) bytes[c] = s->prof_bytes[c];
+    if (count) count[c] = s->prof_count[c];
+    if (reset) { s->prof_ms[c] = 0; s->prof_bytes[c] = 0; s->prof_count[c] = 0; }
+  }
+  return CMS_OK;
+}
+
 int cms_solver_ncolors(const cms_solver* s) { return s ? s->hp.G : -1; }
 size_t cms_solver_device_bytes(const cms_solver* s) { return s ? s->bytes : 0; }
 int cms_solver_get_perm(const cms_solver* s, int* perm) {
@@ -607,6 +685,7 @@ void cms_solver_destroy(cms_solver* s) {
   if (!s) return;
   if (s->stream) cudaStreamSynchronize(s->stream);
   for (void* p : s->allocs) cudaFree(p);
+  for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
   if (s->h_st) cudaFreeHost(s->h_st);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;

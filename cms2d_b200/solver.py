@@ -133,6 +133,18 @@ class Solver:
     def stream_handle(self) -> int:
         return _lib.lib().cms_solver_stream(self._h) or 0
 
+    PROFILE_CLASSES = ("prologue", "ilu0", "fwd_sweep", "bwd_sweep", "spmv", "vector", "resid64", "scalar")
+
+    def profile(self, enable: bool = True):
+        _lib.check(_lib.lib().cms_solver_profile(self._h, int(enable)), "cms_solver_profile")
+
+    def profile_read(self, reset: bool = True) -> dict:
+        ms = np.zeros(8); by = np.zeros(8); cnt = np.zeros(8, np.int64)
+        _lib.check(_lib.lib().cms_solver_profile_read(self._h, int(reset), _ptr(ms), _ptr(by), _ptr(cnt)),
+                   "cms_solver_profile_read")
+        return {name: {"ms": float(ms[q]), "bytes": float(by[q]), "launches": int(cnt[q])}
+                for q, name in enumerate(self.PROFILE_CLASSES)}
+
     def perm(self) -> np.ndarray:
         p = np.zeros(self.grid.ncells, np.int32)
         _lib.check(_lib.lib().cms_solver_get_perm(self._h, _ptr(p)), "cms_solver_get_perm")

@@ -117,6 +117,13 @@ size_t cms_solver_device_bytes(const cms_solver* s);
 int cms_solver_get_perm(const cms_solver* s, int* perm);
 /* Kernel launches issued by the handle since creation (counted on the host). */
 long long cms_solver_launches(const cms_solver* s);
+/* Kernel-class timing with CUDA events on the handle's stream.  Classes:
+ * 0 prologue, 1 ILU(0) factor, 2 forward sweep, 3 backward sweep, 4 SpMV,
+ * 5 vector/reduction kernels, 6 FP64 residual, 7 scalar kernels.
+ * profile_read fills ms[8], bytes[8] (algorithmic bytes: every array a
+ * kernel touches counted once) and count[8] (launches); reset=1 clears. */
+int cms_solver_profile(cms_solver* s, int enable);
+int cms_solver_profile_read(cms_solver* s, int reset, double* ms, double* bytes, long long* count);
 /* The stream the handle runs on (a cudaStream_t). */
 void* cms_solver_stream(cms_solver* s);
 

@@ -393,7 +393,7 @@ void build_lu(Pattern& p, Work<R>& w, const R* acoef, const R* ap, bool use_ilu_
 // ratio sum|r|/sum|r0|.
 template <typename R>
 SolveStats pbicgstab(Pattern& p, Work<R>& wk, int nmaxiter, const R* acoef, const R* ap, const R* su, R* phi, int precond,
-                     R tol, int lfil, R droptol, R permtol) {
+                     R tol, int lfil, R droptol, R permtol, int norm) {
   const int n = p.ncells, nmf = p.nmaxfaces;
   const R small = k_small<R>();
   std::vector<R> pk(n), r(n), uk(n), vk(n), r0(n), zzk((size_t)p.ncellsD + 1, R(0));
@@ -405,9 +405,10 @@ SolveStats pbicgstab(Pattern& p, Work<R>& wk, int nmaxiter, const R* acoef, cons
     term = term + su[i - 1] - ap[i - 1] * phi[i - 1];
     r[i - 1] = term + small;
     r0[i - 1] = r[i - 1];
-    res0 = res0 + std::fabs(r0[i - 1]);
+    res0 = res0 + (norm == 2 ? r0[i - 1] * r0[i - 1] : std::fabs(r0[i - 1]));
     pk[i - 1] = uk[i - 1] = vk[i - 1] = R(0);
   }
+  if (norm == 2) res0 = std::sqrt(res0);
   build_lu(p, wk, acoef, ap, /*ilu_cr=*/true, precond, lfil, droptol, permtol);
   // zzk is 1-based over ncellsD (index 0 unused); ghosts stay zero.
   R alf = R(1), bet0 = R(1), gam = R(1);
@@ -443,8 +444,9 @@ SolveStats pbicgstab(Pattern& p, Work<R>& wk, int nmaxiter, const R* acoef, cons
     for (int i = 0; i < n; ++i) {
       phi[i] = phi[i] + alf * zzk[i + 1];
       r[i] = r[i] - alf * vk[i];
-      res = res + std::fabs(r[i]);
+      res = res + (norm == 2 ? r[i] * r[i] : std::fabs(r[i]));
     }
+    if (norm == 2) res = std::sqrt(res);
     st.iters = iter; st.inner = iter; st.relres = (double)(res / res0);
     if (res / res0 < tol) return st;
   }
@@ -551,7 +553,7 @@ struct OracleHandle {
 template <typename R>
 int solve_impl(OracleHandle* h, Work<R>& wk, const R* acoef, R* ss, const R* sp, R* res, R* phi, R relax, int nswp,
                int nsolv, int precond, R tol, int lfil, R droptol, R permtol, R* rmom, int* iters, int* inner,
-               double* relres) {
+               double* relres, int norm) {
   Pattern& p = h->p;
   const int n = p.ncells, nmf = p.nmaxfaces;
   std::vector<R> ap(n);
@@ -569,7 +571,7 @@ int solve_impl(OracleHandle* h, Work<R>& wk, const R* acoef, R* ss, const R* sp,
   }
   *rmom = std::sqrt(adak(n, res) / R(n));
   SolveStats st{0, 0, 0.0};
-  if (nsolv == 3) st = pbicgstab(p, wk, nswp, acoef, ap.data(), ss, phi, precond, tol, lfil, droptol, permtol);
+  if (nsolv == 3) st = pbicgstab(p, wk, nswp, acoef, ap.data(), ss, phi, precond, tol, lfil, droptol, permtol, norm);
   else if (nsolv == 4) st = pgmres(p, wk, nswp, acoef, ap.data(), ss, phi, precond, tol, lfil, droptol, permtol);
   else return -1;
   *iters = st.iters;
@@ -636,18 +638,18 @@ int orc_set_threads(int n) {
 
 int orc_solve_d(void* hv, const double* acoef, double* ss, const double* sp, double* res, double* phi, double relax,
                 int nswp, int nsolv, int precond, double tol, int lfil, double droptol, double permtol, double* rmom,
-                int* iters, int* inner, double* relres) {
+                int* iters, int* inner, double* relres, int norm) {
   auto* h = static_cast<OracleHandle*>(hv);
   return solve_impl<double>(h, h->wd, acoef, ss, sp, res, phi, relax, nswp, nsolv, precond, tol, lfil, droptol, permtol,
-                            rmom, iters, inner, relres);
+                            rmom, iters, inner, relres, norm);
 }
 
 int orc_solve_f(void* hv, const float* acoef, float* ss, const float* sp, float* res, float* phi, float relax, int nswp,
                 int nsolv, int precond, float tol, int lfil, float droptol, float permtol, float* rmom, int* iters,
-                int* inner, double* relres) {
+                int* inner, double* relres, int norm) {
   auto* h = static_cast<OracleHandle*>(hv);
   return solve_impl<float>(h, h->wf, acoef, ss, sp, res, phi, relax, nswp, nsolv, precond, tol, lfil, droptol, permtol,
-                           rmom, iters, inner, relres);
+                           rmom, iters, inner, relres, norm);
 }
 
 // Applies the factor built by the last orc_solve_* call: x = (LU)^-1 y (lusol,

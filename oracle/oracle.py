@@ -48,11 +48,11 @@ def lib():
         ip = C.POINTER(C.c_int)
         dp = C.POINTER(C.c_double)
         L.orc_solve_d.argtypes = [P, f64p, f64p, f64p, f64p, f64p, C.c_double, C.c_int, C.c_int, C.c_int, C.c_double,
-                                  C.c_int, C.c_double, C.c_double, dp, ip, ip, dp]
+                                  C.c_int, C.c_double, C.c_double, dp, ip, ip, dp, C.c_int]
         L.orc_solve_d.restype = C.c_int
         fp = C.POINTER(C.c_float)
         L.orc_solve_f.argtypes = [P, f32p, f32p, f32p, f32p, f32p, C.c_float, C.c_int, C.c_int, C.c_int, C.c_float,
-                                  C.c_int, C.c_float, C.c_float, fp, ip, ip, dp]
+                                  C.c_int, C.c_float, C.c_float, fp, ip, ip, dp, C.c_int]
         L.orc_solve_f.restype = C.c_int
         L.orc_lusol_d.argtypes = [P, f64p, f64p]
         _LIB = L
@@ -89,7 +89,7 @@ class OracleSolver:
         return ia, ja
 
     def solve(self, acoef, ss, sp, res, phi, relax=1.0, nswp=15, nsolv=3, precond=PC_ILU0, tol=1e-3, lfil=None,
-              droptol=1e-3, permtol=0.5):
+              droptol=1e-3, permtol=0.5, norm=1):
         """Arguments mirror solve(acoef,ss,sp,res,phi,n): ss, res and phi are updated in place.
 
         Returns dict(status, rmom, iters, inner, relres).
@@ -104,7 +104,7 @@ class OracleSolver:
         for a in (acoef, ss, sp, res, phi):
             assert a.dtype == dt and a.flags.c_contiguous
         st = fn(self._h, acoef, ss, sp, res, phi, relax, int(nswp), int(nsolv), int(precond), tol, int(lfil), droptol,
-                permtol, C.byref(rm), C.byref(it), C.byref(inner), C.byref(rr))
+                permtol, C.byref(rm), C.byref(it), C.byref(inner), C.byref(rr), int(norm))
         return dict(status=st, rmom=rm.value, iters=it.value, inner=inner.value, relres=rr.value)
 
     def lusol(self, y):
