@@ -154,6 +154,31 @@ int cms_gpu_solve_f(int n, const float* acoef, float* ss, const float* sp, float
 int cms_gpu_last_info(cms_solve_info* info);
 int cms_gpu_finalize(void);
 
+/* ---- allocation-free entry point ------------------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory when they need it (a host that runs under a fixed device-memory
+ * budget of its own pool, or that must not let cudaMalloc/cudaFree synchronise
+ * the device in the middle of its time step): the solve() prologue of
+ * source/solvers/solvers.f90:230-240 -- ap, the under-relaxed ss, the
+ * normalised residual res and rmom = sqrt(sum res^2 / ncells) -- without a
+ * solver handle and without any allocation.
+ *
+ * All array pointers are DEVICE pointers in the solve() layout (1-based
+ * cell2cell, [ncellsD][nmaxfaces] acoef); ss is updated in place, res is
+ * written, rmom is a HOST double.  stream is a cudaStream_t (NULL: the legacy
+ * default stream); the call returns after the result is on the host.
+ * Scratch is a fixed device array inside the library (about 0.5 MB per GPU,
+ * held from load to exit); ncells above CMS_NOALLOC_MAX_CELLS is rejected with
+ * CMS_BAD_ARGUMENT.  The first call on each device resolves the array's
+ * address (cudaGetSymbolAddress) with that device current; make that first
+ * call before any stream capture.  Every call shares the one array, so calls
+ * that overlap on the GPU (other streams or threads) race: serialise them. */
+#define CMS_NOALLOC_MAX_CELLS 16777216
+int cms_solve_residual_noalloc_d(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, const int* ncface,
+                                 const int* iwet, const double* acoef, double* ss, const double* sp, double* res,
+                                 const double* phi, double relax, double* rmom, void* stream);
+const char* cms_noalloc_last_error(void);
+
 /* Library version string. */
 const char* cms_gpu_version(void);
 /* Text of the last error a call reported (device or argument errors). */
