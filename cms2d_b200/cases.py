@@ -1,0 +1,153 @@
+"""Seeded synthetic flow cases with the shapes of the benchmark configurations.
+
+tidal_basin:  rectangular basin on a uniform Cartesian grid (default 200 x 100
+              cells at 20 m), depth a linear slope from 2 m at the shore to
+              10 m offshore plus seeded Gaussian bumps (0.2 m standard
+              deviation), an M2 water level (0.5 m, 12.42 h) on the open
+              offshore (north) edge, walls elsewhere, Manning n = 0.025.
+tidal_inlet:  three-level telescoping grid (40/20/10 m) of about 1.0M active
+              cells: ocean to the north, a barrier strip (inactive land) cut by
+              a 300 m wide, 8 m deep inlet channel, an ebb shoal of 2-6 m in
+              front of it and a back bay; lognormal Manning n (median 0.025,
+              sigma_log 0.2); M2 + K1 water level (0.6 m / 0.2 m) on the north
+              edge.
+
+A case carries the grid (cms2d_b200.grid.Grid), bed elevation zb (= -depth,
+ncellsD values; dummies copy their parent cell), coefman (ncells), the
+water-level string (1-based cells and faces of the open edge) and the tide.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import grid as G
+
+M2_HOURS = 12.42
+K1_HOURS = 23.93
+
+
+@dataclass
+class Case:
+    name: str
+    grid: G.Grid
+    zb: np.ndarray
+    coefman: np.ndarray
+    th_cells: np.ndarray
+    th_faces: np.ndarray
+    tide: list  # [(amplitude m, period h)]
+    dt: float
+    nsteps: int
+
+    def wse(self, t_seconds: float) -> float:
+        th = t_seconds / 3600.0
+        return float(sum(a * np.cos(2.0 * np.pi * th / T) for a, T in self.tide))
+
+    def wsebnd(self, t_seconds: float) -> np.ndarray:
+        return np.full(self.th_cells.size, self.wse(t_seconds))
+
+
+def _smooth_field(shape, corr_cells: float, rng) -> np.ndarray:
+    """Unit-variance Gaussian random field with a Gaussian correlation (FFT filter)."""
+    ny, nx = shape
+    w = rng.standard_normal(shape)
+    ky = np.fft.fftfreq(ny)[:, None]
+    kx = np.fft.fftfreq(nx)[None, :]
+    filt = np.exp(-2.0 * (np.pi * corr_cells) ** 2 * (kx ** 2 + ky ** 2))
+    f = np.real(np.fft.ifft2(np.fft.fft2(w) * filt))
+    s = f.std()
+    return f / s if s > 0 else f
+
+
+def _north_string(g: G.Grid):
+    """Active cells whose north face leads to a dummy, with that face (1-based)."""
+    n = g.ncells
+    cells, faces = [], []
+    for k in range(g.nmaxfaces):
+        c = g.cell2cell[:n, k]
+        m = (k < g.ncface[:n]) & (c > n) & (g.idirface[:n, k] == G.N_)
+        idx = np.nonzero(m)[0]
+        cells.append(idx + 1); faces.append(np.full(idx.size, k + 1))
+    cells = np.concatenate(cells); faces = np.concatenate(faces)
+    o = np.argsort(cells, kind="stable")
+    return cells[o].astype(np.int32), faces[o].astype(np.int32)
+
+
+def _fill_dummies(g: G.Grid, vals_active: np.ndarray) -> np.ndarray:
+    """Extends a cell field to the dummies (each copies the cell it hangs off)."""
+    out = np.zeros(g.ncellsD)
+    out[: g.ncells] = vals_active
+    parent = np.zeros(g.ncellsD, np.int64)
+    for k in range(g.nmaxfaces):
+        c = g.cell2cell[g.ncells:, k]
+        m = c > 0
+        parent[g.ncells:][m] = c[m] - 1
+    out[g.ncells:] = vals_active[parent[g.ncells:]]
+    return out
+
+
+def tidal_basin(nx: int = 200, ny: int = 100, dx: float = 20.0, seed: int = 0, amp: float = 0.5,
+                manning: float = 0.025, dt: float = 600.0, hours: float = 24.0) -> Case:
+    rng = np.random.default_rng(seed)
+    g = G.cartesian_grid(nx, ny, dx)
+    n = g.ncells
+    jrow = (g.y[:n] / dx - 0.5)  # 0 .. ny-1
+    depth = 2.0 + 8.0 * jrow / max(ny - 1, 1)
+    bumps = _smooth_field((ny, nx), 6.0, rng) * 0.2
+    depth = depth + bumps.ravel()  # natural order is row-major (y then x)
+    zb = _fill_dummies(g, -depth)
+    th_cells, th_faces = _north_string(g)
+    return Case("tidal_basin", g, zb, np.full(n, manning), th_cells, th_faces, [(amp, M2_HOURS)], dt,
+                int(round(hours * 3600.0 / dt)))
+
+
+def tidal_inlet(target_cells: int = 1_000_000, seed: int = 0, dt: float = 300.0, nsteps: int = 48) -> Case:
+    """Three-level telescoping tidal inlet of about target_cells active cells."""
+    rng = np.random.default_rng(seed)
+    dx0 = 40.0
+    # parent lattice scaled so that the active count lands near the target
+    # (the refined zones roughly double the parent count)
+    P = target_cells / 2.07
+    ny = int(round(np.sqrt(P / 1.7)))
+    nx = int(round(1.7 * ny))
+    xc = nx // 2
+    yb0 = int(0.45 * ny)                 # barrier strip rows [yb0, yb1)
+    yb1 = yb0 + max(4, ny // 60)
+    lev = np.zeros((ny, nx), dtype=np.int64)
+    # level 1: wide zone around the inlet; level 2: the channel and ebb shoal core
+    w1x, w1y = int(0.22 * nx), int(0.30 * ny)
+    w2x, w2y = int(0.06 * nx), int(0.12 * ny)
+    lev[max(0, (yb0 + yb1) // 2 - w1y): min(ny, (yb0 + yb1) // 2 + w1y), max(0, xc - w1x): min(nx, xc + w1x)] = 1
+    lev[max(0, (yb0 + yb1) // 2 - w2y): min(ny, (yb0 + yb1) // 2 + w2y), max(0, xc - w2x): min(nx, xc + w2x)] = 2
+    x_in = (xc + 0.5) * dx0  # inlet centre x
+    half_w = 150.0           # 300 m channel
+
+    def active(x, y, s):
+        in_barrier = (y > yb0 * dx0) & (y < yb1 * dx0)
+        in_gap = np.abs(x - x_in) < half_w
+        return ~(in_barrier & ~in_gap)
+
+    g = G.telescoping_grid(lev, dx0, active=active, nmaxfaces=6)
+    n = g.ncells
+    x, y = g.x[:n], g.y[:n]
+    yb = 0.5 * (yb0 + yb1) * dx0
+    Ly = ny * dx0
+    # depth: bay 3 m, ocean 5 m near the barrier rising to 14 m offshore,
+    # ebb shoal mound (2 m crest) in front of the inlet, 8 m channel in the gap
+    off = np.clip((y - yb) / (Ly - yb), 0.0, 1.0)
+    depth = np.where(y < yb, 3.0, 5.0 + 9.0 * off)
+    r2 = ((x - x_in) / 1200.0) ** 2 + ((y - (yb + 900.0)) / 700.0) ** 2
+    shoal = np.exp(-r2)
+    depth = np.where(y >= yb, depth - (depth - 2.0) * shoal, depth)
+    chan = (np.abs(x - x_in) < half_w) & (np.abs(y - yb) < (yb1 - yb0) * dx0)
+    depth = np.where(chan, 8.0, depth)
+    depth = np.maximum(depth, 2.0)
+    zb = _fill_dummies(g, -depth)
+    # lognormal Manning n on a smooth field (correlation ~12 parents)
+    fld = _smooth_field((ny, nx), 12.0, rng)
+    pi = np.clip((x / dx0).astype(np.int64), 0, nx - 1)
+    pj = np.clip((y / dx0).astype(np.int64), 0, ny - 1)
+    coefman = 0.025 * np.exp(0.2 * fld[pj, pi])
+    th_cells, th_faces = _north_string(g)
+    return Case("tidal_inlet", g, zb, coefman, th_cells, th_faces, [(0.6, M2_HOURS), (0.2, K1_HOURS)], dt, nsteps)

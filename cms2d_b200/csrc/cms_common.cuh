@@ -26,6 +26,7 @@ enum Slot : int {
   S_RMOM = 51,
   S_TRUE0 = 52,
   S_TRUE1 = 53,
+  S_IRSCALE = 54, // refinement: norm of the residual handed to the FP32 solve
   S_NSLOTS = 64
 };
 

@@ -1,0 +1,700 @@
+// Device kernels of the implicit flow step (SIMPLEC outer iteration).
+//
+// Layout.  Cells are numbered in the solver's device order: active cells
+// 0..n-1 (colour groups, natural order inside a group), then the dummy cells
+// n..nD-1 in their natural order.  Face arrays are slot-major,
+// A[k * nD + r] for face k (0..nmf-1) of cell r, so a warp reading face k of
+// 32 consecutive cells touches one contiguous segment.  A face shared by two
+// cells is evaluated once by the cell that owns it (the reference's no-repeat
+// face lists) and mirrored into the neighbour's slot, as the reference does.
+#pragma once
+#include "cms_common.cuh"
+
+namespace cms {
+
+struct FlowDev {
+  int n, nD, nmf, nsc, ider;
+  // connectivity (device numbering)
+  const int* ncface;          // [nD]
+  const int* nb;              // [nmf][nD] neighbour (dummies >= n), -1 none
+  const signed char* back;    // [nmf][nD] face index seen from the neighbour
+  const signed char* dir;     // [nmf][nD] 1..4 = N,E,S,W
+  const unsigned char* owned; // [nD] bit k: face k is on the cell's no-repeat list
+  const unsigned char* thm;   // [nD] bit k: face k is on a water-level string
+  const unsigned char* joint; // [nD]
+  const int* iwet;            // [nD]
+  // metrics
+  const double *ds, *dn, *dsxy, *rx, *ry, *rpx, *rpy, *fintp;  // [nmf][nD]
+  const double *areap, *zb, *coefman;                          // [nD]
+  // gradient operator (wet cells): [q][n] stencils
+  const int *ncx, *ncy, *icx, *icy, *ngx, *ngy, *igx, *igy;
+  const double *wcx, *wcy, *wgxy, *wgyx;
+  // parameters
+  double grav, gravinv, hmin, hdry, relax_uv, relax_p, facpp, cviscon, cvisbot, cvishor2areaavg, cvismax, wallfac;
+};
+
+__device__ __forceinline__ int fidx(const FlowDev& G, int k, int r) { return k * G.nD + r; }
+__device__ __forceinline__ double fnxd(int d) { return d == 2 ? 1.0 : (d == 4 ? -1.0 : 0.0); }
+__device__ __forceinline__ double fnyd(int d) { return d == 1 ? 1.0 : (d == 3 ? -1.0 : 0.0); }
+
+__device__ __forceinline__ double expcoef(double dk, double fk) {  // comp_lib.f90:96-109
+  const double absfk = fabs(fk);
+  const double peck = absfk / fmax(fmax(dk, 1.0e-6), absfk);
+  return dk * peck / fmax(exp(peck) - 1.0, 1.0e-6) + fmax(0.0, -fk);
+}
+__device__ __forceinline__ double upwcoef(double dk, double fk) { return dk + fmax(0.0, -fk); }
+__device__ __forceinline__ double wallcoef(double yp, double y0) {  // fric_lib.f90:162-194
+  const double y0lim = fmin(fmax(y0, 1.0e-6), yp * 0.9999);
+  const double c = 0.4 / log(yp / y0lim);
+  return c * c;
+}
+
+struct FlowState {
+  double *p, *h, *u, *v, *pp, *vis, *vis0, *vis1, *cfrict, *z0, *uv, *bsvel, *eta;
+  double *u1, *v1, *p1, *h1;
+  double *su, *sv, *sp, *spu, *spv, *ssu0, *ssv0, *spuv0, *sppp0, *sspp0, *apuareap, *sumu, *Hu, *Hv, *res;
+  double *flux, *visk, *hk, *pk, *acoef, *zbk;  // faces
+  // gradients, two copies each (the cell-reconstruction correction reads the previous one)
+  double *dpx[2], *dpy[2], *dux[2], *duy[2], *dvx[2], *dvy[2], *dppx[2], *dppy[2];
+  double *dHux[2], *dHuy[2], *dHvx[2], *dHvy[2], *dapx[2], *dapy[2], *dzbx[2], *dzby[2];
+  double* wsebnd;      // [nth]
+  int* flag;           // [4] device status flags: 0 drying reached, 1 non-finite
+};
+
+// ----------------------------------------------------------------------------
+// flow_srcsnk_static, ntsch = 1 (flow_imp.F90:336-346), plus the depth update of
+// flow_wetdry(0) (flow.F90:1247-1255) for the fixed wet set.
+__global__ void __launch_bounds__(TPB) kf_static(FlowDev G, FlowState S, double dt) {
+  const int r = blockIdx.x * TPB + threadIdx.x;
+  if (r >= G.nD) return;
+  double hh = S.p[r] * G.gravinv - G.zb[r];
+  if (hh < G.hdry) {
+    hh = fmax(hh, G.hmin);
+    if (r < G.n && G.iwet[r] == 1) S.flag[0] = 1;
+  }
+  S.h[r] = hh;
+  if (r >= G.n) return;
+  const double fac1 = G.areap[r] * S.h1[r] / dt;
+  S.spuv0[r] = -fac1;
+  S.ssu0[r] = fac1 * S.u1[r];
+  S.ssv0[r] = fac1 * S.v1[r];
+  S.sppp0[r] = -G.areap[r] / (G.grav * dt);
+  S.sspp0[r] = -S.p1[r] * S.sppp0[r];
+}
+
+// skew term of face k of joint cell r, owner-side formula of defcorparagradvec
+// (computational.F90:175-213) evaluated for (owner o, its face ko).
+__device__ __forceinline__ void defcor_face(const FlowDev& G, const FlowState& S, int o, int ko, const double* dux,
+                                            const double* duy, const double* dvx, const double* dvy, double& us,
+                                            double& vs) {
+  us = 0.0; vs = 0.0;
+  const int f = fidx(G, ko, o);
+  const int nck = G.nb[f];
+  if (G.iwet[o] == 0 || nck >= G.n || G.iwet[nck] == 0) return;
+  const int jcn = G.back[f];
+  const int fb = fidx(G, jcn, nck);
+  const int d = G.dir[f];
+  const bool xface = (d == 2 || d == 4);
+  const double rpk = xface ? G.rpy[f] : G.rpx[f];
+  const double rpn = xface ? G.rpy[fb] : G.rpx[fb];
+  // acoef of the face from its own inputs (the momentum coefficient of (ko, o))
+  const double a = expcoef(S.visk[f] * S.hk[f] * G.dsxy[f], S.flux[f]);
+  if (fabs(rpk) > 1.0e-6) {
+    const double val = (a + S.flux[f]) * rpk;
+    us = val * (xface ? duy[o] : dux[o]);
+    vs = val * (xface ? dvy[o] : dvx[o]);
+  } else if (fabs(rpn) > 1.0e-6) {
+    const double val = -a * rpn;
+    us = val * (xface ? duy[nck] : dux[nck]);
+    vs = val * (xface ? dvy[nck] : dvx[nck]);
+  }
+}
+
+// coeffsourcesink_uv(exponentialcoef) (flow_imp.F90:409-466), the skewness
+// deferred correction of joint cells (defcorparagradvec), and bound_uv
+// (boundaries.F90:3310-3490): water-level string faces (bnd_vel_openwse,
+// bnd_vel.f90:35-95) then wall friction (wallfric) or dry-cell rows.
+__global__ void __launch_bounds__(TPB) kf_coef_uv(FlowDev G, FlowState S, const double* dux, const double* duy,
+                                                  const double* dvx, const double* dvy, const double* dpx,
+                                                  const double* dpy) {
+  const int r = blockIdx.x * TPB + threadIdx.x;
+  if (r >= G.n) return;
+  const double h = S.h[r], A = G.areap[r];
+  const double fc = 0.0;  // Coriolis parameter (fcoriolis = 0, flow.F90:60)
+  double su = S.ssu0[r] + (fc * S.v[r] - dpx[r]) * h * A;
+  double sv = S.ssv0[r] + (-fc * S.u[r] - dpy[r]) * h * A;
+  const double cb = 1.0 * S.cfrict[r] * S.uv[r] * A;
+  double sp = S.spuv0[r] - cb;
+  const int nf = G.ncface[r];
+  for (int k = 0; k < nf; ++k) {
+    const int f = fidx(G, k, r);
+    S.acoef[f] = expcoef(S.visk[f] * S.hk[f] * G.dsxy[f], S.flux[f]);
+  }
+  if (G.ider == 2 && G.joint[r]) {
+    double ssu = 0.0, ssv = 0.0;
+    for (int k = 0; k < nf; ++k) {
+      double us = 0.0, vs = 0.0;
+      if ((G.owned[r] >> k) & 1) {
+        defcor_face(G, S, r, k, dux, duy, dvx, dvy, us, vs);
+      } else {
+        const int nck = G.nb[fidx(G, k, r)];
+        if (nck < G.n && G.joint[nck]) {
+          defcor_face(G, S, nck, G.back[fidx(G, k, r)], dux, duy, dvx, dvy, us, vs);
+          us = -us; vs = -vs;
+        }
+      }
+      ssu = ssu + us;
+      ssv = ssv + vs;
+    }
+    su = su - ssu;
+    sv = sv - ssv;
+  }
+  // water-level string faces
+  const unsigned char tm = G.thm[r];
+  if (tm) {
+    for (int k = 0; k < nf; ++k) {
+      if (!((tm >> k) & 1)) continue;
+      const int f = fidx(G, k, r);
+      const int nck = G.nb[f];
+      const double a = upwcoef(S.visk[f] * S.hk[f] * G.dsxy[f], S.flux[f]);
+      const int d = G.dir[f];
+      if (d == 1 || d == 3) {
+        S.u[nck] = G.iwet[r] * S.u[r] * h / S.h[nck];
+        const double vg = fnyd(d) * S.flux[f] / (G.ds[f] * S.hk[f]);
+        S.v[nck] = vg;
+        sv = sv + a * vg;
+      } else {
+        const double ug = fnxd(d) * S.flux[f] / (G.ds[f] * S.hk[f]);
+        S.u[nck] = ug;
+        S.v[nck] = G.iwet[r] * S.v[r] * h / S.h[nck];
+        su = su + a * ug;
+      }
+      sp = sp - a;
+      S.acoef[f] = 0.0;
+    }
+  }
+  double spu = sp, spv = sp;
+  if (G.iwet[r] == 1) {
+    for (int k = 0; k < nf; ++k) {
+      const int f = fidx(G, k, r);
+      const int nck = G.nb[f];
+      if (G.iwet[nck] != 0) continue;
+      const double z0w = S.z0[r] * G.wallfac;
+      const int d = G.dir[f];
+      if (d == 1 || d == 3) {
+        spu = spu - G.ds[f] * S.hk[f] * wallcoef(fabs(G.ry[f]), z0w) * fabs(S.u[r]);
+      } else {
+        spv = spv - G.ds[f] * S.hk[f] * wallcoef(fabs(G.rx[f]), z0w) * fabs(S.v[r]);
+      }
+    }
+  } else {
+    S.u[r] = 0.0; S.v[r] = 0.0;
+    spu = -1.0; spv = -1.0; sp = -1.0;
+    su = 0.0; sv = 0.0;
+  }
+  S.su[r] = su; S.sv[r] = sv; S.sp[r] = sp; S.spu[r] = spu; S.spv[r] = spv;
+}
+
+// coefsourcesink_pp, cell part (flow_imp.F90:604-617)
+__global__ void __launch_bounds__(TPB) kf_pp_cell(FlowDev G, FlowState S, const double* dpx, const double* dpy) {
+  const int r = blockIdx.x * TPB + threadIdx.x;
+  if (r >= G.n) return;
+  double asum = 0.0;
+  const int nf = G.ncface[r];
+  for (int k = 0; k < nf; ++k) asum = asum + S.acoef[fidx(G, k, r)];
+  const double apu = G.iwet[r] * G.relax_uv / fmax(asum - S.sp[r], 1.0e-6);
+  const double ap = apu * G.areap[r];
+  S.apuareap[r] = ap;
+  S.sumu[r] = asum * apu;
+  S.Hu[r] = G.iwet[r] * (S.u[r] + ap * dpx[r] * S.h[r]);
+  S.Hv[r] = G.iwet[r] * (S.v[r] + ap * dpy[r] * S.h[r]);
+}
+
+// Cell-based Green-Gauss gradient of one or two scalars (der_grad_eval,
+// der_lib.f90:726-842; der_gradvec_eval 936-1049) with the lagged
+// cell-reconstruction correction of joint cells (reads the previous gradient).
+template <int NV>
+__global__ void __launch_bounds__(TPB) kf_grad(FlowDev G, const double* a, const double* b, double* ax, double* ay,
+                                               double* bx, double* by, const double* axm, const double* aym,
+                                               const double* bxm, const double* bym) {
+  const int r = blockIdx.x * TPB + threadIdx.x;
+  if (r >= G.n) return;
+  double gax = 0.0, gbx = 0.0, gay = 0.0, gby = 0.0;
+  const int nx = G.ncx[r], ny = G.ncy[r];
+  for (int q = 0; q < nx; ++q) {
+    const int c = G.icx[q * G.n + r];
+    const double w = G.wcx[q * G.n + r];
+    gax = gax + w * a[c];
+    if (NV == 2) gbx = gbx + w * b[c];
+  }
+  for (int q = 0; q < ny; ++q) {
+    const int c = G.icy[q * G.n + r];
+    const double w = G.wcy[q * G.n + r];
+    gay = gay + w * a[c];
+    if (NV == 2) gby = gby + w * b[c];
+  }
+  if (G.ider == 2 && G.joint[r]) {
+    const int mx = G.ngx[r], my = G.ngy[r];
+    for (int q = 0; q < mx; ++q) {
+      const int c = G.igx[q * G.n + r];
+      const double w = G.wgxy[q * G.n + r];
+      gax = gax + w * aym[c];
+      if (NV == 2) gbx = gbx + w * bym[c];
+    }
+    for (int q = 0; q < my; ++q) {
+      const int c = G.igy[q * G.n + r];
+      const double w = G.wgyx[q * G.n + r];
+      gay = gay + w * axm[c];
+      if (NV == 2) gby = gby + w * bxm[c];
+    }
+  }
+  ax[r] = gax; ay[r] = gay;
+  if (NV == 2) { bx[r] = gbx; by[r] = gby; }
+}
+
+// Pressure-correction coefficients on owned faces, mirrored (flow_imp.F90:
+// 622-649), and the Rhie-Chow face flux (flow_imp_flux_skew, flow_imp_flux.f90:
+// 2-169, or _noskew 361-409).
+__global__ void __launch_bounds__(TPB) kf_pp_face(FlowDev G, FlowState S, int skew, const double* dHuy,
+                                                  const double* dHvx, const double* dapx, const double* dapy,
+                                                  const double* dpx, const double* dpy) {
+  const int r = blockIdx.x * TPB + threadIdx.x;
+  if (r >= G.n) return;
+  const unsigned char own = G.owned[r];
+  const int nf = G.ncface[r];
+  const bool jr = skew && G.joint[r];
+  for (int k = 0; k < nf; ++k) {
+    if (!((own >> k) & 1)) continue;
+    const int f = fidx(G, k, r);
+    const int nck = G.nb[f];
+    const int fb = fidx(G, G.back[f], nck);
+    const double hk = S.hk[f], ds = G.ds[f], dn = G.dn[f];
+    double a, fl;
+    const int d = G.dir[f];
+    const double fnx = fnxd(d), fny = fnyd(d);
+    if (G.iwet[r] * G.iwet[nck] == 0) {
+      a = 0.0;
+      fl = 0.0;
+    } else if (nck >= G.n) {
+      a = hk * hk * ds * S.apuareap[r] / (1.0 - S.sumu[r]) / dn;
+      if (skew) {
+        const bool xface = (d == 2 || d == 4);
+        fl = hk * ds * ((xface ? fnx * S.Hu[r] : fny * S.Hv[r]) - S.apuareap[r] * hk * (S.p[nck] - S.p[r]) / dn);
+      } else {
+        fl = hk * ds * ((fnx * S.Hu[r] + fny * S.Hv[r]) - S.apuareap[r] * hk * (S.p[nck] - S.p[r]) / dn);
+      }
+    } else {
+      const double fk = G.fintp[f], fp = 1.0 - fk;
+      const double apv = fk * S.apuareap[nck] + fp * S.apuareap[r];
+      const double suf = fk * S.sumu[nck] + fp * S.sumu[r];
+      a = hk * hk * ds * apv / (1.0 - suf) / dn;
+      if (!skew) {
+        const double huf = fk * S.Hu[nck] + fp * S.Hu[r], hvf = fk * S.Hv[nck] + fp * S.Hv[r];
+        fl = hk * ds * ((fnx * huf + fny * hvf) - apv * hk * (S.p[nck] - S.p[r]) / dn);
+      } else {
+        const bool xface = (d == 2 || d == 4);
+        const double fn = xface ? fnx : fny;
+        const double* H = xface ? S.Hu : S.Hv;
+        if (!jr) {
+          const double hf = fk * H[nck] + fp * H[r];
+          fl = hk * ds * (fn * hf - apv * hk * (S.p[nck] - S.p[r]) / dn);
+        } else {
+          const double rpk = xface ? G.rpy[f] : G.rpx[f];
+          const double rpn = xface ? G.rpy[fb] : G.rpx[fb];
+          const double* dap = xface ? dapy : dapx;
+          const double* dH = xface ? dHuy : dHvx;
+          const double* dp = xface ? dpy : dpx;
+          double ap2, hf, dpf;
+          if (fabs(rpk) > 1.0e-6) {
+            ap2 = fk * S.apuareap[nck] + fp * (S.apuareap[r] + rpk * dap[r]);
+            hf = fk * H[nck] + fp * (H[r] + rpk * dH[r]);
+            dpf = (S.p[nck] - S.p[r] - rpk * dp[r]) / dn;
+          } else if (fabs(rpn) > 1.0e-6) {
+            ap2 = fk * (S.apuareap[nck] + rpn * dap[nck]) + fp * S.apuareap[r];
+            hf = fk * (H[nck] + rpn * dH[nck]) + fp * H[r];
+            dpf = (S.p[nck] + rpn * dp[nck] - S.p[r]) / dn;
+          } else {
+            ap2 = apv;
+            hf = fk * H[nck] + fp * H[r];
+            dpf = (S.p[nck] - S.p[r]) / dn;
+          }
+          fl = hk * ds * (fn * hf - ap2 * hk * dpf);
+        }
+      }
+    }
+    S.acoef[f] = a;
+    S.acoef[fb] = a;
+    S.flux[f] = fl;
+    S.flux[fb] = -fl;
+  }
+}
+
+// skew term fcorr of face (ko, o) for the pressure-correction source
+// (flow_imp.F90:720-765), owner side
+__device__ __forceinline__ double fcorr_face(const FlowDev& G, const FlowState& S, int o, int ko, const double* dppx,
+                                             const double* dppy) {
+  const int f = fidx(G, ko, o);
+  const int nck = G.nb[f];
+  if (G.iwet[o] == 0 || G.iwet[nck] == 0) return 0.0;
+  const int fb = fidx(G, G.back[f], nck);
+  const int d = G.dir[f];
+  const bool xface = (d == 2 || d == 4);
+  const double rpk = xface ? G.rpy[f] : G.rpx[f];
+  const double rpn = (nck < G.nD) ? (xface ? G.rpy[fb] : G.rpx[fb]) : 0.0;
+  const double* dpp = xface ? dppy : dppx;
+  if (fabs(rpk) > 1.0e-6) return -S.acoef[f] * rpk * dpp[o];
+  if (fabs(rpn) > 1.0e-6) return S.acoef[f] * rpn * dpp[nck];
+  return 0.0;
+}
+
+// Pressure-correction source terms (flow_imp.F90:699-711, skew 713-789) and
+// bound_pp for water-level strings (bnd_pp, boundaries.F90:4767-4795) and dry
+// rows (3493-3537).
+__global__ void __launch_bounds__(TPB) kf_pp_src(FlowDev G, FlowState S, int skew, const double* dppx,
+                                                 const double* dppy, const double* wse_of_cell) {
+  const int r = blockIdx.x * TPB + threadIdx.x;
+  if (r >= G.n) return;
+  const int nf = G.ncface[r];
+  double sp = S.sppp0[r];
+  double sf = 0.0;
+  for (int k = 0; k < nf; ++k) sf = sf + S.flux[fidx(G, k, r)];
+  double su = S.sspp0[r] - sf + S.p[r] * sp;
+  if (skew && G.joint[r]) {
+    double fc = 0.0;
+    for (int k = 0; k < nf; ++k) {
+      double v = 0.0;
+      if ((G.owned[r] >> k) & 1) {
+        v = fcorr_face(G, S, r, k, dppx, dppy);
+      } else {
+        const int nck = G.nb[fidx(G, k, r)];
+        if (nck < G.n && G.joint[nck]) v = -fcorr_face(G, S, nck, G.back[fidx(G, k, r)], dppx, dppy);
+      }
+      fc = fc + v;
+    }
+    su = su + 0.2 * fc;
+  }
+  if (G.iwet[r] == 0) {
+    int sumwet = 0;
+    for (int k = 0; k < nf; ++k) { const int c = G.nb[fidx(G, k, r)]; if (c < G.n) sumwet += G.iwet[c]; }
+    double aploc = 0.0;
+    su = 0.0;
+    for (int k = 0; k < nf; ++k) {
+      const int f = fidx(G, k, r), c = G.nb[f];
+      double a;
+      if (sumwet >= 1) a = G.iwet[c];
+      else if (c >= G.n) { S.acoef[f] = 0.0; continue; }
+      else a = G.dsxy[f];
+      S.acoef[f] = a;
+      aploc = aploc + a;
+      su = su + a * S.p[c];
+    }
+    su = su - aploc * S.p[r];
+    sp = 0.0;
+  }
+  const unsigned char tm = G.thm[r];
+  if (tm) {
+    for (int k = 0; k < nf; ++k) {
+      if (!((tm >> k) & 1)) continue;
+      const int f = fidx(G, k, r), c = G.nb[f];
+      const double ppg = wse_of_cell[c] * G.grav - S.p[c];
+      S.pp[c] = ppg;
+      su = su + S.acoef[f] * ppg;
+      sp = sp - S.acoef[f];
+      S.acoef[f] = 0.0;
+    }
+  }
+  S.su[r] = su;
+  S.sp[r] = sp;
+}
+
+// pvfc (flow_imp.F90:797-1072), part 1: wall dummies take pp of their cell.
+__global__ void kf_wall_copy(const int* wc, const int* wg, int nw, double* a) {
+  const int j = blockIdx.x * TPB + threadIdx.x;
+  if (j < nw) a[wg[j]] = a[wc[j]];
+}
+
+// pvfc part 2: velocity and flux corrections (owned faces, mirrored), skew
+// corrections of joint cells' flux.
+__global__ void __launch_bounds__(TPB) kf_pvfc(FlowDev G, FlowState S, int skew, const double* dppx,
+                                               const double* dppy) {
+  const int r = blockIdx.x * TPB + threadIdx.x;
+  if (r >= G.n || G.iwet[r] == 0) return;
+  const double val = S.h[r] * S.apuareap[r] / (1.0 - S.sumu[r] + 1.0e-15);
+  S.u[r] = S.u[r] - val * dppx[r];
+  S.v[r] = S.v[r] - val * dppy[r];
+  const unsigned char own = G.owned[r];
+  const int nf = G.ncface[r];
+  const bool jr = skew && G.joint[r];
+  for (int k = 0; k < nf; ++k) {
+    if (!((own >> k) & 1)) continue;
+    const int f = fidx(G, k, r), nck = G.nb[f];
+    if (G.iwet[nck] == 0) continue;
+    const int fb = fidx(G, G.back[f], nck);
+    double fl = S.flux[f] - S.acoef[f] * (S.pp[nck] - S.pp[r]);
+    if (jr && nck < G.n) {
+      const int d = G.dir[f];
+      const bool xface = (d == 2 || d == 4);
+      const double rpk = xface ? G.rpy[f] : G.rpx[f];
+      const double rpn = xface ? G.rpy[fb] : G.rpx[fb];
+      const double* dpp = xface ? dppy : dppx;
+      if (fabs(rpk) > 1.0e-6) fl = fl + S.acoef[f] * rpk * dpp[r];
+      else if (fabs(rpn) > 1.0e-6) fl = fl - S.acoef[f] * rpn * dpp[nck];
+    }
+    S.flux[f] = fl;
+    S.flux[fb] = -fl;
+  }
+}
+
+// pvfc part 3: p += relax*pp; h = max(hmin, p/g - zb); pp *= facpp (all cells)
+__global__ void __launch_bounds__(TPB) kf_pvfc_p(FlowDev G, FlowState S) {
+  const int r = blockIdx.x * TPB + threadIdx.x;
+  if (r >= G.nD) return;
+  const double p = S.p[r] + G.relax_p * S.pp[r];
+  S.p[r] = p;
+  S.h[r] = fmax(G.hmin, p * G.gravinv - G.zb[r]);
+  S.pp[r] = G.facpp * S.pp[r];
+}
+
+// interp_scal_cell2face (interp_lib.f90:2727-2906) on owned faces, mirrored:
+// ibc 0 (no treatment), 1 (zero gradient at wet/dry faces) or 3 (zero at dry
+// faces), with the skewness correction of joint cells when dphix is given.
+__global__ void __launch_bounds__(TPB) kf_interp(FlowDev G, const double* phi, int ibc, double* phik,
+                                                 const double* dphix, const double* dphiy) {
+  const int r = blockIdx.x * TPB + threadIdx.x;
+  if (r >= G.n) return;
+  const unsigned char own = G.owned[r];
+  const int nf = G.ncface[r];
+  const bool corr = dphix != nullptr && G.joint[r];
+  for (int k = 0; k < nf; ++k) {
+    if (!((own >> k) & 1)) continue;
+    const int f = fidx(G, k, r), nck = G.nb[f];
+    const int fb = fidx(G, G.back[f], nck);
+    const double fk = G.fintp[f];
+    const int wr = G.iwet[r], wn = G.iwet[nck];
+    double v;
+    if (ibc == 0) v = fk * phi[nck] + (1.0 - fk) * phi[r];
+    else if (ibc == 1) {
+      if (wr * wn == 1) v = fk * phi[nck] + (1.0 - fk) * phi[r];
+      else if (wr == 1) v = phi[r];
+      else if (wn == 1) v = phi[nck];
+      else v = 0.5 * (phi[r] + phi[nck]);
+    } else {
+      v = (wr * wn == 1) ? fk * phi[nck] + (1.0 - fk) * phi[r] : 0.0;
+    }
+    if (corr) {
+      const int d = G.dir[f];
+      if (d == 2 || d == 4)
+        v = v + fk * G.rpy[fb] * dphiy[nck] + (1.0 - fk) * G.rpy[f] * dphiy[r];
+      else
+        v = v + fk * G.rpx[fb] * dphix[nck] + (1.0 - fk) * G.rpx[f] * dphix[r];
+      v = fmin(fmax(v, fmin(phi[r], phi[nck])), fmax(phi[r], phi[nck]));
+    }
+    phik[f] = v;
+    phik[fb] = v;
+  }
+}
+
+// flow_grad_interp, cell part (flow_imp.F90:1117-1127): dpx, dpy from face
+// pressures and the face depths hk.
+__global__ void __launch_bounds__(TPB) kf_dp_hk(FlowDev G, FlowState S, double* dpx, double* dpy) {
+  const int r = blockIdx.x * TPB + threadIdx.x;
+  if (r >= G.n) return;
+  double ax = 0.0, ay = 0.0;
+  const int nf = G.ncface[r];
+  for (int k = 0; k < nf; ++k) {
+    const int f = fidx(G, k, r);
+    const int d = G.dir[f];
+    const double pk = S.pk[f];
+    ax = ax + fnxd(d) * G.ds[f] * pk;
+    ay = ay + fnyd(d) * G.ds[f] * pk;
+    S.hk[f] = fmax(G.hmin, pk * G.gravinv - S.zbk[f]);
+  }
+  dpx[r] = ax / G.areap[r];
+  dpy[r] = ay / G.areap[r];
+}
+
+// fric_eval: Manning (friction.F90:647-662, fric_lib.f90:944-996) and
+// fric_curmean_quad (877-905); the eddy viscosity of wet cells, mturbul = 5
+// (flow_eddyvis.f90:136-146).
+__global__ void __launch_bounds__(TPB) kf_fric_vis(FlowDev G, FlowState S, const double* dux, const double* duy,
+                                                   const double* dvx, const double* dvy, int do_vis) {
+  const int r = blockIdx.x * TPB + threadIdx.x;
+  if (r >= G.n) return;
+  const double h = S.h[r];
+  const double cman = G.coefman[r];
+  const double hh = fmax(fmin(10.0, h), 0.1 * cman);
+  const double cd = G.grav * cman * cman / pow(hh, 0.3333);
+  S.cfrict[r] = cd;
+  if (cd != 0.0) S.z0[r] = fmax(h / exp(0.4 / sqrt(cd) + 1.0), 1.0e-6);
+  const double um = sqrt(S.u[r] * S.u[r] + S.v[r] * S.v[r]);
+  S.uv[r] = um;
+  const double taum = 1025.0 * cd * um * um;
+  const double bsv = sqrt(taum / 1025.0 + 1.0e-15);
+  S.bsvel[r] = bsv;
+  if (!do_vis) return;
+  double vis;
+  if (G.iwet[r] == 1) {
+    const double a = dux[r], b = dvy[r], c = duy[r] + dvx[r];
+    const double st = sqrt(2.0 * (a * a + b * b) + c * c);
+    vis = fmin(G.cviscon + G.cvisbot * bsv * h + G.cvishor2areaavg * st, G.cvismax);
+  } else {
+    vis = 1.0e-6;
+  }
+  S.vis[r] = vis;
+}
+
+// eddy viscosity next to dry/dummy neighbours (flow_eddyvis.f90:169-186),
+// run level by level so that the natural-order recurrence is reproduced:
+// wl_cells is one level's list; rd_cur bit kk says the opposite neighbour
+// across face kk is an earlier list cell (read the updated value), otherwise
+// the value before this pass (vis0) is read.
+__global__ void kf_vis_wall(FlowDev G, FlowState S, const int* cells, const unsigned char* rd_cur, int m) {
+  const int j = blockIdx.x * TPB + threadIdx.x;
+  if (j >= m) return;
+  const int r = cells[j];
+  const unsigned char cur = rd_cur[j];
+  const int nf = G.ncface[r];
+  static constexpr int kk_of[5] = {0, 3, 4, 1, 2};
+  for (int k = 0; k < nf; ++k) {
+    const int f = fidx(G, k, r), nck = G.nb[f];
+    if (!(G.iwet[nck] == 0 || nck >= G.n)) continue;
+    const int kkdf = kk_of[G.dir[f]];
+    double cid = 0.0, vs = 0.0;
+    for (int kk = 0; kk < nf; ++kk) {
+      const int fk = fidx(G, kk, r);
+      if (G.dir[fk] != kkdf) continue;
+      const int c = G.nb[fk];
+      // own dummies are written earlier in this same loop: read them as updated
+      const double vc = (((cur >> kk) & 1) || c >= G.n) ? S.vis[c] : S.vis0[c];
+      cid = cid + 1.0;
+      vs = vs + vc - G.cviscon;
+    }
+    const double vi = G.cviscon + vs / (cid + 1.0e-15);
+    S.vis[r] = vi;
+    S.vis[nck] = vi;
+  }
+}
+
+// corner cells (flow_eddyvis.f90:199-209), level by level like kf_vis_wall
+__global__ void kf_vis_corner(FlowDev G, FlowState S, const int* cells, const unsigned char* rd_cur, int m) {
+  const int j = blockIdx.x * TPB + threadIdx.x;
+  if (j >= m) return;
+  const int r = cells[j];
+  const unsigned char cur = rd_cur[j];
+  const int nf = G.ncface[r];
+  double cid = 0.0, vs = 0.0;
+  for (int k = 0; k < nf; ++k) {
+    const int c = G.nb[fidx(G, k, r)];
+    const double w = G.iwet[c];
+    const double vc = ((cur >> k) & 1) ? S.vis[c] : S.vis1[c];
+    cid = cid + w;
+    vs = vs + (vc - G.cviscon) * w;
+  }
+  S.vis[r] = G.cviscon + vs / (cid + 1.0e-15);
+}
+
+// a[idx[j]] = vals[j]
+__global__ void kf_scatter_vals(const int* idx, const double* vals, int m, double* a) {
+  const int j = blockIdx.x * TPB + threadIdx.x;
+  if (j < m) a[idx[j]] = vals[j];
+}
+
+// string dummies take the value of their cell (bndcopy2ghost, boundaries.F90:4417-4437)
+__global__ void kf_copy_to_dummy(const int* cells, const int* dummies, int m, double* a) {
+  const int j = blockIdx.x * TPB + threadIdx.x;
+  if (j < m) a[dummies[j]] = a[cells[j]];
+}
+
+// velface_eta (flow_imp.F90:1245-1573), Cartesian/telescoping branch
+__global__ void __launch_bounds__(TPB) kf_velface_eta(FlowDev G, FlowState S) {
+  const int r = blockIdx.x * TPB + threadIdx.x;
+  if (r >= G.n) return;
+  if (S.h[r] > G.hmin && G.iwet[r] == 1) {
+    double umin = 1e6, umax = -1e6, vmin = 1e6, vmax = -1e6;
+    const int nf = G.ncface[r];
+    for (int k = 0; k < nf; ++k) {
+      const int f = fidx(G, k, r);
+      const double vel = S.flux[f] / (S.hk[f] * G.ds[f]);
+      const int d = G.dir[f];
+      const double uf = fnxd(d) * vel, vf = fnyd(d) * vel;
+      umin = fmin(umin, uf); umax = fmax(umax, uf);
+      vmin = fmin(vmin, vf); vmax = fmax(vmax, vf);
+    }
+    const double u = fmin(fmax(S.u[r], umin), umax), v = fmin(fmax(S.v[r], vmin), vmax);
+    S.u[r] = u; S.v[r] = v;
+    S.eta[r] = S.p[r] * G.gravinv;
+    S.uv[r] = sqrt(u * u + v * v);
+  } else {
+    S.h[r] = fmax(G.hmin, S.h[r]);
+    S.u[r] = 0.0; S.v[r] = 0.0; S.uv[r] = 0.0; S.eta[r] = -999.0;
+  }
+}
+
+// flow_update (CMS_Flow.f90:243-300): time levels; pp and its gradient reset
+__global__ void __launch_bounds__(TPB) kf_update(FlowDev G, FlowState S, double* dppx0, double* dppy0, double* dppx1,
+                                                 double* dppy1) {
+  const int r = blockIdx.x * TPB + threadIdx.x;
+  if (r >= G.nD) return;
+  S.u1[r] = S.u[r]; S.v1[r] = S.v[r]; S.p1[r] = S.p[r]; S.h1[r] = S.h[r];
+  S.pp[r] = 0.0;
+  dppx0[r] = 0.0; dppy0[r] = 0.0; dppx1[r] = 0.0; dppy1[r] = 0.0;
+}
+
+// Solve prologue on device-order face arrays (solvers.f90:230-240): the same
+// arithmetic as k_prologue with acoef read slot-major from the flow state.
+template <typename TS>
+__global__ void __launch_bounds__(TPB) kf_solve_prologue(FlowDev G, const double* __restrict__ acoef, double* ss,
+                                                         const double* __restrict__ sp, double* __restrict__ res,
+                                                         const double* __restrict__ phi,
+                                                         const signed char* __restrict__ fslot_dev, double relax,
+                                                         double* __restrict__ aoff, double* __restrict__ diag,
+                                                         double* __restrict__ b, double* __restrict__ x,
+                                                         TS* __restrict__ aoff2, TS* __restrict__ diag2,
+                                                         double* partials, DevState* st) {
+  double v[1] = {0.0};
+  for (int r = blockIdx.x * TPB + threadIdx.x; r < G.n; r += gridDim.x * TPB) {
+    const double rinv = 1.0 / relax, relaxm = 1.0 - relax;
+    const int nf = G.ncface[r];
+    const double phir = phi[r];
+    double sa = 0.0, sn = 0.0, gh = 0.0;
+    for (int k = 0; k < nf; ++k) {
+      const int f = fidx(G, k, r);
+      const double a = acoef[f];
+      const int c = G.nb[f];
+      const double pn = phi[c];
+      sa = sa + a;
+      sn = sn + a * pn;
+      const int s = fslot_dev[k * G.n + r];
+      if (s >= 0) {
+        aoff[(size_t)s * G.n + r] = a;
+        if (aoff2) aoff2[(size_t)s * G.n + r] = (TS)a;
+      } else {
+        gh = gh + a * pn;
+      }
+    }
+    const double ap = (sa - sp[r]) * rinv;
+    const double ssr = ss[r] + relaxm * phir * ap;
+    ss[r] = ssr;
+    const double rr = G.iwet[r] * (sn + ssr - ap * phir) / ap;
+    res[r] = rr;
+    diag[r] = ap;
+    if (diag2) diag2[r] = (TS)ap;
+    b[r] = ssr + gh;
+    x[r] = phir;
+    v[0] += rr * rr;
+  }
+  if (grid_sum<1>(v, partials, &st->ticket[0])) st->s[S_RMOM] = sqrt(v[0] / (double)G.n);
+}
+
+__global__ void __launch_bounds__(TPB) kf_copy(int n, const double* __restrict__ a, double* __restrict__ b) {
+  const int r = blockIdx.x * TPB + threadIdx.x;
+  if (r < n) b[r] = a[r];
+}
+
+// non-finite scan of the water level (sets flag[1])
+__global__ void __launch_bounds__(TPB) kf_check(FlowDev G, FlowState S) {
+  const int r = blockIdx.x * TPB + threadIdx.x;
+  if (r < G.n && !(isfinite(S.p[r]) && isfinite(S.u[r]) && isfinite(S.v[r]))) S.flag[1] = 1;
+}
+
+}  // namespace cms

@@ -1,0 +1,702 @@
+// Host driver of the device flow step (included at the end of cms_solver.cu so
+// that it shares the solver's handle internals).
+//
+// One cms_flow handle owns the grid metrics in device order, the flow state,
+// and a solver handle whose device order it adopts, so that the assembly
+// kernels write the three systems straight into the solver's matrix buffers.
+#pragma once
+#include <algorithm>
+#include <vector>
+
+#include "cms_flow.cuh"
+#include "cms_flow_geom.h"
+
+struct cms_flow {
+  cms_solver* S = nullptr;
+  cms::FlowGeom geom;
+  cms::FlowDev G{};
+  cms::FlowState st{};
+  cms_flow_opts opts{};
+  int n = 0, nD = 0, nmf = 0;
+  std::vector<int> d2n, n2d;  // device <-> natural numbering of all nD cells
+  std::vector<void*> allocs;
+  size_t bytes = 0;
+  // water-level string (device numbering)
+  int nth = 0;
+  int *d_th_cell = nullptr, *d_th_dummy = nullptr;
+  double* d_wse = nullptr;       // [nth] values of the current step
+  double* d_wse_cell = nullptr;  // [nD] the same, at the dummy cells
+  // wall string
+  int nw = 0;
+  int *d_w_cell = nullptr, *d_w_dummy = nullptr;
+  // eddy-viscosity recurrences, level by level
+  std::vector<int> wall_lvl, corner_lvl;  // level starts (size levels+1)
+  int *d_wall_cells = nullptr, *d_corner_cells = nullptr;
+  unsigned char *d_wall_rd = nullptr, *d_corner_rd = nullptr;
+  signed char* d_fslot_dev = nullptr;  // [nmf][n] ELL slot of face k of device row r
+  // gradient copies: index of the current one
+  int cur_dppx = 0, cur_duv = 0, cur_dH = 0, cur_dap = 0;
+  int* h_flag = nullptr;
+  cms_flow_info last{};
+  cms_solve_info last_solve[3]{};  // u, v, pp of the last outer iteration
+  long long launches = 0;
+  double t_sim = 0.0;
+  double nfaces = 0.0;  // faces of active cells (sum of ncface), for byte counts
+
+  template <typename P>
+  int alloc(P** p, size_t count) {
+    const size_t nb = std::max<size_t>(count, 1) * sizeof(P);
+    if (cudaMalloc((void**)p, nb) != cudaSuccess) return CMS_DEVICE_ERROR;
+    if (cudaMemsetAsync(*p, 0, nb, S->stream) != cudaSuccess) return CMS_DEVICE_ERROR;
+    allocs.push_back((void*)*p);
+    bytes += nb;
+    return CMS_OK;
+  }
+  template <typename P>
+  int upload(P** p, const std::vector<P>& h) {
+    int rc = alloc(p, h.size());
+    if (rc) return rc;
+    if (!h.empty() && cudaMemcpyAsync(*p, h.data(), h.size() * sizeof(P), cudaMemcpyHostToDevice, S->stream))
+      return CMS_DEVICE_ERROR;
+    return CMS_OK;
+  }
+};
+
+namespace cms {
+
+using Flow = ::cms_flow;
+
+#define FCHK(...)                     \
+  do {                                \
+    int rc_ = (__VA_ARGS__);          \
+    if (rc_ != CMS_OK) return rc_;    \
+  } while (0)
+
+// Launch of a flow kernel with error check, launch count and optional timing
+// (profiled under the solver handle's flow class).
+#define FLAUNCH(F, ...) FLAUNCHB(F, 0.0, __VA_ARGS__)
+#define FLAUNCHB(F, BYTES, ...)                                                                   \
+  do {                                                                                            \
+    prof_begin((F)->S);                                                                           \
+    __VA_ARGS__;                                                                                  \
+    (F)->launches++;                                                                              \
+    cudaError_t e_ = cudaGetLastError();                                                          \
+    if (e_ != cudaSuccess) {                                                                      \
+      std::snprintf(g_last_error, sizeof(g_last_error), "flow launch: %s", cudaGetErrorString(e_)); \
+      return CMS_DEVICE_ERROR;                                                                    \
+    }                                                                                             \
+    prof_end((F)->S, P_FLOW, (double)(BYTES));                                                    \
+  } while (0)
+
+// Krylov solve of the system a flow prologue wrote into the FP64 buffers
+// (A64, W64.b, W64.x; A32 too for refinement); the solution stays in W64.x.
+static int solve_core64(Solver* S, int nsolv, int nswp, cms_solve_info* info) {
+  std::memset(info, 0, sizeof(*info));
+  info->ncolors = S->hp.G;
+  info->true_relres = -1.0;
+  if (nsolv != 3 && nsolv != 4) return info->status = CMS_UNSUPPORTED;
+  const int maxit = S->opts.max_iters > 0 ? S->opts.max_iters : nswp;
+  const double tol = S->opts.tol > 0 ? S->opts.tol : 1e-3;
+  const int norm = S->opts.norm == 2 ? 2 : 1;
+  const bool refine = S->opts.precision == CMS_PREC_FP32_REFINE;
+  if (refine) CHK(run_refine(S, nsolv, maxit, tol, info));
+  else CHK(run_krylov<double>(S, S->A64, S->W64, nsolv, maxit, norm, tol, 0));
+  CMS_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, S->stream));
+  CMS_CUDA(cudaStreamSynchronize(S->stream));
+  const DevState& h = *S->h_st;
+  info->rmom = h.s[S_RMOM];
+  if (!refine) {
+    info->iters = h.iter;
+    info->inner = (nsolv == 4) ? h.inner : h.iter;
+    info->relres = h.s[S_RELRES];
+    if (h.nonfinite) info->status = CMS_NONFINITE;
+    else if (!h.converged) info->status = CMS_NOT_CONVERGED;
+  }
+  return info->status;
+}
+
+// Level schedule of an in-place natural-order recurrence over a cell list:
+// cell c reads cells reads[c]; a read of an earlier list cell must see its
+// updated value (next level), any other read sees the value before the pass.
+static void level_schedule(const std::vector<int>& list_nat, const std::vector<std::vector<std::pair<int, int>>>& reads,
+                           const std::vector<int>& n2d, std::vector<int>& lvl_start, std::vector<int>& cells_dev,
+                           std::vector<unsigned char>& rd_cur) {
+  const int m = (int)list_nat.size();
+  std::vector<int> pos_of(n2d.size(), -1), level(m, 0);
+  for (int j = 0; j < m; ++j) pos_of[list_nat[j]] = j;
+  std::vector<unsigned char> mask(m, 0);
+  for (int j = 0; j < m; ++j) {
+    int l = 0;
+    for (auto& rk : reads[j]) {  // (face k, natural cell read)
+      const int q = pos_of[rk.second];
+      if (q >= 0 && q < j) {  // an earlier list cell: read its update
+        l = std::max(l, level[q] + 1);
+        mask[j] |= (unsigned char)(1u << rk.first);
+      }
+    }
+    level[j] = l;
+  }
+  int L = 0;
+  for (int j = 0; j < m; ++j) L = std::max(L, level[j] + 1);
+  lvl_start.assign(L + 1, 0);
+  for (int j = 0; j < m; ++j) lvl_start[level[j] + 1]++;
+  for (int l = 0; l < L; ++l) lvl_start[l + 1] += lvl_start[l];
+  cells_dev.assign(m, 0);
+  rd_cur.assign(m, 0);
+  std::vector<int> fill(lvl_start.begin(), lvl_start.end() - 1);
+  for (int j = 0; j < m; ++j) {
+    const int at = fill[level[j]]++;
+    cells_dev[at] = n2d[list_nat[j]];
+    rd_cur[at] = mask[j];
+  }
+}
+
+static int flow_create(int ncells, int ncellsD, int nmf, const int* c2c, const int* ncface, const int* idirface,
+                       const double* x, const double* y, const double* dx, const double* dy, const double* zb,
+                       const double* coefman, int nth, const int* th_cells, const int* th_faces,
+                       const cms_flow_opts* opts, Flow** out) {
+  if (!out || !c2c || !ncface || !idirface || !x || !y || !dx || !dy || !zb || !coefman || nth < 0 ||
+      (nth > 0 && (!th_cells || !th_faces)))
+    return CMS_BAD_ARGUMENT;
+  auto* F = new Flow();
+  cms_flow_default_opts(&F->opts);
+  if (opts) F->opts = *opts;
+  F->n = ncells; F->nD = ncellsD; F->nmf = nmf;
+  auto fail = [&](int rc) { cms_flow_destroy(F); return rc; };
+  // wet set: active cells and string dummies wet, other dummies are walls
+  std::vector<int> iwet(ncellsD, 0);
+  for (int i = 0; i < ncells; ++i) iwet[i] = 1;
+  std::vector<unsigned char> thm(ncellsD, 0);
+  for (int j = 0; j < nth; ++j) {
+    const int i = th_cells[j] - 1, k = th_faces[j] - 1;
+    if (i < 0 || i >= ncells || k < 0 || k >= nmf) return fail(CMS_BAD_ARGUMENT);
+    const int g = c2c[(size_t)i * nmf + k] - 1;
+    if (g < ncells || g >= ncellsD) return fail(CMS_BAD_ARGUMENT);
+    if (thm[i] & (1u << k)) return fail(CMS_BAD_ARGUMENT);
+    thm[i] |= (unsigned char)(1u << k);
+    iwet[g] = 1;
+  }
+  std::string err = build_flow_geom(ncells, ncellsD, nmf, c2c, ncface, idirface, x, y, dx, dy, zb, iwet.data(),
+                                    F->opts.skewcor != 0, F->geom);
+  if (!err.empty()) {
+    std::snprintf(g_last_error, sizeof(g_last_error), "%s", err.c_str());
+    return fail(CMS_BAD_ARGUMENT);
+  }
+  const FlowGeom& g = F->geom;
+  const bool skew = F->opts.skewcor && g.njoint > 0;
+  F->opts.skewcor = skew ? 1 : 0;
+  // solver on the same grid (its device order is the flow's)
+  cms_solver_opts so;
+  cms_solver_default_opts(&so);
+  so.ordering = F->opts.ordering;
+  so.precision = F->opts.precision;
+  so.tol = F->opts.tol;
+  so.norm = F->opts.norm;
+  so.verify = 0;
+  so.inner_tol = F->opts.inner_tol;
+  so.inner_max = F->opts.inner_max;
+  int rc = cms_solver_create(ncells, ncellsD, nmf, c2c, ncface, iwet.data(), &so, &F->S);
+  if (rc) return fail(rc);
+  Solver* S = F->S;
+  const HostPattern& P = S->hp;
+  const int n = ncells, nD = ncellsD;
+  F->d2n.resize(nD); F->n2d.resize(nD);
+  for (int r = 0; r < n; ++r) { F->d2n[r] = P.perm[r]; F->n2d[P.perm[r]] = r; }
+  for (int i = n; i < nD; ++i) { F->d2n[i] = i; F->n2d[i] = i; }
+  // slot-major face arrays in device order
+  auto faceperm_d = [&](const std::vector<double>& a) {
+    std::vector<double> o((size_t)nmf * nD, 0.0);
+    for (int r = 0; r < nD; ++r)
+      for (int k = 0; k < nmf; ++k) o[(size_t)k * nD + r] = a[(size_t)F->d2n[r] * nmf + k];
+    return o;
+  };
+  auto cellperm_d = [&](const std::vector<double>& a) {
+    std::vector<double> o(nD, 0.0);
+    for (int r = 0; r < nD; ++r) o[r] = a[F->d2n[r]];
+    return o;
+  };
+  std::vector<int> nb((size_t)nmf * nD, -1), ncf(nD);
+  std::vector<signed char> back((size_t)nmf * nD, -1), dir((size_t)nmf * nD, 0), fsd((size_t)nmf * n, -1);
+  std::vector<unsigned char> owned(nD, 0), thd(nD, 0), joint(nD, 0);
+  std::vector<int> iwd(nD);
+  for (int r = 0; r < nD; ++r) {
+    const int i = F->d2n[r];
+    ncf[r] = g.ncface[i];
+    iwd[r] = g.iwet[i];
+    joint[r] = g.joint[i];
+    thd[r] = thm[i];
+    for (int k = 0; k < nmf; ++k) {
+      const int j = g.nb[(size_t)i * nmf + k];
+      nb[(size_t)k * nD + r] = (k < g.ncface[i] && j >= 0) ? F->n2d[j] : -1;
+      back[(size_t)k * nD + r] = (signed char)g.back[(size_t)i * nmf + k];
+      dir[(size_t)k * nD + r] = (signed char)g.dir[(size_t)i * nmf + k];
+      if (g.owned[(size_t)i * nmf + k]) owned[r] |= (unsigned char)(1u << k);
+      if (r < n) fsd[(size_t)k * n + r] = P.fslot[(size_t)i * nmf + k];
+    }
+  }
+  FlowDev& D = F->G;
+  D.n = n; D.nD = nD; D.nmf = nmf; D.nsc = g.nsc; D.ider = g.ider;
+  int *p_ncf, *p_nb, *p_iwet;
+  signed char *p_back, *p_dir;
+  unsigned char *p_owned, *p_thm, *p_joint;
+  if ((rc = F->upload(&p_ncf, ncf)) || (rc = F->upload(&p_nb, nb)) || (rc = F->upload(&p_iwet, iwd)) ||
+      (rc = F->upload(&p_back, back)) || (rc = F->upload(&p_dir, dir)) || (rc = F->upload(&p_owned, owned)) ||
+      (rc = F->upload(&p_thm, thd)) || (rc = F->upload(&p_joint, joint)) || (rc = F->upload(&F->d_fslot_dev, fsd)))
+    return fail(rc);
+  D.ncface = p_ncf; D.nb = p_nb; D.iwet = p_iwet; D.back = p_back; D.dir = p_dir; D.owned = p_owned; D.thm = p_thm;
+  D.joint = p_joint;
+  double *p_ds, *p_dn, *p_dsxy, *p_rx, *p_ry, *p_rpx, *p_rpy, *p_fintp, *p_area, *p_zb, *p_man;
+  if ((rc = F->upload(&p_ds, faceperm_d(g.ds))) || (rc = F->upload(&p_dn, faceperm_d(g.dn))) ||
+      (rc = F->upload(&p_dsxy, faceperm_d(g.dsxy))) || (rc = F->upload(&p_rx, faceperm_d(g.rx))) ||
+      (rc = F->upload(&p_ry, faceperm_d(g.ry))) || (rc = F->upload(&p_rpx, faceperm_d(g.rpx))) ||
+      (rc = F->upload(&p_rpy, faceperm_d(g.rpy))) || (rc = F->upload(&p_fintp, faceperm_d(g.fintp))) ||
+      (rc = F->upload(&p_area, cellperm_d(g.areap))) || (rc = F->upload(&p_zb, cellperm_d(g.zb))))
+    return fail(rc);
+  {
+    std::vector<double> man(nD, 0.0);
+    for (int r = 0; r < n; ++r) man[r] = coefman[F->d2n[r]];
+    if ((rc = F->upload(&p_man, man))) return fail(rc);
+  }
+  D.ds = p_ds; D.dn = p_dn; D.dsxy = p_dsxy; D.rx = p_rx; D.ry = p_ry; D.rpx = p_rpx; D.rpy = p_rpy;
+  D.fintp = p_fintp; D.areap = p_area; D.zb = p_zb; D.coefman = p_man;
+  // gradient operator (wet cells), [q][n] in device numbering
+  {
+    const int nsc = g.nsc;
+    std::vector<int> ncx(n), ncy(n), ngx(n), ngy(n), icx((size_t)nsc * n), icy((size_t)nsc * n),
+        igx((size_t)nsc * n), igy((size_t)nsc * n);
+    std::vector<double> wcx((size_t)nsc * n), wcy((size_t)nsc * n), wgxy((size_t)nsc * n), wgyx((size_t)nsc * n);
+    for (int r = 0; r < n; ++r) {
+      const int i = F->d2n[r];
+      ncx[r] = g.gw_ncx[i]; ncy[r] = g.gw_ncy[i]; ngx[r] = g.gw_ngx[i]; ngy[r] = g.gw_ngy[i];
+      for (int q = 0; q < nsc; ++q) {
+        const size_t s = (size_t)i * nsc + q, d = (size_t)q * n + r;
+        icx[d] = F->n2d[g.gw_icx[s]]; icy[d] = F->n2d[g.gw_icy[s]];
+        igx[d] = F->n2d[g.gw_igx[s]]; igy[d] = F->n2d[g.gw_igy[s]];
+        wcx[d] = g.gw_wcx[s]; wcy[d] = g.gw_wcy[s]; wgxy[d] = g.gw_wgxy[s]; wgyx[d] = g.gw_wgyx[s];
+      }
+    }
+    int *a1, *a2, *a3, *a4, *a5, *a6, *a7, *a8;
+    double *b1, *b2, *b3, *b4;
+    if ((rc = F->upload(&a1, ncx)) || (rc = F->upload(&a2, ncy)) || (rc = F->upload(&a3, icx)) ||
+        (rc = F->upload(&a4, icy)) || (rc = F->upload(&a5, ngx)) || (rc = F->upload(&a6, ngy)) ||
+        (rc = F->upload(&a7, igx)) || (rc = F->upload(&a8, igy)) || (rc = F->upload(&b1, wcx)) ||
+        (rc = F->upload(&b2, wcy)) || (rc = F->upload(&b3, wgxy)) || (rc = F->upload(&b4, wgyx)))
+      return fail(rc);
+    D.ncx = a1; D.ncy = a2; D.icx = a3; D.icy = a4; D.ngx = a5; D.ngy = a6; D.igx = a7; D.igy = a8;
+    D.wcx = b1; D.wcy = b2; D.wgxy = b3; D.wgyx = b4;
+  }
+  // parameters (flow.F90:21-168, friction.F90:44-49)
+  D.grav = 9.81; D.gravinv = 1.0 / 9.81; D.hmin = 0.05; D.hdry = 0.05; D.relax_uv = 0.8; D.relax_p = 1.0;
+  D.facpp = 0.2; D.cviscon = 1.0e-6; D.cvisbot = 0.0667; D.cvismax = 20.0; D.wallfac = 1.0;
+  D.cvishor2areaavg = 0.2 * 0.2 * g.areaavg;
+  // state
+  FlowState& T = F->st;
+  double** cellarrs[] = {&T.p, &T.h, &T.u, &T.v, &T.pp, &T.vis, &T.vis0, &T.vis1, &T.cfrict, &T.z0, &T.uv,
+                         &T.bsvel, &T.eta, &T.u1, &T.v1, &T.p1, &T.h1, &T.su, &T.sv, &T.sp, &T.spu, &T.spv,
+                         &T.ssu0, &T.ssv0, &T.spuv0, &T.sppp0, &T.sspp0, &T.apuareap, &T.sumu, &T.Hu, &T.Hv, &T.res};
+  for (double** a : cellarrs)
+    if ((rc = F->alloc(a, nD))) return fail(rc);
+  double** facearrs[] = {&T.flux, &T.visk, &T.hk, &T.pk, &T.acoef, &T.zbk};
+  for (double** a : facearrs)
+    if ((rc = F->alloc(a, (size_t)nmf * nD))) return fail(rc);
+  for (int c = 0; c < 2; ++c) {
+    double** g2[] = {&T.dpx[c], &T.dpy[c], &T.dux[c], &T.duy[c], &T.dvx[c], &T.dvy[c], &T.dppx[c], &T.dppy[c],
+                     &T.dHux[c], &T.dHuy[c], &T.dHvx[c], &T.dHvy[c], &T.dapx[c], &T.dapy[c], &T.dzbx[c], &T.dzby[c]};
+    for (double** a : g2)
+      if ((rc = F->alloc(a, nD))) return fail(rc);
+  }
+  if ((rc = F->alloc(&T.wsebnd, std::max(nth, 1))) || (rc = F->alloc(&T.flag, 4))) return fail(rc);
+  if ((rc = F->alloc(&F->d_wse_cell, nD))) return fail(rc);
+  F->d_wse = T.wsebnd;
+  if (cudaMallocHost((void**)&F->h_flag, 4 * sizeof(int)) != cudaSuccess) return fail(CMS_DEVICE_ERROR);
+  // strings
+  {
+    F->nth = nth;
+    std::vector<int> tc(nth), tg(nth);
+    for (int j = 0; j < nth; ++j) {
+      const int i = th_cells[j] - 1, k = th_faces[j] - 1;
+      tc[j] = F->n2d[i];
+      tg[j] = F->n2d[c2c[(size_t)i * nmf + k] - 1];
+    }
+    if ((rc = F->upload(&F->d_th_cell, tc)) || (rc = F->upload(&F->d_th_dummy, tg))) return fail(rc);
+    std::vector<int> wc, wg;
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k < g.ncface[i]; ++k) {
+        const int j = g.nb[(size_t)i * nmf + k];
+        if (j >= n && !(thm[i] & (1u << k))) { wc.push_back(F->n2d[i]); wg.push_back(F->n2d[j]); }
+      }
+    F->nw = (int)wc.size();
+    if ((rc = F->upload(&F->d_w_cell, wc)) || (rc = F->upload(&F->d_w_dummy, wg))) return fail(rc);
+  }
+  // eddy-viscosity recurrences next to dry/dummy neighbours and at corners
+  {
+    static const int kk_of[5] = {0, 3, 4, 1, 2};
+    std::vector<int> wl;
+    std::vector<std::vector<std::pair<int, int>>> wr;
+    for (int i = 0; i < n; ++i) {
+      if (g.iwet[i] != 1) continue;
+      bool hit = false;
+      std::vector<std::pair<int, int>> reads;
+      for (int k = 0; k < g.ncface[i]; ++k) {
+        const int j = g.nb[(size_t)i * nmf + k];
+        if (!(g.iwet[j] == 0 || j >= n)) continue;
+        hit = true;
+        const int kkdf = kk_of[g.dir[(size_t)i * nmf + k]];
+        for (int kk = 0; kk < g.ncface[i]; ++kk)
+          if (g.dir[(size_t)i * nmf + kk] == kkdf) reads.push_back({kk, g.nb[(size_t)i * nmf + kk]});
+      }
+      if (hit) { wl.push_back(i); wr.push_back(reads); }
+    }
+    std::vector<int> cells;
+    std::vector<unsigned char> rd;
+    level_schedule(wl, wr, F->n2d, F->wall_lvl, cells, rd);
+    if ((rc = F->upload(&F->d_wall_cells, cells)) || (rc = F->upload(&F->d_wall_rd, rd))) return fail(rc);
+    std::vector<int> cl;
+    std::vector<std::vector<std::pair<int, int>>> cr;
+    for (int i = 0; i < n; ++i) {
+      if (!g.icorner[i]) continue;
+      std::vector<std::pair<int, int>> reads;
+      for (int k = 0; k < g.ncface[i]; ++k) reads.push_back({k, g.nb[(size_t)i * nmf + k]});
+      cl.push_back(i);
+      cr.push_back(reads);
+    }
+    level_schedule(cl, cr, F->n2d, F->corner_lvl, cells, rd);
+    if ((rc = F->upload(&F->d_corner_cells, cells)) || (rc = F->upload(&F->d_corner_rd, rd))) return fail(rc);
+  }
+  for (int i = 0; i < n; ++i) F->nfaces += g.ncface[i];
+  if (cudaStreamSynchronize(S->stream) != cudaSuccess) return fail(CMS_DEVICE_ERROR);
+  *out = F;
+  return CMS_OK;
+}
+
+static inline int fblk(int m) { return (m + TPB - 1) / TPB; }
+// algorithmic bytes of a flow kernel: c cell doubles per active cell, f face
+// doubles per face, plus per-dummy-cell doubles d (connectivity included as
+// 8 bytes per face read)
+static inline double fbytes(const Flow* F, double c, double f, double d = 0.0) {
+  return 8.0 * (c * F->n + f * F->nfaces + d * (F->nD - F->n));
+}
+
+// gradient into the other copy, reading the current one as "previous"
+static int grad1(Flow* F, const double* a, double* const* gx, double* const* gy, int& cur) {
+  const int nx = 1 - cur;
+  FLAUNCHB(F, fbytes(F, 9, 1.5), (kf_grad<1><<<fblk(F->n), TPB, 0, F->S->stream>>>(F->G, a, nullptr, gx[nx], gy[nx], nullptr, nullptr,
+                                                               gx[cur], gy[cur], nullptr, nullptr)));
+  cur = nx;
+  return CMS_OK;
+}
+static int grad2(Flow* F, const double* a, const double* b, double* const* ax, double* const* ay, double* const* bx,
+                 double* const* by, int& cur) {
+  const int nx = 1 - cur;
+  FLAUNCHB(F, fbytes(F, 13, 3), (kf_grad<2><<<fblk(F->n), TPB, 0, F->S->stream>>>(F->G, a, b, ax[nx], ay[nx], bx[nx], by[nx], ax[cur],
+                                                               ay[cur], bx[cur], by[cur])));
+  cur = nx;
+  return CMS_OK;
+}
+
+// solve(acoef,ss,sp,res,phi,n) on the flow state (device order)
+static int flow_solve(Flow* F, double* ss, const double* sp, double* phi, double relax, int nswp, double* rmom,
+                      cms_solve_info* info) {
+  Solver* S = F->S;
+  const bool refine = S->opts.precision == CMS_PREC_FP32_REFINE;
+  // reduction kernel: its grid must stay within the solver's partials buffer
+  FLAUNCHB(F, fbytes(F, 9, 2.6), (kf_solve_prologue<float><<<gsz(F->n), TPB, 0, S->stream>>>(
+                 F->G, F->st.acoef, ss, sp, F->st.res, phi, F->d_fslot_dev, relax, S->A64.aoff, S->A64.diag,
+                 S->W64.b, S->W64.x, refine ? S->A32.aoff : nullptr, refine ? S->A32.diag : nullptr, S->d_part,
+                 S->d_st)));
+  const int rc = solve_core64(S, F->opts.nsolv, nswp, info);
+  if (rc == CMS_DEVICE_ERROR || rc == CMS_UNSUPPORTED || rc == CMS_BAD_ARGUMENT) return rc;
+  FLAUNCHB(F, fbytes(F, 2, 0), (kf_copy<<<fblk(F->n), TPB, 0, S->stream>>>(F->n, S->W64.x, phi)));
+  *rmom = info->rmom;
+  return CMS_OK;
+}
+
+// eddy viscosity with the boundary recurrences and its face values
+static int flow_vis(Flow* F, const double* dux, const double* duy, const double* dvx, const double* dvy) {
+  cudaStream_t s = F->S->stream;
+  FLAUNCHB(F, fbytes(F, 15, 0), (kf_fric_vis<<<fblk(F->n), TPB, 0, s>>>(F->G, F->st, dux, duy, dvx, dvy, 1)));
+  if (F->nth)
+    FLAUNCH(F, (kf_copy_to_dummy<<<fblk(F->nth), TPB, 0, s>>>(F->d_th_cell, F->d_th_dummy, F->nth, F->st.vis)));
+  FLAUNCHB(F, fbytes(F, 2, 0, 2), (kf_copy<<<fblk(F->nD), TPB, 0, s>>>(F->nD, F->st.vis, F->st.vis0)));
+  for (size_t l = 0; l + 1 < F->wall_lvl.size(); ++l) {
+    const int a = F->wall_lvl[l], m = F->wall_lvl[l + 1] - a;
+    FLAUNCH(F, (kf_vis_wall<<<fblk(m), TPB, 0, s>>>(F->G, F->st, F->d_wall_cells + a, F->d_wall_rd + a, m)));
+  }
+  FLAUNCHB(F, fbytes(F, 2, 0, 2), (kf_copy<<<fblk(F->nD), TPB, 0, s>>>(F->nD, F->st.vis, F->st.vis1)));
+  for (size_t l = 0; l + 1 < F->corner_lvl.size(); ++l) {
+    const int a = F->corner_lvl[l], m = F->corner_lvl[l + 1] - a;
+    FLAUNCH(F, (kf_vis_corner<<<fblk(m), TPB, 0, s>>>(F->G, F->st, F->d_corner_cells + a, F->d_corner_rd + a, m)));
+  }
+  FLAUNCHB(F, fbytes(F, 2, 2.5), (kf_interp<<<fblk(F->n), TPB, 0, s>>>(F->G, F->st.vis, 3, F->st.visk, nullptr, nullptr)));
+  return CMS_OK;
+}
+
+// flow_grad_interp: velocity gradients, face pressure, dp/dx, dp/dy, hk
+static int flow_grad_interp(Flow* F) {
+  FlowState& T = F->st;
+  cudaStream_t s = F->S->stream;
+  FCHK(grad2(F, T.u, T.v, T.dux, T.duy, T.dvx, T.dvy, F->cur_duv));
+  const bool skew = F->opts.skewcor != 0;
+  FLAUNCHB(F, fbytes(F, 4, 2.5), (kf_interp<<<fblk(F->n), TPB, 0, s>>>(F->G, T.p, 1, T.pk, skew ? T.dpx[0] : nullptr,
+                                                     skew ? T.dpy[0] : nullptr)));
+  FLAUNCHB(F, fbytes(F, 3, 4.2), (kf_dp_hk<<<fblk(F->n), TPB, 0, s>>>(F->G, T, T.dpx[0], T.dpy[0])));
+  return CMS_OK;
+}
+
+static int flow_init(Flow* F, const double* eta0_nat) {
+  FlowState& T = F->st;
+  cudaStream_t s = F->S->stream;
+  const int nD = F->nD;
+  std::vector<double> p(nD), h(nD), eta(nD);
+  for (int r = 0; r < nD; ++r) {
+    const int i = F->d2n[r];
+    p[r] = eta0_nat[i] * F->G.grav;
+    double hh = p[r] * F->G.gravinv - F->geom.zb[i];
+    if (hh < F->G.hdry) hh = std::max(hh, F->G.hmin);
+    h[r] = hh;
+    eta[r] = F->geom.iwet[i] ? p[r] * F->G.gravinv : -999.0;
+  }
+  CMS_CUDA(cudaMemcpyAsync(T.p, p.data(), nD * sizeof(double), cudaMemcpyHostToDevice, s));
+  CMS_CUDA(cudaMemcpyAsync(T.h, h.data(), nD * sizeof(double), cudaMemcpyHostToDevice, s));
+  CMS_CUDA(cudaMemcpyAsync(T.eta, eta.data(), nD * sizeof(double), cudaMemcpyHostToDevice, s));
+  const size_t cb = nD * sizeof(double), fb = (size_t)F->nmf * nD * sizeof(double);
+  for (double* a : {T.u, T.v, T.pp, T.vis, T.cfrict, T.uv, T.bsvel})
+    CMS_CUDA(cudaMemsetAsync(a, 0, cb, s));
+  for (double* a : {T.flux, T.visk, T.hk, T.pk, T.acoef, T.zbk}) CMS_CUDA(cudaMemsetAsync(a, 0, fb, s));
+  for (int c = 0; c < 2; ++c)
+    for (double* a : {T.dpx[c], T.dpy[c], T.dux[c], T.duy[c], T.dvx[c], T.dvy[c], T.dppx[c], T.dppy[c], T.dHux[c],
+                      T.dHuy[c], T.dHvx[c], T.dHvy[c], T.dapx[c], T.dapy[c], T.dzbx[c], T.dzby[c]})
+      CMS_CUDA(cudaMemsetAsync(a, 0, cb, s));
+  F->cur_dppx = F->cur_duv = F->cur_dH = F->cur_dap = 0;
+  CMS_CUDA(cudaMemsetAsync(T.flag, 0, 4 * sizeof(int), s));
+  // bed slope with the all-cells operator and the face bed elevation (prestart.f90:317-318)
+  {
+    const FlowGeom& g = F->geom;
+    const int n = F->n, nsc = g.nsc;
+    std::vector<double> zbr(nD), zx(nD, 0.0), zy(nD, 0.0);
+    for (int r = 0; r < nD; ++r) zbr[r] = g.zb[F->d2n[r]];
+    for (int i = 0; i < n; ++i) {
+      double ax = 0, ay = 0;
+      for (int q = 0; q < g.ga_ncx[i]; ++q) ax += g.ga_wcx[(size_t)i * nsc + q] * g.zb[g.ga_icx[(size_t)i * nsc + q]];
+      for (int q = 0; q < g.ga_ncy[i]; ++q) ay += g.ga_wcy[(size_t)i * nsc + q] * g.zb[g.ga_icy[(size_t)i * nsc + q]];
+      zx[F->n2d[i]] = ax; zy[F->n2d[i]] = ay;
+    }
+    CMS_CUDA(cudaMemcpyAsync(T.dzbx[0], zx.data(), cb, cudaMemcpyHostToDevice, s));
+    CMS_CUDA(cudaMemcpyAsync(T.dzby[0], zy.data(), cb, cudaMemcpyHostToDevice, s));
+    CMS_CUDA(cudaStreamSynchronize(s));
+    FLAUNCH(F, (kf_interp<<<fblk(n), TPB, 0, s>>>(F->G, F->G.zb, 0, T.zbk, F->opts.skewcor ? T.dzbx[0] : nullptr,
+                                                  F->opts.skewcor ? T.dzby[0] : nullptr)));
+  }
+  FCHK(flow_grad_interp(F));
+  FCHK(flow_vis(F, T.dux[F->cur_duv], T.duy[F->cur_duv], T.dvx[F->cur_duv], T.dvy[F->cur_duv]));
+  // time levels
+  FLAUNCH(F, (kf_update<<<fblk(nD), TPB, 0, s>>>(F->G, T, T.dppx[0], T.dppy[0], T.dppx[1], T.dppy[1])));
+  CMS_CUDA(cudaStreamSynchronize(s));
+  F->t_sim = 0.0;
+  return CMS_OK;
+}
+
+// check_conv (flow_imp.F90:1576-1747), dtvar off: 0 divergent, 1 continue, 2 converged
+static int check_conv(const double rm[4], double rmom0[4], double rmom1[4], int niter, int maxit) {
+  if (niter <= 2)
+    for (int q = 1; q <= 3; ++q) { rmom0[q] = std::max(rm[q], 1e-15); rmom1[q] = rmom0[q]; }
+  const double rmommax = std::max(rm[1], std::max(rm[2], rm[3]));
+  if (rmommax > 5.0) return 0;
+  if (niter <= 5) return 1;
+  const int nhalf = maxit / 2;
+  const double rp = rm[1] / rmom0[1];
+  const double ruv = std::max(rm[2] / rmom0[2], rm[3] / rmom0[3]);
+  if ((rp >= 0.5 * 10.0 || ruv >= 1.0 * 10.0) && rm[1] > 1e-4) return 0;
+  if (niter == maxit && (rp >= 0.5 || ruv >= 1.0) && rm[1] > 1e-3) return 0;
+  if (niter == maxit && (rp >= 0.5 / 5.0 || ruv >= 1.0 / 5.0) && rm[1] > 1e-4) return 0;
+  const double rmomuv = std::max(rm[2], rm[3]);
+  if (rm[1] <= 1e-8 && rmomuv <= 1e-7) return 2;
+  if (niter == maxit && (rm[1] > 1e-3 || rmomuv > 1e-2)) return 0;
+  if (niter == maxit && (rm[1] > 1e-4 || rmomuv > 1e-3)) return 0;
+  if (niter <= nhalf || niter % 2 != 0) return 1;
+  const double rchp = rmom1[1] - rm[1];
+  const double rchuv = std::max(rmom1[2], rmom1[3]) - rmomuv;
+  if (rchp < 0.0 || rchuv < 0.0) return 1;
+  if (rchp <= 1e-8 && rchuv <= 1e-7) return 2;
+  for (int q = 1; q <= 3; ++q) rmom1[q] = rm[q];
+  return 1;
+}
+
+static int flow_step(Flow* F, double dt, const double* wsebnd, cms_flow_info* info) {
+  FlowState& T = F->st;
+  Solver* S = F->S;
+  cudaStream_t s = S->stream;
+  cms_flow_info loc{};
+  if (!info) info = &loc;
+  std::memset(info, 0, sizeof(*info));
+  if (F->nth) {  // water levels of the string, placed on the string's dummies
+    CMS_CUDA(cudaMemcpyAsync(F->d_wse, wsebnd, F->nth * sizeof(double), cudaMemcpyHostToDevice, s));
+    FLAUNCH(F, (kf_scatter_vals<<<fblk(F->nth), TPB, 0, s>>>(F->d_th_dummy, F->d_wse, F->nth, F->d_wse_cell)));
+  }
+  FLAUNCHB(F, fbytes(F, 13, 0, 3), (kf_static<<<fblk(F->nD), TPB, 0, s>>>(F->G, T, dt)));
+  const int maxit = F->opts.maxit > 0 ? F->opts.maxit : 20 + F->n / 10000;
+  double rm[4] = {0, 0, 0, 0}, rmom0[4] = {0, 0, 0, 0}, rmom1[4] = {0, 0, 0, 0};
+  int iconv = 1, niter = 0;
+  long long kry = 0;
+  const bool skew = F->opts.skewcor != 0;
+  for (niter = 1; niter <= maxit; ++niter) {
+    const int cd = F->cur_duv;
+    FLAUNCHB(F, fbytes(F, 16.5, 5.6), (kf_coef_uv<<<fblk(F->n), TPB, 0, s>>>(F->G, T, T.dux[cd], T.duy[cd], T.dvx[cd], T.dvy[cd], T.dpx[0],
+                                                      T.dpy[0])));
+    cms_solve_info* si = F->last_solve;
+    std::memset(si, 0, 3 * sizeof(cms_solve_info));
+    FCHK(flow_solve(F, T.su, T.spu, T.u, F->G.relax_uv, F->opts.nswp_uv, &rm[2], &si[0]));
+    kry += si[0].iters;
+    if (si[0].status == CMS_NONFINITE) { iconv = 0; break; }
+    FCHK(flow_solve(F, T.sv, T.spv, T.v, F->G.relax_uv, F->opts.nswp_uv, &rm[3], &si[1]));
+    kry += si[1].iters;
+    if (si[1].status == CMS_NONFINITE) { iconv = 0; break; }
+    FLAUNCHB(F, fbytes(F, 11.5, 1), (kf_pp_cell<<<fblk(F->n), TPB, 0, s>>>(F->G, T, T.dpx[0], T.dpy[0])));
+    if (skew) {
+      FCHK(grad2(F, T.Hu, T.Hv, T.dHux, T.dHuy, T.dHvx, T.dHvy, F->cur_dH));
+      FCHK(grad1(F, T.apuareap, T.dapx, T.dapy, F->cur_dap));
+    }
+    FLAUNCHB(F, fbytes(F, 8, 5), (kf_pp_face<<<fblk(F->n), TPB, 0, s>>>(F->G, T, skew ? 1 : 0, T.dHuy[F->cur_dH], T.dHvx[F->cur_dH],
+                                                      T.dapx[F->cur_dap], T.dapy[F->cur_dap], T.dpx[0], T.dpy[0])));
+    FLAUNCHB(F, fbytes(F, 6, 1.2), (kf_pp_src<<<fblk(F->n), TPB, 0, s>>>(F->G, T, skew ? 1 : 0, T.dppx[F->cur_dppx], T.dppy[F->cur_dppx],
+                                                     F->d_wse_cell)));
+    FCHK(flow_solve(F, T.su, T.sp, T.pp, 1.0, F->opts.nswp_pp, &rm[1], &si[2]));
+    kry += si[2].iters;
+    if (si[2].status == CMS_NONFINITE) { iconv = 0; break; }
+    if (F->nw) FLAUNCH(F, (kf_wall_copy<<<fblk(F->nw), TPB, 0, s>>>(F->d_w_cell, F->d_w_dummy, F->nw, T.pp)));
+    FCHK(grad1(F, T.pp, T.dppx, T.dppy, F->cur_dppx));
+    FLAUNCHB(F, fbytes(F, 9, 2.5), (kf_pvfc<<<fblk(F->n), TPB, 0, s>>>(F->G, T, skew ? 1 : 0, T.dppx[F->cur_dppx], T.dppy[F->cur_dppx])));
+    FLAUNCHB(F, fbytes(F, 6, 0, 6), (kf_pvfc_p<<<fblk(F->nD), TPB, 0, s>>>(F->G, T)));
+    if (F->nw) FLAUNCH(F, (kf_wall_copy<<<fblk(F->nw), TPB, 0, s>>>(F->d_w_cell, F->d_w_dummy, F->nw, T.p)));
+    FCHK(flow_grad_interp(F));
+    const int c2 = F->cur_duv;
+    FCHK(flow_vis(F, T.dux[c2], T.duy[c2], T.dvx[c2], T.dvy[c2]));
+    iconv = check_conv(rm, rmom0, rmom1, niter, maxit);
+    if (iconv == 0 || iconv == 2) break;
+  }
+  if (niter > maxit) niter = maxit;
+  FLAUNCHB(F, fbytes(F, 8, 3.2), (kf_velface_eta<<<fblk(F->n), TPB, 0, s>>>(F->G, T)));
+  FLAUNCH(F, (kf_fric_vis<<<fblk(F->n), TPB, 0, s>>>(F->G, T, nullptr, nullptr, nullptr, nullptr, 0)));
+  FLAUNCHB(F, fbytes(F, 13, 0, 13), (kf_update<<<fblk(F->nD), TPB, 0, s>>>(F->G, T, T.dppx[0], T.dppy[0], T.dppx[1], T.dppy[1])));
+  FLAUNCH(F, (kf_check<<<fblk(F->n), TPB, 0, s>>>(F->G, T)));
+  CMS_CUDA(cudaMemcpyAsync(F->h_flag, T.flag, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CMS_CUDA(cudaStreamSynchronize(s));
+  F->t_sim += dt;
+  info->niter = niter;
+  info->iconv = iconv;
+  info->rmom_p = rm[1]; info->rmom_u = rm[2]; info->rmom_v = rm[3];
+  info->krylov_iters = kry;
+  info->status = CMS_OK;
+  if (F->h_flag[0]) info->status = CMS_UNSUPPORTED;       // a wet cell fell below the drying depth
+  if (F->h_flag[1] || iconv == 0) info->status = CMS_NONFINITE;
+  F->last = *info;
+  return info->status;
+}
+
+}  // namespace cms
+
+extern "C" {
+
+void cms_flow_default_opts(cms_flow_opts* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->nsolv = 4;
+  o->ordering = CMS_ORDER_MULTICOLOR;
+  o->precision = CMS_PREC_FP64;
+  o->norm = 1;
+  o->tol = 1.0e-3;
+  o->nswp_pp = 20;
+  o->nswp_uv = 5;
+  o->maxit = 0;
+  o->skewcor = 1;
+  o->inner_tol = 1.0e-2;
+  o->inner_max = 50;
+}
+
+int cms_flow_create(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, const int* ncface,
+                    const int* idirface, const double* x, const double* y, const double* dx, const double* dy,
+                    const double* zb, const double* coefman, int nth, const int* th_cells, const int* th_faces,
+                    const cms_flow_opts* opts, cms_flow** out) {
+  return cms::flow_create(ncells, ncellsD, nmaxfaces, cell2cell, ncface, idirface, x, y, dx, dy, zb, coefman, nth,
+                          th_cells, th_faces, opts, out);
+}
+
+int cms_flow_init(cms_flow* f, const double* eta0) {
+  if (!f || !eta0) return CMS_BAD_ARGUMENT;
+  return cms::flow_init(f, eta0);
+}
+
+int cms_flow_step(cms_flow* f, double dt, const double* wsebnd, cms_flow_info* info) {
+  if (!f || dt <= 0.0 || (f->nth > 0 && !wsebnd)) return CMS_BAD_ARGUMENT;
+  return cms::flow_step(f, dt, wsebnd, info);
+}
+
+int cms_flow_get(cms_flow* f, int which, double* out) {
+  if (!f || !out) return CMS_BAD_ARGUMENT;
+  const int nD = f->nD, nmf = f->nmf;
+  cms::FlowState& T = f->st;
+  const double* cell = nullptr;
+  const double* face = nullptr;
+  switch (which) {
+    case CMS_FLOW_P: cell = T.p; break;
+    case CMS_FLOW_H: cell = T.h; break;
+    case CMS_FLOW_U: cell = T.u; break;
+    case CMS_FLOW_V: cell = T.v; break;
+    case CMS_FLOW_ETA: cell = T.eta; break;
+    case CMS_FLOW_VIS: cell = T.vis; break;
+    case CMS_FLOW_CFRICT: cell = T.cfrict; break;
+    case CMS_FLOW_DPX: cell = T.dpx[0]; break;
+    case CMS_FLOW_DPY: cell = T.dpy[0]; break;
+    case CMS_FLOW_FLUX: face = T.flux; break;
+    case CMS_FLOW_VISK: face = T.visk; break;
+    case CMS_FLOW_HK: face = T.hk; break;
+    case CMS_FLOW_ACOEF: face = T.acoef; break;
+    case CMS_FLOW_FINTP: face = f->G.fintp; break;
+    case CMS_FLOW_ZBK: face = T.zbk; break;
+    default: return CMS_BAD_ARGUMENT;
+  }
+  cudaStream_t s = f->S->stream;
+  if (cell) {
+    std::vector<double> h(nD);
+    if (cudaMemcpyAsync(h.data(), cell, nD * sizeof(double), cudaMemcpyDeviceToHost, s) ||
+        cudaStreamSynchronize(s))
+      return CMS_DEVICE_ERROR;
+    for (int r = 0; r < nD; ++r) out[f->d2n[r]] = h[r];
+  } else {
+    std::vector<double> h((size_t)nmf * nD);
+    if (cudaMemcpyAsync(h.data(), face, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s) ||
+        cudaStreamSynchronize(s))
+      return CMS_DEVICE_ERROR;
+    for (int r = 0; r < nD; ++r)
+      for (int k = 0; k < nmf; ++k) out[(size_t)f->d2n[r] * nmf + k] = h[(size_t)k * nD + r];
+  }
+  return CMS_OK;
+}
+
+int cms_flow_last_info(const cms_flow* f, cms_flow_info* info) {
+  if (!f || !info) return CMS_BAD_ARGUMENT;
+  *info = f->last;
+  return CMS_OK;
+}
+
+int cms_flow_last_solves(const cms_flow* f, cms_solve_info* info3) {
+  if (!f || !info3) return CMS_BAD_ARGUMENT;
+  for (int q = 0; q < 3; ++q) info3[q] = f->last_solve[q];
+  return CMS_OK;
+}
+
+cms_solver* cms_flow_solver(cms_flow* f) { return f ? f->S : nullptr; }
+long long cms_flow_launches(const cms_flow* f) { return f ? f->launches + (f->S ? f->S->launches : 0) : 0; }
+size_t cms_flow_device_bytes(const cms_flow* f) { return f ? f->bytes + (f->S ? f->S->bytes : 0) : 0; }
+int cms_flow_njoint(const cms_flow* f) { return f ? f->geom.njoint : -1; }
+
+void cms_flow_destroy(cms_flow* f) {
+  if (!f) return;
+  if (f->S) cudaStreamSynchronize(f->S->stream);
+  for (void* p : f->allocs) cudaFree(p);
+  if (f->h_flag) cudaFreeHost(f->h_flag);
+  if (f->S) cms_solver_destroy(f->S);
+  delete f;
+}
+
+}  // extern "C"

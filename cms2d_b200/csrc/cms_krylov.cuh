@@ -32,9 +32,8 @@ __global__ void __launch_bounds__(TPB) k_prologue(int n, int nmf, const T* __res
                                                   T* __restrict__ diag, T* __restrict__ b, T* __restrict__ x,
                                                   TS* __restrict__ aoff2, TS* __restrict__ diag2,
                                                   double* partials, DevState* st) {
-  const int i = blockIdx.x * TPB + threadIdx.x;
   double v[1] = {0.0};
-  if (i < n) {
+  for (int i = blockIdx.x * TPB + threadIdx.x; i < n; i += gridDim.x * TPB) {
     const T rinv = T(1) / relax;
     const T relaxm = T(1) - relax;
     const int nf = ncface[i];
@@ -67,7 +66,7 @@ __global__ void __launch_bounds__(TPB) k_prologue(int n, int nmf, const T* __res
     if (diag2) diag2[r] = (TS)ap;
     b[r] = ssi + gh;
     x[r] = phii;
-    v[0] = (double)resi * (double)resi;
+    v[0] += (double)resi * (double)resi;
   }
   if (grid_sum<1>(v, partials, &st->ticket[0])) {
     st->s[S_RMOM] = sqrt(v[0] / (double)n);
@@ -78,8 +77,7 @@ __global__ void __launch_bounds__(TPB) k_prologue(int n, int nmf, const T* __res
 template <typename TD, typename TS>
 __global__ void __launch_bounds__(TPB) k_scatter(int n, const int* __restrict__ perm, const TS* __restrict__ x,
                                                  TD* __restrict__ phi) {
-  const int r = blockIdx.x * TPB + threadIdx.x;
-  if (r < n) phi[perm[r]] = (TD)x[r];
+  for (int r = blockIdx.x * TPB + threadIdx.x; r < n; r += gridDim.x * TPB) phi[perm[r]] = (TD)x[r];
 }
 
 // ----------------------------------------------------------------------------
@@ -88,12 +86,12 @@ __global__ void __launch_bounds__(TPB) k_scatter(int n, const int* __restrict__ 
 // l = a_rj / u_jj; then every upper entry (j,k) of row j updates the diagonal
 // (k == r) or an entry of row r with the same column.
 template <typename T>
-__global__ void __launch_bounds__(TPB) k_ilu0(int n, int r0, int r1, int KL, int kl, int ku,
-                                              const int* __restrict__ col, const signed char* __restrict__ nup,
-                                              const T* __restrict__ aoff, const T* __restrict__ diag, T* luoff,
-                                              T* invd) {
-  const int r = r0 + blockIdx.x * TPB + threadIdx.x;
-  if (r >= r1) return;
+__global__ void __launch_bounds__(TPB) k_ilu0(int n, int r0, int r1, int KL, int klg, int kug,
+                                              const int* __restrict__ col, const signed char* __restrict__ nlo,
+                                              const signed char* __restrict__ nup, const T* __restrict__ aoff,
+                                              const T* __restrict__ diag, T* luoff, T* invd) {
+ for (int r = r0 + blockIdx.x * TPB + threadIdx.x; r < r1; r += gridDim.x * TPB) {
+  const int kl = min(klg, (int)nlo[r]), ku = min(kug, (int)nup[r]);
   T al[KMAX], au[KMAX];
   int cl[KMAX], cu[KMAX];
 #pragma unroll
@@ -136,6 +134,7 @@ __global__ void __launch_bounds__(TPB) k_ilu0(int n, int r0, int r1, int KL, int
     if (s < kl) luoff[(size_t)s * n + r] = al[s];
     if (s < ku) luoff[(size_t)(KL + s) * n + r] = au[s];
   }
+ }
 }
 
 // ----------------------------------------------------------------------------
@@ -154,19 +153,23 @@ struct GmVecs {
 };
 
 template <typename T, int MODE>
-__global__ void __launch_bounds__(TPB) k_fwd(int n, int r0, int r1, int kl, int step, const int* __restrict__ col,
-                                             const T* __restrict__ luoff, T* z, const T* __restrict__ yin, T* p,
-                                             T* r_, const T* __restrict__ u, T* x, GmVecs gv, const DevState* st) {
+__global__ void __launch_bounds__(TPB) k_fwd(int n, int r0, int r1, int klg, int step, const int* __restrict__ col,
+                                             const signed char* __restrict__ nlo, const T* __restrict__ luoff, T* z,
+                                             const T* __restrict__ yin, T* p, T* r_, const T* __restrict__ u, T* x,
+                                             GmVecs gv, const DevState* st) {
   if (st->done) return;
   if (MODE == FWD_GM_SCALE && !st->active) return;
-  const int r = r0 + blockIdx.x * TPB + threadIdx.x;
-  if (r >= r1) return;
+ for (int r = r0 + blockIdx.x * TPB + threadIdx.x; r < r1; r += gridDim.x * TPB) {
+  const int kl = klg > 0 ? (int)nlo[r] : 0;
   T y;
   if (MODE == FWD_PLAIN) {
     y = yin[r];
   } else if (MODE == FWD_BICG_P) {
-    const T bet = (T)st->s[S_BET], gam = (T)st->s[S_GAM], alf = (T)st->s[S_ALF], bet0 = (T)st->s[S_BET0];
-    const T omg = bet * gam / (alf * bet0 + (T)SMALL);
+    // scalars are formed in FP64 (an FP32 solve of a tiny right-hand side
+    // would otherwise underflow them to 0/0) and applied in T
+    const double bet = st->s[S_BET], gam = st->s[S_GAM], alfd = st->s[S_ALF], bet0 = st->s[S_BET0];
+    const T omg = (T)(bet * gam / (alfd * bet0 + SMALL));
+    const T alf = (T)alfd;
     y = r_[r] + omg * (p[r] - alf * u[r]);
     p[r] = y;
   } else if (MODE == FWD_BICG_R) {
@@ -190,18 +193,20 @@ __global__ void __launch_bounds__(TPB) k_fwd(int n, int r0, int r1, int kl, int 
   for (int s = 0; s < KMAX; ++s)
     if (s < kl) acc = acc - luoff[(size_t)s * n + r] * z[col[(size_t)s * n + r]];
   z[r] = acc;
+ }
 }
 
 // Backward sweep of one group: z_r = invd_r * (z_r - sum_{upper} u_rk z_k)
 // (sparse.f90:256-261); FINAL also adds the result to x (pgmres.f90:226).
 template <typename T, bool FINAL>
-__global__ void __launch_bounds__(TPB) k_bwd(int n, int r0, int r1, int KL, int ku, const int* __restrict__ col,
-                                             const T* __restrict__ luoff, const T* __restrict__ invd, T* z, T* x,
-                                             int need_active, const DevState* st) {
+__global__ void __launch_bounds__(TPB) k_bwd(int n, int r0, int r1, int KL, int kug, const int* __restrict__ col,
+                                             const signed char* __restrict__ nup, const T* __restrict__ luoff,
+                                             const T* __restrict__ invd, T* z, T* x, int need_active,
+                                             const DevState* st) {
   if (st->done) return;
   if (need_active && !st->active) return;
-  const int r = r0 + blockIdx.x * TPB + threadIdx.x;
-  if (r >= r1) return;
+ for (int r = r0 + blockIdx.x * TPB + threadIdx.x; r < r1; r += gridDim.x * TPB) {
+  const int ku = kug > 0 ? (int)nup[r] : 0;
   T acc = z[r];
 #pragma unroll
   for (int t = 0; t < KMAX; ++t)
@@ -209,6 +214,7 @@ __global__ void __launch_bounds__(TPB) k_bwd(int n, int r0, int r1, int KL, int 
   const T zr = invd[r] * acc;
   z[r] = zr;
   if (FINAL) x[r] = x[r] + zr;
+ }
 }
 
 // ----------------------------------------------------------------------------
@@ -222,18 +228,20 @@ enum SpmvMode : int {
 
 template <typename T, int MODE>
 __global__ void __launch_bounds__(TPB) k_spmv(int n, int KL, GroupTab tab, int step, const int* __restrict__ col,
-                                              const T* __restrict__ aoff, const T* __restrict__ diag,
-                                              const T* __restrict__ z, T* __restrict__ y, const T* __restrict__ d1,
-                                              double* partials, DevState* st) {
+                                              const signed char* __restrict__ nlo,
+                                              const signed char* __restrict__ nup, const T* __restrict__ aoff,
+                                              const T* __restrict__ diag, const T* __restrict__ z,
+                                              T* __restrict__ y, const T* __restrict__ d1, double* partials,
+                                              DevState* st) {
   if (st->done) return;
   if (MODE == SPMV_GM && !st->active) return;
   const int g = tab_group(tab, blockIdx.x);
-  const int r = tab.start[g] + (blockIdx.x - tab.blk[g]) * TPB + threadIdx.x;
+  const int stride = (tab.blk[g + 1] - tab.blk[g]) * TPB;
   double v[MODE == SPMV_BICG_V ? 2 : 1];
 #pragma unroll
   for (int q = 0; q < (MODE == SPMV_BICG_V ? 2 : 1); ++q) v[q] = 0.0;
-  if (r < tab.start[g + 1]) {
-    const int kl = tab.kl[g], ku = tab.ku[g];
+  for (int r = tab.start[g] + (blockIdx.x - tab.blk[g]) * TPB + threadIdx.x; r < tab.start[g + 1]; r += stride) {
+    const int kl = tab.kl[g] > 0 ? (int)nlo[r] : 0, ku = tab.ku[g] > 0 ? (int)nup[r] : 0;
     T sum = T(0);
 #pragma unroll
     for (int s = 0; s < KMAX; ++s)
@@ -243,19 +251,19 @@ __global__ void __launch_bounds__(TPB) k_spmv(int n, int KL, GroupTab tab, int s
       if (t < ku) sum = sum + aoff[(size_t)(KL + t) * n + r] * z[col[(size_t)(KL + t) * n + r]];
     const T yr = diag[r] * z[r] - sum;
     y[r] = yr;
-    if (MODE == SPMV_BICG_U) v[0] = (double)yr * (double)d1[r];
-    if (MODE == SPMV_BICG_V) { v[0] = (double)yr * (double)d1[r]; v[1] = (double)yr * (double)yr; }
-    if (MODE == SPMV_GM) v[0] = (double)d1[r] * (double)yr;
+    if (MODE == SPMV_BICG_U) v[0] += (double)yr * (double)d1[r];
+    if (MODE == SPMV_BICG_V) { v[0] += (double)yr * (double)d1[r]; v[1] += (double)yr * (double)yr; }
+    if (MODE == SPMV_GM) v[0] += (double)d1[r] * (double)yr;
   }
   if (grid_sum(v, partials, &st->ticket[1])) {
     if (MODE == SPMV_BICG_U) {
       st->s[S_UKR0] = v[0];
-      st->s[S_GAM] = (double)((T)st->s[S_BET] / (T)v[0]);
+      st->s[S_GAM] = st->s[S_BET] / v[0];
       st->s[S_BET0] = st->s[S_BET];
     } else if (MODE == SPMV_BICG_V) {
       st->s[S_SUM1] = v[0];
       st->s[S_SUM2] = v[1];
-      st->s[S_ALF] = (double)((T)v[0] / max((T)v[1], (T)SMALL));
+      st->s[S_ALF] = v[0] / fmax(v[1], SMALL);
     } else {
       st->s[S_HH + 0 * 3 + (step - 1)] = v[0];
     }
@@ -268,19 +276,20 @@ __global__ void __launch_bounds__(TPB) k_spmv(int n, int KL, GroupTab tab, int s
 template <typename T>
 __global__ void __launch_bounds__(TPB) k_bicg_init(int n, int KL, GroupTab tab, int xzero, int maxit, int norm,
                                                    double tol, const int* __restrict__ col,
-                                                   const T* __restrict__ aoff, const T* __restrict__ diag,
-                                                   const T* __restrict__ b, T* x, T* r_, T* r0, T* p, T* u, T* v_,
-                                                   double* partials, DevState* st) {
+                                                   const signed char* __restrict__ nlo,
+                                                   const signed char* __restrict__ nup, const T* __restrict__ aoff,
+                                                   const T* __restrict__ diag, const T* __restrict__ b, T* x, T* r_,
+                                                   T* r0, T* p, T* u, T* v_, double* partials, DevState* st) {
   const int g = tab_group(tab, blockIdx.x);
-  const int r = tab.start[g] + (blockIdx.x - tab.blk[g]) * TPB + threadIdx.x;
+  const int stride = (tab.blk[g + 1] - tab.blk[g]) * TPB;
   double v[2] = {0.0, 0.0};
-  if (r < tab.start[g + 1]) {
+  for (int r = tab.start[g] + (blockIdx.x - tab.blk[g]) * TPB + threadIdx.x; r < tab.start[g + 1]; r += stride) {
     T term;
     if (xzero) {
       x[r] = T(0);
       term = b[r];
     } else {
-      const int kl = tab.kl[g], ku = tab.ku[g];
+      const int kl = tab.kl[g] > 0 ? (int)nlo[r] : 0, ku = tab.ku[g] > 0 ? (int)nup[r] : 0;
       T sum = T(0);
 #pragma unroll
       for (int s = 0; s < KMAX; ++s)
@@ -296,8 +305,8 @@ __global__ void __launch_bounds__(TPB) k_bicg_init(int n, int KL, GroupTab tab, 
     p[r] = T(0);
     u[r] = T(0);
     v_[r] = T(0);
-    v[0] = fabs((double)rr);
-    v[1] = (double)rr * (double)rr;
+    v[0] += fabs((double)rr);
+    v[1] += (double)rr * (double)rr;
   }
   if (grid_sum(v, partials, &st->ticket[2])) {
     st->s[S_RES0] = (norm == 1) ? v[0] : sqrt(v[1]);
@@ -324,16 +333,15 @@ __global__ void __launch_bounds__(TPB) k_bicg_update(int n, const T* __restrict_
                                                      T* __restrict__ x, T* __restrict__ r_,
                                                      const T* __restrict__ r0, double* partials, DevState* st) {
   if (st->done) return;
-  const int i = blockIdx.x * TPB + threadIdx.x;
   double v[3] = {0.0, 0.0, 0.0};
-  if (i < n) {
-    const T alf = (T)st->s[S_ALF];
+  const T alf = (T)st->s[S_ALF];
+  for (int i = blockIdx.x * TPB + threadIdx.x; i < n; i += gridDim.x * TPB) {
     x[i] = x[i] + alf * z[i];
     const T ri = r_[i] - alf * v_[i];
     r_[i] = ri;
-    v[0] = fabs((double)ri);
-    v[1] = (double)ri * (double)ri;
-    v[2] = (double)ri * (double)r0[i];
+    v[0] += fabs((double)ri);
+    v[1] += (double)ri * (double)ri;
+    v[2] += (double)ri * (double)r0[i];
   }
   if (grid_sum(v, partials, &st->ticket[3])) {
     st->iter += 1;
@@ -352,15 +360,17 @@ __global__ void __launch_bounds__(TPB) k_bicg_update(int n, const T* __restrict_
 // GMRES(3) (pgmres.f90): restart residual v_1 = b - A x, ro = sqrt(sum v_1^2 + small)
 template <typename T>
 __global__ void __launch_bounds__(TPB) k_gm_resid(int n, int KL, GroupTab tab, const int* __restrict__ col,
-                                                  const T* __restrict__ aoff, const T* __restrict__ diag,
-                                                  const T* __restrict__ b, const T* __restrict__ x, T* __restrict__ v1,
-                                                  double* partials, DevState* st) {
+                                                  const signed char* __restrict__ nlo,
+                                                  const signed char* __restrict__ nup, const T* __restrict__ aoff,
+                                                  const T* __restrict__ diag, const T* __restrict__ b,
+                                                  const T* __restrict__ x, T* __restrict__ v1, double* partials,
+                                                  DevState* st) {
   if (st->done) return;
   const int g = tab_group(tab, blockIdx.x);
-  const int r = tab.start[g] + (blockIdx.x - tab.blk[g]) * TPB + threadIdx.x;
+  const int stride = (tab.blk[g + 1] - tab.blk[g]) * TPB;
   double v[1] = {0.0};
-  if (r < tab.start[g + 1]) {
-    const int kl = tab.kl[g], ku = tab.ku[g];
+  for (int r = tab.start[g] + (blockIdx.x - tab.blk[g]) * TPB + threadIdx.x; r < tab.start[g + 1]; r += stride) {
+    const int kl = tab.kl[g] > 0 ? (int)nlo[r] : 0, ku = tab.ku[g] > 0 ? (int)nup[r] : 0;
     T sum = T(0);
 #pragma unroll
     for (int s = 0; s < KMAX; ++s)
@@ -370,16 +380,16 @@ __global__ void __launch_bounds__(TPB) k_gm_resid(int n, int KL, GroupTab tab, c
       if (t < ku) sum = sum + aoff[(size_t)(KL + t) * n + r] * x[col[(size_t)(KL + t) * n + r]];
     const T vr = sum + b[r] - diag[r] * x[r];
     v1[r] = vr;
-    v[0] = (double)vr * (double)vr;
+    v[0] += (double)vr * (double)vr;
   }
   if (grid_sum(v, partials, &st->ticket[2])) {
-    const double ro = (double)sqrt((T)v[0] + (T)SMALL);
+    const double ro = sqrt(v[0] + SMALL);
     if (st->iter == 0) {
       st->s[S_EPS11] = st->s[S_TOL] * ro;
       st->s[S_RO0] = ro;
     }
     st->s[S_RO] = ro;
-    st->s[S_SCALE1] = (double)(T(1) / ((T)ro + (T)SMALL));
+    st->s[S_SCALE1] = 1.0 / (ro + SMALL);
     st->s[S_RS1 + 1] = ro;
     st->active = 1;
     st->ifinal = 0;
@@ -394,16 +404,15 @@ __global__ void __launch_bounds__(TPB) k_gm_resid(int n, int KL, GroupTab tab, c
 template <typename T>
 __global__ void __launch_bounds__(TPB) k_mgs(int n, int j, int i, GmVecs gv, double* partials, DevState* st) {
   if (st->done || !st->active) return;
-  const int q = blockIdx.x * TPB + threadIdx.x;
   T* w = (T*)gv.v[i + 1];
   const T* vj = (const T*)gv.v[j];
   const T h = (T)st->s[S_HH + (j - 1) * 3 + (i - 1)];
   double v[1] = {0.0};
-  if (q < n) {
+  for (int q = blockIdx.x * TPB + threadIdx.x; q < n; q += gridDim.x * TPB) {
     T wq = w[q];
     if (h != T(0)) { wq = wq + (-h) * vj[q]; w[q] = wq; }
-    if (j < i) v[0] = (double)((const T*)gv.v[j + 1])[q] * (double)wq;
-    else v[0] = (double)wq * (double)wq;
+    if (j < i) v[0] += (double)((const T*)gv.v[j + 1])[q] * (double)wq;
+    else v[0] += (double)wq * (double)wq;
   }
   if (grid_sum(v, partials, &st->ticket[4])) {
     double* s = st->s;
@@ -413,43 +422,43 @@ __global__ void __launch_bounds__(TPB) k_mgs(int n, int j, int i, GmVecs gv, dou
       return;
     }
     const int i1 = i + 1;
-    T t = sqrt((T)v[0] + (T)SMALL);
+    double t = sqrt(v[0] + SMALL);
     HH(i1, i) = t;
-    s[S_SCALE1 + i] = (double)(T(1) / max(t, (T)SMALL));
+    s[S_SCALE1 + i] = 1.0 / fmax(t, SMALL);
     for (int k = 2; k <= i; ++k) {
       const int k1 = k - 1;
-      const T tt = (T)HH(k1, i);
-      const T ck = (T)s[S_C + k1], sk = (T)s[S_S + k1];
-      HH(k1, i) = ck * tt + sk * (T)HH(k, i);
-      HH(k, i) = -sk * tt + ck * (T)HH(k, i);
+      const double tt = HH(k1, i);
+      const double ck = s[S_C + k1], sk = s[S_S + k1];
+      HH(k1, i) = ck * tt + sk * HH(k, i);
+      HH(k, i) = -sk * tt + ck * HH(k, i);
     }
-    T gam = sqrt((T)HH(i, i) * (T)HH(i, i) + (T)HH(i1, i) * (T)HH(i1, i));
-    if (gam == T(0)) gam = (T)SMALL;
-    const T ci = (T)HH(i, i) / gam, si = (T)HH(i1, i) / gam;
+    double gam = sqrt(HH(i, i) * HH(i, i) + HH(i1, i) * HH(i1, i));
+    if (gam == 0.0) gam = SMALL;
+    const double ci = HH(i, i) / gam, si = HH(i1, i) / gam;
     s[S_C + i] = ci;
     s[S_S + i] = si;
-    s[S_RS1 + i1] = -si * (T)s[S_RS1 + i];
-    s[S_RS1 + i] = ci * (T)s[S_RS1 + i];
-    HH(i, i) = ci * (T)HH(i, i) + si * (T)HH(i1, i);
-    const T ro = fabs((T)s[S_RS1 + i1]);
+    s[S_RS1 + i1] = -si * s[S_RS1 + i];
+    s[S_RS1 + i] = ci * s[S_RS1 + i];
+    HH(i, i) = ci * HH(i, i) + si * HH(i1, i);
+    const double ro = fabs(s[S_RS1 + i1]);
     s[S_RO] = ro;
     st->inner += 1;
-    if (i < 3 && ro > (T)s[S_EPS11]) return;  // next Arnoldi step
+    if (i < 3 && ro > s[S_EPS11]) return;  // next Arnoldi step
     st->active = 0;
     st->ifinal = i;
-    T rs[4];
-    for (int k = 1; k <= i; ++k) rs[k] = (T)s[S_RS1 + k];
-    rs[i] = rs[i] / (T)HH(i, i);
+    double rs[4];
+    for (int k = 1; k <= i; ++k) rs[k] = s[S_RS1 + k];
+    rs[i] = rs[i] / HH(i, i);
     for (int ii = 2; ii <= i; ++ii) {
       const int k = i - ii + 1, k1 = k + 1;
-      T tt = rs[k];
-      for (int jj = k1; jj <= i; ++jj) tt = tt - (T)HH(k, jj) * rs[jj];
-      rs[k] = tt / (T)HH(k, k);
+      double tt = rs[k];
+      for (int jj = k1; jj <= i; ++jj) tt = tt - HH(k, jj) * rs[jj];
+      rs[k] = tt / HH(k, k);
     }
     for (int k = 1; k <= i; ++k) s[S_Y + k] = rs[k];
     s[S_RELRES] = (double)ro / s[S_RO0];
     if (!isfinite((double)ro)) { st->nonfinite = 1; st->stop = 1; }
-    if (ro <= (T)s[S_EPS11]) st->stop = 1;
+    if (ro <= s[S_EPS11]) st->stop = 1;
   }
 }
 
@@ -484,15 +493,17 @@ __global__ void k_gm_start(DevState* st, int maxit, double tol) {
 // into S_NRM2 (slot_out).  Optionally stores r (FP64) and its FP32 copy.
 template <typename TA, typename TX>
 __global__ void __launch_bounds__(TPB) k_resid64(int n, int KL, GroupTab tab, const int* __restrict__ col,
-                                                 const TA* __restrict__ aoff, const TA* __restrict__ diag,
-                                                 const double* __restrict__ b, const TX* __restrict__ x,
-                                                 double* __restrict__ rout, float* __restrict__ rout32, int slot_out,
-                                                 double* partials, DevState* st) {
+                                                 const signed char* __restrict__ nlo,
+                                                 const signed char* __restrict__ nup, const TA* __restrict__ aoff,
+                                                 const TA* __restrict__ diag, const double* __restrict__ b,
+                                                 const TX* __restrict__ x, double* __restrict__ rout,
+                                                 float* __restrict__ rout32, int slot_out, double* partials,
+                                                 DevState* st) {
   const int g = tab_group(tab, blockIdx.x);
-  const int r = tab.start[g] + (blockIdx.x - tab.blk[g]) * TPB + threadIdx.x;
+  const int stride = (tab.blk[g + 1] - tab.blk[g]) * TPB;
   double v[1] = {0.0};
-  if (r < tab.start[g + 1]) {
-    const int kl = tab.kl[g], ku = tab.ku[g];
+  for (int r = tab.start[g] + (blockIdx.x - tab.blk[g]) * TPB + threadIdx.x; r < tab.start[g + 1]; r += stride) {
+    const int kl = tab.kl[g] > 0 ? (int)nlo[r] : 0, ku = tab.ku[g] > 0 ? (int)nup[r] : 0;
     double sum = 0.0;
 #pragma unroll
     for (int s = 0; s < KMAX; ++s)
@@ -503,21 +514,30 @@ __global__ void __launch_bounds__(TPB) k_resid64(int n, int KL, GroupTab tab, co
     const double rr = b[r] - ((double)diag[r] * (double)x[r] - sum);
     if (rout) rout[r] = rr;
     if (rout32) rout32[r] = (float)rr;
-    v[0] = rr * rr;
+    v[0] += rr * rr;
   }
   if (grid_sum(v, partials, &st->ticket[5])) st->s[slot_out] = v[0];
 }
 
-// x64 += d32 (refinement correction)
-__global__ void __launch_bounds__(TPB) k_ir_correct(int n, const float* __restrict__ d, double* __restrict__ x) {
-  const int i = blockIdx.x * TPB + threadIdx.x;
-  if (i < n) x[i] += (double)d[i];
+// x64 += scale * d32 (refinement correction; scale undoes the normalisation)
+__global__ void __launch_bounds__(TPB) k_ir_correct(int n, const float* __restrict__ d, double* __restrict__ x,
+                                                    const DevState* st) {
+  const double scale = st->s[S_IRSCALE];
+  for (int i = blockIdx.x * TPB + threadIdx.x; i < n; i += gridDim.x * TPB) x[i] += scale * (double)d[i];
+}
+
+// r32 = r64 / ||r64||_2 (the FP32 correction solve sees a unit-norm right-hand side)
+__global__ void __launch_bounds__(TPB) k_ir_scale(int n, const double* __restrict__ r, float* __restrict__ r32,
+                                                  DevState* st) {
+  const double nrm = sqrt(st->s[S_NRM2]);
+  const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
+  for (int i = blockIdx.x * TPB + threadIdx.x; i < n; i += gridDim.x * TPB) r32[i] = (float)(r[i] * inv);
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->s[S_IRSCALE] = nrm;
 }
 
 template <typename TD, typename TS>
 __global__ void __launch_bounds__(TPB) k_convert(int n, const TS* __restrict__ a, TD* __restrict__ b) {
-  const int i = blockIdx.x * TPB + threadIdx.x;
-  if (i < n) b[i] = (TD)a[i];
+  for (int i = blockIdx.x * TPB + threadIdx.x; i < n; i += gridDim.x * TPB) b[i] = (TD)a[i];
 }
 
 }  // namespace cms

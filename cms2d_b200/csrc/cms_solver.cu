@@ -66,7 +66,7 @@ struct cms_solver {
   // pattern
   int *d_perm = nullptr, *d_iperm = nullptr, *d_c2c = nullptr, *d_ncface = nullptr, *d_iwet = nullptr,
       *d_col = nullptr;
-  signed char *d_fslot = nullptr, *d_nup = nullptr;
+  signed char *d_fslot = nullptr, *d_nlo = nullptr, *d_nup = nullptr;
   int K = 0;
   cms::GroupTab tab{};           // all-row launches
   std::vector<int> gblocks; // blocks per group
@@ -91,7 +91,7 @@ struct cms_solver {
   size_t ev_used = 0;
   struct ProfRec { int cat; size_t ev; double bytes; };
   std::vector<ProfRec> prof_recs;
-  double prof_ms[16] = {0};
+  double prof_ms[16] = {0};  // per ProfCat
   double prof_bytes[16] = {0};
   long long prof_count[16] = {0};
 
@@ -111,6 +111,11 @@ namespace cms {
 using Solver = ::cms_solver;
 
 static inline int nblk(int rows) { return (rows + TPB - 1) / TPB; }
+// Grid of a row kernel: one row per thread up to 8 blocks of 256 threads per
+// SM on the 148 SMs, grid-stride beyond that (fewer block partials to reduce,
+// more rows in flight per thread).
+constexpr int GRID_CAP = 148 * 8;
+static inline int gsz(int rows) { return std::max(1, std::min(nblk(rows), GRID_CAP)); }
 
 #define CHK(...)                     \
   do {                               \
@@ -131,7 +136,7 @@ static inline int nblk(int rows) { return (rows + TPB - 1) / TPB; }
 // Kernel classes timed by the profiler (cms_solver_profile_*).
 enum ProfCat : int {
   P_PROLOGUE = 0, P_ILU0 = 1, P_FWD = 2, P_BWD = 3, P_SPMV = 4, P_VEC = 5, P_RESID64 = 6, P_SCALAR = 7,
-  P_NCAT = 8
+  P_FLOW = 8, P_NCAT = 9
 };
 
 static void prof_begin(Solver* S) {
@@ -220,7 +225,7 @@ static int create(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, 
   const size_t n = P.n, nD = P.nD, nmf = P.nmf, K = std::max(S->K, 1);
   if ((rc = S->alloc(&S->d_perm, n)) || (rc = S->alloc(&S->d_iperm, n)) || (rc = S->alloc(&S->d_c2c, nD * nmf)) ||
       (rc = S->alloc(&S->d_ncface, nD)) || (rc = S->alloc(&S->d_iwet, nD)) || (rc = S->alloc(&S->d_col, K * n)) ||
-      (rc = S->alloc(&S->d_fslot, n * nmf)) || (rc = S->alloc(&S->d_nup, n)))
+      (rc = S->alloc(&S->d_fslot, n * nmf)) || (rc = S->alloc(&S->d_nlo, n)) || (rc = S->alloc(&S->d_nup, n)))
     return fail(rc);
   cudaStream_t s = S->stream;
   if (cudaMemcpyAsync(S->d_perm, P.perm.data(), n * sizeof(int), cudaMemcpyHostToDevice, s) ||
@@ -229,6 +234,7 @@ static int create(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, 
       cudaMemcpyAsync(S->d_ncface, ncface, nD * sizeof(int), cudaMemcpyHostToDevice, s) ||
       cudaMemcpyAsync(S->d_col, P.col.data(), P.col.size() * sizeof(int), cudaMemcpyHostToDevice, s) ||
       cudaMemcpyAsync(S->d_fslot, P.fslot.data(), n * nmf, cudaMemcpyHostToDevice, s) ||
+      cudaMemcpyAsync(S->d_nlo, P.nlo.data(), n, cudaMemcpyHostToDevice, s) ||
       cudaMemcpyAsync(S->d_nup, P.nup.data(), n, cudaMemcpyHostToDevice, s))
     return fail(CMS_DEVICE_ERROR);
   {
@@ -242,7 +248,9 @@ static int create(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, 
   S->gblocks.resize(P.G);
   int tot = 0;
   for (int g = 0; g < P.G; ++g) {
-    S->gblocks[g] = nblk(P.gstart[g + 1] - P.gstart[g]);
+    const int rows = P.gstart[g + 1] - P.gstart[g];
+    const long long prop = ((long long)GRID_CAP * rows + P.n - 1) / P.n;
+    S->gblocks[g] = std::max(1, (int)std::min<long long>(nblk(rows), std::max<long long>(prop, 1)));
     tot += S->gblocks[g];
   }
   GroupTab& t = S->tab;
@@ -264,11 +272,12 @@ static int create(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, 
     t.start[0] = 0;
     t.start[1] = P.n;
     t.blk[0] = 0;
-    t.blk[1] = nblk(P.n);
+    t.blk[1] = gsz(P.n);
     t.kl[0] = P.KL;
     t.ku[0] = P.KU;
   }
-  S->max_blocks = std::max(tot, std::max(t.blk[t.ng], nblk(P.n))) + 1;
+  // every reduction kernel launches at most max(GRID_CAP, table blocks) blocks
+  S->max_blocks = std::max(std::max(tot, GRID_CAP), std::max(t.blk[t.ng], gsz(P.n))) + 1;
   if ((rc = S->alloc(&S->d_part, (size_t)3 * S->max_blocks)) || (rc = S->alloc(&S->d_st, 1))) return fail(rc);
   if (cudaMallocHost((void**)&S->h_st, sizeof(DevState)) != cudaSuccess) return fail(CMS_DEVICE_ERROR);
   if ((rc = alloc_precision(S, S->A64, S->W64)) || (rc = alloc_precision(S, S->A32, S->W32))) return fail(rc);
@@ -289,8 +298,8 @@ static int factor(Solver* S, Mat<T>& A) {
     if (r1 <= r0) continue;
     const double R = r1 - r0, E = (double)(P.glo[g] + P.gup[g]);
     KLAUNCH(S, P_ILU0, R * (3 * s + 1) + E * (2 * s + 4),
-            (k_ilu0<T><<<nblk(r1 - r0), TPB, 0, S->stream>>>(P.n, r0, r1, P.KL, P.gkl[g], P.gku[g], S->d_col,
-                                                              S->d_nup, A.aoff, A.diag, A.luoff, A.invd)));
+            (k_ilu0<T><<<gsz(r1 - r0), TPB, 0, S->stream>>>(P.n, r0, r1, P.KL, P.gkl[g], P.gku[g], S->d_col,
+                                                             S->d_nlo, S->d_nup, A.aoff, A.diag, A.luoff, A.invd)));
   }
   return CMS_OK;
 }
@@ -308,8 +317,8 @@ static int sweep_fwd(Solver* S, Mat<T>& A, Work<T>& W, int step, const T* yin, T
     if (r1 <= r0) continue;
     const double R = r1 - r0, E = (double)P.glo[g];
     KLAUNCH(S, P_FWD, R * s * vec + E * (s + 4) + (E > 0 ? R * s : 0.0),
-            (k_fwd<T, MODE><<<nblk(r1 - r0), TPB, 0, S->stream>>>(P.n, r0, r1, P.gkl[g], step, S->d_col, A.luoff,
-                                                                   W.z, yin, p, r, u, x, gv, S->d_st)));
+            (k_fwd<T, MODE><<<gsz(r1 - r0), TPB, 0, S->stream>>>(P.n, r0, r1, P.gkl[g], step, S->d_col, S->d_nlo,
+                                                                  A.luoff, W.z, yin, p, r, u, x, gv, S->d_st)));
   }
   return CMS_OK;
 }
@@ -323,8 +332,8 @@ static int sweep_bwd(Solver* S, Mat<T>& A, Work<T>& W, T* x, int need_active) {
     if (r1 <= r0) continue;
     const double R = r1 - r0, E = (double)P.gup[g];
     KLAUNCH(S, P_BWD, R * s * (FINAL ? 5 : 3) + E * (s + 4) + (E > 0 ? R * s : 0.0),
-            (k_bwd<T, FINAL><<<nblk(r1 - r0), TPB, 0, S->stream>>>(P.n, r0, r1, P.KL, P.gku[g], S->d_col, A.luoff,
-                                                                    A.invd, W.z, x, need_active, S->d_st)));
+            (k_bwd<T, FINAL><<<gsz(r1 - r0), TPB, 0, S->stream>>>(P.n, r0, r1, P.KL, P.gku[g], S->d_col, S->d_nup,
+                                                                   A.luoff, A.invd, W.z, x, need_active, S->d_st)));
   }
   return CMS_OK;
 }
@@ -350,15 +359,17 @@ static int bicg_iter(Solver* S, Mat<T>& A, Work<T>& W) {
   CHK((sweep_fwd<T, FWD_BICG_P>(S, A, W, 0, nullptr, W.p, W.r, W.u, W.x)));
   CHK((sweep_bwd<T, false>(S, A, W, nullptr, 0)));
   KLAUNCH(S, P_SPMV, spmv_bytes<T>(S, 3),
-          (k_spmv<T, SPMV_BICG_U><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, 0, S->d_col, A.aoff, A.diag, W.z,
-                                                                  W.u, W.r0, S->d_part, S->d_st)));
+          (k_spmv<T, SPMV_BICG_U><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, 0, S->d_col, S->d_nlo, S->d_nup,
+                                                                  A.aoff, A.diag, W.z, W.u, W.r0, S->d_part,
+                                                                  S->d_st)));
   CHK((sweep_fwd<T, FWD_BICG_R>(S, A, W, 0, nullptr, W.p, W.r, W.u, W.x)));
   CHK((sweep_bwd<T, false>(S, A, W, nullptr, 0)));
   KLAUNCH(S, P_SPMV, spmv_bytes<T>(S, 3),
-          (k_spmv<T, SPMV_BICG_V><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, 0, S->d_col, A.aoff, A.diag, W.z,
-                                                                  W.v, W.r, S->d_part, S->d_st)));
+          (k_spmv<T, SPMV_BICG_V><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, 0, S->d_col, S->d_nlo, S->d_nup,
+                                                                  A.aoff, A.diag, W.z, W.v, W.r, S->d_part,
+                                                                  S->d_st)));
   KLAUNCH(S, P_VEC, (double)P.n * sizeof(T) * 7,
-          (k_bicg_update<T><<<nblk(P.n), TPB, 0, S->stream>>>(P.n, W.z, W.v, W.x, W.r, W.r0, S->d_part, S->d_st)));
+          (k_bicg_update<T><<<gsz(P.n), TPB, 0, S->stream>>>(P.n, W.z, W.v, W.x, W.r, W.r0, S->d_part, S->d_st)));
   return CMS_OK;
 }
 
@@ -370,9 +381,9 @@ static int run_bicgstab(Solver* S, Mat<T>& A, Work<T>& W, int maxit, int norm, d
   const int nb_all = S->tab.blk[S->tab.ng];
   if (do_factor) CHK(factor<T>(S, A));
   KLAUNCH(S, P_VEC, xzero ? (double)P.n * sizeof(T) * 7 : spmv_bytes<T>(S, 7),
-          (k_bicg_init<T><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, xzero, maxit, norm, tol, S->d_col, A.aoff,
-                                                          A.diag, W.b, W.x, W.r, W.r0, W.p, W.u, W.v, S->d_part,
-                                                          S->d_st)));
+          (k_bicg_init<T><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, xzero, maxit, norm, tol, S->d_col,
+                                                          S->d_nlo, S->d_nup, A.aoff, A.diag, W.b, W.x, W.r, W.r0,
+                                                          W.p, W.u, W.v, S->d_part, S->d_st)));
   int issued = 0, chunk = S->prof_on ? 1 : 2;
   while (issued < maxit) {
     const int c = std::min(chunk, maxit - issued);
@@ -398,16 +409,17 @@ static int run_gmres(Solver* S, Mat<T>& A, Work<T>& W, int maxit, double tol, bo
   for (int j = 0; j < 5; ++j) gv.v[j] = W.vv[j];
   for (int cyc = 0; cyc < maxit; ++cyc) {
     KLAUNCH(S, P_VEC, spmv_bytes<T>(S, 3),
-            (k_gm_resid<T><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, S->d_col, A.aoff, A.diag, W.b, W.x,
-                                                           W.vv[1], S->d_part, S->d_st)));
+            (k_gm_resid<T><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, S->d_col, S->d_nlo, S->d_nup, A.aoff,
+                                                           A.diag, W.b, W.x, W.vv[1], S->d_part, S->d_st)));
     for (int i = 1; i <= 3; ++i) {
       CHK((sweep_fwd<T, FWD_GM_SCALE>(S, A, W, i, nullptr, nullptr, nullptr, nullptr, nullptr)));
       CHK((sweep_bwd<T, false>(S, A, W, nullptr, 1)));
       KLAUNCH(S, P_SPMV, spmv_bytes<T>(S, 3),
-              (k_spmv<T, SPMV_GM><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, i, S->d_col, A.aoff, A.diag, W.z,
-                                                                  W.vv[i + 1], W.vv[1], S->d_part, S->d_st)));
+              (k_spmv<T, SPMV_GM><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, i, S->d_col, S->d_nlo, S->d_nup,
+                                                                  A.aoff, A.diag, W.z, W.vv[i + 1], W.vv[1],
+                                                                  S->d_part, S->d_st)));
       for (int j = 1; j <= i; ++j) {
-        KLAUNCH(S, P_VEC, vb * 4, (k_mgs<T><<<nblk(P.n), TPB, 0, S->stream>>>(P.n, j, i, gv, S->d_part, S->d_st)));
+        KLAUNCH(S, P_VEC, vb * 4, (k_mgs<T><<<gsz(P.n), TPB, 0, S->stream>>>(P.n, j, i, gv, S->d_part, S->d_st)));
       }
     }
     CHK((sweep_fwd<T, FWD_GM_COMB>(S, A, W, 0, nullptr, nullptr, nullptr, nullptr, nullptr)));
@@ -441,9 +453,9 @@ static int resid64(Solver* S, Mat<TA>& A, const double* b, const TX* x, double* 
   const double bytes = (double)P.n * (sizeof(TA) + 8 + sizeof(TX) + (rout ? 8 : 0) + (rout32 ? 4 : 0)) +
                        (double)P.nnz_off * (sizeof(TA) + 4);
   KLAUNCH(S, P_RESID64, bytes,
-          (k_resid64<TA, TX><<<S->tab.blk[S->tab.ng], TPB, 0, S->stream>>>(P.n, P.KL, S->tab, S->d_col, A.aoff, A.diag,
-                                                                            b, x, rout, rout32, slot, S->d_part,
-                                                                            S->d_st)));
+          (k_resid64<TA, TX><<<S->tab.blk[S->tab.ng], TPB, 0, S->stream>>>(P.n, P.KL, S->tab, S->d_col, S->d_nlo,
+                                                                            S->d_nup, A.aoff, A.diag, b, x, rout,
+                                                                            rout32, slot, S->d_part, S->d_st)));
   return CMS_OK;
 }
 
@@ -459,7 +471,7 @@ static int run_refine(Solver* S, int nsolv, int maxit, double tol, cms_solve_inf
   const int imax = S->opts.inner_max > 0 ? S->opts.inner_max : 50;
   const int rmax = S->opts.max_refine > 0 ? S->opts.max_refine : 30;
   for (;;) {
-    CHK(resid64<double, double>(S, S->A64, S->W64.b, S->W64.x, nullptr, S->W32.b, S_NRM2));
+    CHK(resid64<double, double>(S, S->A64, S->W64.b, S->W64.x, S->W64.r, nullptr, S_NRM2));
     CMS_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, S->stream));
     CMS_CUDA(cudaStreamSynchronize(S->stream));
     const double nrm = std::sqrt(S->h_st->s[S_NRM2]);
@@ -470,7 +482,8 @@ static int run_refine(Solver* S, int nsolv, int maxit, double tol, cms_solve_inf
       break;
     }
     if (rel <= tol || steps >= rmax || inner_total >= maxit) break;
-    // inner FP32 solve A32 d = r32 from d = 0 (factor already built)
+    // inner FP32 solve A32 d = r/||r|| from d = 0 (factor already built)
+    KLAUNCH(S, P_VEC, (double)n * 12, (k_ir_scale<<<gsz(n), TPB, 0, S->stream>>>(n, S->W64.r, S->W32.b, S->d_st)));
     if (nsolv == 3) {
       CHK(run_bicgstab<float>(S, S->A32, S->W32, imax, 2, itol, 1, false));
     } else {
@@ -480,7 +493,8 @@ static int run_refine(Solver* S, int nsolv, int maxit, double tol, cms_solve_inf
     CMS_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, S->stream));
     CMS_CUDA(cudaStreamSynchronize(S->stream));
     inner_total += (nsolv == 3) ? S->h_st->iter : S->h_st->inner;
-    KLAUNCH(S, P_VEC, (double)n * 20, (k_ir_correct<<<nblk(n), TPB, 0, S->stream>>>(n, S->W32.x, S->W64.x)));
+    KLAUNCH(S, P_VEC, (double)n * 20,
+            (k_ir_correct<<<gsz(n), TPB, 0, S->stream>>>(n, S->W32.x, S->W64.x, S->d_st)));
     ++steps;
   }
   info->iters = inner_total;
@@ -517,7 +531,7 @@ static int solve_dev(Solver* S, const T* acoef, T* ss, const T* sp, T* res, T* p
     const double sz = sizeof(T);
     const double per = P.nmf * (sz + 4 + 1) + 4 + 4 + 4 + sz * 7 + (a2 ? 4 : 0);
     KLAUNCH(S, P_PROLOGUE, (double)P.n * per + (double)P.nnz_off * (sz + (a2 ? 4 : 0)),
-            (k_prologue<T, float><<<nblk(P.n), TPB, 0, S->stream>>>(P.n, P.nmf, acoef, ss, sp, res, phi, S->d_c2c,
+            (k_prologue<T, float><<<gsz(P.n), TPB, 0, S->stream>>>(P.n, P.nmf, acoef, ss, sp, res, phi, S->d_c2c,
                                                                      S->d_ncface, S->d_iwet, S->d_fslot, S->d_iperm,
                                                                      relax, A.aoff, A.diag, W.b, W.x, a2, d2,
                                                                      S->d_part, S->d_st)));
@@ -526,7 +540,7 @@ static int solve_dev(Solver* S, const T* acoef, T* ss, const T* sp, T* res, T* p
     if (is64) CHK((resid64<double, double>(S, S->A64, S->W64.b, S->W64.x, nullptr, nullptr, S_TRUE0)));
     else {
       KLAUNCH(S, P_VEC, (double)P.n * 12,
-              (k_convert<double, float><<<nblk(P.n), TPB, 0, S->stream>>>(P.n, S->W32.b, S->W64.r)));
+              (k_convert<double, float><<<gsz(P.n), TPB, 0, S->stream>>>(P.n, S->W32.b, S->W64.r)));
       CHK((resid64<float, float>(S, S->A32, S->W64.r, S->W32.x, nullptr, nullptr, S_TRUE0)));
     }
   }
@@ -540,7 +554,7 @@ static int solve_dev(Solver* S, const T* acoef, T* ss, const T* sp, T* res, T* p
     else CHK((resid64<float, float>(S, S->A32, S->W64.r, S->W32.x, nullptr, nullptr, S_TRUE1)));
   }
   KLAUNCH(S, P_VEC, (double)P.n * (4 + 2 * sizeof(T)),
-          (k_scatter<T, T><<<nblk(P.n), TPB, 0, S->stream>>>(P.n, S->d_perm, W.x, phi)));
+          (k_scatter<T, T><<<gsz(P.n), TPB, 0, S->stream>>>(P.n, S->d_perm, W.x, phi)));
   CMS_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, S->stream));
   CMS_CUDA(cudaStreamSynchronize(S->stream));
   const DevState& h = *S->h_st;
@@ -767,3 +781,6 @@ const char* cms_gpu_version(void) { return "cmsgpu 0.1 (sm_100a)"; }
 const char* cms_gpu_last_error(void) { return g_last_error; }
 
 }  // extern "C"
+
+// The device flow step shares this translation unit (and the handle internals).
+#include "cms_flow_host.cuh"

@@ -133,13 +133,14 @@ class Solver:
     def stream_handle(self) -> int:
         return _lib.lib().cms_solver_stream(self._h) or 0
 
-    PROFILE_CLASSES = ("prologue", "ilu0", "fwd_sweep", "bwd_sweep", "spmv", "vector", "resid64", "scalar")
+    PROFILE_CLASSES = ("prologue", "ilu0", "fwd_sweep", "bwd_sweep", "spmv", "vector", "resid64", "scalar", "flow")
 
     def profile(self, enable: bool = True):
         _lib.check(_lib.lib().cms_solver_profile(self._h, int(enable)), "cms_solver_profile")
 
     def profile_read(self, reset: bool = True) -> dict:
-        ms = np.zeros(8); by = np.zeros(8); cnt = np.zeros(8, np.int64)
+        k = len(self.PROFILE_CLASSES)
+        ms = np.zeros(k); by = np.zeros(k); cnt = np.zeros(k, np.int64)
         _lib.check(_lib.lib().cms_solver_profile_read(self._h, int(reset), _ptr(ms), _ptr(by), _ptr(cnt)),
                    "cms_solver_profile_read")
         return {name: {"ms": float(ms[q]), "bytes": float(by[q]), "launches": int(cnt[q])}

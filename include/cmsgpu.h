@@ -119,9 +119,12 @@ int cms_solver_get_perm(const cms_solver* s, int* perm);
 long long cms_solver_launches(const cms_solver* s);
 /* Kernel-class timing with CUDA events on the handle's stream.  Classes:
  * 0 prologue, 1 ILU(0) factor, 2 forward sweep, 3 backward sweep, 4 SpMV,
- * 5 vector/reduction kernels, 6 FP64 residual, 7 scalar kernels.
- * profile_read fills ms[8], bytes[8] (algorithmic bytes: every array a
- * kernel touches counted once) and count[8] (launches); reset=1 clears. */
+ * 5 vector/reduction kernels, 6 FP64 residual, 7 scalar kernels, 8 flow-step
+ * assembly/correction kernels (a flow handle's solver).
+ * profile_read fills ms[CMS_PROF_CLASSES], bytes[..] (algorithmic bytes:
+ * every array a kernel touches counted once) and count[..] (launches);
+ * reset=1 clears. */
+#define CMS_PROF_CLASSES 9
 int cms_solver_profile(cms_solver* s, int enable);
 int cms_solver_profile_read(cms_solver* s, int reset, double* ms, double* bytes, long long* count);
 /* The stream the handle runs on (a cudaStream_t). */
@@ -136,6 +139,77 @@ void cms_solver_destroy(cms_solver* s);
  * number of groups G (> 0) or -CMS_BAD_ARGUMENT. */
 int cms_order_build(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, const int* ncface, int ordering,
                     int* perm, int* gstart, int* kl_ku);
+
+/* ---- implicit flow step (flow_imp, source/flow/flow_imp.F90:29-312) ------
+ * One SIMPLEC time step on the device: static sources, per outer iteration
+ * momentum coefficients (exponential scheme) + skewness corrections + BCs,
+ * u and v solves, pressure-correction coefficients + Rhie-Chow fluxes,
+ * pp solve, velocity/flux/water-level correction, gradients, face values,
+ * Manning friction, eddy viscosity and check_conv; then velface_eta and
+ * the time-level update.  Cartesian and telescoping grids, ntsch = 1,
+ * water-level (TH/H) strings on dummy faces, walls elsewhere.  Wetting and
+ * drying is not handled: a step that would dry a cell returns
+ * CMS_UNSUPPORTED.  Water levels of the string are inputs of each step
+ * (the host keeps bnd_eval). */
+typedef struct cms_flow cms_flow;
+
+typedef struct cms_flow_opts {
+  int nsolv;         /* 3 BiCGStab, 4 GMRES (solvers.f90:8)                        */
+  int ordering;      /* CMS_ORDER_*                                                */
+  int precision;     /* CMS_PREC_FP64 or CMS_PREC_FP32_REFINE (the solves)         */
+  int norm;          /* BiCGStab stopping norm (1 = L1 as the reference)           */
+  double tol;        /* inner relative tolerance (reference 1e-3)                  */
+  int nswp_pp;       /* iteration caps (flow.F90:779-792): pp 20/15, u/v 5         */
+  int nswp_uv;
+  int maxit;         /* outer iterations; 0: 20 + ncells/10000 (flow.F90:784,792)  */
+  int skewcor;       /* skewness corrections on telescoping grids (flow.F90:108)   */
+  double inner_tol;  /* refinement: FP32 solve tolerance                           */
+  int inner_max;
+} cms_flow_opts;
+
+typedef struct cms_flow_info {
+  int status;        /* CMS_*                                                      */
+  int niter;         /* outer iterations run                                       */
+  int iconv;         /* check_conv: 0 divergent, 1 continue (maxit reached), 2 converged */
+  double rmom_p, rmom_u, rmom_v;  /* last normalised residuals (rmom(1:3))        */
+  long long krylov_iters;         /* Krylov iterations of all solves of the step  */
+} cms_flow_info;
+
+enum {
+  CMS_FLOW_P = 0, CMS_FLOW_H = 1, CMS_FLOW_U = 2, CMS_FLOW_V = 3, CMS_FLOW_ETA = 4, CMS_FLOW_VIS = 5,
+  CMS_FLOW_CFRICT = 6, CMS_FLOW_DPX = 7, CMS_FLOW_DPY = 8,
+  CMS_FLOW_FLUX = 100, CMS_FLOW_VISK = 101, CMS_FLOW_HK = 102, CMS_FLOW_ACOEF = 103, CMS_FLOW_FINTP = 104,
+  CMS_FLOW_ZBK = 105
+};
+
+void cms_flow_default_opts(cms_flow_opts* opts);
+/* Grid in the reference layout: cell2cell/idirface [ncellsD][nmaxfaces]
+ * (1-based ids, direction 1..4 = N,E,S,W), cell centres/sizes x,y,dx,dy and
+ * bed elevation zb (ncellsD, zb = -depth), Manning n per active cell, and one
+ * water-level string given as 1-based (cell, face) pairs whose faces lead to
+ * dummy cells.  All other dummy faces are walls (geo_init_cart,
+ * geospatial.F90:1400-1833; bnd_init). */
+int cms_flow_create(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, const int* ncface,
+                    const int* idirface, const double* x, const double* y, const double* dx, const double* dy,
+                    const double* zb, const double* coefman, int nth, const int* th_cells, const int* th_faces,
+                    const cms_flow_opts* opts, cms_flow** out);
+/* Cold start at rest from the water level eta0 (ncellsD values, natural
+ * order), as prestart does (prestart.f90:302-325). */
+int cms_flow_init(cms_flow* f, const double* eta0);
+/* One time step of length dt; wsebnd holds the string's water levels at the
+ * new time level (one per string entry). */
+int cms_flow_step(cms_flow* f, double dt, const double* wsebnd, cms_flow_info* info);
+/* Host copy (natural order) of a state array CMS_FLOW_*: ncellsD values for
+ * cell arrays, [ncellsD][nmaxfaces] for face arrays. */
+int cms_flow_get(cms_flow* f, int which, double* out);
+int cms_flow_last_info(const cms_flow* f, cms_flow_info* info);
+/* Solve records (u, v, pp) of the last outer iteration of the last step. */
+int cms_flow_last_solves(const cms_flow* f, cms_solve_info* info3);
+cms_solver* cms_flow_solver(cms_flow* f);
+long long cms_flow_launches(const cms_flow* f);
+size_t cms_flow_device_bytes(const cms_flow* f);
+int cms_flow_njoint(const cms_flow* f);
+void cms_flow_destroy(cms_flow* f);
 
 /* ---- reference-shaped global API (one implicit handle, like solv_def) ---- */
 

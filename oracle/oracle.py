@@ -111,3 +111,92 @@ class OracleSolver:
         x = np.zeros_like(y)
         lib().orc_lusol_d(self._h, np.ascontiguousarray(y, np.float64), x)
         return x
+
+
+class FlowOracle:
+    """CPU restatement of one implicit flow step (flow_imp, flow_imp.F90:29-312)."""
+
+    CELL = {"p": 0, "h": 1, "u": 2, "v": 3, "eta": 4, "vis": 5, "cfrict": 6, "dpx": 7, "dpy": 8}
+    FACE = {"flux": 100, "visk": 101, "hk": 102, "acoef": 103, "fintp": 104, "zbk": 105}
+
+    def __init__(self, case, skewcor: bool = True):
+        L = lib()
+        if not hasattr(L, "_flow_bound"):
+            P = C.c_void_p
+            L.orcf_create.restype = P
+            i32 = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+            f64 = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+            L.orcf_create.argtypes = [C.c_int, C.c_int, C.c_int, i32, i32, i32, f64, f64, f64, f64, f64, f64, C.c_int,
+                                      i32, i32, C.c_int]
+            L.orcf_destroy.argtypes = [P]
+            L.orcf_set_solver.argtypes = [P, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int]
+            L.orcf_init.argtypes = [P, f64]
+            L.orcf_step.argtypes = [P, C.c_double, f64, C.c_int, C.POINTER(C.c_int), f64]
+            L.orcf_step.restype = C.c_int
+            L.orcf_get.argtypes = [P, C.c_int, f64]
+            L.orcf_get.restype = C.c_longlong
+            L.orcf_solve_iters.argtypes = [P]
+            L.orcf_solve_iters.restype = C.c_longlong
+            L.orcf_njoint.argtypes = [P]
+            L.orcf_set_order.argtypes = [P, i32]
+            L._flow_bound = True
+        g = case.grid
+        self.case = case
+        self.g = g
+        self._h = L.orcf_create(g.ncells, g.ncellsD, g.nmaxfaces, np.ascontiguousarray(g.cell2cell, np.int32),
+                                np.ascontiguousarray(g.ncface, np.int32), np.ascontiguousarray(g.idirface, np.int32),
+                                np.ascontiguousarray(g.x), np.ascontiguousarray(g.y), np.ascontiguousarray(g.dx),
+                                np.ascontiguousarray(g.dy), np.ascontiguousarray(case.zb, np.float64),
+                                np.ascontiguousarray(case.coefman, np.float64), int(case.th_cells.size),
+                                np.ascontiguousarray(case.th_cells, np.int32),
+                                np.ascontiguousarray(case.th_faces, np.int32), int(skewcor))
+        self.t = 0.0
+        self.steps = 0
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().orcf_destroy(h)
+            self._h = None
+
+    def set_solver(self, nsolv=4, precond=PC_ILU0, tol=1e-3, nswp_pp=20, nswp_uv=5, norm=1):
+        lib().orcf_set_solver(self._h, nsolv, precond, tol, nswp_pp, nswp_uv, norm)
+
+    def set_order(self, perm):
+        """Solve in another unknown order (perm[r] = natural 0-based cell of solver row r)."""
+        lib().orcf_set_order(self._h, np.ascontiguousarray(perm, np.int32))
+
+    def init(self, eta0=None):
+        if eta0 is None:
+            eta0 = np.full(self.g.ncellsD, self.case.wse(0.0))
+        lib().orcf_init(self._h, np.ascontiguousarray(eta0, np.float64))
+
+    def step(self, maxit=None, dt=None):
+        dt = self.case.dt if dt is None else dt
+        if maxit is None:
+            maxit = 20 + self.g.ncells // 10000  # flow.F90:784,792
+        wse = np.ascontiguousarray(self.case.wsebnd(self.t + dt), np.float64)
+        ni = C.c_int()
+        rm = np.zeros(3)
+        st = lib().orcf_step(self._h, dt, wse, int(maxit), C.byref(ni), rm)
+        self.t += dt
+        self.steps += 1
+        return dict(status=st, niter=ni.value, rmom=rm.copy())
+
+    def get(self, name):
+        g = self.g
+        if name in self.CELL:
+            out = np.zeros(g.ncellsD)
+            lib().orcf_get(self._h, self.CELL[name], out)
+            return out
+        out = np.zeros(g.ncellsD * g.nmaxfaces)
+        lib().orcf_get(self._h, self.FACE[name], out)
+        return out.reshape(g.ncellsD, g.nmaxfaces)
+
+    @property
+    def solve_iters(self):
+        return lib().orcf_solve_iters(self._h)
+
+    @property
+    def njoint(self):
+        return lib().orcf_njoint(self._h)

@@ -57,3 +57,22 @@ def test_order_build_host_only():
     # red cells (i+j even) first
     i = perm % 8; j = perm // 8
     assert np.all(((i + j) % 2)[: gstart[1]] == 0)
+
+
+def test_flow_entry_points_marshal_and_reject_bad_grids():
+    """The flow binding's argument lists match the C-ABI (checked without a GPU)."""
+    from cms2d_b200 import flow as F
+    L = _lib.lib()
+    F._bind(L)
+    o = F.FlowOpts()
+    L.cms_flow_default_opts(C.byref(o))
+    assert o.nsolv == 4 and o.nswp_pp == 20 and o.nswp_uv == 5 and o.skewcor == 1
+    z = np.zeros(16, np.int32)
+    zd = np.zeros(16)
+    h = C.c_void_p()
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    rc = L.cms_flow_create(0, 0, 4, p(z), p(z), p(z), p(zd), p(zd), p(zd), p(zd), p(zd), p(zd), 0, None, None,
+                           C.byref(o), C.byref(h))
+    assert rc == _lib.CMS_BAD_ARGUMENT
+    info = F.FlowInfo()
+    assert L.cms_flow_step(None, 1.0, None, C.byref(info)) == _lib.CMS_BAD_ARGUMENT

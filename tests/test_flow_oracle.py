@@ -1,0 +1,61 @@
+"""CPU checks of the flow oracle (the checker of the GPU flow step)."""
+import numpy as np
+
+from cms2d_b200 import cases
+from oracle import oracle as O
+
+
+def test_basin_follows_tide_and_stays_finite():
+    c = cases.tidal_basin(40, 20, seed=0)
+    f = O.FlowOracle(c)
+    f.set_solver(nsolv=4, tol=1e-3)
+    f.init()
+    for _ in range(6):
+        r = f.step()
+        assert r["status"] == 0 and 1 <= r["niter"] <= 20 + c.grid.ncells // 10000
+    n = c.grid.ncells
+    eta = f.get("eta")[:n]
+    assert np.all(np.isfinite(eta))
+    assert abs(eta.mean() - c.wse(f.t)) < 0.01
+    # a falling tide drains the basin through the north edge: northward velocity
+    assert f.get("v")[:n].mean() > 0
+
+
+def test_flux_antisymmetry_and_mass_balance():
+    """flux(k,i) = -flux(back face, neighbour); volume change = net boundary inflow."""
+    c = cases.tidal_basin(30, 16, seed=2)
+    f = O.FlowOracle(c)
+    f.set_solver(nsolv=3, tol=1e-12, nswp_pp=400, nswp_uv=400)
+    f.init()
+    g = c.grid
+    n = g.ncells
+    h0 = f.get("h")[:n].copy()
+    r = f.step(maxit=30)
+    assert r["status"] == 0
+    flux = f.get("flux")
+    for k in range(g.nmaxfaces):
+        j = g.cell2cell[:n, k] - 1
+        m = (k < g.ncface[:n]) & (j < n)
+        i = np.nonzero(m)[0]
+        # find the back face of each interior face
+        for ii, jj in zip(i[:200], j[m][:200]):
+            kb = int(np.nonzero(g.cell2cell[jj, : g.ncface[jj]] == ii + 1)[0][0])
+            assert abs(flux[ii, k] + flux[jj, kb]) <= 1e-12 * max(1.0, abs(flux[ii, k]))
+    # continuity of the converged step: A (h - h1)/dt + sum_k flux = 0 per cell
+    h1 = f.get("h")[:n]
+    area = g.dx[:n] * g.dy[:n]
+    net = np.array([flux[i, : g.ncface[i]].sum() for i in range(n)])
+    resid = area * (h1 - h0) / c.dt + net
+    # the SIMPLEC outer loop stops at check_conv, leaving a small continuity defect
+    assert np.abs(resid).max() <= 1e-4 * np.abs(net).max() + 1e-9
+
+
+def test_telescoping_joint_cells_present():
+    c = cases.tidal_inlet(15000, seed=1)
+    f = O.FlowOracle(c)
+    assert f.njoint > 0
+    f.set_solver(nsolv=4, tol=1e-3)
+    f.init()
+    r = f.step()
+    assert r["status"] == 0
+    assert np.all(np.isfinite(f.get("u")[: c.grid.ncells]))
