@@ -131,7 +131,7 @@ def run_solve_ours(args):
     g, acoef, ss, sp, phi = build_solve_case(args.cells, seed=17 + rank)
     N = g.ncells
     solver = S.Solver(g, precision=args.precision, tol=1e-6, norm=2, verify=False, inner_tol=args.inner_tol,
-                      inner_max=args.inner_max, nsolv=3)
+                      inner_max=args.inner_max, nsolv=3, multi_kernel=args.multi_kernel)
     nswp = 5000
     # device-resident inputs
     t_acoef = torch.from_numpy(acoef).to(dev)
@@ -333,7 +333,7 @@ def run_flow_ours(args):
     g = case.grid
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
     settings = dict(FLOW_SOLVER, nswp_pp=args.nswp, nswp_uv=args.nswp, inner_tol=args.inner_tol,
-                    inner_max=args.inner_max)
+                    inner_max=args.inner_max, multi_kernel=args.multi_kernel)
     precs = [args.precision]
     if not args.no_companion:
         precs.append("fp64" if args.precision == "fp32_refine" else "fp32_refine")
@@ -428,6 +428,7 @@ def run_flow_ours(args):
                                f"dt={case.dt:g} s, ILU0-BiCGStab solves to 1e-6 rel. L2 residual",
                    "cells": g.ncells, "precision": args.precision, "ordering": "multicolor",
                    "solver": "BiCGStab + ILU(0)", "parallelism": f"replicas x{world}",
+                   "solver_kernels": "per-phase launches" if args.multi_kernel else "persistent cooperative",
                    "l2": "flushed between steps (256 MB write)"},
         "outer_iters_per_step": head["outer_iters"],
         "krylov_iters_per_step": head["krylov_iters_per_step"],
@@ -528,6 +529,8 @@ def main():
     ap.add_argument("--inner-max", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ncu", action="store_true", help="warm-up and timed steps only (profiler runs)")
+    ap.add_argument("--multi-kernel", action="store_true",
+                    help="BiCGStab as one launch per phase instead of one persistent launch per solve")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -22,7 +22,8 @@ PREC_FP64, PREC_FP32_REFINE, PREC_FP32 = 0, 1, 2
 class SolverOpts(C.Structure):
     _fields_ = [("ordering", C.c_int), ("precision", C.c_int), ("norm", C.c_int), ("tol", C.c_double),
                 ("max_iters", C.c_int), ("inner_tol", C.c_double), ("inner_max", C.c_int),
-                ("max_refine", C.c_int), ("verify", C.c_int)]
+                ("max_refine", C.c_int), ("verify", C.c_int), ("multi_kernel", C.c_int),
+                ("inner_relax", C.c_int)]
 
 
 class SolveInfo(C.Structure):

@@ -30,6 +30,14 @@ enum Slot : int {
   S_NSLOTS = 64
 };
 
+// Grid barrier of the persistent solver kernel (cms_persist.cuh).
+struct GridBar {
+  unsigned int count;  // blocks arrived at the current barrier
+  unsigned int gen;    // barrier generation
+  int err;             // 1: a block gave up waiting (bounded spin)
+  int pad;
+};
+
 struct DevState {
   double s[S_NSLOTS];
   int done;       // 1: the solve has stopped (converged or capped)
@@ -42,7 +50,8 @@ struct DevState {
   int inner;      // GMRES: Arnoldi steps in total
   int converged;  // 1 when the stopping test passed
   int nonfinite;  // 1 when a non-finite value reached a reduction
-  int pad[6];
+  GridBar bar;
+  int pad[2];
   unsigned int ticket[8];
 };
 

@@ -195,6 +195,7 @@ static int flow_create(int ncells, int ncellsD, int nmf, const int* c2c, const i
   so.verify = 0;
   so.inner_tol = F->opts.inner_tol;
   so.inner_max = F->opts.inner_max;
+  so.multi_kernel = F->opts.multi_kernel;
   int rc = cms_solver_create(ncells, ncellsD, nmf, c2c, ncface, iwet.data(), &so, &F->S);
   if (rc) return fail(rc);
   Solver* S = F->S;

@@ -20,6 +20,7 @@
 #include "cms_common.cuh"
 #include "cms_krylov.cuh"
 #include "cms_order.h"
+#include "cms_persist.cuh"
 #include "cmsgpu.h"
 
 static char g_last_error[512] = "";
@@ -80,6 +81,13 @@ struct cms_solver {
   cms::DevState* h_st = nullptr;  // pinned mirror
   double* d_part = nullptr;
   int max_blocks = 0;
+  // persistent BiCGStab: slots per group, tile tables, block partials [2][3][tiles]
+  int *d_gkl = nullptr, *d_gku = nullptr;
+  int *d_toff = nullptr, *d_dep_ptr = nullptr, *d_dep_idx = nullptr;
+  unsigned int* d_progress = nullptr;
+  double* d_ppart = nullptr;
+  int ptiles = 0;  // tiles (= blocks) of the persistent kernel; 0 not built, -1 not launchable
+  int cur_relax = 0;  // the FP32 factor in A32 is the two-phase one (k_ilu0_relax)
   cms::Staging<double> S64;
   cms::Staging<float> S32;
   size_t bytes = 0;
@@ -136,7 +144,7 @@ static inline int gsz(int rows) { return std::max(1, std::min(nblk(rows), GRID_C
 // Kernel classes timed by the profiler (cms_solver_profile_*).
 enum ProfCat : int {
   P_PROLOGUE = 0, P_ILU0 = 1, P_FWD = 2, P_BWD = 3, P_SPMV = 4, P_VEC = 5, P_RESID64 = 6, P_SCALAR = 7,
-  P_FLOW = 8, P_NCAT = 9
+  P_FLOW = 8, P_PERSIST = 9, P_NCAT = 10
 };
 
 static void prof_begin(Solver* S) {
@@ -279,6 +287,12 @@ static int create(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, 
   // every reduction kernel launches at most max(GRID_CAP, table blocks) blocks
   S->max_blocks = std::max(std::max(tot, GRID_CAP), std::max(t.blk[t.ng], gsz(P.n))) + 1;
   if ((rc = S->alloc(&S->d_part, (size_t)3 * S->max_blocks)) || (rc = S->alloc(&S->d_st, 1))) return fail(rc);
+  if ((rc = S->alloc(&S->d_gkl, P.G)) || (rc = S->alloc(&S->d_gku, P.G)) ||
+      (rc = S->alloc(&S->d_ppart, (size_t)6 * GRID_CAP)))
+    return fail(rc);
+  if (cudaMemcpyAsync(S->d_gkl, P.gkl.data(), P.G * sizeof(int), cudaMemcpyHostToDevice, s) ||
+      cudaMemcpyAsync(S->d_gku, P.gku.data(), P.G * sizeof(int), cudaMemcpyHostToDevice, s))
+    return fail(CMS_DEVICE_ERROR);
   if (cudaMallocHost((void**)&S->h_st, sizeof(DevState)) != cudaSuccess) return fail(CMS_DEVICE_ERROR);
   if ((rc = alloc_precision(S, S->A64, S->W64)) || (rc = alloc_precision(S, S->A32, S->W32))) return fail(rc);
   if (cudaStreamSynchronize(s) != cudaSuccess) return fail(CMS_DEVICE_ERROR);
@@ -373,6 +387,154 @@ static int bicg_iter(Solver* S, Mat<T>& A, Work<T>& W) {
   return CMS_OK;
 }
 
+// Tiles of the persistent kernel: one block per tile, every block resident
+// (cooperative launch), at most one block per 256 rows.  Builds the tile
+// tables on first use; 0 when the device cannot launch the kernel or a group
+// does not keep natural order.
+static int persist_tiles(Solver* S) {
+  if (S->ptiles != 0) return std::max(S->ptiles, 0);
+  S->ptiles = -1;
+  const HostPattern& P = S->hp;
+  int coop = 0, nsm = 0, per32 = 0, per64 = 0;
+  if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, S->dev) != cudaSuccess || !coop ||
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, S->dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per32, k_bicg_persistent<float>, TPB, 0) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per64, k_bicg_persistent<double>, TPB, 0) != cudaSuccess ||
+      std::min(per32, per64) <= 0) {
+    cudaGetLastError();
+    return 0;
+  }
+  const int n = P.n;
+  const int nt = std::max(1, std::min(std::min(std::min(per32, per64) * nsm, nblk(n)), GRID_CAP));
+  // tile t = natural cells [tstart[t], tstart[t+1])
+  std::vector<int> tstart(nt + 1), tile_nat(n);
+  for (int t = 0; t <= nt; ++t) tstart[t] = (int)((long long)t * n / nt);
+  for (int t = 0; t < nt; ++t)
+    for (int i = tstart[t]; i < tstart[t + 1]; ++i) tile_nat[i] = t;
+  std::vector<int> toff((size_t)P.G * (nt + 1));
+  for (int g = 0; g < P.G; ++g) {
+    int r = P.gstart[g];
+    for (int q = r + 1; q < P.gstart[g + 1]; ++q)
+      if (P.perm[q] <= P.perm[q - 1]) return 0;  // rows of a group must keep natural order
+    for (int t = 0; t <= nt; ++t) {
+      while (r < P.gstart[g + 1] && P.perm[r] < tstart[t]) ++r;
+      toff[(size_t)g * (nt + 1) + t] = r;
+    }
+  }
+  // neighbour tiles (symmetric): tiles holding a row coupled to one of ours
+  std::vector<std::vector<int>> dep(nt);
+  auto add = [&](int a, int b) {
+    for (int q : dep[a]) if (q == b) return;
+    dep[a].push_back(b);
+  };
+  for (int r = 0; r < n; ++r) {
+    const int ti = tile_nat[P.perm[r]];
+    for (int s = 0; s < S->K; ++s) {
+      const int j = P.col[(size_t)s * n + r];
+      if (j == r) continue;
+      const int tj = tile_nat[P.perm[j]];
+      if (tj != ti) { add(ti, tj); add(tj, ti); }
+    }
+  }
+  std::vector<int> dptr(nt + 1, 0), didx;
+  for (int t = 0; t < nt; ++t) {
+    std::sort(dep[t].begin(), dep[t].end());
+    didx.insert(didx.end(), dep[t].begin(), dep[t].end());
+    dptr[t + 1] = (int)didx.size();
+  }
+  if (S->alloc(&S->d_toff, toff.size()) || S->alloc(&S->d_dep_ptr, nt + 1) ||
+      S->alloc(&S->d_dep_idx, std::max<size_t>(didx.size(), 1)) || S->alloc(&S->d_progress, nt))
+    return 0;
+  cudaStream_t s = S->stream;
+  if (cudaMemcpyAsync(S->d_toff, toff.data(), toff.size() * sizeof(int), cudaMemcpyHostToDevice, s) ||
+      cudaMemcpyAsync(S->d_dep_ptr, dptr.data(), dptr.size() * sizeof(int), cudaMemcpyHostToDevice, s) ||
+      (!didx.empty() &&
+       cudaMemcpyAsync(S->d_dep_idx, didx.data(), didx.size() * sizeof(int), cudaMemcpyHostToDevice, s)) ||
+      cudaStreamSynchronize(s))
+    return 0;
+  S->ptiles = nt;
+  return nt;
+}
+
+// Algorithmic bytes of one persistent launch (each array a phase touches
+// counted once per phase): the start, then per iteration two preconditioner
+// applications (forward phases with their right-hand side formed in place,
+// backward phases), two SpMVs with their dot products and the x/r update.
+// The last forward group does its backward step in place (relax: every group
+// after the first); with spmv0 the backward phase of group 0 also forms the
+// SpMV of its rows from the same column indices and gathered values.
+template <typename T>
+static double persist_bytes(const Solver* S, int iters, bool xzero, bool relax, bool spmv0) {
+  const HostPattern& P = S->hp;
+  const double s = sizeof(T), n = P.n;
+  const bool fuse = relax || (P.G > 0 && P.gku[P.G - 1] == 0);
+  double fwd = 0.0, bwd = 0.0, spmv_rest = 0.0;
+  for (int g = 0; g < P.G; ++g) {
+    const double R = P.gstart[g + 1] - P.gstart[g], El = P.glo[g], Eu = P.gup[g];
+    fwd += El * (s + 4) + (El > 0 ? R * s : 0.0);  // factor entries, columns, gathered values
+    const bool last = fuse && (g == P.G - 1 || (relax && g >= 1));
+    if (last) fwd += R * s;                         // invd
+    else bwd += R * s * 3 + Eu * (s + 4) + (Eu > 0 ? R * s : 0.0);
+    // SpMV: diag, own value, output, dot operand, matrix entries, columns, gathers
+    const double sp = R * s * 4 + (El + Eu) * (s + 4) + (El + Eu > 0 ? R * s : 0.0);
+    if (g == 0 && spmv0) bwd += R * s * 3 + Eu * s;  // diag, output, dot operand, A's entries
+    else spmv_rest += sp;
+  }
+  // forward right-hand sides: p-update reads r, p, u, writes p, z (5); x/r
+  // update reads z, x, r, u, writes x, r, z (7)
+  const double it = 2 * (fwd + bwd + spmv_rest) + n * s * (5 + 7) + n * s * 7;
+  const double start = xzero ? n * s * 7 : spmv_bytes<T>(S, 7);
+  return start + iters * it;
+}
+
+// The whole BiCGStab solve as one cooperative launch.  Returns 1 (nothing
+// enqueued but a memset) when the launch was refused for its size, so the
+// caller can fall back to the per-phase kernels.
+template <typename T>
+static int run_bicgstab_persistent(Solver* S, Mat<T>& A, Work<T>& W, int tiles, int maxit, int norm, double tol,
+                                   int xzero) {
+  const HostPattern& P = S->hp;
+  PersistArgs<T> a;
+  a.n = P.n; a.KL = P.KL; a.G = P.G; a.gku_last = P.gku[P.G - 1];
+  a.relax = S->cur_relax;
+  a.g1 = P.G > 1 ? P.gstart[1] : P.n;
+  a.spmv0 = (P.gkl[0] == 0 && ((a.relax || a.gku_last == 0) ? P.G >= 2 : P.G >= 1)) ? 1 : 0;
+  a.gkl = S->d_gkl; a.gku = S->d_gku;
+  a.toff = S->d_toff; a.dep_ptr = S->d_dep_ptr; a.dep_idx = S->d_dep_idx; a.progress = S->d_progress;
+  a.col = S->d_col; a.nlo = S->d_nlo; a.nup = S->d_nup;
+  a.aoff = A.aoff; a.diag = A.diag; a.luoff = A.luoff; a.invd = A.invd;
+  a.b = W.b; a.x = W.x; a.r = W.r; a.r0 = W.r0; a.p = W.p; a.u = W.u; a.v = W.v; a.z = W.z;
+  a.part = S->d_ppart; a.bar = &S->d_st->bar; a.st = S->d_st;
+  a.maxit = maxit; a.norm = norm; a.xzero = xzero; a.tol = tol;
+  CMS_CUDA(cudaMemsetAsync(&S->d_st->bar, 0, sizeof(GridBar), S->stream));
+  CMS_CUDA(cudaMemsetAsync(S->d_progress, 0, sizeof(unsigned int) * tiles, S->stream));
+  void* args[] = {&a};
+  prof_begin(S);
+  const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_bicg_persistent<T>, dim3(tiles), dim3(TPB), args,
+                                                    0, S->stream);
+  if (e == cudaErrorCooperativeLaunchTooLarge) {
+    cudaGetLastError();
+    S->ptiles = -1;
+    return 1;
+  }
+  if (e != cudaSuccess) {
+    std::snprintf(g_last_error, sizeof(g_last_error), "cooperative launch: %s", cudaGetErrorString(e));
+    return CMS_DEVICE_ERROR;
+  }
+  S->launches++;
+  const size_t nrec = S->prof_recs.size();
+  prof_end(S, P_PERSIST, 0.0);
+  const bool recorded = S->prof_recs.size() > nrec;
+  CMS_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, S->stream));
+  CMS_CUDA(cudaStreamSynchronize(S->stream));
+  if (S->h_st->bar.err) {
+    std::snprintf(g_last_error, sizeof(g_last_error), "persistent BiCGStab: a grid barrier wait timed out");
+    return CMS_DEVICE_ERROR;
+  }
+  if (recorded) S->prof_recs.back().bytes = persist_bytes<T>(S, S->h_st->iter, xzero != 0, a.relax != 0, a.spmv0 != 0);
+  return CMS_OK;
+}
+
 // BiCGStab from x (or 0) on b, ending when the device stopping test fires.
 template <typename T>
 static int run_bicgstab(Solver* S, Mat<T>& A, Work<T>& W, int maxit, int norm, double tol, int xzero,
@@ -380,6 +542,17 @@ static int run_bicgstab(Solver* S, Mat<T>& A, Work<T>& W, int maxit, int norm, d
   const HostPattern& P = S->hp;
   const int nb_all = S->tab.blk[S->tab.ng];
   if (do_factor) CHK(factor<T>(S, A));
+  if (!S->opts.multi_kernel) {
+    const int tiles = persist_tiles(S);
+    if (tiles > 0) {
+      const int rc = run_bicgstab_persistent<T>(S, A, W, tiles, maxit, norm, tol, xzero);
+      if (rc != 1) return rc;
+    }
+  }
+  if (S->cur_relax) {  // the per-phase kernels need the exact factor
+    S->cur_relax = 0;
+    CHK(factor<T>(S, A));
+  }
   KLAUNCH(S, P_VEC, xzero ? (double)P.n * sizeof(T) * 7 : spmv_bytes<T>(S, 7),
           (k_bicg_init<T><<<nb_all, TPB, 0, S->stream>>>(P.n, P.KL, S->tab, xzero, maxit, norm, tol, S->d_col,
                                                           S->d_nlo, S->d_nup, A.aoff, A.diag, W.b, W.x, W.r, W.r0,
@@ -463,8 +636,23 @@ static int resid64(Solver* S, Mat<TA>& A, const double* b, const TX* x, double* 
 static int run_refine(Solver* S, int nsolv, int maxit, double tol, cms_solve_info* info) {
   const HostPattern& P = S->hp;
   const int n = P.n;
-  // A32 was written by the prologue; b64/x64 live in W64.b / W64.x.
-  CHK(factor<float>(S, S->A32));
+  // A32 was written by the prologue; b64/x64 live in W64.b / W64.x.  The FP32
+  // factor is the two-phase one when the persistent BiCGStab will run it.
+  const bool relax = nsolv == 3 && S->opts.inner_relax && S->opts.ordering == CMS_ORDER_MULTICOLOR && P.G > 2 &&
+                     !S->opts.multi_kernel && persist_tiles(S) > 0;
+  struct RelaxScope {  // the flag describes A32's factor only while this solve runs
+    Solver* s;
+    ~RelaxScope() { s->cur_relax = 0; }
+  } relax_scope{S};
+  if (relax) {
+    KLAUNCH(S, P_ILU0, (double)n * (3 * 4 + 2) + (double)(P.nnz_off) * (2 * 4 + 4),
+            (k_ilu0_relax<float><<<gsz(n), TPB, 0, S->stream>>>(n, P.KL, P.gstart[1], S->d_col, S->d_nlo,
+                                                                 S->d_nup, S->A32.aoff, S->A32.diag, S->A32.luoff,
+                                                                 S->A32.invd)));
+    S->cur_relax = 1;
+  } else {
+    CHK(factor<float>(S, S->A32));
+  }
   int steps = 0, inner_total = 0;
   double nrm0 = -1.0, rel = 1.0;
   const double itol = S->opts.inner_tol > 0 ? S->opts.inner_tol : 1e-2;
@@ -614,6 +802,8 @@ void cms_solver_default_opts(cms_solver_opts* o) {
   o->inner_max = 50;
   o->max_refine = 30;
   o->verify = 1;
+  o->multi_kernel = 0;
+  o->inner_relax = 1;
 }
 
 int cms_solver_create(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, const int* ncface,

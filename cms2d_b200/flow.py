@@ -24,7 +24,8 @@ FACE = {"flux": 100, "visk": 101, "hk": 102, "acoef": 103, "fintp": 104, "zbk": 
 class FlowOpts(C.Structure):
     _fields_ = [("nsolv", C.c_int), ("ordering", C.c_int), ("precision", C.c_int), ("norm", C.c_int),
                 ("tol", C.c_double), ("nswp_pp", C.c_int), ("nswp_uv", C.c_int), ("maxit", C.c_int),
-                ("skewcor", C.c_int), ("inner_tol", C.c_double), ("inner_max", C.c_int)]
+                ("skewcor", C.c_int), ("inner_tol", C.c_double), ("inner_max", C.c_int),
+                ("multi_kernel", C.c_int)]
 
 
 class FlowInfo(C.Structure):
@@ -65,7 +66,8 @@ class FlowModel:
 
     def __init__(self, case, nsolv: int = 4, ordering: str = "multicolor", precision: str = "fp64",
                  tol: float = 1e-3, norm: int = 1, nswp_pp: int | None = None, nswp_uv: int | None = None,
-                 maxit: int = 0, skewcor: bool = True, inner_tol: float = 1e-2, inner_max: int = 50):
+                 maxit: int = 0, skewcor: bool = True, inner_tol: float = 1e-2, inner_max: int = 50,
+                 multi_kernel: bool = False):
         L = _lib.lib()
         _bind(L)
         self.case = case
@@ -85,6 +87,7 @@ class FlowModel:
         o.skewcor = int(skewcor)
         o.inner_tol = inner_tol
         o.inner_max = inner_max
+        o.multi_kernel = int(multi_kernel)
         self.opts = o
         self._keep = [np.ascontiguousarray(a) for a in (
             g.cell2cell.astype(np.int32), g.ncface.astype(np.int32), g.idirface.astype(np.int32),

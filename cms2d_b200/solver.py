@@ -67,7 +67,8 @@ class Solver:
 
     def __init__(self, grid, iwet=None, ordering: str = "multicolor", precision: str = "fp64", tol: float = 1e-3,
                  norm: int = 1, max_iters: int = 0, inner_tol: float = 1e-2, inner_max: int = 50,
-                 max_refine: int = 30, verify: bool = True, nsolv: int = NSOLV_DEFAULT):
+                 max_refine: int = 30, verify: bool = True, nsolv: int = NSOLV_DEFAULT,
+                 multi_kernel: bool = False, inner_relax: bool = True):
         L = _lib.lib()
         self.grid = grid
         self.nsolv = nsolv
@@ -82,6 +83,8 @@ class Solver:
         self.opts.inner_max = inner_max
         self.opts.max_refine = max_refine
         self.opts.verify = int(verify)
+        self.opts.multi_kernel = int(multi_kernel)
+        self.opts.inner_relax = int(inner_relax)
         self._c2c = np.ascontiguousarray(grid.cell2cell, np.int32)
         self._ncf = np.ascontiguousarray(grid.ncface, np.int32)
         self._iwet = np.ones(grid.ncellsD, np.int32) if iwet is None else np.ascontiguousarray(iwet, np.int32)
@@ -133,7 +136,8 @@ class Solver:
     def stream_handle(self) -> int:
         return _lib.lib().cms_solver_stream(self._h) or 0
 
-    PROFILE_CLASSES = ("prologue", "ilu0", "fwd_sweep", "bwd_sweep", "spmv", "vector", "resid64", "scalar", "flow")
+    PROFILE_CLASSES = ("prologue", "ilu0", "fwd_sweep", "bwd_sweep", "spmv", "vector", "resid64", "scalar", "flow",
+                       "bicgstab_persistent")
 
     def profile(self, enable: bool = True):
         _lib.check(_lib.lib().cms_solver_profile(self._h, int(enable)), "cms_solver_profile")

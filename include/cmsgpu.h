@@ -62,6 +62,15 @@ typedef struct cms_solver_opts {
   int max_refine;    /* refinement: cap on FP64 residual/correction steps              */
   int verify;        /* 1: compute the FP64 true residual after the solve (one extra
                         pass); 0: skip it (true_relres = -1)                           */
+  int multi_kernel;  /* 0: each BiCGStab solve is one persistent cooperative launch
+                        (grid barriers between colour phases, dot products reduced
+                        in the kernel); 1: one launch per phase with host polling.
+                        Both run the same arithmetic.                                  */
+  int inner_relax;   /* refinement with BiCGStab on a grid that needs more than two
+                        colours: 1 (default) factors the FP32 inner system without the
+                        couplings among rows of colours >= 2, so its sweeps take two
+                        phases like a red/black grid; 0: exact multicolour ILU(0).
+                        The FP64 residual makes either converge to the same answer.   */
 } cms_solver_opts;
 
 typedef struct cms_solve_info {
@@ -120,11 +129,12 @@ long long cms_solver_launches(const cms_solver* s);
 /* Kernel-class timing with CUDA events on the handle's stream.  Classes:
  * 0 prologue, 1 ILU(0) factor, 2 forward sweep, 3 backward sweep, 4 SpMV,
  * 5 vector/reduction kernels, 6 FP64 residual, 7 scalar kernels, 8 flow-step
- * assembly/correction kernels (a flow handle's solver).
+ * assembly/correction kernels (a flow handle's solver), 9 persistent
+ * BiCGStab (factor + every iteration in one launch).
  * profile_read fills ms[CMS_PROF_CLASSES], bytes[..] (algorithmic bytes:
  * every array a kernel touches counted once) and count[..] (launches);
  * reset=1 clears. */
-#define CMS_PROF_CLASSES 9
+#define CMS_PROF_CLASSES 10
 int cms_solver_profile(cms_solver* s, int enable);
 int cms_solver_profile_read(cms_solver* s, int reset, double* ms, double* bytes, long long* count);
 /* The stream the handle runs on (a cudaStream_t). */
@@ -165,6 +175,7 @@ typedef struct cms_flow_opts {
   int skewcor;       /* skewness corrections on telescoping grids (flow.F90:108)   */
   double inner_tol;  /* refinement: FP32 solve tolerance                           */
   int inner_max;
+  int multi_kernel;  /* solver kernels, as cms_solver_opts.multi_kernel            */
 } cms_flow_opts;
 
 typedef struct cms_flow_info {

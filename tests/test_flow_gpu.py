@@ -3,10 +3,13 @@
 Same algorithm on both sides: every solve runs a fixed number of Krylov
 iterations (the tolerance is never met) and the oracle solves in the GPU's
 unknown order (natural/level order or multicolour).  The only differences are
-FP64 rounding: the GPU sums dot products and face terms in another order, and
-unconverged Krylov iterations amplify those last bits.  Observed: water level
-within 1e-10 m, velocities and fluxes within 1e-7 relative to their largest
-value; the bounds below are 1e-9 m and 1e-6.  The outer iteration count is
+FP64 rounding: the GPU sums dot products and face terms in another order.
+The iteration counts are chosen so that no solve runs on after its residual
+has reached rounding level (there BiCGStab's scalars are formed from noise and
+the two sides drift apart): on the small basin the velocity systems reach
+1e-15 within a few iterations.  Observed: water level within 1e-10 m,
+velocities and fluxes within 1e-8 relative to their largest value; the bounds
+below are 1e-9 m and 1e-6.  The outer iteration count is
 fixed at 4 (check_conv only tests divergence before the sixth iteration).
 FP32 + FP64 refinement is compared with the FP64 oracle on converged solves
 (1e-5).
@@ -20,7 +23,8 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-FIXED = dict(nsolv=3, tol=1e-30, nswp_pp=12, nswp_uv=8)
+FIXED = {"inlet": dict(nsolv=3, tol=1e-30, nswp_pp=12, nswp_uv=8),
+         "basin": dict(nsolv=3, tol=1e-30, nswp_pp=8, nswp_uv=4)}
 
 
 def _pair(case, steps, maxit=4, precision="fp64", ordering="multicolor", same_order=True, **solver):
@@ -70,7 +74,7 @@ def test_geometry_matches_oracle():
 @pytest.mark.parametrize("kind", ["basin", "inlet"])
 def test_flow_step_matches_oracle(kind, ordering):
     c = cases.tidal_basin(40, 30, seed=1) if kind == "basin" else cases.tidal_inlet(12000, seed=3)
-    o, m = _pair(c, steps=2, ordering=ordering, **FIXED)
+    o, m = _pair(c, steps=2, ordering=ordering, **FIXED[kind])
     e = _errors(o, m, c.grid)
     print(kind, ordering, e)
     assert e["eta_m"] <= 1e-9

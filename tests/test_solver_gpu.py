@@ -41,15 +41,16 @@ def _oracle_on_device_order(g, perm, acoef, ss, sp, phi, **kw):
 
 @pytest.mark.parametrize("kind", ["cart", "tel"])
 @pytest.mark.parametrize("ordering", ["natural", "multicolor"])
-@pytest.mark.parametrize("nsolv", [3, 4])
-def test_fp64_parity(kind, ordering, nsolv):
+@pytest.mark.parametrize("nsolv,multi", [(3, False), (3, True), (4, False)])
+def test_fp64_parity(kind, ordering, nsolv, multi):
+    """BiCGStab runs both as one persistent launch and as per-phase kernels."""
     g = _grids()[kind]
     acoef, ss, sp, phi = G.random_system(g, seed=21)
     phi[: g.ncells] = np.random.default_rng(1).standard_normal(g.ncells) * 0.1
     relax = 0.8
     nswp = 40 if nsolv == 3 else 15
     tol = 1e-8
-    s = S.Solver(g, ordering=ordering, tol=tol)
+    s = S.Solver(g, ordering=ordering, tol=tol, multi_kernel=multi)
     a, b, c, p = _copy(acoef, ss, sp, phi)
     res = np.zeros_like(b)
     info = s.solve(a, b, c, res, p, relax=relax, nswp=nswp, nsolv=nsolv)
@@ -217,3 +218,54 @@ def test_large_system_residual_property(n_target):
         info = s.solve(a, b, c, res, p, relax=1.0, nswp=1000, nsolv=3)
         assert info["status"] == 0, info
         assert 0 <= info["true_relres"] <= 2e-6, info
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32_refine", "fp32"])
+@pytest.mark.parametrize("kind", ["tel", "big"])
+def test_persistent_matches_multi_kernel(precision, kind):
+    """The persistent BiCGStab launch and the per-phase kernels run the same
+    arithmetic; only the block partition of the dot products differs, so the
+    iteration counts agree and the solutions agree to rounding."""
+    g = G.solver_test_grid(250_000) if kind == "big" else _grids()["tel"]
+    acoef, ss, sp, phi = G.random_system(g, seed=5)
+    if precision == "fp32":
+        acoef, ss, sp, phi = (x.astype(np.float32) for x in (acoef, ss, sp, phi))
+    out = []
+    for multi in (False, True):
+        # exact multicolour factor on both sides (the two-phase inner factor is
+        # tested on its own below)
+        s = S.Solver(g, precision="fp64" if precision == "fp32" else precision, tol=1e-6, norm=2,
+                     multi_kernel=multi, inner_relax=False)
+        a, b, c, p = _copy(acoef, ss, sp, phi)
+        res = np.zeros_like(b)
+        info = s.solve(a, b, c, res, p, nswp=500, nsolv=3)
+        assert info["status"] == 0, info
+        out.append((info, p[: g.ncells].astype(np.float64)))
+    (i0, p0), (i1, p1) = out
+    assert i0["iters"] == i1["iters"] and i0["refine_steps"] == i1["refine_steps"], (i0, i1)
+    # FP64: rounding only; FP32 solves and refined solves: both within their
+    # stopping tolerance of the same solution
+    tol = {"fp64": 1e-9, "fp32_refine": 1e-5, "fp32": 1e-4}[precision]
+    assert np.abs(p0 - p1).max() <= tol * np.abs(p1).max()
+
+
+@pytest.mark.parametrize("kind", ["tel", "big"])
+def test_two_phase_inner_factor(kind):
+    """FP32 + refinement with the two-phase inner factor (couplings among the
+    rows of colours >= 2 dropped) converges to the FP64 tolerance and to the
+    same solution as the exact multicolour factor."""
+    g = G.solver_test_grid(250_000) if kind == "big" else _grids()["tel"]
+    acoef, ss, sp, phi = G.random_system(g, seed=9)
+    res = {}
+    for relax in (True, False):
+        s = S.Solver(g, precision="fp32_refine", tol=1e-8, norm=2, inner_relax=relax)
+        assert s.last_info is None
+        a, b, c, p = _copy(acoef, ss, sp, phi)
+        r = np.zeros_like(b)
+        info = s.solve(a, b, c, r, p, nswp=2000, nsolv=3)
+        assert info["status"] == 0 and info["ncolors"] > 2, info
+        assert info["true_relres"] <= 1e-8, info
+        res[relax] = (info, p[: g.ncells].copy())
+    print({k: (v[0]["iters"], v[0]["refine_steps"]) for k, v in res.items()})
+    p1, p0 = res[True][1], res[False][1]
+    assert np.abs(p1 - p0).max() <= 1e-6 * np.abs(p0).max()
