@@ -156,6 +156,8 @@ def run_solve_ours(args):
     launches0 = solver.launches
     ms_total = 0.0
     infos = []
+    if args.ncu:  # a profiler started with --profile-from-start off sees the timed steps only
+        torch.cuda.profiler.start()
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             t_ss.copy_(t_ss0); t_phi.copy_(t_phi0)
@@ -168,6 +170,8 @@ def run_solve_ours(args):
             e1.synchronize()
             ms_total += e0.elapsed_time(e1)
     torch.cuda.synchronize(dev)
+    if args.ncu:
+        torch.cuda.profiler.stop()
     launches = solver.launches - launches0
     if world > 1:
         t = torch.tensor([ms_total], device=dev, dtype=torch.float64)
@@ -245,7 +249,8 @@ def run_solve_ours(args):
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": round(e2e_ms, 3)},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "kernel": top, "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(ach / peak, 4), "peak_kind": peak_kind, "traffic": None},
+                     "frac": round(ach / peak, 4), "peak_kind": peak_kind,
+                     "traffic": persist_traffic(prof, top, infos[-1]["iters"], args.steps, args.precision)},
         "kernels": kernels,
     }
     out["clocks"] = clk.summary()
@@ -299,6 +304,20 @@ def run_solve_reference(args):
 
 FLOW_SOLVER = dict(nsolv=3, tol=1e-6, norm=2)
 
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# persistent FP32 BiCGStab kernel per Krylov iteration on a 1M-unknown system,
+# from one ncu capture of its three launches in a 1M solve (1,343 MB over 24
+# iterations; profiles/bicgstab_persistent_solve_1M.md).  The roofline's
+# traffic is this figure times the iterations of an average launch.
+PERSIST_DRAM_BYTES_PER_ITER = 1343.35e6 / 24
+
+
+def persist_traffic(prof, top, iters_per_step, steps, precision):
+    if top != "bicgstab_persistent" or precision != "fp32_refine" or not prof[top]["launches"]:
+        return None
+    per_launch = iters_per_step * steps / prof[top]["launches"]
+    return round(PERSIST_DRAM_BYTES_PER_ITER * per_launch)
+
 
 def flow_case(cells: int, seed: int):
     from cms2d_b200 import cases
@@ -350,18 +369,34 @@ def run_flow_ours(args):
         torch.cuda.synchronize(dev)
         launches0 = m.launches
         ms_total = 0.0
+        t_wall = 0.0
         infos = []
+        # host buffers of the public API: boundary water levels in (pinned),
+        # the new water level out; the device time of each step is taken with
+        # events on the solver stream, the end-to-end time around the call and
+        # the read-back of the result
+        wse_h = torch.zeros(case.th_cells.size, dtype=torch.float64).pin_memory().numpy()
+        eta_h = torch.zeros(g.ncellsD, dtype=torch.float64).pin_memory().numpy()
+        eta_p = eta_h.ctypes.data_as(__import__("ctypes").c_void_p)
+        if args.ncu and prec == args.precision:  # the profiler sees the timed steps only
+            torch.cuda.profiler.start()
         with ClockSampler(local) as clk:
             for _ in range(args.steps):
+                wse_h[:] = case.wsebnd(m.t + case.dt)
                 flush.fill_(1.0)
                 torch.cuda.synchronize(dev)
                 e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+                t0 = time.perf_counter()
                 e0.record(stream)
-                infos.append(m.step())
+                infos.append(m.step(wsebnd=wse_h))
                 e1.record(stream)
+                L.cms_flow_get(m._h, 4, eta_p)
+                t_wall += time.perf_counter() - t0
                 e1.synchronize()
                 ms_total += e0.elapsed_time(e1)
         torch.cuda.synchronize(dev)
+        if args.ncu and prec == args.precision:
+            torch.cuda.profiler.stop()
         launches = m.launches - launches0
         if world > 1:
             t = torch.tensor([ms_total], device=dev, dtype=torch.float64)
@@ -372,22 +407,15 @@ def run_flow_ours(args):
              "krylov_iters_per_step": float(np.mean([i["krylov_iters"] for i in infos])),
              "status": sorted({i["status"] for i in infos}), "gpu_launches": int(launches),
              "clocks": clk.summary()}
+        if world > 1:
+            t = torch.tensor([t_wall], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            t_wall = float(t.item())
+        r["e2e"] = {"value": round(world * args.steps / t_wall, 5), "unit": "timesteps/s",
+                    "h2d_bytes_per_step": int(wse_h.nbytes), "d2h_bytes_per_step": int(eta_h.nbytes),
+                    "ms_per_step": round(1e3 * t_wall / args.steps, 2),
+                    "timing": "wall clock around cms_flow_step and the water-level read-back, same steps"}
         if prec == args.precision and not args.ncu:
-            # e2e: the public API with host buffers: boundary levels in (pinned), water level out
-            wse_h = torch.zeros(case.th_cells.size, dtype=torch.float64).pin_memory().numpy()
-            eta_h = torch.zeros(g.ncellsD, dtype=torch.float64).pin_memory().numpy()
-            ne = max(1, min(args.steps, 3))
-            t_e2e = 0.0
-            for _ in range(ne):
-                wse_h[:] = case.wsebnd(m.t + case.dt)
-                flush.fill_(1.0); torch.cuda.synchronize(dev)
-                t0 = time.perf_counter()
-                m.step(wsebnd=wse_h)
-                L.cms_flow_get(m._h, 4, eta_h.ctypes.data_as(__import__("ctypes").c_void_p))
-                t_e2e += time.perf_counter() - t0
-            r["e2e"] = {"value": round(world * ne / t_e2e, 5), "unit": "timesteps/s",
-                        "h2d_bytes_per_step": int(wse_h.nbytes), "d2h_bytes_per_step": int(eta_h.nbytes),
-                        "ms_per_step": round(1e3 * t_e2e / ne, 2)}
             # roofline: kernel classes timed with events over K profiled steps
             L.cms_solver_profile(h_solver, 1)
             _profile_read(L, h_solver)
@@ -402,7 +430,8 @@ def run_flow_ours(args):
         if world > 1:
             dist.destroy_process_group()
         if rank == 0:
-            print(json.dumps({"ncu_pass": True, "ms_per_step": res[args.precision]["ms_per_step"]}), flush=True)
+            print(json.dumps({"ncu_pass": True, "ms_per_step": res[args.precision]["ms_per_step"],
+                              "gpu_launches": res[args.precision]["gpu_launches"]}), flush=True)
         return
     head = res[args.precision]
     prof = head["profile"]
@@ -437,7 +466,8 @@ def run_flow_ours(args):
         "e2e": head["e2e"],
         "gpu_launches": head["gpu_launches"],
         "roofline": {"bound": "hbm", "kernel": top, "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(ach / peak, 4), "peak_kind": peak_kind, "traffic": None,
+                     "frac": round(ach / peak, 4), "peak_kind": peak_kind,
+                     "traffic": persist_traffic(prof, top, head["krylov_iters_per_step"], args.steps, args.precision),
                      "step_GBps": round(all_bytes / (tot / 1e3) / 1e9, 1) if tot else 0},
         "kernels": kernels,
         "clocks": head["clocks"],
@@ -478,6 +508,14 @@ def flow_cpu_sample(case, outer_per_step, n_outer, threads=None):
             "s_per_outer_iter": round(per_outer, 3)}
 
 
+# Outer SIMPLEC iterations per time step of the timed steps of the flow
+# workload (steps 4-6 of the 1M inlet after 3 warm-up steps; both precisions
+# of the GPU run take 16).  The CPU arm times a bounded number of outer
+# iterations and scales its per-iteration time by this count, since a CPU
+# step takes minutes.
+FLOW_OUTER_PER_STEP = 16
+
+
 def run_flow_reference(args):
     world, rank, local = dist_setup()
     if rank != 0:
@@ -489,26 +527,29 @@ def run_flow_reference(args):
     f = O.FlowOracle(case)
     f.set_solver(nsolv=3, precond=O.PC_ILU0, tol=1e-6, nswp_pp=200, nswp_uv=200, norm=2)
     f.init()
-    # warm-up: one full time step, which also gives the outer iterations per step
-    t0 = time.perf_counter()
-    r = f.step()
-    t_full = time.perf_counter() - t0
-    n_full = max(r["niter"], 1)
-    times = []
+    # warm-up steps: one outer iteration each (untimed)
+    for _ in range(args.warmup):
+        f.step(maxit=1)
+    per_outer = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
         rr = f.step(maxit=args.cpu_outer)
-        times.append((time.perf_counter() - t0) / max(rr["niter"], 1) * n_full)
-    v = args.steps / sum(times)
+        per_outer.append((time.perf_counter() - t0) / max(rr["niter"], 1))
+    t_step = float(np.mean(per_outer)) * FLOW_OUTER_PER_STEP
+    v = 1.0 / t_step
     out = {"impl": "reference", "metric": METRIC, "value": round(v, 6), "unit": "timesteps/s",
-           "n_gpus": world, "steps": args.steps, "warmup": 1,
-           "ms_per_step": round(1e3 * sum(times) / args.steps, 1), "higher_is_better": True, "scaling": "weak",
+           "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": round(1e3 * t_step, 1), "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded telescoping tidal inlet)",
-           "config": {"workload": f"implicit flow step, telescoping tidal inlet {case.grid.ncells} cells, "
-                                  f"CPU oracle port, solves to 1e-6", "cells": case.grid.ncells},
+           "config": {"workload": f"implicit flow step, telescoping tidal inlet {case.grid.ncells} cells (40/20/10 m), "
+                                  f"dt={case.dt:g} s, ILU0-BiCGStab solves to 1e-6 rel. L2 residual",
+                      "cells": case.grid.ncells, "precision": "fp64", "ordering": "natural",
+                      "implementation": "CPU restatement of the reference path (oracle), OpenMP"},
            "cpu_baseline": {"value": round(v, 6), "unit": "timesteps/s", "cores": threads, "kind": "port",
-                            "sample": f"warm-up: one full step ({n_full} outer iterations, {t_full:.1f} s); each "
-                                      f"timed step: {args.cpu_outer} outer iterations scaled to {n_full}"},
+                            "sample": f"{args.warmup} warm-up steps of one outer iteration, then {args.steps} "
+                                      f"steps of {args.cpu_outer} outer iterations each; mean time per outer "
+                                      f"iteration {np.mean(per_outer):.2f} s scaled to {FLOW_OUTER_PER_STEP} "
+                                      f"outer iterations per step"},
            "e2e": {"value": round(v, 6), "unit": "timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
