@@ -63,7 +63,8 @@ __device__ __forceinline__ T ldm(const T* p) { return __ldcg(p); }  // load of d
 
 template <typename T>
 struct PersistArgs {
-  int n, KL, G;
+  int n, KL, KU, G;
+  int klB, kuB;            // slot bounds over groups 1..G-1
   int gku_last;            // upper slots of the last group (0: its backward step is fused)
   int spmv0;               // 1: group 0 has no lower couplings and its own backward
                            // phase; the SpMV of its rows is done in that phase
@@ -209,7 +210,7 @@ __device__ __forceinline__ int2 tile_rows(const PersistArgs<T>& A, int g) {
 // r1 are replaced by the first row of the batch (loads stay in bounds) and
 // marked !ok; their results are not stored.
 template <typename T>
-constexpr int NRT = sizeof(T) == 4 ? 4 : 2;  // rows per thread per batch (register budget)
+constexpr int NRT = 2;  // rows per thread per batch (register budget; measured best for FP32 and FP64)
 template <int NR, typename F>
 __device__ __forceinline__ void for_rows(int r0, int r1, F&& f) {
   for (int base = r0 + (int)threadIdx.x; base < r1; base += NR * (int)blockDim.x) {
@@ -223,6 +224,50 @@ __device__ __forceinline__ void for_rows(int r0, int r1, F&& f) {
     }
     f(r, ok);
   }
+}
+
+// Rows of this tile in groups ga..gb as one index space, so that small groups
+// do not each cost a batch of their own.  With up to GFLAT groups the tile's
+// ranges sit in shared memory (s_lo: first row of each group's range, s_pre:
+// prefix counts); with more groups (level schedules) each group is a loop.
+constexpr int GFLAT = 16;
+template <int NR, typename T, typename F>
+__device__ __forceinline__ void for_rows_g(const PersistArgs<T>& A, const int* s_lo, const int* s_pre, int ga, int gb,
+                                           F&& f) {
+  if (A.G > GFLAT) {
+    for (int g = ga; g <= gb; ++g) {
+      const int2 rr = tile_rows(A, g);
+      for_rows<NR>(rr.x, rr.y, f);
+    }
+    return;
+  }
+  const int k0 = s_pre[ga], k1 = s_pre[gb + 1];
+  for (int base = k0 + (int)threadIdx.x; base < k1; base += NR * (int)blockDim.x) {
+    int r[NR];
+    bool ok[NR];
+#pragma unroll
+    for (int q = 0; q < NR; ++q) {
+      int k = base + q * (int)blockDim.x;
+      ok[q] = k < k1;
+      if (!ok[q]) k = base;
+      int g = ga;
+      while (g < gb && k >= s_pre[g + 1]) ++g;
+      r[q] = s_lo[g] + (k - s_pre[g]);
+    }
+    f(r, ok);
+  }
+}
+
+// rows of this tile in groups ga..gb
+template <typename T>
+__device__ __forceinline__ int tile_count(const PersistArgs<T>& A, const int* s_pre, int ga, int gb) {
+  if (A.G <= GFLAT) return s_pre[gb + 1] - s_pre[ga];
+  int c = 0;
+  for (int g = ga; g <= gb; ++g) {
+    const int2 rr = tile_rows(A, g);
+    c += rr.y - rr.x;
+  }
+  return c;
 }
 
 // Slot sums over NR rows at once, slot loops bounded by the group's slot
@@ -325,8 +370,8 @@ __device__ __forceinline__ void spmv_rows(const PersistArgs<T>& A, T (&y)[NR], c
 // dots[0..1]): those rows couple only to later groups, whose z is final, and
 // the gathered neighbour values serve both sums.
 template <typename T, int MODE>
-__device__ __forceinline__ void pc_apply(const PersistArgs<T>& A, PhaseState& ph, double omg_d, double alf_d,
-                                         double gam_d, double (&dots)[2]) {
+__device__ __forceinline__ void pc_apply(const PersistArgs<T>& A, PhaseState& ph, const int* s_lo, const int* s_pre,
+                                         double omg_d, double alf_d, double gam_d, double (&dots)[2]) {
   constexpr int NR = NRT<T>;
   const T omg = (T)omg_d, alf = (T)alf_d, gam = (T)gam_d;
   const int G = A.G;
@@ -339,18 +384,11 @@ __device__ __forceinline__ void pc_apply(const PersistArgs<T>& A, PhaseState& ph
   const int nfwd = A.relax ? 2 : G;
   for (int ph_i = 0; ph_i < nfwd && ph.ok; ++ph_i) {
     const int ga = ph_i, gb = (A.relax && ph_i == 1) ? G - 1 : ph_i;
-    bool any = false;
-    for (int g = ga; g <= gb; ++g) {
-      const int2 rr = tile_rows(A, g);
-      any = any || (rr.y > rr.x);
-    }
-    if (any) wait_neighbours(A, ph);
-   for (int g = ga; g <= gb; ++g) {
-    const int2 rr = tile_rows(A, g);
-    const int klg = __ldg(&A.gkl[g]);
-    const bool last = fuse && (g == G - 1 || (A.relax && g >= 1));
-    const int cmax = (A.relax && g >= 1) ? A.g1 : 0x7fffffff;
-    for_rows<NR>(rr.x, rr.y, [&](const int (&r)[NR], const bool (&ok)[NR]) {
+    if (tile_count(A, s_pre, ga, gb) > 0) wait_neighbours(A, ph);
+    const int klg = ga == gb ? __ldg(&A.gkl[ga]) : A.klB;
+    const bool last = fuse && (gb == G - 1 || (A.relax && ga >= 1));
+    const int cmax = (A.relax && ga >= 1) ? A.g1 : 0x7fffffff;
+    for_rows_g<NR>(A, s_lo, s_pre, ga, gb, [&](const int (&r)[NR], const bool (&ok)[NR]) {
       T y[NR], xo[NR], zo[NR], iv[NR];
 #pragma unroll
       for (int q = 0; q < NR; ++q) {
@@ -379,7 +417,6 @@ __device__ __forceinline__ void pc_apply(const PersistArgs<T>& A, PhaseState& ph
         A.z[r[q]] = last ? iv[q] * w[q] : w[q];
       }
     });
-   }
     end_phase(A, ph);
   }
   for (int g = A.relax ? 0 : (fuse ? G - 2 : G - 1); g >= 0 && ph.ok; --g) {
@@ -453,15 +490,29 @@ __global__ void __launch_bounds__(TPB, 4) k_bicg_persistent(PersistArgs<T> A) {
   constexpr int NR = NRT<T>;
   const int G = A.G;
   PhaseState ph{0u, 0u, true, true};
+  // this tile's group ranges (groups beyond GFLAT are read per phase)
+  __shared__ int s_lo[GFLAT], s_pre[GFLAT + 1];
+  if (G <= GFLAT && threadIdx.x == 0) {
+    int acc = 0;
+    for (int g = 0; g < G; ++g) {
+      const int2 rr = tile_rows(A, g);
+      s_lo[g] = rr.x;
+      s_pre[g] = acc;
+      acc += rr.y - rr.x;
+    }
+    s_pre[G] = acc;
+  }
+  __syncthreads();
+  // slot bounds of the SpMV phases (rows of groups spmv0..G-1)
+  const int klS = A.spmv0 ? A.klB : A.KL, kuS = A.spmv0 ? A.kuB : A.KU;
   // start: r = b - A x + small, r0 = r, p = u = v = 0 (x is only read here,
   // or zeroed row by row)
   double res0 = 1.0, bet = 0.0;
   {
     double s2[2] = {0.0, 0.0};
-    for (int g = 0; g < G; ++g) {
-      const int2 rr = tile_rows(A, g);
-      const int klg = __ldg(&A.gkl[g]), kug = __ldg(&A.gku[g]);
-      for_rows<NR>(rr.x, rr.y, [&](const int (&r)[NR], const bool (&ok)[NR]) {
+    {
+      const int klg = A.KL, kug = A.KU;
+      for_rows_g<NR>(A, s_lo, s_pre, 0, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR]) {
         T term[NR], bq[NR], dg[NR], xq[NR];
 #pragma unroll
         for (int q = 0; q < NR; ++q) {
@@ -505,16 +556,15 @@ __global__ void __launch_bounds__(TPB, 4) k_bicg_persistent(PersistArgs<T> A) {
     ++it;
     const double omg = bet * gam / (alf * bet0 + SMALL);
     double dots[2] = {0.0, 0.0};
-    pc_apply<T, 0>(A, ph, omg, alf, gam, dots);
+    pc_apply<T, 0>(A, ph, s_lo, s_pre, omg, alf, gam, dots);
     if (!ph.ok) break;
     // u = A z, u.r0 (rows of later groups)
     {
       double s1[1] = {dots[0]};
       wait_neighbours(A, ph);
-      for (int g = A.spmv0; g < G; ++g) {
-        const int2 rr = tile_rows(A, g);
-        const int klg = __ldg(&A.gkl[g]), kug = __ldg(&A.gku[g]);
-        for_rows<NR>(rr.x, rr.y, [&](const int (&r)[NR], const bool (&ok)[NR]) {
+      {
+        const int klg = klS, kug = kuS;
+        for_rows_g<NR>(A, s_lo, s_pre, A.spmv0, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR]) {
           T ur[NR], d1[NR];
 #pragma unroll
           for (int q = 0; q < NR; ++q) d1[q] = ldm(&A.r0[r[q]]);
@@ -537,16 +587,15 @@ __global__ void __launch_bounds__(TPB, 4) k_bicg_persistent(PersistArgs<T> A) {
       bet0 = bet;
     }
     dots[0] = dots[1] = 0.0;
-    pc_apply<T, 1>(A, ph, omg, alf, gam, dots);
+    pc_apply<T, 1>(A, ph, s_lo, s_pre, omg, alf, gam, dots);
     if (!ph.ok) break;
     // v = A z, v.r, v.v (rows of later groups)
     {
       double s2[2] = {dots[0], dots[1]};
       wait_neighbours(A, ph);
-      for (int g = A.spmv0; g < G; ++g) {
-        const int2 rr = tile_rows(A, g);
-        const int klg = __ldg(&A.gkl[g]), kug = __ldg(&A.gku[g]);
-        for_rows<NR>(rr.x, rr.y, [&](const int (&r)[NR], const bool (&ok)[NR]) {
+      {
+        const int klg = klS, kug = kuS;
+        for_rows_g<NR>(A, s_lo, s_pre, A.spmv0, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR]) {
           T vr[NR], d1[NR];
 #pragma unroll
           for (int q = 0; q < NR; ++q) d1[q] = ldm(&A.r[r[q]]);
@@ -572,9 +621,8 @@ __global__ void __launch_bounds__(TPB, 4) k_bicg_persistent(PersistArgs<T> A) {
     {
       const T a = (T)alf;
       double s3[3] = {0.0, 0.0, 0.0};
-      for (int g = 0; g < G; ++g) {
-        const int2 rr = tile_rows(A, g);
-        for_rows<NR>(rr.x, rr.y, [&](const int (&r)[NR], const bool (&ok)[NR]) {
+      {
+        for_rows_g<NR>(A, s_lo, s_pre, 0, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR]) {
           T xn[NR], rn[NR], r0v[NR];
 #pragma unroll
           for (int q = 0; q < NR; ++q) {

@@ -495,7 +495,12 @@ static int run_bicgstab_persistent(Solver* S, Mat<T>& A, Work<T>& W, int tiles, 
                                    int xzero) {
   const HostPattern& P = S->hp;
   PersistArgs<T> a;
-  a.n = P.n; a.KL = P.KL; a.G = P.G; a.gku_last = P.gku[P.G - 1];
+  a.n = P.n; a.KL = P.KL; a.KU = P.KU; a.G = P.G; a.gku_last = P.gku[P.G - 1];
+  a.klB = a.kuB = 0;
+  for (int g = 1; g < P.G; ++g) {
+    a.klB = std::max(a.klB, P.gkl[g]);
+    a.kuB = std::max(a.kuB, P.gku[g]);
+  }
   a.relax = S->cur_relax;
   a.g1 = P.G > 1 ? P.gstart[1] : P.n;
   a.spmv0 = (P.gkl[0] == 0 && ((a.relax || a.gku_last == 0) ? P.G >= 2 : P.G >= 1)) ? 1 : 0;
