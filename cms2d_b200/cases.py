@@ -88,18 +88,41 @@ def _fill_dummies(g: G.Grid, vals_active: np.ndarray) -> np.ndarray:
 
 
 def tidal_basin(nx: int = 200, ny: int = 100, dx: float = 20.0, seed: int = 0, amp: float = 0.5,
-                manning: float = 0.025, dt: float = 600.0, hours: float = 24.0) -> Case:
+                manning: float = 0.025, dt: float = 600.0, hours: float = 24.0, depth_shore: float = 2.0,
+                depth_off: float = 10.0) -> Case:
     rng = np.random.default_rng(seed)
     g = G.cartesian_grid(nx, ny, dx)
     n = g.ncells
     jrow = (g.y[:n] / dx - 0.5)  # 0 .. ny-1
-    depth = 2.0 + 8.0 * jrow / max(ny - 1, 1)
+    depth = depth_shore + (depth_off - depth_shore) * jrow / max(ny - 1, 1)
     bumps = _smooth_field((ny, nx), 6.0, rng) * 0.2
     depth = depth + bumps.ravel()  # natural order is row-major (y then x)
     zb = _fill_dummies(g, -depth)
     th_cells, th_faces = _north_string(g)
     return Case("tidal_basin", g, zb, np.full(n, manning), th_cells, th_faces, [(amp, M2_HOURS)], dt,
                 int(round(hours * 3600.0 / dt)))
+
+
+def ensemble_basins(nmembers: int = 64, seed: int = 0, nmin: int = 50_000, nmax: int = 400_000,
+                    dt: float = 600.0, steps: int = 24) -> list:
+    """Independent tidal basins of uneven size: uniform Cartesian grids at
+    20 m with nmin..nmax cells and aspect ratios 1:1 to 4:1, each with its own
+    M2 amplitude (0.3-1.0 m), Manning n (0.015-0.035) and depth profile
+    (shore 1.5-3 m, offshore 6-14 m, its own seeded bumps)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(nmembers):
+        ncell = rng.uniform(nmin, nmax)
+        aspect = rng.uniform(1.0, 4.0)
+        long_side = int(round(np.sqrt(ncell * aspect)))
+        short_side = max(4, int(round(ncell / long_side)))
+        nx, ny = (long_side, short_side) if rng.random() < 0.5 else (short_side, long_side)
+        c = tidal_basin(nx, ny, 20.0, seed=int(rng.integers(1 << 30)), amp=float(rng.uniform(0.3, 1.0)),
+                        manning=float(rng.uniform(0.015, 0.035)), dt=dt, hours=steps * dt / 3600.0,
+                        depth_shore=float(rng.uniform(1.5, 3.0)), depth_off=float(rng.uniform(6.0, 14.0)))
+        c.name = f"basin{k:02d}"
+        out.append(c)
+    return out
 
 
 def tidal_inlet(target_cells: int = 1_000_000, seed: int = 0, dt: float = 300.0, nsteps: int = 48) -> Case:

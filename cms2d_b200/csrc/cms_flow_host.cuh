@@ -42,6 +42,9 @@ struct cms_flow {
   long long launches = 0;
   double t_sim = 0.0;
   double nfaces = 0.0;  // faces of active cells (sum of ncface), for byte counts
+  // outer-loop state of the step in progress (check_conv's residual history)
+  double it_rm[4] = {0, 0, 0, 0}, it_rmom0[4] = {0, 0, 0, 0}, it_rmom1[4] = {0, 0, 0, 0};
+  long long it_kry = 0;
 
   template <typename P>
   int alloc(P** p, size_t count) {
@@ -396,8 +399,9 @@ static int grad2(Flow* F, const double* a, const double* b, double* const* ax, d
 }
 
 // solve(acoef,ss,sp,res,phi,n) on the flow state (device order)
-static int flow_solve(Flow* F, double* ss, const double* sp, double* phi, double relax, int nswp, double* rmom,
-                      cms_solve_info* info) {
+// solve() prologue of one flow system: the device-order system (and its FP32
+// copy for refinement) from the face coefficients, and rmom.
+static int flow_solve_begin(Flow* F, double* ss, const double* sp, double* phi, double relax) {
   Solver* S = F->S;
   const bool refine = S->opts.precision == CMS_PREC_FP32_REFINE;
   // reduction kernel: its grid must stay within the solver's partials buffer
@@ -405,11 +409,22 @@ static int flow_solve(Flow* F, double* ss, const double* sp, double* phi, double
                  F->G, F->st.acoef, ss, sp, F->st.res, phi, F->d_fslot_dev, relax, S->A64.aoff, S->A64.diag,
                  S->W64.b, S->W64.x, refine ? S->A32.aoff : nullptr, refine ? S->A32.diag : nullptr, S->d_part,
                  S->d_st)));
-  const int rc = solve_core64(S, F->opts.nsolv, nswp, info);
-  if (rc == CMS_DEVICE_ERROR || rc == CMS_UNSUPPORTED || rc == CMS_BAD_ARGUMENT) return rc;
-  FLAUNCHB(F, fbytes(F, 2, 0), (kf_copy<<<fblk(F->n), TPB, 0, S->stream>>>(F->n, S->W64.x, phi)));
+  return CMS_OK;
+}
+
+// The solution back into the flow field.
+static int flow_solve_end(Flow* F, double* phi, double* rmom, const cms_solve_info* info) {
+  FLAUNCHB(F, fbytes(F, 2, 0), (kf_copy<<<fblk(F->n), TPB, 0, F->S->stream>>>(F->n, F->S->W64.x, phi)));
   *rmom = info->rmom;
   return CMS_OK;
+}
+
+static int flow_solve(Flow* F, double* ss, const double* sp, double* phi, double relax, int nswp, double* rmom,
+                      cms_solve_info* info) {
+  CHK(flow_solve_begin(F, ss, sp, phi, relax));
+  const int rc = solve_core64(F->S, F->opts.nsolv, nswp, info);
+  if (rc == CMS_DEVICE_ERROR || rc == CMS_UNSUPPORTED || rc == CMS_BAD_ARGUMENT) return rc;
+  return flow_solve_end(F, phi, rmom, info);
 }
 
 // eddy viscosity with the boundary recurrences and its face values
@@ -523,75 +538,122 @@ static int check_conv(const double rm[4], double rmom0[4], double rmom1[4], int 
   return 1;
 }
 
-static int flow_step(Flow* F, double dt, const double* wsebnd, cms_flow_info* info) {
+// Stages of one time step (flow_imp.F90:29-312), shared by the single-model
+// step and the ensemble step.
+
+// before the outer loop: string water levels, static sources
+static int step_begin(Flow* F, double dt, const double* wsebnd) {
   FlowState& T = F->st;
-  Solver* S = F->S;
-  cudaStream_t s = S->stream;
-  cms_flow_info loc{};
-  if (!info) info = &loc;
-  std::memset(info, 0, sizeof(*info));
+  cudaStream_t s = F->S->stream;
   if (F->nth) {  // water levels of the string, placed on the string's dummies
     CMS_CUDA(cudaMemcpyAsync(F->d_wse, wsebnd, F->nth * sizeof(double), cudaMemcpyHostToDevice, s));
     FLAUNCH(F, (kf_scatter_vals<<<fblk(F->nth), TPB, 0, s>>>(F->d_th_dummy, F->d_wse, F->nth, F->d_wse_cell)));
   }
   FLAUNCHB(F, fbytes(F, 13, 0, 3), (kf_static<<<fblk(F->nD), TPB, 0, s>>>(F->G, T, dt)));
-  const int maxit = F->opts.maxit > 0 ? F->opts.maxit : 20 + F->n / 10000;
-  double rm[4] = {0, 0, 0, 0}, rmom0[4] = {0, 0, 0, 0}, rmom1[4] = {0, 0, 0, 0};
-  int iconv = 1, niter = 0;
-  long long kry = 0;
+  for (int q = 0; q < 4; ++q) F->it_rm[q] = F->it_rmom0[q] = F->it_rmom1[q] = 0.0;
+  F->it_kry = 0;
+  std::memset(F->last_solve, 0, 3 * sizeof(cms_solve_info));
+  return CMS_OK;
+}
+
+static int flow_maxit(const Flow* F) { return F->opts.maxit > 0 ? F->opts.maxit : 20 + F->n / 10000; }
+
+// momentum coefficients (before the u and v solves)
+static int stage_uv(Flow* F) {
+  FlowState& T = F->st;
+  const int cd = F->cur_duv;
+  FLAUNCHB(F, fbytes(F, 16.5, 5.6), (kf_coef_uv<<<fblk(F->n), TPB, 0, F->S->stream>>>(F->G, T, T.dux[cd], T.duy[cd],
+                                                                                       T.dvx[cd], T.dvy[cd], T.dpx[0],
+                                                                                       T.dpy[0])));
+  return CMS_OK;
+}
+
+// pressure-correction system (after the u and v solves)
+static int stage_pp(Flow* F) {
+  FlowState& T = F->st;
+  cudaStream_t s = F->S->stream;
   const bool skew = F->opts.skewcor != 0;
-  for (niter = 1; niter <= maxit; ++niter) {
-    const int cd = F->cur_duv;
-    FLAUNCHB(F, fbytes(F, 16.5, 5.6), (kf_coef_uv<<<fblk(F->n), TPB, 0, s>>>(F->G, T, T.dux[cd], T.duy[cd], T.dvx[cd], T.dvy[cd], T.dpx[0],
-                                                      T.dpy[0])));
-    cms_solve_info* si = F->last_solve;
-    std::memset(si, 0, 3 * sizeof(cms_solve_info));
-    FCHK(flow_solve(F, T.su, T.spu, T.u, F->G.relax_uv, F->opts.nswp_uv, &rm[2], &si[0]));
-    kry += si[0].iters;
-    if (si[0].status == CMS_NONFINITE) { iconv = 0; break; }
-    FCHK(flow_solve(F, T.sv, T.spv, T.v, F->G.relax_uv, F->opts.nswp_uv, &rm[3], &si[1]));
-    kry += si[1].iters;
-    if (si[1].status == CMS_NONFINITE) { iconv = 0; break; }
-    FLAUNCHB(F, fbytes(F, 11.5, 1), (kf_pp_cell<<<fblk(F->n), TPB, 0, s>>>(F->G, T, T.dpx[0], T.dpy[0])));
-    if (skew) {
-      FCHK(grad2(F, T.Hu, T.Hv, T.dHux, T.dHuy, T.dHvx, T.dHvy, F->cur_dH));
-      FCHK(grad1(F, T.apuareap, T.dapx, T.dapy, F->cur_dap));
-    }
-    FLAUNCHB(F, fbytes(F, 8, 5), (kf_pp_face<<<fblk(F->n), TPB, 0, s>>>(F->G, T, skew ? 1 : 0, T.dHuy[F->cur_dH], T.dHvx[F->cur_dH],
-                                                      T.dapx[F->cur_dap], T.dapy[F->cur_dap], T.dpx[0], T.dpy[0])));
-    FLAUNCHB(F, fbytes(F, 6, 1.2), (kf_pp_src<<<fblk(F->n), TPB, 0, s>>>(F->G, T, skew ? 1 : 0, T.dppx[F->cur_dppx], T.dppy[F->cur_dppx],
-                                                     F->d_wse_cell)));
-    FCHK(flow_solve(F, T.su, T.sp, T.pp, 1.0, F->opts.nswp_pp, &rm[1], &si[2]));
-    kry += si[2].iters;
-    if (si[2].status == CMS_NONFINITE) { iconv = 0; break; }
-    if (F->nw) FLAUNCH(F, (kf_wall_copy<<<fblk(F->nw), TPB, 0, s>>>(F->d_w_cell, F->d_w_dummy, F->nw, T.pp)));
-    FCHK(grad1(F, T.pp, T.dppx, T.dppy, F->cur_dppx));
-    FLAUNCHB(F, fbytes(F, 9, 2.5), (kf_pvfc<<<fblk(F->n), TPB, 0, s>>>(F->G, T, skew ? 1 : 0, T.dppx[F->cur_dppx], T.dppy[F->cur_dppx])));
-    FLAUNCHB(F, fbytes(F, 6, 0, 6), (kf_pvfc_p<<<fblk(F->nD), TPB, 0, s>>>(F->G, T)));
-    if (F->nw) FLAUNCH(F, (kf_wall_copy<<<fblk(F->nw), TPB, 0, s>>>(F->d_w_cell, F->d_w_dummy, F->nw, T.p)));
-    FCHK(flow_grad_interp(F));
-    const int c2 = F->cur_duv;
-    FCHK(flow_vis(F, T.dux[c2], T.duy[c2], T.dvx[c2], T.dvy[c2]));
-    iconv = check_conv(rm, rmom0, rmom1, niter, maxit);
-    if (iconv == 0 || iconv == 2) break;
+  FLAUNCHB(F, fbytes(F, 11.5, 1), (kf_pp_cell<<<fblk(F->n), TPB, 0, s>>>(F->G, T, T.dpx[0], T.dpy[0])));
+  if (skew) {
+    CHK(grad2(F, T.Hu, T.Hv, T.dHux, T.dHuy, T.dHvx, T.dHvy, F->cur_dH));
+    CHK(grad1(F, T.apuareap, T.dapx, T.dapy, F->cur_dap));
   }
-  if (niter > maxit) niter = maxit;
+  FLAUNCHB(F, fbytes(F, 8, 5), (kf_pp_face<<<fblk(F->n), TPB, 0, s>>>(F->G, T, skew ? 1 : 0, T.dHuy[F->cur_dH],
+                                                                     T.dHvx[F->cur_dH], T.dapx[F->cur_dap],
+                                                                     T.dapy[F->cur_dap], T.dpx[0], T.dpy[0])));
+  FLAUNCHB(F, fbytes(F, 6, 1.2), (kf_pp_src<<<fblk(F->n), TPB, 0, s>>>(F->G, T, skew ? 1 : 0, T.dppx[F->cur_dppx],
+                                                                      T.dppy[F->cur_dppx], F->d_wse_cell)));
+  return CMS_OK;
+}
+
+// corrections after the pressure-correction solve, then check_conv
+static int stage_corr(Flow* F, int niter, int maxit, int* iconv) {
+  FlowState& T = F->st;
+  cudaStream_t s = F->S->stream;
+  const bool skew = F->opts.skewcor != 0;
+  if (F->nw) FLAUNCH(F, (kf_wall_copy<<<fblk(F->nw), TPB, 0, s>>>(F->d_w_cell, F->d_w_dummy, F->nw, T.pp)));
+  CHK(grad1(F, T.pp, T.dppx, T.dppy, F->cur_dppx));
+  FLAUNCHB(F, fbytes(F, 9, 2.5), (kf_pvfc<<<fblk(F->n), TPB, 0, s>>>(F->G, T, skew ? 1 : 0, T.dppx[F->cur_dppx],
+                                                                    T.dppy[F->cur_dppx])));
+  FLAUNCHB(F, fbytes(F, 6, 0, 6), (kf_pvfc_p<<<fblk(F->nD), TPB, 0, s>>>(F->G, T)));
+  if (F->nw) FLAUNCH(F, (kf_wall_copy<<<fblk(F->nw), TPB, 0, s>>>(F->d_w_cell, F->d_w_dummy, F->nw, T.p)));
+  CHK(flow_grad_interp(F));
+  const int c2 = F->cur_duv;
+  CHK(flow_vis(F, T.dux[c2], T.duy[c2], T.dvx[c2], T.dvy[c2]));
+  *iconv = check_conv(F->it_rm, F->it_rmom0, F->it_rmom1, niter, maxit);
+  return CMS_OK;
+}
+
+// after the outer loop: face velocities and levels, time levels, checks
+static int step_end(Flow* F, double dt, int niter, int iconv, cms_flow_info* info) {
+  FlowState& T = F->st;
+  cudaStream_t s = F->S->stream;
   FLAUNCHB(F, fbytes(F, 8, 3.2), (kf_velface_eta<<<fblk(F->n), TPB, 0, s>>>(F->G, T)));
   FLAUNCH(F, (kf_fric_vis<<<fblk(F->n), TPB, 0, s>>>(F->G, T, nullptr, nullptr, nullptr, nullptr, 0)));
-  FLAUNCHB(F, fbytes(F, 13, 0, 13), (kf_update<<<fblk(F->nD), TPB, 0, s>>>(F->G, T, T.dppx[0], T.dppy[0], T.dppx[1], T.dppy[1])));
+  FLAUNCHB(F, fbytes(F, 13, 0, 13), (kf_update<<<fblk(F->nD), TPB, 0, s>>>(F->G, T, T.dppx[0], T.dppy[0], T.dppx[1],
+                                                                           T.dppy[1])));
   FLAUNCH(F, (kf_check<<<fblk(F->n), TPB, 0, s>>>(F->G, T)));
   CMS_CUDA(cudaMemcpyAsync(F->h_flag, T.flag, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
   CMS_CUDA(cudaStreamSynchronize(s));
   F->t_sim += dt;
+  std::memset(info, 0, sizeof(*info));
   info->niter = niter;
   info->iconv = iconv;
-  info->rmom_p = rm[1]; info->rmom_u = rm[2]; info->rmom_v = rm[3];
-  info->krylov_iters = kry;
+  info->rmom_p = F->it_rm[1]; info->rmom_u = F->it_rm[2]; info->rmom_v = F->it_rm[3];
+  info->krylov_iters = F->it_kry;
   info->status = CMS_OK;
   if (F->h_flag[0]) info->status = CMS_UNSUPPORTED;       // a wet cell fell below the drying depth
   if (F->h_flag[1] || iconv == 0) info->status = CMS_NONFINITE;
   F->last = *info;
   return info->status;
+}
+
+static int flow_step(Flow* F, double dt, const double* wsebnd, cms_flow_info* info) {
+  FlowState& T = F->st;
+  cms_flow_info loc{};
+  if (!info) info = &loc;
+  CHK(step_begin(F, dt, wsebnd));
+  const int maxit = flow_maxit(F);
+  int iconv = 1, niter = 0;
+  cms_solve_info* si = F->last_solve;
+  for (niter = 1; niter <= maxit; ++niter) {
+    CHK(stage_uv(F));
+    std::memset(si, 0, 3 * sizeof(cms_solve_info));
+    FCHK(flow_solve(F, T.su, T.spu, T.u, F->G.relax_uv, F->opts.nswp_uv, &F->it_rm[2], &si[0]));
+    F->it_kry += si[0].iters;
+    if (si[0].status == CMS_NONFINITE) { iconv = 0; break; }
+    FCHK(flow_solve(F, T.sv, T.spv, T.v, F->G.relax_uv, F->opts.nswp_uv, &F->it_rm[3], &si[1]));
+    F->it_kry += si[1].iters;
+    if (si[1].status == CMS_NONFINITE) { iconv = 0; break; }
+    CHK(stage_pp(F));
+    FCHK(flow_solve(F, T.su, T.sp, T.pp, 1.0, F->opts.nswp_pp, &F->it_rm[1], &si[2]));
+    F->it_kry += si[2].iters;
+    if (si[2].status == CMS_NONFINITE) { iconv = 0; break; }
+    CHK(stage_corr(F, niter, maxit, &iconv));
+    if (iconv == 0 || iconv == 2) break;
+  }
+  if (niter > maxit) niter = maxit;
+  return step_end(F, dt, niter, iconv, info);
 }
 
 }  // namespace cms

@@ -72,10 +72,12 @@ struct PersistArgs {
   int g1;                  // first row of group 1
   const int* gkl;          // [G] lower slots per group
   const int* gku;          // [G] upper slots per group
-  const int* toff;         // [G][gridDim+1] tile row ranges per group
-  const int* dep_ptr;      // [gridDim+1]
+  int ntiles;              // tiles (blocks) of this system
+  int tile;                // this block's tile (set in the block's own copy)
+  const int* toff;         // [G][ntiles+1] tile row ranges per group
+  const int* dep_ptr;      // [ntiles+1]
   const int* dep_idx;      // neighbour tiles of each tile
-  unsigned int* progress;  // [gridDim] phases completed per tile (zero at launch)
+  unsigned int* progress;  // [ntiles] phases completed per tile (zero at launch)
   const int* col;
   const signed char* nlo;
   const signed char* nup;
@@ -91,7 +93,7 @@ struct PersistArgs {
   T* u;
   T* v;
   T* z;
-  double* part;  // [2][3][gridDim]
+  double* part;  // [2][3][ntiles]
   GridBar* bar;  // count: barrier arrivals (zero at launch); err: a wait gave up
   DevState* st;
   int maxit, norm, xzero;
@@ -115,7 +117,7 @@ __device__ __forceinline__ void wait_neighbours(const PersistArgs<T>& A, PhaseSt
   if (ph.fresh) { ph.fresh = false; return; }
   if (threadIdx.x < 32) {
     int fail = 0;
-    const int d0 = A.dep_ptr[blockIdx.x], d1 = A.dep_ptr[blockIdx.x + 1];
+    const int d0 = A.dep_ptr[A.tile], d1 = A.dep_ptr[A.tile + 1];
     for (int i = d0 + (int)threadIdx.x; i < d1 && !fail; i += 32) {
       const unsigned int* f = A.progress + A.dep_idx[i];
       unsigned int spins = 0;
@@ -137,7 +139,7 @@ __device__ __forceinline__ void end_phase(const PersistArgs<T>& A, PhaseState& p
   __syncthreads();
   ++ph.done;
   ph.fresh = false;
-  if (threadIdx.x == 0) st_release(A.progress + blockIdx.x, ph.done);
+  if (threadIdx.x == 0) st_release(A.progress + A.tile, ph.done);
 }
 
 // Grid-wide barrier on a monotone arrival counter.
@@ -145,7 +147,7 @@ template <typename T>
 __device__ __forceinline__ void grid_barrier(const PersistArgs<T>& A, PhaseState& ph) {
   __shared__ int s_fail;
   __syncthreads();
-  ph.target += gridDim.x;
+  ph.target += A.ntiles;
   if (threadIdx.x == 0) {
     int fail = 0;
     if (bar_failed(A.bar)) {
@@ -166,25 +168,25 @@ __device__ __forceinline__ void grid_barrier(const PersistArgs<T>& A, PhaseState
 }
 
 // Writes this block's partial sums of NS values into buffer buf.
-template <int NS>
-__device__ __forceinline__ void put_partials(double (&v)[NS], double* part, int buf) {
+template <int NS, typename T>
+__device__ __forceinline__ void put_partials(const PersistArgs<T>& A, double (&v)[NS], int buf) {
   block_sum<NS>(v);
   if (threadIdx.x == 0) {
 #pragma unroll
-    for (int q = 0; q < NS; ++q) part[((size_t)buf * 3 + q) * gridDim.x + blockIdx.x] = v[q];
+    for (int q = 0; q < NS; ++q) A.part[((size_t)buf * 3 + q) * A.ntiles + A.tile] = v[q];
   }
 }
 
 // After a grid barrier: every thread of every block gets the grid totals.
-template <int NS>
-__device__ __forceinline__ void get_totals(double (&tot)[NS], const double* part, int buf) {
+template <int NS, typename T>
+__device__ __forceinline__ void get_totals(const PersistArgs<T>& A, double (&tot)[NS], int buf) {
   __shared__ double bc[NS];
   double acc[NS];
 #pragma unroll
   for (int q = 0; q < NS; ++q) {
     acc[q] = 0.0;
-    for (int bb = threadIdx.x; bb < (int)gridDim.x; bb += blockDim.x)
-      acc[q] += __ldcg(&part[((size_t)buf * 3 + q) * gridDim.x + bb]);
+    for (int bb = threadIdx.x; bb < A.ntiles; bb += blockDim.x)
+      acc[q] += __ldcg(&A.part[((size_t)buf * 3 + q) * A.ntiles + bb]);
   }
   block_sum<NS>(acc);
   if (threadIdx.x == 0) {
@@ -200,7 +202,7 @@ __device__ __forceinline__ void get_totals(double (&tot)[NS], const double* part
 // Rows of this block's tile in group g.
 template <typename T>
 __device__ __forceinline__ int2 tile_rows(const PersistArgs<T>& A, int g) {
-  const int* o = A.toff + (size_t)g * (gridDim.x + 1) + blockIdx.x;
+  const int* o = A.toff + (size_t)g * (A.ntiles + 1) + A.tile;
   return make_int2(__ldg(o), __ldg(o + 1));
 }
 
@@ -485,8 +487,9 @@ __device__ __forceinline__ void pc_apply(const PersistArgs<T>& A, PhaseState& ph
   }
 }
 
+// The solve run by one block (tile A.tile of the system A describes).
 template <typename T>
-__global__ void __launch_bounds__(TPB, 4) k_bicg_persistent(PersistArgs<T> A) {
+__device__ __forceinline__ void bicg_body(const PersistArgs<T>& A) {
   constexpr int NR = NRT<T>;
   const int G = A.G;
   PhaseState ph{0u, 0u, true, true};
@@ -540,11 +543,11 @@ __global__ void __launch_bounds__(TPB, 4) k_bicg_persistent(PersistArgs<T> A) {
         }
       });
     }
-    put_partials<2>(s2, A.part, 0);
+    put_partials<2>(A, s2, 0);
     end_phase(A, ph);
     grid_barrier(A, ph);
     if (ph.ok) {
-      get_totals<2>(s2, A.part, 0);
+      get_totals<2>(A, s2, 0);
       res0 = (A.norm == 1) ? s2[0] : sqrt(s2[1]);
       bet = s2[1];
     }
@@ -577,11 +580,11 @@ __global__ void __launch_bounds__(TPB, 4) k_bicg_persistent(PersistArgs<T> A) {
           }
         });
       }
-      put_partials<1>(s1, A.part, buf);
+      put_partials<1>(A, s1, buf);
       end_phase(A, ph);
       grid_barrier(A, ph);
       if (!ph.ok) break;
-      get_totals<1>(s1, A.part, buf);
+      get_totals<1>(A, s1, buf);
       buf ^= 1;
       gam = bet / s1[0];
       bet0 = bet;
@@ -609,11 +612,11 @@ __global__ void __launch_bounds__(TPB, 4) k_bicg_persistent(PersistArgs<T> A) {
           }
         });
       }
-      put_partials<2>(s2, A.part, buf);
+      put_partials<2>(A, s2, buf);
       end_phase(A, ph);
       grid_barrier(A, ph);
       if (!ph.ok) break;
-      get_totals<2>(s2, A.part, buf);
+      get_totals<2>(A, s2, buf);
       buf ^= 1;
       alf = s2[0] / fmax(s2[1], SMALL);
     }
@@ -641,11 +644,11 @@ __global__ void __launch_bounds__(TPB, 4) k_bicg_persistent(PersistArgs<T> A) {
           }
         });
       }
-      put_partials<3>(s3, A.part, buf);
+      put_partials<3>(A, s3, buf);
       end_phase(A, ph);
       grid_barrier(A, ph);
       if (!ph.ok) break;
-      get_totals<3>(s3, A.part, buf);
+      get_totals<3>(A, s3, buf);
       buf ^= 1;
       const double res = (A.norm == 1) ? s3[0] : sqrt(s3[1]);
       rel = res / res0;
@@ -654,7 +657,7 @@ __global__ void __launch_bounds__(TPB, 4) k_bicg_persistent(PersistArgs<T> A) {
       if (rel < A.tol) { converged = 1; break; }
     }
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (A.tile == 0 && threadIdx.x == 0) {
     A.st->iter = it;
     A.st->s[S_RELRES] = rel;
     A.st->s[S_RES0] = res0;
@@ -663,6 +666,36 @@ __global__ void __launch_bounds__(TPB, 4) k_bicg_persistent(PersistArgs<T> A) {
     A.st->done = 1;
     A.st->s[S_BET] = bet;
   }
+}
+
+// One system: block b works on tile b.
+template <typename T>
+__global__ void __launch_bounds__(TPB, 4) k_bicg_persistent(PersistArgs<T> A) {
+  __shared__ PersistArgs<T> sA;
+  if (threadIdx.x == 0) {
+    sA = A;
+    sA.ntiles = gridDim.x;
+    sA.tile = blockIdx.x;
+  }
+  __syncthreads();
+  bicg_body<T>(sA);
+}
+
+// Several independent systems (an ensemble) in one launch: bmap[b] = (member,
+// tile) of block b.  Each member has its own tiles, progress counters,
+// partial sums, barrier and device state, so members share nothing but the
+// launch and each stops at its own stopping test.
+template <typename T>
+__global__ void __launch_bounds__(TPB, 4) k_bicg_batched(const PersistArgs<T>* __restrict__ members,
+                                                         const int2* __restrict__ bmap) {
+  __shared__ PersistArgs<T> sA;
+  if (threadIdx.x == 0) {
+    const int2 mt = bmap[blockIdx.x];
+    sA = members[mt.x];
+    sA.tile = mt.y;
+  }
+  __syncthreads();
+  bicg_body<T>(sA);
 }
 
 // Factor of the two-phase preconditioner: ILU(0) of A without the couplings

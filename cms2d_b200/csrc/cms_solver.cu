@@ -87,6 +87,7 @@ struct cms_solver {
   unsigned int* d_progress = nullptr;
   double* d_ppart = nullptr;
   int ptiles = 0;  // tiles (= blocks) of the persistent kernel; 0 not built, -1 not launchable
+  size_t cap_toff = 0, cap_dep = 0;  // capacities of d_toff / d_dep_idx
   int cur_relax = 0;  // the FP32 factor in A32 is the two-phase one (k_ilu0_relax)
   cms::Staging<double> S64;
   cms::Staging<float> S32;
@@ -387,25 +388,45 @@ static int bicg_iter(Solver* S, Mat<T>& A, Work<T>& W) {
   return CMS_OK;
 }
 
-// Tiles of the persistent kernel: one block per tile, every block resident
-// (cooperative launch), at most one block per 256 rows.  Builds the tile
-// tables on first use; 0 when the device cannot launch the kernel or a group
-// does not keep natural order.
-static int persist_tiles(Solver* S) {
-  if (S->ptiles != 0) return std::max(S->ptiles, 0);
-  S->ptiles = -1;
-  const HostPattern& P = S->hp;
-  int coop = 0, nsm = 0, per32 = 0, per64 = 0;
-  if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, S->dev) != cudaSuccess || !coop ||
-      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, S->dev) != cudaSuccess ||
+// Blocks of the persistent kernels that can be resident at once on the
+// device (cooperative launch limit); 0 when it cannot be launched.
+static int persist_capacity(int dev) {
+  int coop = 0, nsm = 0, per32 = 0, per64 = 0, perb = 0;
+  if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop ||
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per32, k_bicg_persistent<float>, TPB, 0) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per64, k_bicg_persistent<double>, TPB, 0) != cudaSuccess ||
-      std::min(per32, per64) <= 0) {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perb, k_bicg_batched<float>, TPB, 0) != cudaSuccess ||
+      std::min(std::min(per32, per64), perb) <= 0) {
     cudaGetLastError();
     return 0;
   }
+  return std::min(std::min(std::min(per32, per64), perb) * nsm, GRID_CAP);
+}
+
+static int build_tiles(Solver* S, int nt);
+
+// Tiles of the persistent kernel: one block per tile, every block resident,
+// at most one block per 256 rows.  Builds the tile tables on first use; 0
+// when the device cannot launch the kernel or a group does not keep natural
+// order.
+static int persist_tiles(Solver* S) {
+  if (S->ptiles != 0) return std::max(S->ptiles, 0);
+  const int cap = persist_capacity(S->dev);
+  if (cap <= 0) {
+    S->ptiles = -1;
+    return 0;
+  }
+  return build_tiles(S, std::min(cap, nblk(S->hp.n)));
+}
+
+// Tile tables for nt tiles (tile t = natural cells [t n / nt, (t+1) n / nt)).
+static int build_tiles(Solver* S, int nt) {
+  const HostPattern& P = S->hp;
   const int n = P.n;
-  const int nt = std::max(1, std::min(std::min(std::min(per32, per64) * nsm, nblk(n)), GRID_CAP));
+  nt = std::max(1, std::min(std::min(nt, nblk(n)), GRID_CAP));
+  if (S->ptiles == nt) return nt;
+  S->ptiles = -1;
   // tile t = natural cells [tstart[t], tstart[t+1])
   std::vector<int> tstart(nt + 1), tile_nat(n);
   for (int t = 0; t <= nt; ++t) tstart[t] = (int)((long long)t * n / nt);
@@ -442,9 +463,16 @@ static int persist_tiles(Solver* S) {
     didx.insert(didx.end(), dep[t].begin(), dep[t].end());
     dptr[t + 1] = (int)didx.size();
   }
-  if (S->alloc(&S->d_toff, toff.size()) || S->alloc(&S->d_dep_ptr, nt + 1) ||
-      S->alloc(&S->d_dep_idx, std::max<size_t>(didx.size(), 1)) || S->alloc(&S->d_progress, nt))
-    return 0;
+  // buffers sized for the largest table built so far
+  if (toff.size() > S->cap_toff) {
+    if (S->alloc(&S->d_toff, toff.size())) return 0;
+    S->cap_toff = toff.size();
+  }
+  if (didx.size() + 1 > S->cap_dep) {
+    if (S->alloc(&S->d_dep_idx, didx.size() + 1)) return 0;
+    S->cap_dep = didx.size() + 1;
+  }
+  if (!S->d_dep_ptr && (S->alloc(&S->d_dep_ptr, GRID_CAP + 1) || S->alloc(&S->d_progress, GRID_CAP))) return 0;
   cudaStream_t s = S->stream;
   if (cudaMemcpyAsync(S->d_toff, toff.data(), toff.size() * sizeof(int), cudaMemcpyHostToDevice, s) ||
       cudaMemcpyAsync(S->d_dep_ptr, dptr.data(), dptr.size() * sizeof(int), cudaMemcpyHostToDevice, s) ||
@@ -487,23 +515,21 @@ static double persist_bytes(const Solver* S, int iters, bool xzero, bool relax, 
   return start + iters * it;
 }
 
-// The whole BiCGStab solve as one cooperative launch.  Returns 1 (nothing
-// enqueued but a memset) when the launch was refused for its size, so the
-// caller can fall back to the per-phase kernels.
+// Arguments of the persistent kernel for one system (tile count set by the
+// caller: gridDim for one system, the member's tiles in a batch).
 template <typename T>
-static int run_bicgstab_persistent(Solver* S, Mat<T>& A, Work<T>& W, int tiles, int maxit, int norm, double tol,
-                                   int xzero) {
+static PersistArgs<T> make_args(Solver* S, Mat<T>& A, Work<T>& W, int tiles, int maxit, int norm, double tol,
+                                int xzero) {
   const HostPattern& P = S->hp;
   PersistArgs<T> a;
+  std::memset(&a, 0, sizeof(a));
   a.n = P.n; a.KL = P.KL; a.KU = P.KU; a.G = P.G; a.gku_last = P.gku[P.G - 1];
   a.klB = a.kuB = 0;
   for (int g = 1; g < P.G; ++g) {
     a.klB = std::max(a.klB, P.gkl[g]);
     a.kuB = std::max(a.kuB, P.gku[g]);
   }
-  a.relax = S->cur_relax;
-  a.g1 = P.G > 1 ? P.gstart[1] : P.n;
-  a.spmv0 = (P.gkl[0] == 0 && ((a.relax || a.gku_last == 0) ? P.G >= 2 : P.G >= 1)) ? 1 : 0;
+  a.ntiles = tiles;
   a.gkl = S->d_gkl; a.gku = S->d_gku;
   a.toff = S->d_toff; a.dep_ptr = S->d_dep_ptr; a.dep_idx = S->d_dep_idx; a.progress = S->d_progress;
   a.col = S->d_col; a.nlo = S->d_nlo; a.nup = S->d_nup;
@@ -511,6 +537,19 @@ static int run_bicgstab_persistent(Solver* S, Mat<T>& A, Work<T>& W, int tiles, 
   a.b = W.b; a.x = W.x; a.r = W.r; a.r0 = W.r0; a.p = W.p; a.u = W.u; a.v = W.v; a.z = W.z;
   a.part = S->d_ppart; a.bar = &S->d_st->bar; a.st = S->d_st;
   a.maxit = maxit; a.norm = norm; a.xzero = xzero; a.tol = tol;
+  a.relax = S->cur_relax;
+  a.g1 = P.G > 1 ? P.gstart[1] : P.n;
+  a.spmv0 = (P.gkl[0] == 0 && ((a.relax || a.gku_last == 0) ? P.G >= 2 : P.G >= 1)) ? 1 : 0;
+  return a;
+}
+
+// The whole BiCGStab solve as one cooperative launch.  Returns 1 (nothing
+// enqueued but a memset) when the launch was refused for its size, so the
+// caller can fall back to the per-phase kernels.
+template <typename T>
+static int run_bicgstab_persistent(Solver* S, Mat<T>& A, Work<T>& W, int tiles, int maxit, int norm, double tol,
+                                   int xzero) {
+  PersistArgs<T> a = make_args<T>(S, A, W, tiles, maxit, norm, tol, xzero);
   CMS_CUDA(cudaMemsetAsync(&S->d_st->bar, 0, sizeof(GridBar), S->stream));
   CMS_CUDA(cudaMemsetAsync(S->d_progress, 0, sizeof(unsigned int) * tiles, S->stream));
   void* args[] = {&a};
@@ -979,3 +1018,4 @@ const char* cms_gpu_last_error(void) { return g_last_error; }
 
 // The device flow step shares this translation unit (and the handle internals).
 #include "cms_flow_host.cuh"
+#include "cms_ensemble_host.cuh"

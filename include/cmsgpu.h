@@ -222,6 +222,32 @@ size_t cms_flow_device_bytes(const cms_flow* f);
 int cms_flow_njoint(const cms_flow* f);
 void cms_flow_destroy(cms_flow* f);
 
+/* ---- Ensembles of independent flow models --------------------------------
+ * (no counterpart in the reference: CMS-Flow runs one grid per process)
+ * Members are cms_flow handles created as usual; an ensemble steps them
+ * together.  When every member solves with BiCGStab in FP32 + refinement
+ * (and the device can launch the persistent kernel), each of the three solves
+ * of an outer iteration runs for all members in one batched persistent
+ * launch; otherwise the members solve one after another.  Each member's
+ * results are those of its own cms_flow_step up to rounding (dot products
+ * are split over a different number of blocks). */
+typedef struct cms_ensemble cms_ensemble;
+int cms_ensemble_create(int nmembers, cms_flow* const* members, cms_ensemble** out);
+/* Layout: blocks of the batched launch, split among members by unknowns
+ * (0 = the device's resident capacity).  CMS_UNSUPPORTED when not batched. */
+int cms_ensemble_set_tiles(cms_ensemble* e, int total_tiles);
+/* Blocks of the batched launch in use; per_member (may be NULL) gets each
+ * member's share. */
+int cms_ensemble_tiles(const cms_ensemble* e, int* per_member);
+int cms_ensemble_capacity(const cms_ensemble* e);
+int cms_ensemble_batched(const cms_ensemble* e);
+/* One time step of every member; wsebnd[i] holds member i's string levels
+ * (NULL allowed for members without a string); infos: one per member. */
+int cms_ensemble_step(cms_ensemble* e, double dt, const double* const* wsebnd, cms_flow_info* infos);
+long long cms_ensemble_launches(const cms_ensemble* e);
+/* Frees the ensemble, not its members. */
+void cms_ensemble_destroy(cms_ensemble* e);
+
 /* ---- reference-shaped global API (one implicit handle, like solv_def) ---- */
 
 /* solv_init: source/solvers/solvers.f90:93-202. */

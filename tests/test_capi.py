@@ -76,3 +76,17 @@ def test_flow_entry_points_marshal_and_reject_bad_grids():
     assert rc == _lib.CMS_BAD_ARGUMENT
     info = F.FlowInfo()
     assert L.cms_flow_step(None, 1.0, None, C.byref(info)) == _lib.CMS_BAD_ARGUMENT
+
+
+def test_ensemble_entry_points_reject_bad_arguments():
+    """cms_ensemble_* argument checks run before any device work."""
+    from cms2d_b200 import ensemble as E
+    L = _lib.lib()
+    E._bind(L)
+    h = C.c_void_p()
+    assert L.cms_ensemble_create(0, None, C.byref(h)) == _lib.CMS_BAD_ARGUMENT
+    arr = (C.c_void_p * 2)(None, None)
+    assert L.cms_ensemble_create(2, arr, C.byref(h)) == _lib.CMS_BAD_ARGUMENT
+    assert L.cms_ensemble_step(None, 1.0, None, None) == _lib.CMS_BAD_ARGUMENT
+    assert L.cms_ensemble_set_tiles(None, 4) == _lib.CMS_BAD_ARGUMENT
+    assert L.cms_ensemble_batched(None) == 0
