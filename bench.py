@@ -250,7 +250,7 @@ def run_solve_ours(args):
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "kernel": top, "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(ach / peak, 4), "peak_kind": peak_kind,
-                     "traffic": persist_traffic(prof, top, infos[-1]["iters"], args.steps, args.precision)},
+                     "traffic": persist_traffic(prof, top, infos[-1]["iters"], args.steps, args.precision, N)},
         "kernels": kernels,
     }
     out["clocks"] = clk.summary()
@@ -312,16 +312,35 @@ FLOW_SOLVER = dict(nsolv=3, tol=1e-6, norm=2)
 PERSIST_DRAM_BYTES_PER_ITER = 1343.35e6 / 24
 
 
-def persist_traffic(prof, top, iters_per_step, steps, precision):
+PERSIST_CAPTURE_UNKNOWNS = 1_000_405
+
+
+def persist_traffic(prof, top, iters_per_step, steps, precision, unknowns):
+    """DRAM bytes of an average persistent launch, from the 1M capture; only
+    for workloads of that size (a smaller system stays in L2, a larger one
+    does not, so the figure does not scale)."""
     if top != "bicgstab_persistent" or precision != "fp32_refine" or not prof[top]["launches"]:
+        return None
+    if not 0.8 <= unknowns / PERSIST_CAPTURE_UNKNOWNS <= 1.25:
         return None
     per_launch = iters_per_step * steps / prof[top]["launches"]
     return round(PERSIST_DRAM_BYTES_PER_ITER * per_launch)
 
 
-def flow_case(cells: int, seed: int):
+def flow_case(args, seed: int):
+    """--case inlet: the telescoping tidal inlet of about --cells cells;
+    --case basin: the 200 x 100 Cartesian tidal basin at 20 m."""
     from cms2d_b200 import cases
-    return cases.tidal_inlet(cells, seed=seed)
+    if args.case == "basin":
+        return cases.tidal_basin(200, 100, 20.0, seed=seed)
+    return cases.tidal_inlet(args.cells, seed=seed)
+
+
+def case_label(case):
+    g = case.grid
+    if case.name == "tidal_basin":
+        return f"Cartesian tidal basin {g.ncells} cells (20 m), dt={case.dt:g} s"
+    return f"telescoping tidal inlet {g.ncells} cells (40/20/10 m), dt={case.dt:g} s"
 
 
 def _profile_read(L, h):
@@ -348,7 +367,7 @@ def run_flow_ours(args):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     L = _lib.lib()
-    case = flow_case(args.cells, seed=11 + rank)
+    case = flow_case(args, seed=11 + rank)
     g = case.grid
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
     settings = dict(FLOW_SOLVER, nswp_pp=args.nswp, nswp_uv=args.nswp, inner_tol=args.inner_tol,
@@ -452,9 +471,9 @@ def run_flow_ours(args):
         "ms_per_step": round(head["ms_per_step"], 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64 refine" if args.precision == "fp32_refine" else "f64",
-        "data": "synthetic (seeded telescoping tidal inlet)",
-        "config": {"workload": f"implicit flow step, telescoping tidal inlet {g.ncells} cells (40/20/10 m), "
-                               f"dt={case.dt:g} s, ILU0-BiCGStab solves to 1e-6 rel. L2 residual",
+        "data": f"synthetic (seeded {case.name.replace('_', ' ')})",
+        "config": {"workload": f"implicit flow step, {case_label(case)}, "
+                               f"ILU0-BiCGStab solves to 1e-6 rel. L2 residual",
                    "cells": g.ncells, "precision": args.precision, "ordering": "multicolor",
                    "solver": "BiCGStab + ILU(0)", "parallelism": f"replicas x{world}",
                    "solver_kernels": "per-phase launches" if args.multi_kernel else "persistent cooperative",
@@ -467,7 +486,8 @@ def run_flow_ours(args):
         "gpu_launches": head["gpu_launches"],
         "roofline": {"bound": "hbm", "kernel": top, "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(ach / peak, 4), "peak_kind": peak_kind,
-                     "traffic": persist_traffic(prof, top, head["krylov_iters_per_step"], args.steps, args.precision),
+                     "traffic": persist_traffic(prof, top, head["krylov_iters_per_step"], args.steps, args.precision,
+                                                g.ncells),
                      "step_GBps": round(all_bytes / (tot / 1e3) / 1e9, 1) if tot else 0},
         "kernels": kernels,
         "clocks": head["clocks"],
@@ -502,8 +522,9 @@ def flow_cpu_sample(case, outer_per_step, n_outer, threads=None):
     per_outer = dt / max(r["niter"], 1)
     t_step = per_outer * max(outer_per_step, 1.0)
     return {"value": round(1.0 / t_step, 6), "unit": "timesteps/s", "cores": threads, "kind": "port",
-            "sample": f"{r['niter']} outer SIMPLEC iterations of time step 1 on the same {case.grid.ncells}-cell "
-                      f"inlet (natural-order ILU0-BiCGStab, serial factor/sweeps as in the reference), "
+            "sample": f"{r['niter']} outer SIMPLEC iterations of time step 1 on the same case ({case.name}, "
+                      f"{case.grid.ncells} cells; natural-order ILU0-BiCGStab, serial factor/sweeps as in the "
+                      f"reference), "
                       f"{dt:.1f} s, scaled to {outer_per_step:.1f} outer iterations per step",
             "s_per_outer_iter": round(per_outer, 3)}
 
@@ -521,35 +542,46 @@ def run_flow_reference(args):
     if rank != 0:
         return
     from oracle import oracle as O
-    case = flow_case(args.cells, seed=11)
+    case = flow_case(args, seed=11)
     threads = os.cpu_count()
     O.set_threads(threads)
     f = O.FlowOracle(case)
     f.set_solver(nsolv=3, precond=O.PC_ILU0, tol=1e-6, nswp_pp=200, nswp_uv=200, norm=2)
     f.init()
-    # warm-up steps: one outer iteration each (untimed)
-    for _ in range(args.warmup):
-        f.step(maxit=1)
-    per_outer = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        rr = f.step(maxit=args.cpu_outer)
-        per_outer.append((time.perf_counter() - t0) / max(rr["niter"], 1))
-    t_step = float(np.mean(per_outer)) * FLOW_OUTER_PER_STEP
+    if case.grid.ncells <= 100_000:  # small cases: whole steps, as the GPU arm
+        for _ in range(args.warmup):
+            f.step()
+        times = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            f.step()
+            times.append(time.perf_counter() - t0)
+        t_step = float(np.mean(times))
+        sample = f"{args.warmup} warm-up steps, then {args.steps} whole timed steps"
+    else:
+        # warm-up steps: one outer iteration each (untimed)
+        for _ in range(args.warmup):
+            f.step(maxit=1)
+        per_outer = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            rr = f.step(maxit=args.cpu_outer)
+            per_outer.append((time.perf_counter() - t0) / max(rr["niter"], 1))
+        t_step = float(np.mean(per_outer)) * FLOW_OUTER_PER_STEP
+        sample = (f"{args.warmup} warm-up steps of one outer iteration, then {args.steps} steps of "
+                  f"{args.cpu_outer} outer iterations each; mean time per outer iteration "
+                  f"{np.mean(per_outer):.2f} s scaled to {FLOW_OUTER_PER_STEP} outer iterations per step")
     v = 1.0 / t_step
     out = {"impl": "reference", "metric": METRIC, "value": round(v, 6), "unit": "timesteps/s",
            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": round(1e3 * t_step, 1), "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded telescoping tidal inlet)",
-           "config": {"workload": f"implicit flow step, telescoping tidal inlet {case.grid.ncells} cells (40/20/10 m), "
-                                  f"dt={case.dt:g} s, ILU0-BiCGStab solves to 1e-6 rel. L2 residual",
+           "vs_baseline": None, "dtype": "f64", "data": f"synthetic (seeded {case.name.replace('_', ' ')})",
+           "config": {"workload": f"implicit flow step, {case_label(case)}, ILU0-BiCGStab solves to 1e-6 "
+                                  f"rel. L2 residual",
                       "cells": case.grid.ncells, "precision": "fp64", "ordering": "natural",
                       "implementation": "CPU restatement of the reference path (oracle), OpenMP"},
            "cpu_baseline": {"value": round(v, 6), "unit": "timesteps/s", "cores": threads, "kind": "port",
-                            "sample": f"{args.warmup} warm-up steps of one outer iteration, then {args.steps} "
-                                      f"steps of {args.cpu_outer} outer iterations each; mean time per outer "
-                                      f"iteration {np.mean(per_outer):.2f} s scaled to {FLOW_OUTER_PER_STEP} "
-                                      f"outer iterations per step"},
+                            "sample": sample},
            "e2e": {"value": round(v, 6), "unit": "timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
@@ -639,11 +671,14 @@ def run_ensemble_ours(args):
     }
     if args.ens_sequential and rank == 0:
         # the same members stepped one after another with their own solver launches
+        for m in e.members:  # each member's solver on the whole GPU again
+            L.cms_solver_set_tiles(m.solver_handle, 0)
         t0 = time.perf_counter()
         for m in e.members:
             m.step()
         sync()
         out["sequential_member_steps_per_s"] = round(args.members / (time.perf_counter() - t0), 4)
+        out["sequential"] = "one step of each member after the timed steps, members one after another"
     if world > 1:
         dist.destroy_process_group()
     e.close()
@@ -667,6 +702,8 @@ def main():
     ap.add_argument("--no-companion", action="store_true", help="flow: skip the other-precision run")
     ap.add_argument("--cpu-outer", type=int, default=3, help="flow CPU sample: outer iterations timed")
     ap.add_argument("--cells", type=int, default=1_000_000)
+    ap.add_argument("--case", default="inlet", choices=["inlet", "basin"],
+                    help="flow workload: 1M telescoping inlet (default) or the 200x100 basin")
     ap.add_argument("--precision", default="fp32_refine", choices=["fp32_refine", "fp64"])
     ap.add_argument("--inner-tol", type=float, default=1e-2)
     ap.add_argument("--inner-max", type=int, default=50)

@@ -79,6 +79,7 @@ def lib():
     L.cms_solver_launches.restype = C.c_longlong
     L.cms_solver_profile.argtypes = [vp, i]
     L.cms_solver_profile_read.argtypes = [vp, i, vp, vp, vp]
+    L.cms_solver_set_tiles.argtypes = [vp, i]
     L.cms_solver_stream.argtypes = [vp]
     L.cms_solver_stream.restype = vp
     L.cms_solver_destroy.argtypes = [vp]

@@ -864,6 +864,14 @@ int cms_solver_update_wet(cms_solver* s, const int* iwet) {
   return CMS_OK;
 }
 
+int cms_solver_set_tiles(cms_solver* s, int tiles) {
+  if (!s || tiles < 0) return -CMS_BAD_ARGUMENT;
+  const int cap = cms::persist_capacity(s->dev);
+  if (cap <= 0) return -CMS_UNSUPPORTED;
+  const int nt = cms::build_tiles(s, tiles == 0 ? std::min(cap, cms::nblk(s->hp.n)) : std::min(tiles, cap));
+  return nt > 0 ? nt : -CMS_UNSUPPORTED;
+}
+
 int cms_solver_set_opts(cms_solver* s, const cms_solver_opts* o) {
   if (!s || !o) return CMS_BAD_ARGUMENT;
   if (o->ordering != s->opts.ordering) return CMS_BAD_ARGUMENT;  // the ordering is fixed at creation

@@ -137,6 +137,10 @@ long long cms_solver_launches(const cms_solver* s);
 #define CMS_PROF_CLASSES 10
 int cms_solver_profile(cms_solver* s, int enable);
 int cms_solver_profile_read(cms_solver* s, int reset, double* ms, double* bytes, long long* count);
+/* Blocks (tiles) of the handle's persistent BiCGStab launch: 0 restores the
+ * default (the device's resident capacity, at most one block per 256 rows);
+ * returns the count in use, or a negative CMS_* code. */
+int cms_solver_set_tiles(cms_solver* s, int tiles);
 /* The stream the handle runs on (a cudaStream_t). */
 void* cms_solver_stream(cms_solver* s);
 
