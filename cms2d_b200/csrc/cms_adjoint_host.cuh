@@ -1,0 +1,156 @@
+// Adjoint of solve() (included at the end of cms_solver.cu).
+//
+// solve() turns (acoef, ss, sp, phi) into A x = b with
+//   A_ii = ap_i = (sum_k acoef(k,i) - sp_i) / relax,   A_ic = -acoef(k,i)  (c active),
+//   b_i  = ss_i + (1 - relax) phi_i ap_i + sum_{k: c dummy} acoef(k,i) phi_c
+// (solvers.f90:230-240).  For a loss L(x) with g = dL/dx the adjoint solve is
+// A^T lam = g, and
+//   dL/dss_i       = lam_i
+//   dL/dsp_i       = lam_i (x_i - (1 - relax) phi_i) / relax
+//   dL/dacoef(k,i) = lam_i ((1 - relax) phi_i - x_i) / relax + lam_i x_c
+// where x_c is the solution at an active neighbour and phi_c at a dummy.
+//
+// A^T has A's sparsity pattern: its ELL values are A's entries read through a
+// transpose map (slot e of row r holds the slot of row col[e] that points back
+// to r).  It is solved by the same ILU(0)-BiCGStab (ILU(0) of A^T in the same
+// device order), FP64.
+#pragma once
+
+namespace cms {
+
+// aT[e] = a[tslot[e]] (0 where the slot is padding)
+template <typename T>
+__global__ void __launch_bounds__(TPB) k_transpose_vals(size_t m, const int* __restrict__ tslot,
+                                                        const T* __restrict__ a, T* __restrict__ aT) {
+  for (size_t e = (size_t)blockIdx.x * TPB + threadIdx.x; e < m; e += (size_t)gridDim.x * TPB) {
+    const int t = tslot[e];
+    aT[e] = t >= 0 ? a[t] : T(0);
+  }
+}
+
+// b[r] = g[perm[r]] (natural -> device order)
+__global__ void __launch_bounds__(TPB) k_gather_rhs(int n, const int* __restrict__ perm, const double* __restrict__ g,
+                                                    double* __restrict__ b) {
+  for (int r = blockIdx.x * TPB + threadIdx.x; r < n; r += gridDim.x * TPB) b[r] = g[perm[r]];
+}
+
+// gradients with respect to the solve() inputs, natural order (see above)
+__global__ void __launch_bounds__(TPB) k_solve_grads(int n, int nmf, const int* __restrict__ c2c,
+                                                     const int* __restrict__ ncface, const int* __restrict__ iperm,
+                                                     const double* __restrict__ lam_dev,
+                                                     const double* __restrict__ x, const double* __restrict__ phi0,
+                                                     double relax, double* __restrict__ lam, double* __restrict__ gac,
+                                                     double* __restrict__ gss, double* __restrict__ gsp) {
+  for (int i = blockIdx.x * TPB + threadIdx.x; i < n; i += gridDim.x * TPB) {
+    const double l = lam_dev[iperm[i]];
+    const double xi = x[i];
+    const double dap = l * ((1.0 - relax) * phi0[i] - xi) / relax;  // dL/d(acoef) through ap and b
+    if (lam) lam[i] = l;
+    if (gss) gss[i] = l;
+    if (gsp) gsp[i] = -dap;
+    if (gac) {
+      const int nf = ncface[i];
+      for (int k = 0; k < nmf; ++k) {
+        double v = 0.0;
+        if (k < nf) v = dap + l * x[c2c[(size_t)i * nmf + k] - 1];
+        gac[(size_t)i * nmf + k] = v;
+      }
+    }
+  }
+}
+
+// transpose map and buffers of A^T (first use)
+static int adjoint_setup(Solver* S) {
+  if (S->d_tslot) return CMS_OK;
+  const HostPattern& P = S->hp;
+  const size_t n = P.n, K = std::max(S->K, 1);
+  std::vector<int> ts(K * n, -1);
+  for (size_t r = 0; r < n; ++r) {
+    const int kl = P.nlo[r], ku = P.nup[r];
+    for (int s = 0; s < S->K; ++s) {
+      const bool valid = s < P.KL ? s < kl : (s - P.KL) < ku;
+      if (!valid) continue;
+      const int j = P.col[(size_t)s * n + r];
+      // row j's slot pointing back to r: an upper slot of j when j < r
+      const int a0 = j < (int)r ? P.KL : 0, a1 = j < (int)r ? P.KL + P.nup[j] : P.nlo[j];
+      for (int s2 = a0; s2 < a1; ++s2)
+        if (P.col[(size_t)s2 * n + j] == (int)r) {
+          ts[(size_t)s * n + r] = (int)((size_t)s2 * n + j);
+          break;
+        }
+      if (ts[(size_t)s * n + r] < 0) {
+        std::snprintf(g_last_error, sizeof(g_last_error), "adjoint: pattern is not symmetric at row %zu", r);
+        return CMS_UNSUPPORTED;
+      }
+    }
+  }
+  int* d = nullptr;
+  CHK(S->alloc(&d, K * n));
+  CMS_CUDA(cudaMemcpyAsync(d, ts.data(), K * n * sizeof(int), cudaMemcpyHostToDevice, S->stream));
+  CHK(S->alloc(&S->AT64.aoff, K * n));
+  CHK(S->alloc(&S->AT64.luoff, K * n));
+  CHK(S->alloc(&S->AT64.invd, n));
+  CMS_CUDA(cudaStreamSynchronize(S->stream));
+  S->d_tslot = d;
+  return CMS_OK;
+}
+
+// A^T lam = g and the gradients of solve()'s inputs (all natural order,
+// device pointers; see cms_solver_adjoint_dev_d).
+static int solve_adjoint(Solver* S, const double* acoef, const double* ss, const double* sp, const double* phi0,
+                         const double* x, double relax, const double* g, double tol, int maxit, double* lam,
+                         double* gac, double* gss, double* gsp, cms_solve_info* info) {
+  const HostPattern& P = S->hp;
+  const int n = P.n;
+  cms_solve_info loc{};
+  if (!info) info = &loc;
+  std::memset(info, 0, sizeof(*info));
+  info->ncolors = P.G;
+  info->true_relres = -1.0;
+  CHK(adjoint_setup(S));
+  CHK(alloc_staging<double>(S, S->S64));
+  cudaStream_t st = S->stream;
+  const size_t nD = P.nD, nmf = P.nmf;
+  // the forward system again (ss on a copy: the prologue updates it in place)
+  CMS_CUDA(cudaMemcpyAsync(S->S64.ss, ss, nD * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  KLAUNCH(S, P_PROLOGUE, 0.0,
+          (k_prologue<double, float><<<gsz(n), TPB, 0, st>>>(n, (int)nmf, acoef, S->S64.ss, sp, S->S64.res, phi0,
+                                                              S->d_c2c, S->d_ncface, S->d_iwet, S->d_fslot,
+                                                              S->d_iperm, relax, S->A64.aoff, S->A64.diag,
+                                                              S->W64.b, S->W64.x, nullptr, nullptr, S->d_part,
+                                                              S->d_st)));
+  const size_t m = (size_t)std::max(S->K, 1) * n;
+  S->AT64.diag = S->A64.diag;
+  KLAUNCH(S, P_VEC, (double)m * 20,
+          (k_transpose_vals<double><<<gsz(n), TPB, 0, st>>>(m, S->d_tslot, S->A64.aoff, S->AT64.aoff)));
+  KLAUNCH(S, P_VEC, (double)n * 20, (k_gather_rhs<<<gsz(n), TPB, 0, st>>>(n, S->d_perm, g, S->W64.b)));
+  const int saved_relax = S->cur_relax;
+  S->cur_relax = 0;
+  CHK(run_bicgstab<double>(S, S->AT64, S->W64, maxit, 2, tol, 1, true));
+  S->cur_relax = saved_relax;
+  CMS_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, st));
+  CMS_CUDA(cudaStreamSynchronize(st));
+  const DevState& h = *S->h_st;
+  info->iters = h.iter;
+  info->inner = h.iter;
+  info->relres = h.s[S_RELRES];
+  if (h.nonfinite) info->status = CMS_NONFINITE;
+  else if (!h.converged) info->status = CMS_NOT_CONVERGED;
+  KLAUNCH(S, P_VEC, (double)n * (8 * 6 + nmf * 20),
+          (k_solve_grads<<<gsz(n), TPB, 0, st>>>(n, (int)nmf, S->d_c2c, S->d_ncface, S->d_iperm, S->W64.x, x, phi0,
+                                                 relax, lam, gac, gss, gsp)));
+  CMS_CUDA(cudaStreamSynchronize(st));
+  return info->status;
+}
+
+}  // namespace cms
+
+extern "C" int cms_solver_adjoint_dev_d(cms_solver* s, const double* acoef, const double* ss, const double* sp,
+                                        const double* phi0, const double* x, double relax, const double* g,
+                                        double tol, int maxit, double* lam, double* grad_acoef, double* grad_ss,
+                                        double* grad_sp, cms_solve_info* info) {
+  if (!s || !acoef || !ss || !sp || !phi0 || !x || !g || relax <= 0.0 || tol <= 0.0 || maxit <= 0)
+    return CMS_BAD_ARGUMENT;
+  return cms::solve_adjoint(s, acoef, ss, sp, phi0, x, relax, g, tol, maxit, lam, grad_acoef, grad_ss, grad_sp,
+                            info);
+}

@@ -74,6 +74,8 @@ struct cms_solver {
   // numeric buffers
   cms::Mat<double> A64;
   cms::Mat<float> A32;
+  cms::Mat<double> AT64;     // adjoint: A^T's values and its factor (diag shared with A64)
+  int* d_tslot = nullptr;    // adjoint: transpose map of the ELL slots
   cms::Work<double> W64;
   cms::Work<float> W32;
   double* ir_r64 = nullptr;  // refinement: FP64 residual scratch (unused when null)
@@ -1027,3 +1029,4 @@ const char* cms_gpu_last_error(void) { return g_last_error; }
 // The device flow step shares this translation unit (and the handle internals).
 #include "cms_flow_host.cuh"
 #include "cms_ensemble_host.cuh"
+#include "cms_adjoint_host.cuh"

@@ -185,6 +185,10 @@ class Solver:
             raise TypeError("float32 or float64 arrays expected")
         L = _lib.lib()
         info = _lib.SolveInfo()
+        if dev and hasattr(acoef, "device"):
+            # the handle's own stream reads the tensors: finish the work that produced them
+            import torch
+            torch.cuda.current_stream(acoef.device).synchronize()
         fn = {(True, False): L.cms_solver_solve_d, (False, False): L.cms_solver_solve_f,
               (True, True): L.cms_solver_solve_dev_d, (False, True): L.cms_solver_solve_dev_f}[(is64, dev)]
         rc = fn(self._h, *[_ptr(a) for a in arrs], float(relax), int(nswp), int(nsolv), C.byref(info))

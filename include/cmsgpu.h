@@ -137,6 +137,18 @@ long long cms_solver_launches(const cms_solver* s);
 #define CMS_PROF_CLASSES 10
 int cms_solver_profile(cms_solver* s, int enable);
 int cms_solver_profile_read(cms_solver* s, int reset, double* ms, double* bytes, long long* count);
+/* Adjoint of solve() (no counterpart in the reference), FP64, device
+ * pointers in the solve() layout (natural order, acoef [ncellsD][nmaxfaces]):
+ * given the inputs of a forward solve (acoef, ss and sp as passed in, phi0 =
+ * phi before the solve), its solution x (phi after the solve, ncellsD values,
+ * dummies unchanged) and g = dL/dx, solves A^T lam = g (ILU(0)-BiCGStab to
+ * ||r||2/||g||2 < tol, at most maxit iterations) and writes lam and the
+ * gradients dL/dacoef, dL/dss, dL/dsp (rows of active cells; any output may be
+ * NULL). */
+int cms_solver_adjoint_dev_d(cms_solver* s, const double* acoef, const double* ss, const double* sp,
+                             const double* phi0, const double* x, double relax, const double* g, double tol,
+                             int maxit, double* lam, double* grad_acoef, double* grad_ss, double* grad_sp,
+                             cms_solve_info* info);
 /* Blocks (tiles) of the handle's persistent BiCGStab launch: 0 restores the
  * default (the device's resident capacity, at most one block per 256 rows);
  * returns the count in use, or a negative CMS_* code. */
