@@ -705,7 +705,8 @@ def main():
     ap.add_argument("--case", default="inlet", choices=["inlet", "basin"],
                     help="flow workload: 1M telescoping inlet (default) or the 200x100 basin")
     ap.add_argument("--precision", default="fp32_refine", choices=["fp32_refine", "fp64"])
-    ap.add_argument("--inner-tol", type=float, default=1e-2)
+    ap.add_argument("--inner-tol", type=float, default=1e-3,
+                    help="refinement: relative residual reduction asked of each FP32 inner solve")
     ap.add_argument("--inner-max", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ncu", action="store_true", help="warm-up and timed steps only (profiler runs)")

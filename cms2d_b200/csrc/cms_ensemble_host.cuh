@@ -98,7 +98,7 @@ static int refine_batched(Ens* E, const std::vector<int>& act, const std::vector
     rm.info = infos[j];
     rm.maxit = S->opts.max_iters > 0 ? S->opts.max_iters : nswp[j];
     rm.tol = S->opts.tol > 0 ? S->opts.tol : 1e-3;
-    rm.itol = S->opts.inner_tol > 0 ? S->opts.inner_tol : 1e-2;
+    rm.itol = S->opts.inner_tol > 0 ? S->opts.inner_tol : 1e-3;
     rm.imax = S->opts.inner_max > 0 ? S->opts.inner_max : 50;
     rm.rmax = S->opts.max_refine > 0 ? S->opts.max_refine : 30;
     const bool relax = S->opts.inner_relax && S->opts.ordering == CMS_ORDER_MULTICOLOR && P.G > 2;

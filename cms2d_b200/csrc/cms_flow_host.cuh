@@ -672,7 +672,7 @@ void cms_flow_default_opts(cms_flow_opts* o) {
   o->nswp_uv = 5;
   o->maxit = 0;
   o->skewcor = 1;
-  o->inner_tol = 1.0e-2;
+  o->inner_tol = 1.0e-3;
   o->inner_max = 50;
 }
 

@@ -701,7 +701,7 @@ static int run_refine(Solver* S, int nsolv, int maxit, double tol, cms_solve_inf
   }
   int steps = 0, inner_total = 0;
   double nrm0 = -1.0, rel = 1.0;
-  const double itol = S->opts.inner_tol > 0 ? S->opts.inner_tol : 1e-2;
+  const double itol = S->opts.inner_tol > 0 ? S->opts.inner_tol : 1e-3;
   const int imax = S->opts.inner_max > 0 ? S->opts.inner_max : 50;
   const int rmax = S->opts.max_refine > 0 ? S->opts.max_refine : 30;
   for (;;) {
@@ -844,7 +844,7 @@ void cms_solver_default_opts(cms_solver_opts* o) {
   o->norm = 1;
   o->tol = 1.0e-3;
   o->max_iters = 0;
-  o->inner_tol = 1.0e-2;
+  o->inner_tol = 1.0e-3;
   o->inner_max = 50;
   o->max_refine = 30;
   o->verify = 1;

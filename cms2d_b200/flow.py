@@ -66,7 +66,7 @@ class FlowModel:
 
     def __init__(self, case, nsolv: int = 4, ordering: str = "multicolor", precision: str = "fp64",
                  tol: float = 1e-3, norm: int = 1, nswp_pp: int | None = None, nswp_uv: int | None = None,
-                 maxit: int = 0, skewcor: bool = True, inner_tol: float = 1e-2, inner_max: int = 50,
+                 maxit: int = 0, skewcor: bool = True, inner_tol: float = 1e-3, inner_max: int = 50,
                  multi_kernel: bool = False):
         L = _lib.lib()
         _bind(L)

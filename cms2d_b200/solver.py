@@ -66,7 +66,7 @@ class Solver:
     """
 
     def __init__(self, grid, iwet=None, ordering: str = "multicolor", precision: str = "fp64", tol: float = 1e-3,
-                 norm: int = 1, max_iters: int = 0, inner_tol: float = 1e-2, inner_max: int = 50,
+                 norm: int = 1, max_iters: int = 0, inner_tol: float = 1e-3, inner_max: int = 50,
                  max_refine: int = 30, verify: bool = True, nsolv: int = NSOLV_DEFAULT,
                  multi_kernel: bool = False, inner_relax: bool = True):
         L = _lib.lib()
