@@ -88,7 +88,12 @@ static int refine_batched(Ens* E, const std::vector<int>& act, const std::vector
   struct Reset {  // cur_relax describes A32's factor only during this solve
     Ens* e;
     const std::vector<int>& a;
-    ~Reset() { for (int i : a) e->m[i]->S->cur_relax = 0; }
+    ~Reset() {
+      for (int i : a) {
+        e->m[i]->S->cur_relax = 0;
+        e->m[i]->S->cur_fuse = 0;
+      }
+    }
   } reset{E, act};
   for (int j = 0; j < A_; ++j) {
     Solver* S = E->m[act[j]]->S;
@@ -102,6 +107,7 @@ static int refine_batched(Ens* E, const std::vector<int>& act, const std::vector
     rm.imax = S->opts.inner_max > 0 ? S->opts.inner_max : 50;
     rm.rmax = S->opts.max_refine > 0 ? S->opts.max_refine : 30;
     const bool relax = S->opts.inner_relax && S->opts.ordering == CMS_ORDER_MULTICOLOR && P.G > 2;
+    S->cur_fuse = 1;
     if (relax) {
       KLAUNCH(S, P_ILU0, (double)n * (3 * 4 + 2) + (double)(P.nnz_off) * (2 * 4 + 4),
               (k_ilu0_relax<float><<<gsz(n), TPB, 0, S->stream>>>(n, P.KL, P.gstart[1], S->d_col, S->d_nlo,

@@ -45,6 +45,7 @@
 namespace cms {
 
 constexpr unsigned int kSpinLimit = 1u << 22;
+constexpr int NSMAX = 6;  // sums per reduction (partial-sum buffer stride)
 
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
   unsigned int v;
@@ -69,6 +70,8 @@ struct PersistArgs {
   int spmv0;               // 1: group 0 has no lower couplings and its own backward
                            // phase; the SpMV of its rows is done in that phase
   int relax;               // 1: two-phase preconditioner (factor from k_ilu0_relax)
+  int fuse_upd;            // 1 (L2 stopping test only): the x/r update is done in the next
+                           // iteration's forward phases, its sums come from identities
   int g1;                  // first row of group 1
   const int* gkl;          // [G] lower slots per group
   const int* gku;          // [G] upper slots per group
@@ -93,7 +96,7 @@ struct PersistArgs {
   T* u;
   T* v;
   T* z;
-  double* part;  // [2][3][ntiles]
+  double* part;  // [2][NSMAX][ntiles]
   GridBar* bar;  // count: barrier arrivals (zero at launch); err: a wait gave up
   DevState* st;
   int maxit, norm, xzero;
@@ -173,7 +176,7 @@ __device__ __forceinline__ void put_partials(const PersistArgs<T>& A, double (&v
   block_sum<NS>(v);
   if (threadIdx.x == 0) {
 #pragma unroll
-    for (int q = 0; q < NS; ++q) A.part[((size_t)buf * 3 + q) * A.ntiles + A.tile] = v[q];
+    for (int q = 0; q < NS; ++q) A.part[((size_t)buf * NSMAX + q) * A.ntiles + A.tile] = v[q];
   }
 }
 
@@ -186,7 +189,7 @@ __device__ __forceinline__ void get_totals(const PersistArgs<T>& A, double (&tot
   for (int q = 0; q < NS; ++q) {
     acc[q] = 0.0;
     for (int bb = threadIdx.x; bb < A.ntiles; bb += blockDim.x)
-      acc[q] += __ldcg(&A.part[((size_t)buf * 3 + q) * A.ntiles + bb]);
+      acc[q] += __ldcg(&A.part[((size_t)buf * NSMAX + q) * A.ntiles + bb]);
   }
   block_sum<NS>(acc);
   if (threadIdx.x == 0) {
@@ -373,7 +376,8 @@ __device__ __forceinline__ void spmv_rows(const PersistArgs<T>& A, T (&y)[NR], c
 // the gathered neighbour values serve both sums.
 template <typename T, int MODE>
 __device__ __forceinline__ void pc_apply(const PersistArgs<T>& A, PhaseState& ph, const int* s_lo, const int* s_pre,
-                                         double omg_d, double alf_d, double gam_d, double (&dots)[2]) {
+                                         double omg_d, double alf_d, double gam_d, bool pending,
+                                         double (&dots)[5]) {
   constexpr int NR = NRT<T>;
   const T omg = (T)omg_d, alf = (T)alf_d, gam = (T)gam_d;
   const int G = A.G;
@@ -391,15 +395,23 @@ __device__ __forceinline__ void pc_apply(const PersistArgs<T>& A, PhaseState& ph
     const bool last = fuse && (gb == G - 1 || (A.relax && ga >= 1));
     const int cmax = (A.relax && ga >= 1) ? A.g1 : 0x7fffffff;
     for_rows_g<NR>(A, s_lo, s_pre, ga, gb, [&](const int (&r)[NR], const bool (&ok)[NR]) {
-      T y[NR], xo[NR], zo[NR], iv[NR];
+      T y[NR], xo[NR], zo[NR], iv[NR], rn[NR], r0v[NR];
 #pragma unroll
       for (int q = 0; q < NR; ++q) {
         if (MODE == 0) {
-          y[q] = ldm(&A.r[r[q]]) + omg * (ldm(&A.p[r[q]]) - alf * ldm(&A.u[r[q]]));
+          if (pending) {  // the previous iteration's x += alf z, r -= alf v (own row)
+            zo[q] = ldm(&A.z[r[q]]);
+            xo[q] = ldm(&A.x[r[q]]);
+            rn[q] = ldm(&A.r[r[q]]) - alf * ldm(&A.v[r[q]]);
+          } else {
+            rn[q] = ldm(&A.r[r[q]]);
+          }
+          y[q] = rn[q] + omg * (ldm(&A.p[r[q]]) - alf * ldm(&A.u[r[q]]));
         } else {
           y[q] = ldm(&A.r[r[q]]) - gam * ldm(&A.u[r[q]]);
           xo[q] = ldm(&A.x[r[q]]);
           zo[q] = ldm(&A.z[r[q]]);
+          if (A.fuse_upd) r0v[q] = ldm(&A.r0[r[q]]);
         }
         iv[q] = last ? __ldg(&A.invd[r[q]]) : T(1);
       }
@@ -411,10 +423,18 @@ __device__ __forceinline__ void pc_apply(const PersistArgs<T>& A, PhaseState& ph
       for (int q = 0; q < NR; ++q) {
         if (!ok[q]) continue;
         if (MODE == 0) {
+          if (pending) {
+            A.x[r[q]] = xo[q] + alf * zo[q];
+            A.r[r[q]] = rn[q];
+          }
           A.p[r[q]] = y[q];
         } else {
           A.x[r[q]] = xo[q] + gam * zo[q];
           A.r[r[q]] = y[q];
+          if (A.fuse_upd) {  // r1.r0 and r1.r1 for the identities
+            dots[3] += (double)y[q] * (double)r0v[q];
+            dots[4] += (double)y[q] * (double)y[q];
+          }
         }
         A.z[r[q]] = last ? iv[q] * w[q] : w[q];
       }
@@ -427,7 +447,7 @@ __device__ __forceinline__ void pc_apply(const PersistArgs<T>& A, PhaseState& ph
     if (rr.y > rr.x) wait_neighbours(A, ph);
     if (g == 0 && A.spmv0) {
       for_rows<NR>(rr.x, rr.y, [&](const int (&r)[NR], const bool (&ok)[NR]) {
-        T w[NR], iv[NR], dg[NR], d1[NR], sa[NR];
+        T w[NR], iv[NR], dg[NR], d1[NR], sa[NR], r0v[NR];
         int ku[NR];
 #pragma unroll
         for (int q = 0; q < NR; ++q) {
@@ -435,6 +455,7 @@ __device__ __forceinline__ void pc_apply(const PersistArgs<T>& A, PhaseState& ph
           iv[q] = __ldg(&A.invd[r[q]]);
           dg[q] = __ldg(&A.diag[r[q]]);
           d1[q] = MODE == 0 ? ldm(&A.r0[r[q]]) : ldm(&A.r[r[q]]);
+          if (MODE == 1 && A.fuse_upd) r0v[q] = ldm(&A.r0[r[q]]);
           ku[q] = __ldg(&A.nup[r[q]]);
           sa[q] = T(0);
         }
@@ -465,6 +486,7 @@ __device__ __forceinline__ void pc_apply(const PersistArgs<T>& A, PhaseState& ph
             A.v[r[q]] = y;
             dots[0] += (double)y * (double)d1[q];
             dots[1] += (double)y * (double)y;
+            if (A.fuse_upd) dots[2] += (double)y * (double)r0v[q];
           }
         }
       });
@@ -555,11 +577,13 @@ __device__ __forceinline__ void bicg_body(const PersistArgs<T>& A) {
   double alf = 1.0, bet0 = 1.0, gam = 1.0, rel = 1.0;
   int it = 0, converged = 0, nonfinite = 0;
   int buf = 1;
+  bool pending = false;  // fuse_upd: an x/r update waits for the next forward phases
   while (ph.ok && it < A.maxit) {
     ++it;
     const double omg = bet * gam / (alf * bet0 + SMALL);
-    double dots[2] = {0.0, 0.0};
-    pc_apply<T, 0>(A, ph, s_lo, s_pre, omg, alf, gam, dots);
+    double dots[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    pc_apply<T, 0>(A, ph, s_lo, s_pre, omg, alf, gam, pending, dots);
+    pending = false;
     if (!ph.ok) break;
     // u = A z, u.r0 (rows of later groups)
     {
@@ -589,36 +613,60 @@ __device__ __forceinline__ void bicg_body(const PersistArgs<T>& A) {
       gam = bet / s1[0];
       bet0 = bet;
     }
-    dots[0] = dots[1] = 0.0;
-    pc_apply<T, 1>(A, ph, s_lo, s_pre, omg, alf, gam, dots);
+    for (double& d : dots) d = 0.0;
+    pc_apply<T, 1>(A, ph, s_lo, s_pre, omg, alf, gam, false, dots);
     if (!ph.ok) break;
-    // v = A z, v.r, v.v (rows of later groups)
+    // v = A z, v.r, v.v (rows of later groups); with fuse_upd also v.r0 and
+    // the r1.r0, r1.r1 sums of the forward phases
     {
-      double s2[2] = {dots[0], dots[1]};
+      double s5[5] = {dots[0], dots[1], dots[2], dots[3], dots[4]};
       wait_neighbours(A, ph);
       {
         const int klg = klS, kug = kuS;
         for_rows_g<NR>(A, s_lo, s_pre, A.spmv0, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR]) {
-          T vr[NR], d1[NR];
+          T vr[NR], d1[NR], r0v[NR];
 #pragma unroll
-          for (int q = 0; q < NR; ++q) d1[q] = ldm(&A.r[r[q]]);
+          for (int q = 0; q < NR; ++q) {
+            d1[q] = ldm(&A.r[r[q]]);
+            if (A.fuse_upd) r0v[q] = ldm(&A.r0[r[q]]);
+          }
           spmv_rows(A, vr, A.z, r, klg, kug);
 #pragma unroll
           for (int q = 0; q < NR; ++q) {
             if (!ok[q]) continue;
             A.v[r[q]] = vr[q];
-            s2[0] += (double)vr[q] * (double)d1[q];
-            s2[1] += (double)vr[q] * (double)vr[q];
+            s5[0] += (double)vr[q] * (double)d1[q];
+            s5[1] += (double)vr[q] * (double)vr[q];
+            if (A.fuse_upd) s5[2] += (double)vr[q] * (double)r0v[q];
           }
         });
       }
-      put_partials<2>(A, s2, buf);
+      if (A.fuse_upd) put_partials<5>(A, s5, buf);
+      else {
+        double s2[2] = {s5[0], s5[1]};
+        put_partials<2>(A, s2, buf);
+      }
       end_phase(A, ph);
       grid_barrier(A, ph);
       if (!ph.ok) break;
-      get_totals<2>(A, s2, buf);
+      if (A.fuse_upd) get_totals<5>(A, s5, buf);
+      else {
+        double s2[2];
+        get_totals<2>(A, s2, buf);
+        s5[0] = s2[0]; s5[1] = s2[1];
+      }
       buf ^= 1;
-      alf = s2[0] / fmax(s2[1], SMALL);
+      alf = s5[0] / fmax(s5[1], SMALL);
+      if (A.fuse_upd) {
+        // r = r1 - alf v:  |r|^2 = |r1|^2 - 2 alf v.r1 + alf^2 v.v,  r.r0 = r1.r0 - alf v.r0
+        const double rr = fmax(s5[4] - 2.0 * alf * s5[0] + alf * alf * s5[1], 0.0);
+        rel = sqrt(rr) / res0;
+        bet = s5[3] - alf * s5[2];
+        pending = true;
+        if (!isfinite(rel)) { nonfinite = 1; break; }
+        if (rel < A.tol) { converged = 1; break; }
+        continue;
+      }
     }
     // x += alf z; r -= alf v; stopping test; next bet (own rows only)
     {
@@ -656,6 +704,25 @@ __device__ __forceinline__ void bicg_body(const PersistArgs<T>& A) {
       if (!isfinite(rel)) { nonfinite = 1; break; }
       if (rel < A.tol) { converged = 1; break; }
     }
+  }
+  // fuse_upd: the last iteration's update (own rows; every tile has passed the
+  // last grid barrier, nothing else reads these rows afterwards)
+  if (pending && ph.ok) {
+    const T a = (T)alf;
+    for_rows_g<NR>(A, s_lo, s_pre, 0, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR]) {
+      T xn[NR], rn[NR];
+#pragma unroll
+      for (int q = 0; q < NR; ++q) {
+        xn[q] = ldm(&A.x[r[q]]) + a * ldm(&A.z[r[q]]);
+        rn[q] = ldm(&A.r[r[q]]) - a * ldm(&A.v[r[q]]);
+      }
+#pragma unroll
+      for (int q = 0; q < NR; ++q) {
+        if (!ok[q]) continue;
+        A.x[r[q]] = xn[q];
+        A.r[r[q]] = rn[q];
+      }
+    });
   }
   if (A.tile == 0 && threadIdx.x == 0) {
     A.st->iter = it;

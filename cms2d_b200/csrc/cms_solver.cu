@@ -91,6 +91,7 @@ struct cms_solver {
   int ptiles = 0;  // tiles (= blocks) of the persistent kernel; 0 not built, -1 not launchable
   size_t cap_toff = 0, cap_dep = 0;  // capacities of d_toff / d_dep_idx
   int cur_relax = 0;  // the FP32 factor in A32 is the two-phase one (k_ilu0_relax)
+  int cur_fuse = 0;   // inner solves of refinement: update folded into the next iteration
   cms::Staging<double> S64;
   cms::Staging<float> S32;
   size_t bytes = 0;
@@ -291,7 +292,7 @@ static int create(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, 
   S->max_blocks = std::max(std::max(tot, GRID_CAP), std::max(t.blk[t.ng], gsz(P.n))) + 1;
   if ((rc = S->alloc(&S->d_part, (size_t)3 * S->max_blocks)) || (rc = S->alloc(&S->d_st, 1))) return fail(rc);
   if ((rc = S->alloc(&S->d_gkl, P.G)) || (rc = S->alloc(&S->d_gku, P.G)) ||
-      (rc = S->alloc(&S->d_ppart, (size_t)6 * GRID_CAP)))
+      (rc = S->alloc(&S->d_ppart, (size_t)2 * NSMAX * GRID_CAP)))
     return fail(rc);
   if (cudaMemcpyAsync(S->d_gkl, P.gkl.data(), P.G * sizeof(int), cudaMemcpyHostToDevice, s) ||
       cudaMemcpyAsync(S->d_gku, P.gku.data(), P.G * sizeof(int), cudaMemcpyHostToDevice, s))
@@ -540,6 +541,7 @@ static PersistArgs<T> make_args(Solver* S, Mat<T>& A, Work<T>& W, int tiles, int
   a.part = S->d_ppart; a.bar = &S->d_st->bar; a.st = S->d_st;
   a.maxit = maxit; a.norm = norm; a.xzero = xzero; a.tol = tol;
   a.relax = S->cur_relax;
+  a.fuse_upd = (S->cur_fuse && norm == 2) ? 1 : 0;
   a.g1 = P.G > 1 ? P.gstart[1] : P.n;
   a.spmv0 = (P.gkl[0] == 0 && ((a.relax || a.gku_last == 0) ? P.G >= 2 : P.G >= 1)) ? 1 : 0;
   return a;
@@ -686,10 +688,11 @@ static int run_refine(Solver* S, int nsolv, int maxit, double tol, cms_solve_inf
   // factor is the two-phase one when the persistent BiCGStab will run it.
   const bool relax = nsolv == 3 && S->opts.inner_relax && S->opts.ordering == CMS_ORDER_MULTICOLOR && P.G > 2 &&
                      !S->opts.multi_kernel && persist_tiles(S) > 0;
-  struct RelaxScope {  // the flag describes A32's factor only while this solve runs
+  struct RelaxScope {  // the flags describe A32's factor and its solves only while this solve runs
     Solver* s;
-    ~RelaxScope() { s->cur_relax = 0; }
+    ~RelaxScope() { s->cur_relax = 0; s->cur_fuse = 0; }
   } relax_scope{S};
+  S->cur_fuse = 1;
   if (relax) {
     KLAUNCH(S, P_ILU0, (double)n * (3 * 4 + 2) + (double)(P.nnz_off) * (2 * 4 + 4),
             (k_ilu0_relax<float><<<gsz(n), TPB, 0, S->stream>>>(n, P.KL, P.gstart[1], S->d_col, S->d_nlo,
