@@ -329,10 +329,16 @@ def persist_traffic(prof, top, iters_per_step, steps, precision, unknowns):
 
 def flow_case(args, seed: int):
     """--case inlet: the telescoping tidal inlet of about --cells cells;
-    --case basin: the 200 x 100 Cartesian tidal basin at 20 m."""
+    --case basin: the 200 x 100 Cartesian tidal basin at 20 m;
+    --case flat: a Cartesian intertidal flat of about --cells cells at 20 m
+    (1.6:1), stepped from 2 h after high water so that cells dry every step."""
     from cms2d_b200 import cases
     if args.case == "basin":
         return cases.tidal_basin(200, 100, 20.0, seed=seed)
+    if args.case == "flat":
+        ny = max(8, int(round(np.sqrt(args.cells / 1.6))))
+        nx = max(8, int(round(args.cells / ny)))
+        return cases.tidal_flat(nx, ny, 20.0, seed=seed, dt=300.0, t0_hours=2.0)
     return cases.tidal_inlet(args.cells, seed=seed)
 
 
@@ -340,6 +346,9 @@ def case_label(case):
     g = case.grid
     if case.name == "tidal_basin":
         return f"Cartesian tidal basin {g.ncells} cells (20 m), dt={case.dt:g} s"
+    if case.name == "tidal_flat":
+        return (f"Cartesian intertidal flat {g.ncells} cells (20 m), dt={case.dt:g} s, falling tide "
+                f"(wetting and drying every step)")
     return f"telescoping tidal inlet {g.ncells} cells (40/20/10 m), dt={case.dt:g} s"
 
 
@@ -417,6 +426,7 @@ def run_flow_ours(args):
         if args.ncu and prec == args.precision:
             torch.cuda.profiler.stop()
         launches = m.launches - launches0
+        wd_stats = m.wetdry_stats()
         if world > 1:
             t = torch.tensor([ms_total], device=dev, dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -425,6 +435,9 @@ def run_flow_ours(args):
              "outer_iters": float(np.mean([i["niter"] for i in infos])),
              "krylov_iters_per_step": float(np.mean([i["krylov_iters"] for i in infos])),
              "status": sorted({i["status"] for i in infos}), "gpu_launches": int(launches),
+             "wetdry": {"wet_cells": float(np.mean([i["nwet"] for i in infos])),
+                        "cells_changed_per_step": float(np.mean([i["nchanged"] for i in infos])),
+                        "host_update": wd_stats},
              "clocks": clk.summary()}
         if world > 1:
             t = torch.tensor([t_wall], device=dev, dtype=torch.float64)
@@ -481,6 +494,7 @@ def run_flow_ours(args):
         "outer_iters_per_step": head["outer_iters"],
         "krylov_iters_per_step": head["krylov_iters_per_step"],
         "step_status": head["status"],
+        "wetdry": head["wetdry"],
         "cells_steps_per_s": round(head["value"] * g.ncells, 1),
         "e2e": head["e2e"],
         "gpu_launches": head["gpu_launches"],
@@ -702,8 +716,8 @@ def main():
     ap.add_argument("--no-companion", action="store_true", help="flow: skip the other-precision run")
     ap.add_argument("--cpu-outer", type=int, default=3, help="flow CPU sample: outer iterations timed")
     ap.add_argument("--cells", type=int, default=1_000_000)
-    ap.add_argument("--case", default="inlet", choices=["inlet", "basin"],
-                    help="flow workload: 1M telescoping inlet (default) or the 200x100 basin")
+    ap.add_argument("--case", default="inlet", choices=["inlet", "basin", "flat"],
+                    help="flow workload: 1M telescoping inlet (default), the 200x100 basin or an intertidal flat")
     ap.add_argument("--precision", default="fp32_refine", choices=["fp32_refine", "fp64"])
     ap.add_argument("--inner-tol", type=float, default=1e-3,
                     help="refinement: relative residual reduction asked of each FP32 inner solve")

@@ -11,6 +11,12 @@ tidal_inlet:  three-level telescoping grid (40/20/10 m) of about 1.0M active
               front of it and a back bay; lognormal Manning n (median 0.025,
               sigma_log 0.2); M2 + K1 water level (0.6 m / 0.2 m) on the north
               edge.
+tidal_flat:   intertidal flat that wets and dries over the tide: bed from 1 m
+              above mean sea level at the south shore to 3 m depth at the open
+              north edge, seeded bumps, a one-cell-wide creek cut into the flat
+              and a depression on the upper flat that is cut off at low water;
+              M2 tide of 1 m.  Cartesian, or telescoping with a refined zone
+              around the creek.
 
 A case carries the grid (cms2d_b200.grid.Grid), bed elevation zb (= -depth,
 ncellsD values; dummies copy their parent cell), coefman (ncells), the
@@ -39,9 +45,10 @@ class Case:
     tide: list  # [(amplitude m, period h)]
     dt: float
     nsteps: int
+    t0: float = 0.0  # tide phase: the water level at time t is the tide at t0 + t (seconds)
 
     def wse(self, t_seconds: float) -> float:
-        th = t_seconds / 3600.0
+        th = (t_seconds + self.t0) / 3600.0
         return float(sum(a * np.cos(2.0 * np.pi * th / T) for a, T in self.tide))
 
     def wsebnd(self, t_seconds: float) -> np.ndarray:
@@ -174,3 +181,38 @@ def tidal_inlet(target_cells: int = 1_000_000, seed: int = 0, dt: float = 300.0,
     coefman = 0.025 * np.exp(0.2 * fld[pj, pi])
     th_cells, th_faces = _north_string(g)
     return Case("tidal_inlet", g, zb, coefman, th_cells, th_faces, [(0.6, M2_HOURS), (0.2, K1_HOURS)], dt, nsteps)
+
+
+def tidal_flat(nx: int = 60, ny: int = 40, dx: float = 20.0, seed: int = 0, amp: float = 1.0, dt: float = 300.0,
+               hours: float = 12.42, t0_hours: float = 0.0, refine: bool = False, manning: float = 0.025) -> Case:
+    """Intertidal flat (see the module docstring).  With refine=True the grid is
+    telescoping: parents of 2 dx with a refined (dx) zone around the creek, so
+    that wet/dry fronts cross refinement interfaces."""
+    rng = np.random.default_rng(seed)
+    if refine:
+        pnx, pny = max(4, nx // 2), max(4, ny // 2)
+        lev = np.zeros((pny, pnx), dtype=np.int64)
+        cx = pnx // 3
+        lev[: max(2, (2 * pny) // 3), max(0, cx - pnx // 6): min(pnx, cx + pnx // 6 + 1)] = 1
+        g = G.telescoping_grid(lev, 2.0 * dx, nmaxfaces=6)
+    else:
+        g = G.cartesian_grid(nx, ny, dx)
+    n = g.ncells
+    x, y = g.x[:n], g.y[:n]
+    Lx, Ly = nx * dx, ny * dx
+    depth = -1.0 + 4.0 * np.clip(y / Ly, 0.0, 1.0)
+    fld = _smooth_field((ny, nx), 4.0, rng) * 0.15
+    ii = np.clip((x / dx).astype(np.int64), 0, nx - 1)
+    jj = np.clip((y / dx).astype(np.int64), 0, ny - 1)
+    depth = depth + fld[jj, ii]
+    # one-cell-wide creek from the shore to the middle of the flat
+    xc = (nx // 3 + 0.5) * dx
+    creek = (np.abs(x - xc) < 0.5 * dx) & (y < 0.55 * Ly)
+    depth = np.where(creek, depth + 1.2, depth)
+    # depression on the upper flat
+    r2 = ((x - 0.7 * Lx) / (4.0 * dx)) ** 2 + ((y - 0.2 * Ly) / (4.0 * dx)) ** 2
+    depth = depth + 1.4 * np.exp(-r2)
+    zb = _fill_dummies(g, -depth)
+    th_cells, th_faces = _north_string(g)
+    return Case("tidal_flat", g, zb, np.full(n, manning), th_cells, th_faces, [(amp, M2_HOURS)], dt,
+                int(round(hours * 3600.0 / dt)), t0=t0_hours * 3600.0)

@@ -346,7 +346,7 @@ long long cms_ensemble_launches(const cms_ensemble* e) { return e ? e->launches 
 int cms_ensemble_step(cms_ensemble* e, double dt, const double* const* wsebnd, cms_flow_info* infos) {
   if (!e || dt <= 0.0) return CMS_BAD_ARGUMENT;
   for (size_t i = 0; i < e->m.size(); ++i)
-    if (e->m[i]->nth > 0 && (!wsebnd || !wsebnd[i])) return CMS_BAD_ARGUMENT;
+    if (!e->m[i]->inited || (e->m[i]->nth > 0 && (!wsebnd || !wsebnd[i]))) return CMS_BAD_ARGUMENT;
   return cms::ensemble_step(e, dt, wsebnd, infos);
 }
 

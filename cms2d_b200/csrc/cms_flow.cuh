@@ -22,6 +22,7 @@ struct FlowDev {
   const unsigned char* owned; // [nD] bit k: face k is on the cell's no-repeat list
   const unsigned char* thm;   // [nD] bit k: face k is on a water-level string
   const unsigned char* joint; // [nD]
+  const unsigned char* crmask;  // [nD] bit k: face k takes part in the cell-reconstruction weights
   const int* iwet;            // [nD]
   // metrics
   const double *ds, *dn, *dsxy, *rx, *ry, *rpx, *rpy, *fintp;  // [nmf][nD]
@@ -30,7 +31,15 @@ struct FlowDev {
   const int *ncx, *ncy, *icx, *icy, *ngx, *ngy, *igx, *igy;
   const double *wcx, *wcy, *wgxy, *wgyx;
   // parameters
-  double grav, gravinv, hmin, hdry, relax_uv, relax_p, facpp, cviscon, cvisbot, cvishor2areaavg, cvismax, wallfac;
+  double grav, gravinv, hmin, hdry, hdry1, hdry2, relax_uv, relax_p, facpp, cviscon, cvisbot, cvishor2areaavg,
+      cvismax, wallfac;
+};
+
+// The wet-cell gradient operator as written by kf_gw_rows (the same buffers
+// FlowDev reads).
+struct GWOut {
+  int *ncx, *ncy, *icx, *icy, *ngx, *ngy, *igx, *igy;
+  double *wcx, *wcy, *wgxy, *wgyx;
 };
 
 __device__ __forceinline__ int fidx(const FlowDev& G, int k, int r) { return k * G.nD + r; }
@@ -58,20 +67,22 @@ struct FlowState {
   double *dpx[2], *dpy[2], *dux[2], *duy[2], *dvx[2], *dvy[2], *dppx[2], *dppy[2];
   double *dHux[2], *dHuy[2], *dHvx[2], *dHvy[2], *dapx[2], *dapy[2], *dzbx[2], *dzby[2];
   double* wsebnd;      // [nth]
-  int* flag;           // [4] device status flags: 0 drying reached, 1 non-finite
+  int* flag;           // [4] device status flags: 1 non-finite, 2 depth classes changed
 };
+
+// depth h = p/g - zb with two roundings (as the host and the reference form it)
+__device__ __forceinline__ double depth_of(const FlowDev& G, double p, double zb) {
+  return __dsub_rn(__dmul_rn(p, G.gravinv), zb);
+}
 
 // ----------------------------------------------------------------------------
 // flow_srcsnk_static, ntsch = 1 (flow_imp.F90:336-346), plus the depth update of
-// flow_wetdry(0) (flow.F90:1247-1255) for the fixed wet set.
+// flow_wetdry(0) (flow.F90:1247-1255).
 __global__ void __launch_bounds__(TPB) kf_static(FlowDev G, FlowState S, double dt) {
   const int r = blockIdx.x * TPB + threadIdx.x;
   if (r >= G.nD) return;
-  double hh = S.p[r] * G.gravinv - G.zb[r];
-  if (hh < G.hdry) {
-    hh = fmax(hh, G.hmin);
-    if (r < G.n && G.iwet[r] == 1) S.flag[0] = 1;
-  }
+  double hh = depth_of(G, S.p[r], G.zb[r]);
+  if (hh < G.hdry) hh = fmax(hh, G.hmin);
   S.h[r] = hh;
   if (r >= G.n) return;
   const double fac1 = G.areap[r] * S.h1[r] / dt;
@@ -544,11 +555,19 @@ __global__ void __launch_bounds__(TPB) kf_fric_vis(FlowDev G, FlowState S, const
 }
 
 // eddy viscosity next to dry/dummy neighbours (flow_eddyvis.f90:169-186),
-// run level by level so that the natural-order recurrence is reproduced:
-// wl_cells is one level's list; rd_cur bit kk says the opposite neighbour
-// across face kk is an earlier list cell (read the updated value), otherwise
-// the value before this pass (vis0) is read.
-__global__ void kf_vis_wall(FlowDev G, FlowState S, const int* cells, const unsigned char* rd_cur, int m) {
+// run level by level so that the natural-order recurrence is reproduced.
+// Each wall face of list cell r (a face to a dry cell or a dummy) sets
+// vis(r) and vis of that neighbour from r's cells on the opposite side.
+// Reads: an earlier list cell (rd_cur bit kk) is read updated, a later or
+// unlisted wet cell as it was before this pass (vis0); r's own dummy as it
+// is in memory (only r writes it); a dry active cell as the last write to it
+// in cell order: r's own write at an earlier face kk < k, else the face value
+// of the last earlier list cell that wrote it (src[j*nmf+kk], a face index
+// into wallv; -1: before this pass).  Several list cells can write one dry
+// cell, so those writes go to the face array wallv and kf_vis_wall_final
+// copies the last writer's value in.
+__global__ void kf_vis_wall(FlowDev G, FlowState S, const int* cells, const unsigned char* rd_cur, const int* src,
+                            double* wallv, int m) {
   const int j = blockIdx.x * TPB + threadIdx.x;
   if (j >= m) return;
   const int r = cells[j];
@@ -564,15 +583,29 @@ __global__ void kf_vis_wall(FlowDev G, FlowState S, const int* cells, const unsi
       const int fk = fidx(G, kk, r);
       if (G.dir[fk] != kkdf) continue;
       const int c = G.nb[fk];
-      // own dummies are written earlier in this same loop: read them as updated
-      const double vc = (((cur >> kk) & 1) || c >= G.n) ? S.vis[c] : S.vis0[c];
+      double vc;
+      if (c >= G.n) {
+        vc = S.vis[c];
+      } else if (G.iwet[c] == 0) {
+        const int sf = src[j * G.nmf + kk];
+        vc = kk < k ? wallv[fk] : (sf >= 0 ? wallv[sf] : S.vis0[c]);
+      } else {
+        vc = ((cur >> kk) & 1) ? S.vis[c] : S.vis0[c];
+      }
       cid = cid + 1.0;
       vs = vs + vc - G.cviscon;
     }
     const double vi = G.cviscon + vs / (cid + 1.0e-15);
     S.vis[r] = vi;
-    S.vis[nck] = vi;
+    if (nck >= G.n) S.vis[nck] = vi;
+    else wallv[f] = vi;
   }
+}
+
+// dry active cells written by the wall pass take their last writer's value
+__global__ void kf_vis_wall_final(const int* cells, const int* faces, int m, const double* wallv, double* vis) {
+  const int j = blockIdx.x * TPB + threadIdx.x;
+  if (j < m) vis[cells[j]] = wallv[faces[j]];
 }
 
 // corner cells (flow_eddyvis.f90:199-209), level by level like kf_vis_wall
@@ -695,6 +728,142 @@ __global__ void __launch_bounds__(TPB) kf_copy(int n, const double* __restrict__
 __global__ void __launch_bounds__(TPB) kf_check(FlowDev G, FlowState S) {
   const int r = blockIdx.x * TPB + threadIdx.x;
   if (r < G.n && !(isfinite(S.p[r]) && isfinite(S.u[r]) && isfinite(S.v[r]))) S.flag[1] = 1;
+}
+
+// ---- wetting and drying --------------------------------------------------
+
+// Depth classes of every cell from the water level (the inputs of the wet/dry
+// rules, flow.F90:1259-1271 and 1363-1416); sets flag[2] and stores the new
+// classes when any cell's classes differ from the stored ones.
+__global__ void __launch_bounds__(TPB) kf_wet_codes(FlowDev G, FlowState S, unsigned char* code) {
+  const int r = blockIdx.x * TPB + threadIdx.x;
+  if (r >= G.nD) return;
+  const double h = depth_of(G, S.p[r], G.zb[r]);
+  const unsigned char c = (unsigned char)((h >= G.hdry ? 1 : 0) | (h < G.hdry1 ? 2 : 0) | (h < G.hdry2 ? 4 : 0));
+  if (c != code[r]) {
+    code[r] = c;
+    S.flag[2] = 1;
+  }
+}
+
+// Zero flux and viscosity on every face with a dry side (flow.F90:1501-1524),
+// owned faces mirrored.
+__global__ void __launch_bounds__(TPB) kf_wet_faces(FlowDev G, FlowState S) {
+  const int r = blockIdx.x * TPB + threadIdx.x;
+  if (r >= G.n) return;
+  const unsigned char own = G.owned[r];
+  const int nf = G.ncface[r];
+  const int wr = G.iwet[r];
+  for (int k = 0; k < nf; ++k) {
+    if (!((own >> k) & 1)) continue;
+    const int f = fidx(G, k, r), nck = G.nb[f];
+    if (wr * G.iwet[nck] != 0) continue;
+    const int fb = fidx(G, G.back[f], nck);
+    S.flux[f] = 0.0; S.visk[f] = 0.0;
+    S.flux[fb] = 0.0; S.visk[fb] = 0.0;
+  }
+}
+
+// keeps stencil entries with |w| > 1e-8 in order (screen_weights,
+// der_lib.f90:681-715) into slots [q * n + r]; returns the count
+__device__ __forceinline__ int gw_keep(int nt, const double* w, const int* idx, int n, int r, int* oi, double* ow) {
+  int c = 0;
+  for (int k = 0; k <= nt; ++k)
+    if (fabs(w[k]) > 1.0e-8) {
+      oi[c * n + r] = idx[k];
+      ow[c * n + r] = w[k];
+      ++c;
+    }
+  return c;
+}
+
+// Wet-cell gradient operator of the listed active cells (all when list is
+// null) from the current wet set: der_grad_cbgg (der_lib.f90:272-378) and, for
+// joint cells, der_grad_cbggcr (381-443).  Every product and sum is rounded
+// on its own, as in the host and reference arithmetic, so the weights are the
+// same bits the host would form.
+__global__ void __launch_bounds__(TPB) kf_gw_rows(FlowDev G, GWOut O, const int* list, int m) {
+  const int j = blockIdx.x * TPB + threadIdx.x;
+  if (j >= m) return;
+  const int r = list ? list[j] : j;
+  const int n = G.n, nmf = G.nmf;
+  if (G.iwet[r] == 0) {
+    O.ncx[r] = 0; O.ncy[r] = 0;
+    O.ngx[r] = 0; O.ngy[r] = 0;
+    return;
+  }
+  double tx[9], ty[9];
+  int ti[9], tj[9];
+  const int nf = G.ncface[r];
+  for (int k = 0; k <= nmf; ++k) { tx[k] = 0.0; ty[k] = 0.0; ti[k] = r; tj[k] = r; }
+  const double area = G.areap[r];
+  for (int k = 0; k < nf; ++k) {
+    const int f = fidx(G, k, r), c = G.nb[f], d = G.dir[f];
+    const double dsx = fnxd(d) * G.ds[f], dsy = fnyd(d) * G.ds[f], fk = G.fintp[f];
+    ti[k + 1] = c; tj[k + 1] = c;
+    if (G.iwet[c] == 1) {
+      const double fp = __dsub_rn(1.0, fk);
+      tx[0] = __dadd_rn(tx[0], __dmul_rn(dsx, fp));
+      tx[k + 1] = __dmul_rn(dsx, fk);
+      ty[0] = __dadd_rn(ty[0], __dmul_rn(dsy, fp));
+      ty[k + 1] = __dmul_rn(dsy, fk);
+    } else {
+      tx[0] = __dadd_rn(tx[0], dsx);
+      ty[0] = __dadd_rn(ty[0], dsy);
+    }
+  }
+  for (int k = 0; k <= nmf; ++k) { tx[k] = __ddiv_rn(tx[k], area); ty[k] = __ddiv_rn(ty[k], area); }
+  const int cx = gw_keep(nmf, tx, ti, n, r, O.icx, O.wcx);
+  const int cy = gw_keep(nmf, ty, tj, n, r, O.icy, O.wcy);
+  double sx = 0.0, sy = 0.0;
+  for (int q = 0; q < cx; ++q) sx = __dadd_rn(sx, O.wcx[q * n + r]);
+  for (int q = 0; q < cy; ++q) sy = __dadd_rn(sy, O.wcy[q * n + r]);
+  const double mx = __ddiv_rn(sx, (double)cx), my = __ddiv_rn(sy, (double)cy);
+  for (int q = 0; q < cx; ++q) O.wcx[q * n + r] = __dsub_rn(O.wcx[q * n + r], mx);
+  for (int q = 0; q < cy; ++q) O.wcy[q * n + r] = __dsub_rn(O.wcy[q * n + r], my);
+  O.ncx[r] = cx; O.ncy[r] = cy;
+  if (G.ider != 2 || !G.joint[r]) return;
+  const unsigned char own = G.owned[r], cr = G.crmask[r];
+  for (int k = 0; k <= nmf; ++k) { tx[k] = 0.0; ty[k] = 0.0; ti[k] = 0; tj[k] = 0; }
+  ti[0] = r; tj[0] = r;
+  for (int k = 0; k < nf; ++k) {
+    if (!((own >> k) & 1)) continue;
+    const int f = fidx(G, k, r), c = G.nb[f], d = G.dir[f];
+    const bool xface = (d == 2 || d == 4);
+    if (!xface) tj[k + 1] = c;
+    if (!((cr >> k) & 1) || G.iwet[c] == 0) continue;
+    const int fb = fidx(G, G.back[f], c);
+    const double fk = G.fintp[f], fp = __dsub_rn(1.0, fk);
+    if (xface) {
+      const double dsx = fnxd(d) * G.ds[f];
+      tx[0] = __dadd_rn(tx[0], __ddiv_rn(__dmul_rn(__dmul_rn(dsx, fp), G.rpy[f]), area));
+      tx[k + 1] = __ddiv_rn(__dmul_rn(__dmul_rn(dsx, fk), G.rpy[fb]), area);
+      ti[k + 1] = c;
+    } else {
+      const double dsy = fnyd(d) * G.ds[f];
+      ty[0] = __dadd_rn(ty[0], __ddiv_rn(__dmul_rn(__dmul_rn(dsy, fp), G.rpx[f]), area));
+      ty[k + 1] = __ddiv_rn(__dmul_rn(__dmul_rn(dsy, fk), G.rpx[fb]), area);
+    }
+  }
+  O.ngx[r] = gw_keep(nmf, tx, ti, n, r, O.igx, O.wgxy);
+  O.ngy[r] = gw_keep(nmf, ty, tj, n, r, O.igy, O.wgyx);
+}
+
+// buf[3j..3j+2] = (u, v, vis) of cell idx[j]
+__global__ void kf_gather_uvv(const int* idx, int m, const double* u, const double* v, const double* vis,
+                              double* buf) {
+  const int j = blockIdx.x * TPB + threadIdx.x;
+  if (j >= m) return;
+  const int c = idx[j];
+  buf[3 * j] = u[c]; buf[3 * j + 1] = v[c]; buf[3 * j + 2] = vis[c];
+}
+
+// (u, v, vis) of cell idx[j] = buf[3j..3j+2]
+__global__ void kf_scatter_uvv(const int* idx, int m, const double* buf, double* u, double* v, double* vis) {
+  const int j = blockIdx.x * TPB + threadIdx.x;
+  if (j >= m) return;
+  const int c = idx[j];
+  u[c] = buf[3 * j]; v[c] = buf[3 * j + 1]; vis[c] = buf[3 * j + 2];
 }
 
 }  // namespace cms

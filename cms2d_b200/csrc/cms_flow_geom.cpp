@@ -122,7 +122,7 @@ std::string build_flow_geom(int n, int nD, int nmf, const int* cell2cell, const 
         g.fintp[f] = (d == 2 || d == 4) ? dx[i] / (dx[i] + dx[j]) : dy[i] / (dy[i] + dy[j]);
       }
     }
-  // Green-Gauss operators
+  // Green-Gauss operator of all cells (the wet-cell one is built on the device)
   g.nsc = nmf + 1;
   g.ider = (skewcor && g.njoint > 0) ? 2 : 1;
   const int nsc = g.nsc;
@@ -197,19 +197,33 @@ std::string build_flow_geom(int n, int nD, int nmf, const int* cell2cell, const 
       ngy[i] = keep_nonzero(nmf, ty.data(), tj.data(), &igy[(size_t)i * nsc], &wgyx[(size_t)i * nsc]);
     }
   };
-  gg(1, g.gw_ncx, g.gw_ncy, g.gw_icx, g.gw_icy, g.gw_wcx, g.gw_wcy, g.gw_ngx, g.gw_ngy, g.gw_igx, g.gw_igy, g.gw_wgxy,
-     g.gw_wgyx);
   gg(0, g.ga_ncx, g.ga_ncy, g.ga_icx, g.ga_icy, g.ga_wcx, g.ga_wcy, g.ga_ngx, g.ga_ngy, g.ga_igx, g.ga_igy, g.ga_wgxy,
      g.ga_wgyx);
-  // corner cells: wet cells with more than one dry neighbour
-  g.icorner.assign(nD, 0);
+  // faces of the cell-reconstruction weights (der_grad_cbggcr's skip test)
+  g.crmask.assign(nD, 0);
+  for (int i = 0; i < n; ++i)
+    for (int k = 0; k < g.ncface[i]; ++k) {
+      const size_t f = at(i, k);
+      if (!g.owned[f]) continue;
+      const int j = g.nb[f], d = g.dir[f];
+      if (j >= n) continue;
+      const double ratio = (d == 2 || d == 4) ? dy[i] / dy[j] : dx[i] / dx[j];
+      if (std::fabs(ratio - 1.0) < 0.1) continue;
+      g.crmask[i] |= (unsigned char)(1u << k);
+    }
+  corner_flags(g);
+  return std::string();
+}
+
+void corner_flags(FlowGeom& g) {
+  const int n = g.n, nmf = g.nmf;
+  g.icorner.assign(g.nD, 0);
   for (int i = 0; i < n; ++i) {
     if (g.iwet[i] != 1) continue;
     int nd = 0;
-    for (int k = 0; k < g.ncface[i]; ++k) nd += (g.iwet[g.nb[at(i, k)]] == 0);
+    for (int k = 0; k < g.ncface[i]; ++k) nd += (g.iwet[g.nb[(size_t)i * nmf + k]] == 0);
     g.icorner[i] = nd > 1;
   }
-  return std::string();
 }
 
 }  // namespace cms

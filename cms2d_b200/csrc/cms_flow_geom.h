@@ -17,15 +17,19 @@ struct FlowGeom {
   std::vector<unsigned char> joint;  // joint (refinement-interface) cells
   int njoint = 0;
   double areaavg = 0;
-  // cell-based Green-Gauss operator for wet cells (ibc = 1) and for all cells
-  // (ibc = 0): q-th stencil entry of cell i at [i * nsc + q]
+  // cell-based Green-Gauss operator for all cells (ibc = 0): q-th stencil
+  // entry of cell i at [i * nsc + q].  The wet-cell operator (ibc = 1) is
+  // built and updated on the device from the same metrics.
   int nsc = 0;
-  std::vector<int> gw_ncx, gw_ncy, gw_icx, gw_icy, ga_ncx, ga_ncy, ga_icx, ga_icy;
-  std::vector<double> gw_wcx, gw_wcy, ga_wcx, ga_wcy;
+  std::vector<int> ga_ncx, ga_ncy, ga_icx, ga_icy;
+  std::vector<double> ga_wcx, ga_wcy;
   // cell-reconstruction corrections of joint cells (ider = 2)
-  std::vector<int> gw_ngx, gw_ngy, gw_igx, gw_igy, ga_ngx, ga_ngy, ga_igx, ga_igy;
-  std::vector<double> gw_wgxy, gw_wgyx, ga_wgxy, ga_wgyx;
+  std::vector<int> ga_ngx, ga_ngy, ga_igx, ga_igy;
+  std::vector<double> ga_wgxy, ga_wgyx;
   int ider = 1;
+  // bit k: face k of the cell takes part in the cell-reconstruction weights
+  // (a no-repeat face to an active cell whose size differs by 10 % or more)
+  std::vector<unsigned char> crmask;
   std::vector<int> iwet, icorner;
 };
 
@@ -34,5 +38,9 @@ struct FlowGeom {
 std::string build_flow_geom(int n, int nD, int nmf, const int* cell2cell, const int* ncface, const int* idirface,
                             const double* x, const double* y, const double* dx, const double* dy, const double* zb,
                             const int* iwet, bool skewcor, FlowGeom& g);
+
+// icorner from g.iwet: wet active cells with more than one dry neighbour
+// (flow.F90:1460-1471).
+void corner_flags(FlowGeom& g);
 
 }  // namespace cms

@@ -6,10 +6,12 @@
 // kernels write the three systems straight into the solver's matrix buffers.
 #pragma once
 #include <algorithm>
+#include <chrono>
 #include <vector>
 
 #include "cms_flow.cuh"
 #include "cms_flow_geom.h"
+#include "cms_flow_wetdry.h"
 
 struct cms_flow {
   cms_solver* S = nullptr;
@@ -29,10 +31,27 @@ struct cms_flow {
   // wall string
   int nw = 0;
   int *d_w_cell = nullptr, *d_w_dummy = nullptr;
-  // eddy-viscosity recurrences, level by level
+  // eddy-viscosity recurrences, level by level (buffers hold up to n cells)
   std::vector<int> wall_lvl, corner_lvl;  // level starts (size levels+1)
   int *d_wall_cells = nullptr, *d_corner_cells = nullptr;
   unsigned char *d_wall_rd = nullptr, *d_corner_rd = nullptr;
+  int* d_wall_src = nullptr;    // [n * nmf] per list entry and face slot: wallv face of the dry cell's last writer
+  double* d_wallv = nullptr;    // [nmf][nD] value each wall face wrote
+  int *d_wall_fin_cells = nullptr, *d_wall_fin_faces = nullptr;  // dry cells written, their last writer's face
+  int nwall_fin = 0;
+  // wetting and drying: rules, device depth classes, the wet flags (device
+  // order) and the wet-cell gradient operator they feed
+  cms::WetDryRules wd;
+  unsigned char* d_code = nullptr;  // [nD] depth classes of the last evaluation (device order)
+  int* d_iwet = nullptr;            // [nD] = G.iwet
+  cms::GWOut gw{};
+  int wd_pending = 0;               // depth classes changed at the end of the last step
+  int inited = 0;                   // cms_flow_init has run (it builds the wet set and its operator)
+  int nwet = 0, last_changed = 0;
+  long long wd_updates = 0;
+  double wd_ms[3] = {0, 0, 0};      // host time of the updates: read-back, rules, application
+  int* d_list = nullptr;            // [n + nD] cell lists of an update (device numbering)
+  double* d_buf = nullptr;          // [3 nD] gathered (u, v, vis)
   signed char* d_fslot_dev = nullptr;  // [nmf][n] ELL slot of face k of device row r
   // gradient copies: index of the current one
   int cur_dppx = 0, cur_duv = 0, cur_dH = 0, cur_dap = 0;
@@ -154,6 +173,115 @@ static void level_schedule(const std::vector<int>& list_nat, const std::vector<s
   }
 }
 
+// Eddy-viscosity recurrence lists from the current wet set: wet cells next to
+// a dry or dummy neighbour, and corner cells (flow_eddyvis.f90:169-209), each
+// in level order.
+static int vis_lists(Flow* F) {
+  const FlowGeom& g = F->geom;
+  const int n = F->n, nD = F->nD, nmf = F->nmf;
+  static const int kk_of[5] = {0, 3, 4, 1, 2};
+  auto nbf = [&](int i, int k) { return g.nb[(size_t)i * nmf + k]; };
+  auto drf = [&](int i, int k) { return g.dir[(size_t)i * nmf + k]; };
+  auto wallface = [&](int i, int k) { const int c = nbf(i, k); return c >= n || g.iwet[c] == 0; };
+  // wall cells in cell order; walk them as the reference loop does, noting for
+  // every read of a dry active cell which earlier list cell wrote it last
+  std::vector<int> wl;
+  for (int i = 0; i < n; ++i) {
+    if (g.iwet[i] != 1) continue;
+    for (int k = 0; k < g.ncface[i]; ++k)
+      if (wallface(i, k)) { wl.push_back(i); break; }
+  }
+  const int m = (int)wl.size();
+  std::vector<int> pos(n, -1), level(m, 0), lastw(n, -1), src((size_t)m * nmf, -1);
+  std::vector<unsigned char> cur(m, 0);
+  for (int p = 0; p < m; ++p) pos[wl[p]] = p;
+  for (int p = 0; p < m; ++p) {
+    const int i = wl[p];
+    int l = 0;
+    for (int k = 0; k < g.ncface[i]; ++k) {
+      if (!wallface(i, k)) continue;
+      const int kkdf = kk_of[drf(i, k)];
+      for (int kk = 0; kk < g.ncface[i]; ++kk) {
+        if (drf(i, kk) != kkdf) continue;
+        const int c = nbf(i, kk);
+        if (c >= n) continue;
+        if (g.iwet[c] == 0) {
+          const int w = lastw[c];  // earlier list cells only: i's own writes are noted below
+          src[(size_t)p * nmf + kk] = w;
+          if (w >= 0) l = std::max(l, level[w / nmf] + 1);
+        } else if (pos[c] >= 0 && pos[c] < p) {
+          cur[p] |= (unsigned char)(1u << kk);
+          l = std::max(l, level[pos[c]] + 1);
+        }
+      }
+    }
+    level[p] = l;
+    for (int k = 0; k < g.ncface[i]; ++k) {
+      const int c = nbf(i, k);
+      if (c < n && g.iwet[c] == 0) lastw[c] = p * nmf + k;
+    }
+  }
+  int L = 0;
+  for (int p = 0; p < m; ++p) L = std::max(L, level[p] + 1);
+  F->wall_lvl.assign(L + 1, 0);
+  for (int p = 0; p < m; ++p) F->wall_lvl[level[p] + 1]++;
+  for (int l = 0; l < L; ++l) F->wall_lvl[l + 1] += F->wall_lvl[l];
+  std::vector<int> fill(F->wall_lvl.begin(), F->wall_lvl.end() - 1), cells(m), srcd((size_t)m * nmf, -1);
+  std::vector<unsigned char> rd(m);
+  auto face_dev = [&](int w) { return (w % nmf) * nD + F->n2d[wl[w / nmf]]; };
+  for (int p = 0; p < m; ++p) {
+    const int q = fill[level[p]]++;
+    cells[q] = F->n2d[wl[p]];
+    rd[q] = cur[p];
+    for (int kk = 0; kk < nmf; ++kk) {
+      const int w = src[(size_t)p * nmf + kk];
+      if (w >= 0) srcd[(size_t)q * nmf + kk] = face_dev(w);
+    }
+  }
+  std::vector<int> fin_c, fin_f;
+  for (int c = 0; c < n; ++c)
+    if (lastw[c] >= 0) { fin_c.push_back(F->n2d[c]); fin_f.push_back(face_dev(lastw[c])); }
+  F->nwall_fin = (int)fin_c.size();
+  cudaStream_t s = F->S->stream;
+  if (m > 0) {
+    CMS_CUDA(cudaMemcpyAsync(F->d_wall_cells, cells.data(), m * sizeof(int), cudaMemcpyHostToDevice, s));
+    CMS_CUDA(cudaMemcpyAsync(F->d_wall_rd, rd.data(), m, cudaMemcpyHostToDevice, s));
+    CMS_CUDA(cudaMemcpyAsync(F->d_wall_src, srcd.data(), srcd.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+  }
+  if (F->nwall_fin > 0) {
+    CMS_CUDA(cudaMemcpyAsync(F->d_wall_fin_cells, fin_c.data(), fin_c.size() * sizeof(int), cudaMemcpyHostToDevice,
+                             s));
+    CMS_CUDA(cudaMemcpyAsync(F->d_wall_fin_faces, fin_f.data(), fin_f.size() * sizeof(int), cudaMemcpyHostToDevice,
+                             s));
+  }
+  CMS_CUDA(cudaStreamSynchronize(s));  // the host vectors go out of scope
+  std::vector<int> cl;
+  std::vector<std::vector<std::pair<int, int>>> cr;
+  for (int i = 0; i < n; ++i) {
+    if (!g.icorner[i]) continue;
+    std::vector<std::pair<int, int>> reads;
+    for (int k = 0; k < g.ncface[i]; ++k) reads.push_back({k, g.nb[(size_t)i * nmf + k]});
+    cl.push_back(i);
+    cr.push_back(reads);
+  }
+  level_schedule(cl, cr, F->n2d, F->corner_lvl, cells, rd);
+  if (!cells.empty()) {
+    CMS_CUDA(cudaMemcpyAsync(F->d_corner_cells, cells.data(), cells.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+    CMS_CUDA(cudaMemcpyAsync(F->d_corner_rd, rd.data(), rd.size(), cudaMemcpyHostToDevice, s));
+    CMS_CUDA(cudaStreamSynchronize(s));
+  }
+  return CMS_OK;
+}
+
+// The host wet flags (natural order) into the device copy.
+static int wet_upload(Flow* F) {
+  std::vector<int> w(F->nD);
+  for (int r = 0; r < F->nD; ++r) w[r] = F->geom.iwet[F->d2n[r]];
+  CMS_CUDA(cudaMemcpyAsync(F->d_iwet, w.data(), w.size() * sizeof(int), cudaMemcpyHostToDevice, F->S->stream));
+  CMS_CUDA(cudaStreamSynchronize(F->S->stream));
+  return CMS_OK;
+}
+
 static int flow_create(int ncells, int ncellsD, int nmf, const int* c2c, const int* ncface, const int* idirface,
                        const double* x, const double* y, const double* dx, const double* dy, const double* zb,
                        const double* coefman, int nth, const int* th_cells, const int* th_faces,
@@ -221,13 +349,14 @@ static int flow_create(int ncells, int ncellsD, int nmf, const int* c2c, const i
   };
   std::vector<int> nb((size_t)nmf * nD, -1), ncf(nD);
   std::vector<signed char> back((size_t)nmf * nD, -1), dir((size_t)nmf * nD, 0), fsd((size_t)nmf * n, -1);
-  std::vector<unsigned char> owned(nD, 0), thd(nD, 0), joint(nD, 0);
+  std::vector<unsigned char> owned(nD, 0), thd(nD, 0), joint(nD, 0), crm(nD, 0);
   std::vector<int> iwd(nD);
   for (int r = 0; r < nD; ++r) {
     const int i = F->d2n[r];
     ncf[r] = g.ncface[i];
     iwd[r] = g.iwet[i];
     joint[r] = g.joint[i];
+    crm[r] = g.crmask[i];
     thd[r] = thm[i];
     for (int k = 0; k < nmf; ++k) {
       const int j = g.nb[(size_t)i * nmf + k];
@@ -240,15 +369,16 @@ static int flow_create(int ncells, int ncellsD, int nmf, const int* c2c, const i
   }
   FlowDev& D = F->G;
   D.n = n; D.nD = nD; D.nmf = nmf; D.nsc = g.nsc; D.ider = g.ider;
-  int *p_ncf, *p_nb, *p_iwet;
+  int *p_ncf, *p_nb;
   signed char *p_back, *p_dir;
-  unsigned char *p_owned, *p_thm, *p_joint;
-  if ((rc = F->upload(&p_ncf, ncf)) || (rc = F->upload(&p_nb, nb)) || (rc = F->upload(&p_iwet, iwd)) ||
+  unsigned char *p_owned, *p_thm, *p_joint, *p_crm;
+  if ((rc = F->upload(&p_ncf, ncf)) || (rc = F->upload(&p_nb, nb)) || (rc = F->upload(&F->d_iwet, iwd)) ||
       (rc = F->upload(&p_back, back)) || (rc = F->upload(&p_dir, dir)) || (rc = F->upload(&p_owned, owned)) ||
-      (rc = F->upload(&p_thm, thd)) || (rc = F->upload(&p_joint, joint)) || (rc = F->upload(&F->d_fslot_dev, fsd)))
+      (rc = F->upload(&p_thm, thd)) || (rc = F->upload(&p_joint, joint)) || (rc = F->upload(&p_crm, crm)) ||
+      (rc = F->upload(&F->d_fslot_dev, fsd)))
     return fail(rc);
-  D.ncface = p_ncf; D.nb = p_nb; D.iwet = p_iwet; D.back = p_back; D.dir = p_dir; D.owned = p_owned; D.thm = p_thm;
-  D.joint = p_joint;
+  D.ncface = p_ncf; D.nb = p_nb; D.iwet = F->d_iwet; D.back = p_back; D.dir = p_dir; D.owned = p_owned;
+  D.thm = p_thm; D.joint = p_joint; D.crmask = p_crm;
   double *p_ds, *p_dn, *p_dsxy, *p_rx, *p_ry, *p_rpx, *p_rpy, *p_fintp, *p_area, *p_zb, *p_man;
   if ((rc = F->upload(&p_ds, faceperm_d(g.ds))) || (rc = F->upload(&p_dn, faceperm_d(g.dn))) ||
       (rc = F->upload(&p_dsxy, faceperm_d(g.dsxy))) || (rc = F->upload(&p_rx, faceperm_d(g.rx))) ||
@@ -263,34 +393,41 @@ static int flow_create(int ncells, int ncellsD, int nmf, const int* c2c, const i
   }
   D.ds = p_ds; D.dn = p_dn; D.dsxy = p_dsxy; D.rx = p_rx; D.ry = p_ry; D.rpx = p_rpx; D.rpy = p_rpy;
   D.fintp = p_fintp; D.areap = p_area; D.zb = p_zb; D.coefman = p_man;
-  // gradient operator (wet cells), [q][n] in device numbering
+  // wet-cell gradient operator, [q][n] in device numbering (built by kf_gw_rows)
   {
-    const int nsc = g.nsc;
-    std::vector<int> ncx(n), ncy(n), ngx(n), ngy(n), icx((size_t)nsc * n), icy((size_t)nsc * n),
-        igx((size_t)nsc * n), igy((size_t)nsc * n);
-    std::vector<double> wcx((size_t)nsc * n), wcy((size_t)nsc * n), wgxy((size_t)nsc * n), wgyx((size_t)nsc * n);
-    for (int r = 0; r < n; ++r) {
-      const int i = F->d2n[r];
-      ncx[r] = g.gw_ncx[i]; ncy[r] = g.gw_ncy[i]; ngx[r] = g.gw_ngx[i]; ngy[r] = g.gw_ngy[i];
-      for (int q = 0; q < nsc; ++q) {
-        const size_t s = (size_t)i * nsc + q, d = (size_t)q * n + r;
-        icx[d] = F->n2d[g.gw_icx[s]]; icy[d] = F->n2d[g.gw_icy[s]];
-        igx[d] = F->n2d[g.gw_igx[s]]; igy[d] = F->n2d[g.gw_igy[s]];
-        wcx[d] = g.gw_wcx[s]; wcy[d] = g.gw_wcy[s]; wgxy[d] = g.gw_wgxy[s]; wgyx[d] = g.gw_wgyx[s];
-      }
-    }
-    int *a1, *a2, *a3, *a4, *a5, *a6, *a7, *a8;
-    double *b1, *b2, *b3, *b4;
-    if ((rc = F->upload(&a1, ncx)) || (rc = F->upload(&a2, ncy)) || (rc = F->upload(&a3, icx)) ||
-        (rc = F->upload(&a4, icy)) || (rc = F->upload(&a5, ngx)) || (rc = F->upload(&a6, ngy)) ||
-        (rc = F->upload(&a7, igx)) || (rc = F->upload(&a8, igy)) || (rc = F->upload(&b1, wcx)) ||
-        (rc = F->upload(&b2, wcy)) || (rc = F->upload(&b3, wgxy)) || (rc = F->upload(&b4, wgyx)))
+    const size_t nsc = g.nsc;
+    GWOut& O = F->gw;
+    if ((rc = F->alloc(&O.ncx, n)) || (rc = F->alloc(&O.ncy, n)) || (rc = F->alloc(&O.ngx, n)) ||
+        (rc = F->alloc(&O.ngy, n)) || (rc = F->alloc(&O.icx, nsc * n)) || (rc = F->alloc(&O.icy, nsc * n)) ||
+        (rc = F->alloc(&O.igx, nsc * n)) || (rc = F->alloc(&O.igy, nsc * n)) || (rc = F->alloc(&O.wcx, nsc * n)) ||
+        (rc = F->alloc(&O.wcy, nsc * n)) || (rc = F->alloc(&O.wgxy, nsc * n)) || (rc = F->alloc(&O.wgyx, nsc * n)))
       return fail(rc);
-    D.ncx = a1; D.ncy = a2; D.icx = a3; D.icy = a4; D.ngx = a5; D.ngy = a6; D.igx = a7; D.igy = a8;
-    D.wcx = b1; D.wcy = b2; D.wgxy = b3; D.wgyx = b4;
+    D.ncx = O.ncx; D.ncy = O.ncy; D.icx = O.icx; D.icy = O.icy; D.ngx = O.ngx; D.ngy = O.ngy; D.igx = O.igx;
+    D.igy = O.igy; D.wcx = O.wcx; D.wcy = O.wcy; D.wgxy = O.wgxy; D.wgyx = O.wgyx;
   }
-  // parameters (flow.F90:21-168, friction.F90:44-49)
-  D.grav = 9.81; D.gravinv = 1.0 / 9.81; D.hmin = 0.05; D.hdry = 0.05; D.relax_uv = 0.8; D.relax_p = 1.0;
+  // wetting and drying: closed dummies (every dummy off the string) and the
+  // string's cells and dummies as flow_pond seeds
+  {
+    WetDryRules& R = F->wd;
+    R.closed.assign(nD, 0);
+    for (int i = n; i < nD; ++i) R.closed[i] = 1;
+    for (int j = 0; j < nth; ++j) {
+      const int i = th_cells[j] - 1, k = th_faces[j] - 1;
+      const int gd = c2c[(size_t)i * nmf + k] - 1;
+      R.closed[gd] = 0;
+      R.seed_cells.push_back(i);
+      R.seed_dummies.push_back(gd);
+    }
+    R.ponding = F->opts.ponding != 0;
+    R.narrowchannels = F->opts.narrowchannels != 0;
+    if ((rc = F->alloc(&F->d_code, nD)) || (rc = F->alloc(&F->d_list, (size_t)n + nD)) ||
+        (rc = F->alloc(&F->d_buf, (size_t)3 * nD)))
+      return fail(rc);
+  }
+  // parameters (flow.F90:21-168, 684-694, friction.F90:44-49)
+  const double hdry = F->opts.hdry > 0.0 ? F->opts.hdry : 0.05;
+  D.grav = 9.81; D.gravinv = 1.0 / 9.81; D.hmin = hdry; D.hdry = hdry; D.hdry1 = 5.0 * hdry; D.hdry2 = 2.0 * hdry;
+  D.relax_uv = 0.8; D.relax_p = 1.0;
   D.facpp = 0.2; D.cviscon = 1.0e-6; D.cvisbot = 0.0667; D.cvismax = 20.0; D.wallfac = 1.0;
   D.cvishor2areaavg = 0.2 * 0.2 * g.areaavg;
   // state
@@ -333,40 +470,11 @@ static int flow_create(int ncells, int ncellsD, int nmf, const int* c2c, const i
     if ((rc = F->upload(&F->d_w_cell, wc)) || (rc = F->upload(&F->d_w_dummy, wg))) return fail(rc);
   }
   // eddy-viscosity recurrences next to dry/dummy neighbours and at corners
-  {
-    static const int kk_of[5] = {0, 3, 4, 1, 2};
-    std::vector<int> wl;
-    std::vector<std::vector<std::pair<int, int>>> wr;
-    for (int i = 0; i < n; ++i) {
-      if (g.iwet[i] != 1) continue;
-      bool hit = false;
-      std::vector<std::pair<int, int>> reads;
-      for (int k = 0; k < g.ncface[i]; ++k) {
-        const int j = g.nb[(size_t)i * nmf + k];
-        if (!(g.iwet[j] == 0 || j >= n)) continue;
-        hit = true;
-        const int kkdf = kk_of[g.dir[(size_t)i * nmf + k]];
-        for (int kk = 0; kk < g.ncface[i]; ++kk)
-          if (g.dir[(size_t)i * nmf + kk] == kkdf) reads.push_back({kk, g.nb[(size_t)i * nmf + kk]});
-      }
-      if (hit) { wl.push_back(i); wr.push_back(reads); }
-    }
-    std::vector<int> cells;
-    std::vector<unsigned char> rd;
-    level_schedule(wl, wr, F->n2d, F->wall_lvl, cells, rd);
-    if ((rc = F->upload(&F->d_wall_cells, cells)) || (rc = F->upload(&F->d_wall_rd, rd))) return fail(rc);
-    std::vector<int> cl;
-    std::vector<std::vector<std::pair<int, int>>> cr;
-    for (int i = 0; i < n; ++i) {
-      if (!g.icorner[i]) continue;
-      std::vector<std::pair<int, int>> reads;
-      for (int k = 0; k < g.ncface[i]; ++k) reads.push_back({k, g.nb[(size_t)i * nmf + k]});
-      cl.push_back(i);
-      cr.push_back(reads);
-    }
-    level_schedule(cl, cr, F->n2d, F->corner_lvl, cells, rd);
-    if ((rc = F->upload(&F->d_corner_cells, cells)) || (rc = F->upload(&F->d_corner_rd, rd))) return fail(rc);
-  }
+  if ((rc = F->alloc(&F->d_wall_cells, n)) || (rc = F->alloc(&F->d_wall_rd, n)) ||
+      (rc = F->alloc(&F->d_wall_src, (size_t)n * nmf)) || (rc = F->alloc(&F->d_wallv, (size_t)nmf * nD)) ||
+      (rc = F->alloc(&F->d_wall_fin_cells, n)) || (rc = F->alloc(&F->d_wall_fin_faces, n)) ||
+      (rc = F->alloc(&F->d_corner_cells, n)) || (rc = F->alloc(&F->d_corner_rd, n)) || (rc = vis_lists(F)))
+    return fail(rc);
   for (int i = 0; i < n; ++i) F->nfaces += g.ncface[i];
   if (cudaStreamSynchronize(S->stream) != cudaSuccess) return fail(CMS_DEVICE_ERROR);
   *out = F;
@@ -436,8 +544,12 @@ static int flow_vis(Flow* F, const double* dux, const double* duy, const double*
   FLAUNCHB(F, fbytes(F, 2, 0, 2), (kf_copy<<<fblk(F->nD), TPB, 0, s>>>(F->nD, F->st.vis, F->st.vis0)));
   for (size_t l = 0; l + 1 < F->wall_lvl.size(); ++l) {
     const int a = F->wall_lvl[l], m = F->wall_lvl[l + 1] - a;
-    FLAUNCH(F, (kf_vis_wall<<<fblk(m), TPB, 0, s>>>(F->G, F->st, F->d_wall_cells + a, F->d_wall_rd + a, m)));
+    FLAUNCH(F, (kf_vis_wall<<<fblk(m), TPB, 0, s>>>(F->G, F->st, F->d_wall_cells + a, F->d_wall_rd + a,
+                                                     F->d_wall_src + (size_t)a * F->nmf, F->d_wallv, m)));
   }
+  if (F->nwall_fin)
+    FLAUNCH(F, (kf_vis_wall_final<<<fblk(F->nwall_fin), TPB, 0, s>>>(F->d_wall_fin_cells, F->d_wall_fin_faces,
+                                                                     F->nwall_fin, F->d_wallv, F->st.vis)));
   FLAUNCHB(F, fbytes(F, 2, 0, 2), (kf_copy<<<fblk(F->nD), TPB, 0, s>>>(F->nD, F->st.vis, F->st.vis1)));
   for (size_t l = 0; l + 1 < F->corner_lvl.size(); ++l) {
     const int a = F->corner_lvl[l], m = F->corner_lvl[l + 1] - a;
@@ -459,10 +571,160 @@ static int flow_grad_interp(Flow* F) {
   return CMS_OK;
 }
 
+// Wet-cell gradient operator of the listed cells (device numbering), or of
+// every active cell when cells is null.
+static int gw_rows(Flow* F, const std::vector<int>* cells) {
+  cudaStream_t s = F->S->stream;
+  if (!cells) {
+    FLAUNCH(F, (kf_gw_rows<<<fblk(F->n), TPB, 0, s>>>(F->G, F->gw, nullptr, F->n)));
+    return CMS_OK;
+  }
+  const int m = (int)cells->size();
+  if (m == 0) return CMS_OK;
+  CMS_CUDA(cudaMemcpyAsync(F->d_list, cells->data(), m * sizeof(int), cudaMemcpyHostToDevice, s));
+  FLAUNCH(F, (kf_gw_rows<<<fblk(m), TPB, 0, s>>>(F->G, F->gw, F->d_list, m)));
+  CMS_CUDA(cudaStreamSynchronize(s));  // d_list is reused
+  return CMS_OK;
+}
+
+// Applies a new wet set (natural order, all nD cells): device flags, corner
+// cells and eddy-viscosity lists; then, except at the cold start, the rest of
+// flow_wetdry(0) and der_update (flow.F90:1473-1524, derivatives.f90:204-296):
+// dry-to-wet initialisation of u, v, vis (5 passes in cell order over the
+// newly wet cells), zero flux and viscosity on faces with a dry side, and the
+// gradient operator of every active cell whose state changed and of its
+// neighbours.  At the cold start the whole operator is built from the new set
+// (der_init).
+static int wetdry_apply(Flow* F, const std::vector<int>& neww, bool cold) {
+  FlowGeom& g = F->geom;
+  const int n = F->n, nD = F->nD, nmf = F->nmf;
+  cudaStream_t s = F->S->stream;
+  std::vector<int> old = g.iwet;
+  g.iwet = neww;
+  int changed = 0, changed_all = 0, nwet = 0;
+  for (int i = 0; i < nD; ++i) {
+    const int d = old[i] != neww[i];
+    changed_all += d;
+    if (i < n) { changed += d; nwet += neww[i]; }
+  }
+  F->nwet = nwet;
+  F->last_changed = changed;
+  if (!cold && changed_all == 0) return CMS_OK;
+  corner_flags(g);
+  FCHK(wet_upload(F));
+  FCHK(vis_lists(F));
+  if (cold) return gw_rows(F, nullptr);
+  if (changed == 0) return CMS_OK;  // only dummies changed: der_update looks at active cells
+  // dry-to-wet initialisation on the host from the gathered neighbourhood
+  std::vector<int> newly;
+  for (int i = 0; i < n; ++i)
+    if (neww[i] == 1 && old[i] == 0) newly.push_back(i);
+  if (!newly.empty()) {
+    std::vector<int> pos(nD, -1), gat;
+    auto add = [&](int c) { if (pos[c] < 0) { pos[c] = (int)gat.size(); gat.push_back(c); } };
+    for (int i : newly) {
+      add(i);
+      for (int k = 0; k < g.ncface[i]; ++k) add(g.nb[(size_t)i * nmf + k]);
+    }
+    const int m = (int)gat.size();
+    std::vector<int> gdev(m);
+    for (int q = 0; q < m; ++q) gdev[q] = F->n2d[gat[q]];
+    std::vector<double> buf((size_t)3 * m);
+    CMS_CUDA(cudaMemcpyAsync(F->d_list, gdev.data(), m * sizeof(int), cudaMemcpyHostToDevice, s));
+    FLAUNCH(F, (kf_gather_uvv<<<fblk(m), TPB, 0, s>>>(F->d_list, m, F->st.u, F->st.v, F->st.vis, F->d_buf)));
+    CMS_CUDA(cudaMemcpyAsync(buf.data(), F->d_buf, buf.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CMS_CUDA(cudaStreamSynchronize(s));
+    const double small = 1.0e-15;  // definitions.F90:93
+    for (int pass = 0; pass < 5; ++pass)
+      for (int i : newly) {
+        double us = 0.0, vs = 0.0, viss = 0.0;
+        int ns = 0;
+        for (int k = 0; k < g.ncface[i]; ++k) {
+          const int c = g.nb[(size_t)i * nmf + k], q = pos[c];
+          us = us + buf[3 * q]; vs = vs + buf[3 * q + 1]; viss = viss + buf[3 * q + 2];
+          ns += neww[c];
+        }
+        const int q = pos[i];
+        buf[3 * q] = us / ((double)ns + small) / 1.25;
+        buf[3 * q + 1] = vs / ((double)ns + small) / 1.25;
+        buf[3 * q + 2] = viss / ((double)ns + small);
+      }
+    const int mn = (int)newly.size();
+    std::vector<double> out((size_t)3 * mn);
+    for (int j = 0; j < mn; ++j) {
+      const int q = pos[newly[j]];
+      gdev[j] = F->n2d[newly[j]];
+      for (int c = 0; c < 3; ++c) out[3 * j + c] = buf[3 * q + c];
+    }
+    CMS_CUDA(cudaMemcpyAsync(F->d_list, gdev.data(), mn * sizeof(int), cudaMemcpyHostToDevice, s));
+    CMS_CUDA(cudaMemcpyAsync(F->d_buf, out.data(), out.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    FLAUNCH(F, (kf_scatter_uvv<<<fblk(mn), TPB, 0, s>>>(F->d_list, mn, F->d_buf, F->st.u, F->st.v, F->st.vis)));
+    CMS_CUDA(cudaStreamSynchronize(s));
+  }
+  FLAUNCHB(F, fbytes(F, 1, 4), (kf_wet_faces<<<fblk(n), TPB, 0, s>>>(F->G, F->st)));
+  // der_update's list: changed active cells and their neighbours, active ones only
+  std::vector<unsigned char> chg(nD, 0);
+  for (int i = 0; i < n; ++i)
+    if (neww[i] != old[i]) {
+      chg[i] = 1;
+      for (int k = 0; k < g.ncface[i]; ++k) chg[g.nb[(size_t)i * nmf + k]] = 1;
+    }
+  std::vector<int> list;
+  for (int i = 0; i < n; ++i)
+    if (chg[i]) list.push_back(F->n2d[i]);
+  return gw_rows(F, &list);
+}
+
+// Wet/dry update at the start of a step whose depth classes changed: the
+// rules on the classes the last step ended with, then wetdry_apply.
+static int wetdry_update(Flow* F) {
+  using clk = std::chrono::steady_clock;
+  auto ms = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
+  const auto t0 = clk::now();
+  const int nD = F->nD;
+  std::vector<unsigned char> cd(nD), cn(nD);
+  CMS_CUDA(cudaMemcpyAsync(cd.data(), F->d_code, nD, cudaMemcpyDeviceToHost, F->S->stream));
+  CMS_CUDA(cudaStreamSynchronize(F->S->stream));
+  for (int r = 0; r < nD; ++r) cn[F->d2n[r]] = cd[r];
+  const auto t1 = clk::now();
+  std::vector<int> neww;
+  wetdry_rules(F->geom, cn.data(), F->wd, neww);
+  const auto t2 = clk::now();
+  F->wd_updates++;
+  const int rc = wetdry_apply(F, neww, false);
+  const auto t3 = clk::now();
+  F->wd_ms[0] += ms(t0, t1); F->wd_ms[1] += ms(t1, t2); F->wd_ms[2] += ms(t2, t3);
+  return rc;
+}
+
 static int flow_init(Flow* F, const double* eta0_nat) {
   FlowState& T = F->st;
   cudaStream_t s = F->S->stream;
   const int nD = F->nD;
+  // wet set of the cold start (prestart.f90:308-315): flow_wetdry(0), again
+  // with ponding on when every cell is dry
+  {
+    std::vector<unsigned char> cn(nD), cd(nD);
+    for (int i = 0; i < nD; ++i) {
+      const double pi = eta0_nat[i] * F->G.grav;
+      const double hh = pi * F->G.gravinv - F->geom.zb[i];
+      cn[i] = (unsigned char)((hh >= F->G.hdry ? WD_WET : 0) | (hh < F->G.hdry1 ? WD_LT1 : 0) |
+                              (hh < F->G.hdry2 ? WD_LT2 : 0));
+    }
+    std::vector<int> neww;
+    wetdry_rules(F->geom, cn.data(), F->wd, neww);
+    int nwet = 0;
+    for (int i = 0; i < F->n; ++i) nwet += neww[i];
+    if (nwet == 0 && !F->wd.ponding) {
+      F->wd.ponding = true;
+      wetdry_rules(F->geom, cn.data(), F->wd, neww);
+    }
+    FCHK(wetdry_apply(F, neww, true));
+    for (int r = 0; r < nD; ++r) cd[r] = cn[F->d2n[r]];
+    CMS_CUDA(cudaMemcpyAsync(F->d_code, cd.data(), nD, cudaMemcpyHostToDevice, s));
+    CMS_CUDA(cudaStreamSynchronize(s));
+    F->wd_pending = 0;
+  }
   std::vector<double> p(nD), h(nD), eta(nD);
   for (int r = 0; r < nD; ++r) {
     const int i = F->d2n[r];
@@ -509,6 +771,7 @@ static int flow_init(Flow* F, const double* eta0_nat) {
   FLAUNCH(F, (kf_update<<<fblk(nD), TPB, 0, s>>>(F->G, T, T.dppx[0], T.dppy[0], T.dppx[1], T.dppy[1])));
   CMS_CUDA(cudaStreamSynchronize(s));
   F->t_sim = 0.0;
+  F->inited = 1;
   return CMS_OK;
 }
 
@@ -545,6 +808,11 @@ static int check_conv(const double rm[4], double rmom0[4], double rmom1[4], int 
 static int step_begin(Flow* F, double dt, const double* wsebnd) {
   FlowState& T = F->st;
   cudaStream_t s = F->S->stream;
+  F->last_changed = 0;
+  if (F->wd_pending) {  // flow_wetdry(0) and der_update (flow_imp.F90:73-79)
+    FCHK(wetdry_update(F));
+    F->wd_pending = 0;
+  }
   if (F->nth) {  // water levels of the string, placed on the string's dummies
     CMS_CUDA(cudaMemcpyAsync(F->d_wse, wsebnd, F->nth * sizeof(double), cudaMemcpyHostToDevice, s));
     FLAUNCH(F, (kf_scatter_vals<<<fblk(F->nth), TPB, 0, s>>>(F->d_th_dummy, F->d_wse, F->nth, F->d_wse_cell)));
@@ -613,16 +881,23 @@ static int step_end(Flow* F, double dt, int niter, int iconv, cms_flow_info* inf
   FLAUNCHB(F, fbytes(F, 13, 0, 13), (kf_update<<<fblk(F->nD), TPB, 0, s>>>(F->G, T, T.dppx[0], T.dppy[0], T.dppx[1],
                                                                            T.dppy[1])));
   FLAUNCH(F, (kf_check<<<fblk(F->n), TPB, 0, s>>>(F->G, T)));
+  // depth classes for the next step's flow_wetdry(0) (p does not change in between)
+  FLAUNCHB(F, fbytes(F, 0, 0, 0) + 17.0 * F->nD, (kf_wet_codes<<<fblk(F->nD), TPB, 0, s>>>(F->G, T, F->d_code)));
   CMS_CUDA(cudaMemcpyAsync(F->h_flag, T.flag, 4 * sizeof(int), cudaMemcpyDeviceToHost, s));
   CMS_CUDA(cudaStreamSynchronize(s));
+  if (F->h_flag[2]) {
+    F->wd_pending = 1;
+    CMS_CUDA(cudaMemsetAsync(T.flag + 2, 0, sizeof(int), s));
+  }
   F->t_sim += dt;
   std::memset(info, 0, sizeof(*info));
   info->niter = niter;
   info->iconv = iconv;
   info->rmom_p = F->it_rm[1]; info->rmom_u = F->it_rm[2]; info->rmom_v = F->it_rm[3];
   info->krylov_iters = F->it_kry;
+  info->nwet = F->nwet;
+  info->nchanged = F->last_changed;
   info->status = CMS_OK;
-  if (F->h_flag[0]) info->status = CMS_UNSUPPORTED;       // a wet cell fell below the drying depth
   if (F->h_flag[1] || iconv == 0) info->status = CMS_NONFINITE;
   F->last = *info;
   return info->status;
@@ -674,6 +949,9 @@ void cms_flow_default_opts(cms_flow_opts* o) {
   o->skewcor = 1;
   o->inner_tol = 1.0e-3;
   o->inner_max = 50;
+  o->hdry = 0.05;
+  o->ponding = 0;
+  o->narrowchannels = 0;
 }
 
 int cms_flow_create(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, const int* ncface,
@@ -690,7 +968,7 @@ int cms_flow_init(cms_flow* f, const double* eta0) {
 }
 
 int cms_flow_step(cms_flow* f, double dt, const double* wsebnd, cms_flow_info* info) {
-  if (!f || dt <= 0.0 || (f->nth > 0 && !wsebnd)) return CMS_BAD_ARGUMENT;
+  if (!f || !f->inited || dt <= 0.0 || (f->nth > 0 && !wsebnd)) return CMS_BAD_ARGUMENT;
   return cms::flow_step(f, dt, wsebnd, info);
 }
 
@@ -700,6 +978,10 @@ int cms_flow_get(cms_flow* f, int which, double* out) {
   cms::FlowState& T = f->st;
   const double* cell = nullptr;
   const double* face = nullptr;
+  if (which == CMS_FLOW_IWET) {  // the host copy is the one the device flags were made from
+    for (int i = 0; i < nD; ++i) out[i] = f->geom.iwet[i];
+    return CMS_OK;
+  }
   switch (which) {
     case CMS_FLOW_P: cell = T.p; break;
     case CMS_FLOW_H: cell = T.h; break;
@@ -752,6 +1034,13 @@ cms_solver* cms_flow_solver(cms_flow* f) { return f ? f->S : nullptr; }
 long long cms_flow_launches(const cms_flow* f) { return f ? f->launches + (f->S ? f->S->launches : 0) : 0; }
 size_t cms_flow_device_bytes(const cms_flow* f) { return f ? f->bytes + (f->S ? f->S->bytes : 0) : 0; }
 int cms_flow_njoint(const cms_flow* f) { return f ? f->geom.njoint : -1; }
+
+int cms_flow_wetdry_stats(const cms_flow* f, long long* updates, double* ms3) {
+  if (!f || !updates || !ms3) return CMS_BAD_ARGUMENT;
+  *updates = f->wd_updates;
+  for (int q = 0; q < 3; ++q) ms3[q] = f->wd_ms[q];
+  return CMS_OK;
+}
 
 void cms_flow_destroy(cms_flow* f) {
   if (!f) return;

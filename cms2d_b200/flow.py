@@ -17,7 +17,7 @@ from . import _lib
 _ORDER = {"multicolor": _lib.ORDER_MULTICOLOR, "natural": _lib.ORDER_NATURAL}
 _PREC = {"fp64": _lib.PREC_FP64, "fp32_refine": _lib.PREC_FP32_REFINE}
 
-CELL = {"p": 0, "h": 1, "u": 2, "v": 3, "eta": 4, "vis": 5, "cfrict": 6, "dpx": 7, "dpy": 8}
+CELL = {"p": 0, "h": 1, "u": 2, "v": 3, "eta": 4, "vis": 5, "cfrict": 6, "dpx": 7, "dpy": 8, "iwet": 9}
 FACE = {"flux": 100, "visk": 101, "hk": 102, "acoef": 103, "fintp": 104, "zbk": 105}
 
 
@@ -25,12 +25,13 @@ class FlowOpts(C.Structure):
     _fields_ = [("nsolv", C.c_int), ("ordering", C.c_int), ("precision", C.c_int), ("norm", C.c_int),
                 ("tol", C.c_double), ("nswp_pp", C.c_int), ("nswp_uv", C.c_int), ("maxit", C.c_int),
                 ("skewcor", C.c_int), ("inner_tol", C.c_double), ("inner_max", C.c_int),
-                ("multi_kernel", C.c_int)]
+                ("multi_kernel", C.c_int), ("hdry", C.c_double), ("ponding", C.c_int), ("narrowchannels", C.c_int)]
 
 
 class FlowInfo(C.Structure):
     _fields_ = [("status", C.c_int), ("niter", C.c_int), ("iconv", C.c_int), ("rmom_p", C.c_double),
-                ("rmom_u", C.c_double), ("rmom_v", C.c_double), ("krylov_iters", C.c_longlong)]
+                ("rmom_u", C.c_double), ("rmom_v", C.c_double), ("krylov_iters", C.c_longlong),
+                ("nwet", C.c_int), ("nchanged", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -67,7 +68,8 @@ class FlowModel:
     def __init__(self, case, nsolv: int = 4, ordering: str = "multicolor", precision: str = "fp64",
                  tol: float = 1e-3, norm: int = 1, nswp_pp: int | None = None, nswp_uv: int | None = None,
                  maxit: int = 0, skewcor: bool = True, inner_tol: float = 1e-3, inner_max: int = 50,
-                 multi_kernel: bool = False):
+                 multi_kernel: bool = False, hdry: float = 0.05, ponding: bool = False,
+                 narrowchannels: bool = False):
         L = _lib.lib()
         _bind(L)
         self.case = case
@@ -88,6 +90,9 @@ class FlowModel:
         o.inner_tol = inner_tol
         o.inner_max = inner_max
         o.multi_kernel = int(multi_kernel)
+        o.hdry = hdry
+        o.ponding = int(ponding)
+        o.narrowchannels = int(narrowchannels)
         self.opts = o
         self._keep = [np.ascontiguousarray(a) for a in (
             g.cell2cell.astype(np.int32), g.ncface.astype(np.int32), g.idirface.astype(np.int32),
@@ -163,6 +168,16 @@ class FlowModel:
     def njoint(self) -> int:
         return _lib.lib().cms_flow_njoint(self._h)
 
+    def wetdry_stats(self) -> dict:
+        """Wet/dry updates so far and their host time (ms): read-back, rules, application."""
+        L = _lib.lib()
+        L.cms_flow_wetdry_stats.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        up = C.c_longlong()
+        ms = np.zeros(3)
+        _lib.check(L.cms_flow_wetdry_stats(self._h, C.byref(up), _p(ms)), "cms_flow_wetdry_stats")
+        return {"updates": int(up.value), "readback_ms": float(ms[0]), "rules_ms": float(ms[1]),
+                "apply_ms": float(ms[2])}
+
     @property
     def solver_handle(self):
         return _lib.lib().cms_flow_solver(self._h)
@@ -172,3 +187,24 @@ class FlowModel:
         p = np.zeros(self.g.ncells, np.int32)
         _lib.check(_lib.lib().cms_solver_get_perm(self.solver_handle, _p(p)), "cms_solver_get_perm")
         return p
+
+
+def wetdry_rules(case, eta, hdry: float = 0.05, ponding: bool = False, narrowchannels: bool = False) -> np.ndarray:
+    """Wet flags (ncellsD) that flow_wetdry(0) gives the case's grid for the
+    water level eta (ncellsD values); host computation, no device needed."""
+    L = _lib.lib()
+    if not getattr(L, "_wdr_bound", False):
+        L.cms_wetdry_rules.argtypes = [C.c_int] * 3 + [C.c_void_p] * 5 + [C.c_int, C.c_void_p, C.c_void_p, C.c_double,
+                                                                          C.c_int, C.c_int, C.c_void_p]
+        L._wdr_bound = True
+    g = case.grid
+    arrs = [np.ascontiguousarray(a) for a in (g.cell2cell.astype(np.int32), g.ncface.astype(np.int32),
+                                               g.idirface.astype(np.int32), case.zb.astype(np.float64),
+                                               np.asarray(eta, np.float64), case.th_cells.astype(np.int32),
+                                               case.th_faces.astype(np.int32))]
+    out = np.zeros(g.ncellsD, np.int32)
+    rc = L.cms_wetdry_rules(g.ncells, g.ncellsD, g.nmaxfaces, _p(arrs[0]), _p(arrs[1]), _p(arrs[2]), _p(arrs[3]),
+                            _p(arrs[4]), int(case.th_cells.size), _p(arrs[5]), _p(arrs[6]), float(hdry),
+                            int(ponding), int(narrowchannels), _p(out))
+    _lib.check(rc, "cms_wetdry_rules")
+    return out

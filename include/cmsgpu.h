@@ -192,6 +192,9 @@ typedef struct cms_flow_opts {
   double inner_tol;  /* refinement: FP32 solve tolerance                           */
   int inner_max;
   int multi_kernel;  /* solver kernels, as cms_solver_opts.multi_kernel            */
+  double hdry;       /* drying depth (flow.F90:51, hmin = hdry); 0: 0.05 m          */
+  int ponding;       /* keep isolated water bodies (flow.F90:54; default 0)         */
+  int narrowchannels; /* keep one-cell-wide channels (flow.F90:55; default 0)       */
 } cms_flow_opts;
 
 typedef struct cms_flow_info {
@@ -200,11 +203,13 @@ typedef struct cms_flow_info {
   int iconv;         /* check_conv: 0 divergent, 1 continue (maxit reached), 2 converged */
   double rmom_p, rmom_u, rmom_v;  /* last normalised residuals (rmom(1:3))        */
   long long krylov_iters;         /* Krylov iterations of all solves of the step  */
+  int nwet;          /* wet active cells during the step (number_wet_cells)        */
+  int nchanged;      /* active cells whose wet state changed at the step's start   */
 } cms_flow_info;
 
 enum {
   CMS_FLOW_P = 0, CMS_FLOW_H = 1, CMS_FLOW_U = 2, CMS_FLOW_V = 3, CMS_FLOW_ETA = 4, CMS_FLOW_VIS = 5,
-  CMS_FLOW_CFRICT = 6, CMS_FLOW_DPX = 7, CMS_FLOW_DPY = 8,
+  CMS_FLOW_CFRICT = 6, CMS_FLOW_DPX = 7, CMS_FLOW_DPY = 8, CMS_FLOW_IWET = 9,
   CMS_FLOW_FLUX = 100, CMS_FLOW_VISK = 101, CMS_FLOW_HK = 102, CMS_FLOW_ACOEF = 103, CMS_FLOW_FINTP = 104,
   CMS_FLOW_ZBK = 105
 };
@@ -224,8 +229,20 @@ int cms_flow_create(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell
  * order), as prestart does (prestart.f90:302-325). */
 int cms_flow_init(cms_flow* f, const double* eta0);
 /* One time step of length dt; wsebnd holds the string's water levels at the
- * new time level (one per string entry). */
+ * new time level (one per string entry).  The step starts with wetting and
+ * drying (flow_wetdry(0), flow.F90:1231-1539, and der_update,
+ * derivatives.f90:204-296) when any cell's depth class changed since the
+ * last one. */
 int cms_flow_step(cms_flow* f, double dt, const double* wsebnd, cms_flow_info* info);
+/* Wet set of flow_wetdry(0) (flow.F90:1231-1539; flow_pond 1807-1876) for the
+ * water level eta (ncellsD values): depth rule, every dummy off the water-level
+ * string closed (dry), narrow-channel removal (Cartesian rules; the one-cell
+ * rule when narrowchannels is set), and flow_pond seeded by the string unless
+ * ponding is set.  Host arrays only (no device work); hdry <= 0 means 0.05 m.
+ * Grid arrays as in cms_flow_create; iwet receives ncellsD flags. */
+int cms_wetdry_rules(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, const int* ncface,
+                     const int* idirface, const double* zb, const double* eta, int nth, const int* th_cells,
+                     const int* th_faces, double hdry, int ponding, int narrowchannels, int* iwet);
 /* Host copy (natural order) of a state array CMS_FLOW_*: ncellsD values for
  * cell arrays, [ncellsD][nmaxfaces] for face arrays. */
 int cms_flow_get(cms_flow* f, int which, double* out);
@@ -236,6 +253,11 @@ cms_solver* cms_flow_solver(cms_flow* f);
 long long cms_flow_launches(const cms_flow* f);
 size_t cms_flow_device_bytes(const cms_flow* f);
 int cms_flow_njoint(const cms_flow* f);
+/* Wet/dry updates run so far (steps that started with a changed wet set
+ * candidate) and their host time in ms: ms3[0] depth-class read-back, ms3[1]
+ * rules, ms3[2] application (flags, lists, dry-to-wet initialisation,
+ * gradient-operator rows).  No counterpart in the reference. */
+int cms_flow_wetdry_stats(const cms_flow* f, long long* updates, double* ms3);
 void cms_flow_destroy(cms_flow* f);
 
 /* ---- Ensembles of independent flow models --------------------------------

@@ -5,10 +5,9 @@
 // telescoping grids (simple and joint cells, skewness corrections), ntsch = 1,
 // exponential convection scheme (ndsch = 4), Manning friction without waves,
 // the mturbul = 5 eddy viscosity, tidal/water-level (TH/H) boundary strings and
-// walls.  Water levels on boundary strings are inputs of a step (bnd_eval stays
-// with the caller).  Wetting and drying is not restated: iwet is fixed at
-// creation (active cells wet, wall dummies dry, open-boundary dummies wet) and
-// a step reports an error if a cell falls below the drying depth.
+// walls, wetting and drying (flow_wetdry(0) with flow_pond, der_update).
+// Water levels on boundary strings are inputs of a step (bnd_eval stays with
+// the caller).
 //
 // Only tests/, __graft_entry__.smoke() and bench.py's CPU baseline load it.
 // Arrays are 1-based like the Fortran: index 0 is unused; face arrays are
@@ -23,6 +22,7 @@ extern "C" {
 void* orc_create(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, const int* ncface, const int* iwet,
                  int fix_last_cell);
 void orc_destroy(void* h);
+void orc_set_wet(void* h, const int* iwet);
 int orc_solve_d(void* hv, const double* acoef, double* ss, const double* sp, double* res, double* phi, double relax,
                 int nswp, int nsolv, int precond, double tol, int lfil, double droptol, double permtol, double* rmom,
                 int* iters, int* inner, double* relres, int norm);
@@ -36,6 +36,9 @@ using VI = std::vector<int>;
 struct Params {
   double grav = 9.81;             // flow.F90:34
   double hmin = 0.05, hdry = 0.05;  // flow.F90:50-51
+  double hdry1 = 0.25, hdry2 = 0.1;  // 5 hdry, 2 hdry (flow.F90:52-53, 686-689)
+  double small = 1.0e-15;          // definitions.F90:93
+  bool ponding = false, narrowchannels = false;  // flow.F90:54-55
   double relax_uv = 0.8, relax_pp = 1.0, relax_p = 1.0;  // flow.F90:124-130
   double facpp = 0.2;             // flow.F90:132
   double cviscon = 1.0e-6, cvisbot = 0.0667, cvishor = 0.2, cvismax = 20.0;  // flow.F90:82-96 (mturbul=5)
@@ -67,7 +70,8 @@ struct Flow {
     int ider = 1;
   } gow, goa;
   // state
-  VI iwet, icorner;
+  VI iwet, iwet1, icorner;
+  int last_nlist = 0;  // cells der_update recomputed in the last step
   V p, h, u, v, pp, eta, vis, cfrict, uelwc, uv, bsxy, bsvel, z0, coefman, cmb, fc;
   V u1, v1, p1, h1;
   V flux, visk, hk, pk, acoef;
@@ -227,7 +231,72 @@ void screen(int nt, const double* wxt, const double* wyt, const int* ixt, const 
   }
 }
 
-// der_grad_cbgg (der_lib.f90:272-378) and der_grad_cbggcr (381-443) for all cells.
+// der_grad_cbgg (der_lib.f90:272-378) for cell i: Green-Gauss weights from
+// the current iwet (ibc = 1 uses only wet neighbours, ibc = 0 all).
+void cbgg_cell(Flow& f, Flow::GO& go, int i, int ibc) {
+  const int nmf = f.nmf, nsc = go.nsc;
+  if (f.iwet[i] == 0 && ibc == 1) { go.ncx[i] = 0; go.ncy[i] = 0; return; }
+  std::vector<double> wx(nmf + 1, 0.0), wy(nmf + 1, 0.0);
+  std::vector<int> ix(nmf + 1, 0), iy(nmf + 1, 0);
+  ix[0] = i; iy[0] = i;
+  for (int k = 1; k <= f.ncface[i]; ++k) {
+    int nck = f.C(k, i);
+    ix[k] = nck; iy[k] = nck;
+    if (f.iwet[nck] == 1 || ibc == 0) {
+      wx[0] = wx[0] + f.F(f.dsx, k, i) * (1.0 - f.F(f.fintp, k, i));
+      wx[k] = f.F(f.dsx, k, i) * f.F(f.fintp, k, i);
+      wy[0] = wy[0] + f.F(f.dsy, k, i) * (1.0 - f.F(f.fintp, k, i));
+      wy[k] = f.F(f.dsy, k, i) * f.F(f.fintp, k, i);
+    } else {
+      wx[0] = wx[0] + f.F(f.dsx, k, i);
+      wy[0] = wy[0] + f.F(f.dsy, k, i);
+    }
+  }
+  for (int k = 0; k <= nmf; ++k) { wx[k] = wx[k] / f.areap[i]; wy[k] = wy[k] / f.areap[i]; }
+  int *icx = &go.icx[(size_t)i * (nsc + 1)], *icy = &go.icy[(size_t)i * (nsc + 1)];
+  double *wcx = &go.wcx[(size_t)i * (nsc + 1)], *wcy = &go.wcy[(size_t)i * (nsc + 1)];
+  screen(nmf, wx.data(), wy.data(), ix.data(), iy.data(), go.ncx[i], go.ncy[i], icx, icy, wcx, wcy);
+  double sx = 0, sy = 0;
+  for (int q = 1; q <= go.ncx[i]; ++q) sx = sx + wcx[q];
+  for (int q = 1; q <= go.ncy[i]; ++q) sy = sy + wcy[q];
+  for (int q = 1; q <= go.ncx[i]; ++q) wcx[q] = wcx[q] - sx / (double)go.ncx[i];
+  for (int q = 1; q <= go.ncy[i]; ++q) wcy[q] = wcy[q] - sy / (double)go.ncy[i];
+}
+
+// der_grad_cbggcr (der_lib.f90:381-443) for cell i: cell-reconstruction
+// weights across refinement faces (no-repeat x and y face lists).
+void cbggcr_cell(Flow& f, Flow::GO& go, int i, int ibc) {
+  const int n = f.n, nmf = f.nmf, nsc = go.nsc;
+  if (f.iwet[i] == 0 && ibc == 1) { go.ngx[i] = 0; go.ngy[i] = 0; return; }
+  std::vector<double> gxy(nmf + 1, 0.0), gyx(nmf + 1, 0.0);
+  std::vector<int> igx(nmf + 1, 0), igy(nmf + 1, 0);
+  igx[0] = i; igy[0] = i;
+  for (int j = 1; j <= f.nxface[i]; ++j) {
+    int k = f.FI(f.kxface, j, i), nck = f.C(k, i);
+    if (nck > n || std::fabs(f.dy[i] / f.dy[nck] - 1.0) < 0.1) continue;
+    if (f.iwet[nck] == 0 && ibc == 1) continue;
+    int jcn = f.FI(f.llec, k, i);
+    gxy[0] = gxy[0] + f.F(f.dsx, k, i) * (1.0 - f.F(f.fintp, k, i)) * f.F(f.rpy, k, i) / f.areap[i];
+    gxy[k] = f.F(f.dsx, k, i) * f.F(f.fintp, k, i) * f.F(f.rpy, jcn, nck) / f.areap[i];
+    igx[k] = nck;
+  }
+  for (int j = 1; j <= f.nyface[i]; ++j) {
+    int k = f.FI(f.kyface, j, i), nck = f.C(k, i);
+    igy[k] = nck;
+    if (nck > n || std::fabs(f.dx[i] / f.dx[nck] - 1.0) < 0.1) continue;
+    if (f.iwet[nck] == 0 && ibc == 1) continue;
+    int jcn = f.FI(f.llec, k, i);
+    gyx[0] = gyx[0] + f.F(f.dsy, k, i) * (1.0 - f.F(f.fintp, k, i)) * f.F(f.rpx, k, i) / f.areap[i];
+    gyx[k] = f.F(f.dsy, k, i) * f.F(f.fintp, k, i) * f.F(f.rpx, jcn, nck) / f.areap[i];
+  }
+  screen(nmf, gxy.data(), gyx.data(), igx.data(), igy.data(), go.ngx[i], go.ngy[i],
+         &go.igx[(size_t)i * (nsc + 1)], &go.igy[(size_t)i * (nsc + 1)], &go.wgxy[(size_t)i * (nsc + 1)],
+         &go.wgyx[(size_t)i * (nsc + 1)]);
+}
+
+// der_init's operator build (derivatives.f90:95-150) for the current iwet:
+// cbgg for every cell, cbggcr for the joint cells (its weights are zero
+// elsewhere on these grids, and der_grad_eval applies them to joint cells only).
 void build_go(Flow& f, Flow::GO& go, int ibc) {
   const int n = f.n, nD = f.nD, nmf = f.nmf;
   go.nsc = nmf + 1;  // room for the cell and every face (derivatives.f90:125-131 sizes it the same or larger)
@@ -238,65 +307,183 @@ void build_go(Flow& f, Flow::GO& go, int ibc) {
   go.ngx.assign(nD + 1, 0); go.ngy.assign(nD + 1, 0);
   go.igx = go.icx; go.igy = go.icx; go.wgxy = go.wcx; go.wgyx = go.wcx;
   go.ider = (f.skewcor && !f.idjoint.empty()) ? 2 : 1;
-  std::vector<double> wx(nmf + 1), wy(nmf + 1);
-  std::vector<int> ix(nmf + 1), iy(nmf + 1);
+  for (int i = 1; i <= n; ++i) cbgg_cell(f, go, i, ibc);
+  if (go.ider != 2) return;
+  for (int i : f.idjoint) cbggcr_cell(f, go, i, ibc);
+}
+
+// der_update (derivatives.f90:204-296): the wet-cell operator is recomputed
+// for every active cell whose wet state differs from the previous time level
+// and for its neighbours.  Only active cells' changes are looked at; a dummy
+// whose state changes does not flag its cell.
+int der_update(Flow& f) {
+  const int n = f.n;
+  std::vector<char> ichg(f.nD + 1, 0);
+  for (int i = 1; i <= n; ++i)
+    if (f.iwet[i] != f.iwet1[i]) {
+      ichg[i] = 1;
+      for (int k = 1; k <= f.ncface[i]; ++k) ichg[f.C(k, i)] = 1;
+    }
+  int nlist = 0;
   for (int i = 1; i <= n; ++i) {
-    if (f.iwet[i] == 0 && ibc == 1) { go.ncx[i] = 0; go.ncy[i] = 0; continue; }
-    std::fill(wx.begin(), wx.end(), 0.0); std::fill(wy.begin(), wy.end(), 0.0);
-    ix[0] = i; iy[0] = i;
-    for (int k = 1; k <= f.ncface[i]; ++k) {
-      int nck = f.C(k, i);
-      ix[k] = nck; iy[k] = nck;
-      if (f.iwet[nck] == 1 || ibc == 0) {
-        wx[0] = wx[0] + f.F(f.dsx, k, i) * (1.0 - f.F(f.fintp, k, i));
-        wx[k] = f.F(f.dsx, k, i) * f.F(f.fintp, k, i);
-        wy[0] = wy[0] + f.F(f.dsy, k, i) * (1.0 - f.F(f.fintp, k, i));
-        wy[k] = f.F(f.dsy, k, i) * f.F(f.fintp, k, i);
-      } else {
-        wx[0] = wx[0] + f.F(f.dsx, k, i);
-        wy[0] = wy[0] + f.F(f.dsy, k, i);
+    if (!ichg[i]) continue;
+    ++nlist;
+    cbgg_cell(f, f.gow, i, 1);
+    if (f.gow.ider == 2) cbggcr_cell(f, f.gow, i, 1);
+  }
+  return nlist;
+}
+
+// flow_pond (flow.F90:1807-1876): wet cells not connected through wet cells
+// to a forcing-boundary string are dried.  The string cells and their dummies
+// seed the search; the alternating forward/backward sweeps run until a pass
+// adds nothing.
+void flow_pond(Flow& f) {
+  const int n = f.n, nD = f.nD;
+  std::vector<int> ipond(nD + 1, 0);
+  for (size_t j = 0; j < f.th_cells.size(); ++j) {
+    const int i = f.th_cells[j], k = f.th_faces[j];
+    ipond[i] = f.iwet[i];
+    const int nck = f.C(k, i);
+    ipond[nck] = f.iwet[nck];
+  }
+  int npond = 10;
+  while (npond > 0) {
+    npond = 0;
+    for (int i = 1; i <= n; ++i) {
+      if (ipond[i] != 1) continue;
+      for (int k = 1; k <= f.ncface[i]; ++k) {
+        const int nck = f.C(k, i);
+        npond = npond + std::max(0, f.iwet[nck] - ipond[nck]);
+        ipond[nck] = f.iwet[nck];
       }
     }
-    for (int k = 0; k <= nmf; ++k) { wx[k] = wx[k] / f.areap[i]; wy[k] = wy[k] / f.areap[i]; }
-    int *icx = &go.icx[(size_t)i * (nsc + 1)], *icy = &go.icy[(size_t)i * (nsc + 1)];
-    double *wcx = &go.wcx[(size_t)i * (nsc + 1)], *wcy = &go.wcy[(size_t)i * (nsc + 1)];
-    screen(nmf, wx.data(), wy.data(), ix.data(), iy.data(), go.ncx[i], go.ncy[i], icx, icy, wcx, wcy);
-    double sx = 0, sy = 0;
-    for (int q = 1; q <= go.ncx[i]; ++q) sx = sx + wcx[q];
-    for (int q = 1; q <= go.ncy[i]; ++q) sy = sy + wcy[q];
-    for (int q = 1; q <= go.ncx[i]; ++q) wcx[q] = wcx[q] - sx / (double)go.ncx[i];
-    for (int q = 1; q <= go.ncy[i]; ++q) wcy[q] = wcy[q] - sy / (double)go.ncy[i];
+    for (int i = n; i >= 1; --i) {
+      if (ipond[i] != 1) continue;
+      for (int k = 1; k <= f.ncface[i]; ++k) {
+        const int nck = f.C(k, i);
+        npond = npond + std::max(0, f.iwet[nck] - ipond[nck]);
+        ipond[nck] = f.iwet[nck];
+      }
+    }
   }
-  if (go.ider != 2) return;
-  std::vector<double> gxy(nmf + 1), gyx(nmf + 1);
-  std::vector<int> igx(nmf + 1), igy(nmf + 1);
-  for (int i : f.idjoint) {
-    if (f.iwet[i] == 0 && ibc == 1) { go.ngx[i] = 0; go.ngy[i] = 0; continue; }
-    igx[0] = i; igy[0] = i;
-    for (int k = 1; k <= nmf; ++k) { igx[k] = 0; igy[k] = 0; }
-    std::fill(gxy.begin(), gxy.end(), 0.0);
-    for (int j = 1; j <= f.nxface[i]; ++j) {
-      int k = f.FI(f.kxface, j, i), nck = f.C(k, i);
-      if (nck > n || std::fabs(f.dy[i] / f.dy[nck] - 1.0) < 0.1) continue;
-      if (f.iwet[nck] == 0 && ibc == 1) continue;
-      int jcn = f.FI(f.llec, k, i);
-      gxy[0] = gxy[0] + f.F(f.dsx, k, i) * (1.0 - f.F(f.fintp, k, i)) * f.F(f.rpy, k, i) / f.areap[i];
-      gxy[k] = f.F(f.dsx, k, i) * f.F(f.fintp, k, i) * f.F(f.rpy, jcn, nck) / f.areap[i];
-      igx[k] = nck;
+  for (int i = 1; i <= nD; ++i)
+    if (ipond[i] == 0 && f.iwet[i] == 1) f.iwet[i] = 0;
+}
+
+// flow_wetdry(0) (flow.F90:1231-1539) for Cartesian and telescoping grids
+// (ncellpoly = 0) without structures: depth rule, closed-boundary dummies dry,
+// narrow-channel removal (narrowchannels off) or the one-cell rule
+// (narrowchannels on), flow_pond (ponding off), corner cells, dry-to-wet
+// initialisation (5 passes, in cell order), and zero flux and viscosity on
+// every face with a dry side.
+void flow_wetdry(Flow& f) {
+  const Params& P = f.P;
+  const int n = f.n, nD = f.nD;
+  const double gravinv = 1.0 / P.grav;
+  for (int i = 1; i <= nD; ++i) {
+    f.h[i] = f.p[i] * gravinv - f.zb[i];
+    if (f.h[i] < P.hdry) {
+      f.h[i] = std::max(f.h[i], P.hmin);
+      f.iwet[i] = 0;
+    } else {
+      f.iwet[i] = 1;
     }
-    std::fill(gyx.begin(), gyx.end(), 0.0);
-    for (int j = 1; j <= f.nyface[i]; ++j) {
-      int k = f.FI(f.kyface, j, i), nck = f.C(k, i);
-      igy[k] = nck;
-      if (nck > n || std::fabs(f.dx[i] / f.dx[nck] - 1.0) < 0.1) continue;
-      if (f.iwet[nck] == 0 && ibc == 1) continue;
-      int jcn = f.FI(f.llec, k, i);
-      gyx[0] = gyx[0] + f.F(f.dsy, k, i) * (1.0 - f.F(f.fintp, k, i)) * f.F(f.rpx, k, i) / f.areap[i];
-      gyx[k] = f.F(f.dsy, k, i) * f.F(f.fintp, k, i) * f.F(f.rpx, jcn, nck) / f.areap[i];
+  }
+  for (size_t j = 0; j < f.w_cells.size(); ++j) f.iwet[f.C(f.w_faces[j], f.w_cells[j])] = 0;
+  auto dir = [&](int k, int i) { return f.FI(f.idir, k, i); };
+  if (P.narrowchannels) {
+    int nsw = 1;
+    while (nsw > 0) {
+      nsw = 0;
+      for (int i = 1; i <= n; ++i) {
+        if (f.iwet[i] == 0) continue;
+        int ksum = 0;
+        for (int k = 1; k <= f.ncface[i]; ++k) ksum += f.iwet[f.C(k, i)];
+        if (ksum == 0) { f.iwet[i] = 0; ++nsw; }
+      }
     }
-    screen(nmf, gxy.data(), gyx.data(), igx.data(), igy.data(), go.ngx[i], go.ngy[i],
-           &go.igx[(size_t)i * (nsc + 1)], &go.igy[(size_t)i * (nsc + 1)], &go.wgxy[(size_t)i * (nsc + 1)],
-           &go.wgyx[(size_t)i * (nsc + 1)]);
+  } else {
+    int nsw = 1;
+    while (nsw > 0) {
+      nsw = 0;
+      for (int i = 1; i <= n; ++i) {
+        if (f.iwet[i] == 0) continue;
+        int ksum = 0;
+        for (int k = 1; k <= f.ncface[i]; ++k) ksum += f.iwet[f.C(k, i)];
+        if (ksum <= 1) { f.iwet[i] = 0; ++nsw; }
+        int kns = 0, kew = 0;
+        for (int k = 1; k <= f.ncface[i]; ++k) {
+          const int nck = f.C(k, i), d = dir(k, i);
+          if (d == 1 || d == 3) kns += f.iwet[nck];
+          if (d == 2 || d == 4) kew += f.iwet[nck];
+        }
+        if ((kns == 0 || kew == 0) && f.h[i] < P.hdry1) { f.iwet[i] = 0; ++nsw; }
+        // a direct neighbour on side a plus the cells beyond the neighbour on side b
+        auto pair_sum = [&](int a, int b) {
+          int s = 0;
+          for (int k = 1; k <= f.ncface[i]; ++k) {
+            const int nck = f.C(k, i);
+            if (dir(k, i) == a) s += f.iwet[nck];
+            if (dir(k, i) == b)
+              for (int kk = 1; kk <= f.ncface[nck]; ++kk)
+                if (dir(kk, nck) == b) s += f.iwet[f.C(kk, nck)];
+          }
+          return s;
+        };
+        const int knss = pair_sum(1, 3);
+        if (knss == 0 && f.h[i] < P.hdry2) { f.iwet[i] = 0; ++nsw; }
+        // the north-north count (flow.F90:1384-1392) is formed but the test
+        // that follows reads knss again (flow.F90:1394)
+        if (knss == 0 && f.h[i] < P.hdry2) { f.iwet[i] = 0; ++nsw; }
+        const int keww = pair_sum(2, 4);
+        if (keww == 0 && f.h[i] < P.hdry2) { f.iwet[i] = 0; ++nsw; }
+        const int keew = pair_sum(4, 2);
+        if (keew == 0 && f.h[i] < P.hdry2) { f.iwet[i] = 0; ++nsw; }
+      }
+    }
+  }
+  if (!P.ponding) flow_pond(f);
+  for (int i = 1; i <= n; ++i) {
+    f.icorner[i] = 0;
+    if (f.iwet[i] == 1) {
+      int nd = 0;
+      for (int k = 1; k <= f.ncface[i]; ++k) if (f.iwet[f.C(k, i)] == 0) ++nd;
+      if (nd > 1) f.icorner[i] = 1;
+    }
+  }
+  for (int pass = 0; pass < 5; ++pass)
+    for (int i = 1; i <= n; ++i) {
+      if (!(f.iwet[i] == 1 && f.iwet1[i] == 0)) continue;
+      double us = 0, vs = 0, viss = 0;
+      int ns = 0;
+      for (int k = 1; k <= f.ncface[i]; ++k) {
+        const int nck = f.C(k, i);
+        us = us + f.u[nck]; vs = vs + f.v[nck]; viss = viss + f.vis[nck]; ns += f.iwet[nck];
+      }
+      f.u[i] = us / ((double)ns + P.small) / 1.25;
+      f.v[i] = vs / ((double)ns + P.small) / 1.25;
+      f.vis[i] = viss / ((double)ns + P.small);
+    }
+  for (int i = 1; i <= n; ++i)
+    for (int j = 1; j <= f.nxyface[i]; ++j) {
+      const int k = f.FI(f.kxyface, j, i), nck = f.C(k, i), jcn = f.FI(f.llec, k, i);
+      if (f.iwet[i] * f.iwet[nck] == 0) {
+        f.F(f.flux, k, i) = 0.0; f.F(f.visk, k, i) = 0.0;
+        f.F(f.flux, jcn, nck) = 0.0; f.F(f.visk, jcn, nck) = 0.0;
+      }
+    }
+}
+
+// The solver's residual weights follow iwet (natural and permuted solvers).
+void solver_set_wet(Flow& f) {
+  const int n = f.n, nD = f.nD;
+  std::vector<int> iw(nD);
+  for (int i = 1; i <= nD; ++i) iw[i - 1] = f.iwet[i];
+  orc_set_wet(f.solver, iw.data());
+  if (f.solver_perm) {
+    for (int r = 0; r < nD; ++r) iw[r] = f.iwet[(r < n ? f.perm[r] : r) + 1];
+    orc_set_wet(f.solver_perm, iw.data());
   }
 }
 
@@ -904,15 +1091,10 @@ void velface_eta(Flow& f) {
 }
 
 int flow_step(Flow& f, double dt, int maxit, int* niter_out) {
-  const double gravinv = 1.0 / f.P.grav;
-  // flow_wetdry(0) for the fixed wet set: depth update and the drying check
-  for (int i = 1; i <= f.nD; ++i) {
-    f.h[i] = f.p[i] * gravinv - f.zb[i];
-    if (f.h[i] < f.P.hdry) {
-      f.h[i] = std::max(f.h[i], f.P.hmin);
-      if (i <= f.n && f.iwet[i] == 1) return 5;  // drying is not handled
-    }
-  }
+  // wetting and drying, then the gradient weights of changed cells (flow_imp.F90:73-79)
+  flow_wetdry(f);
+  f.last_nlist = der_update(f);
+  solver_set_wet(f);
   srcsnk_static(f, dt);
   int iconv = 1, niter = 0;
   for (niter = 1; niter <= maxit; ++niter) {
@@ -946,6 +1128,7 @@ int flow_step(Flow& f, double dt, int maxit, int* niter_out) {
   fric_eval(f);
   // flow_update (CMS_Flow.f90:243-300), implicit branch
   for (int i = 1; i <= f.nD; ++i) {
+    f.iwet1[i] = f.iwet[i];
     f.u1[i] = f.u[i]; f.v1[i] = f.v[i]; f.p1[i] = f.p[i]; f.h1[i] = f.h[i];
     f.pp[i] = 0.0; f.dppx[i] = 0.0; f.dppy[i] = 0.0;
   }
@@ -992,6 +1175,7 @@ void* orcf_create(int ncells, int ncellsD, int nmf, const int* c2c, const int* n
   f->skewcor = skewcor != 0;
   geometry(*f);
   if (f->idjoint.empty()) f->skewcor = false;  // flow.F90:832
+  f->iwet1.assign(ncellsD + 1, 1);
   f->icorner.assign(ncellsD + 1, 0);
   for (int i = 1; i <= ncells; ++i) {
     int nd = 0;
@@ -1049,17 +1233,32 @@ void orcf_set_solver(void* h, int nsolv, int precond, double tol, int nswp_pp, i
   f->nsolv = nsolv; f->precond = precond; f->tol = tol; f->nswp_pp = nswp_pp; f->nswp_uv = nswp_uv; f->norm = norm;
 }
 
-// Cold start from the water level eta0 (ncellsD values) at rest (prestart.f90:302-325).
+// Cold start from the water level eta0 (ncellsD values) at rest (prestart.f90:
+// 302-325): flow_wetdry(0) (again with ponding on when every cell is dry),
+// iwet1 = iwet, and the wet-cell gradient operator of that wet set (der_init
+// builds it from the wet set of flow_init's flow_wetdry call, which sees the
+// same water level on a cold start).
 int orcf_init(void* h, const double* eta0) {
   auto* f = static_cast<Flow*>(h);
   const double g = f->P.grav, gravinv = 1.0 / g;
   for (int i = 1; i <= f->nD; ++i) {
     f->p[i] = eta0[i - 1] * g;
-    f->h[i] = f->p[i] * gravinv - f->zb[i];
-    if (f->h[i] < f->P.hdry) f->h[i] = std::max(f->h[i], f->P.hmin);
     f->u[i] = f->v[i] = 0.0;
+    f->iwet1[i] = 1;
+  }
+  flow_wetdry(*f);
+  int nwet = 0;
+  for (int i = 1; i <= f->n; ++i) nwet += f->iwet[i];
+  if (nwet == 0) {
+    f->P.ponding = true;
+    flow_wetdry(*f);
+  }
+  for (int i = 1; i <= f->nD; ++i) {
+    f->iwet1[i] = f->iwet[i];
     f->eta[i] = f->iwet[i] ? f->p[i] * gravinv : -999.0;
   }
+  build_go(*f, f->gow, 1);
+  solver_set_wet(*f);
   grad_eval(*f, f->goa, f->zb, f->dzbx, f->dzby);
   interp_c2f(*f, f->zb, 0, f->zbk, &f->dzbx, &f->dzby);
   flow_grad_interp(*f);
@@ -1071,7 +1270,7 @@ int orcf_init(void* h, const double* eta0) {
 }
 
 // One implicit time step (flow_imp + flow_update).  wsebnd: water level of each
-// TH-string cell.  Returns 0 ok, 2 divergent/non-finite, 5 drying reached.
+// TH-string cell.  Returns 0 ok, 2 divergent/non-finite.
 int orcf_step(void* h, double dt, const double* wsebnd, int maxit, int* niter, double* rmom3) {
   auto* f = static_cast<Flow*>(h);
   for (size_t j = 0; j < f->wsebnd.size(); ++j) f->wsebnd[j] = wsebnd[j];
@@ -1082,9 +1281,15 @@ int orcf_step(void* h, double dt, const double* wsebnd, int maxit, int* niter, d
 
 // Copies a state array: 0 p, 1 h, 2 u, 3 v, 4 eta, 5 vis, 6 cfrict, 7 dpx, 8 dpy
 // (ncellsD values); 100 flux, 101 visk, 102 hk, 103 acoef, 104 fintp, 105 zbk
-// ([ncellsD][nmaxfaces]).  Returns the number of values.
+// ([ncellsD][nmaxfaces]); 200 iwet, 201 icorner (as values).  Returns the
+// number of values.
 long long orcf_get(void* h, int which, double* out) {
   auto* f = static_cast<Flow*>(h);
+  if (which == 200 || which == 201) {
+    const VI& a = which == 200 ? f->iwet : f->icorner;
+    for (int i = 1; i <= f->nD; ++i) out[i - 1] = a[i];
+    return f->nD;
+  }
   const V* cell[] = {&f->p, &f->h, &f->u, &f->v, &f->eta, &f->vis, &f->cfrict, &f->dpx, &f->dpy};
   const V* face[] = {&f->flux, &f->visk, &f->hk, &f->acoef, &f->fintp, &f->zbk};
   if (which >= 0 && which < 9) {
@@ -1101,6 +1306,14 @@ long long orcf_get(void* h, int which, double* out) {
 }
 
 long long orcf_solve_iters(void* h) { return static_cast<Flow*>(h)->solve_iters; }
+// cells der_update recomputed at the start of the last step
+int orcf_last_nlist(void* h) { return static_cast<Flow*>(h)->last_nlist; }
+// ponding and narrowchannels switches (flow.F90:54-55)
+void orcf_set_wetdry(void* h, int ponding, int narrowchannels) {
+  auto* f = static_cast<Flow*>(h);
+  f->P.ponding = ponding != 0;
+  f->P.narrowchannels = narrowchannels != 0;
+}
 int orcf_njoint(void* h) { return (int)static_cast<Flow*>(h)->idjoint.size(); }
 
 }  // extern "C"

@@ -617,6 +617,13 @@ void* orc_create(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, c
 
 void orc_destroy(void* h) { delete static_cast<OracleHandle*>(h); }
 
+// Replaces the wet flags (ncellsD values) that weight the normalised residual
+// (solvers.f90:237-240 reads the module array iwet at every call).
+void orc_set_wet(void* hv, const int* iwet) {
+  auto* h = static_cast<OracleHandle*>(hv);
+  h->p.iwet.assign(iwet, iwet + h->p.ncellsD);
+}
+
 int orc_nnz(void* h) { return static_cast<OracleHandle*>(h)->p.no_zero; }
 
 // Copies the CSR pattern (1-based ia[ncells+1], ja[nnz]) built by indexm.

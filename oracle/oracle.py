@@ -116,7 +116,8 @@ class OracleSolver:
 class FlowOracle:
     """CPU restatement of one implicit flow step (flow_imp, flow_imp.F90:29-312)."""
 
-    CELL = {"p": 0, "h": 1, "u": 2, "v": 3, "eta": 4, "vis": 5, "cfrict": 6, "dpx": 7, "dpy": 8}
+    CELL = {"p": 0, "h": 1, "u": 2, "v": 3, "eta": 4, "vis": 5, "cfrict": 6, "dpx": 7, "dpy": 8, "iwet": 200,
+            "icorner": 201}
     FACE = {"flux": 100, "visk": 101, "hk": 102, "acoef": 103, "fintp": 104, "zbk": 105}
 
     def __init__(self, case, skewcor: bool = True):
@@ -139,6 +140,8 @@ class FlowOracle:
             L.orcf_solve_iters.restype = C.c_longlong
             L.orcf_njoint.argtypes = [P]
             L.orcf_set_order.argtypes = [P, i32]
+            L.orcf_last_nlist.argtypes = [P]
+            L.orcf_set_wetdry.argtypes = [P, C.c_int, C.c_int]
             L._flow_bound = True
         g = case.grid
         self.case = case
@@ -165,6 +168,10 @@ class FlowOracle:
     def set_order(self, perm):
         """Solve in another unknown order (perm[r] = natural 0-based cell of solver row r)."""
         lib().orcf_set_order(self._h, np.ascontiguousarray(perm, np.int32))
+
+    def set_wetdry(self, ponding=False, narrowchannels=False):
+        """The ponding and narrow-channel switches of the wetting and drying rules."""
+        lib().orcf_set_wetdry(self._h, int(ponding), int(narrowchannels))
 
     def init(self, eta0=None):
         if eta0 is None:
@@ -196,6 +203,11 @@ class FlowOracle:
     @property
     def solve_iters(self):
         return lib().orcf_solve_iters(self._h)
+
+    @property
+    def last_nlist(self):
+        """Cells whose gradient weights der_update recomputed at the last step."""
+        return lib().orcf_last_nlist(self._h)
 
     @property
     def njoint(self):

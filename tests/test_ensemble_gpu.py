@@ -85,3 +85,31 @@ def test_layout_autotuner_picks_a_candidate():
     info = e.step()
     assert all(i["status"] == 0 for i in info)
     e.close()
+
+
+def test_ensemble_wetting_and_drying():
+    """Intertidal members (a falling and a rising tide, Cartesian and
+    telescoping): each member's wet set and fields follow its own steps."""
+    cs = [cases.tidal_flat(seed=1, t0_hours=1.0), cases.tidal_flat(50, 36, seed=2, t0_hours=7.0, refine=True)]
+    steps = 4
+    solo, wet = [], []
+    for c in cs:
+        m = FlowModel(c, **SET)
+        m.init()
+        for _ in range(steps):
+            assert m.step()["status"] == 0
+        solo.append({k: m.get(k)[: c.grid.ncells] for k in ("eta", "u", "v")})
+        wet.append(m.get("iwet"))
+        m.close()
+    e = EnsembleModel(cs, **{k: v for k, v in SET.items() if k != "precision"})
+    e.init()
+    changed = 0
+    for _ in range(steps):
+        infos = e.step()
+        assert all(i["status"] == 0 for i in infos), infos
+        changed += sum(i["nchanged"] for i in infos)
+    assert changed > 0
+    for m, w in zip(e.members, wet):
+        assert np.array_equal(m.get("iwet"), w)
+    _compare(e, solo, cs, 1e-10, 1e-8)
+    e.close()
