@@ -67,7 +67,8 @@ struct FlowState {
   double *dpx[2], *dpy[2], *dux[2], *duy[2], *dvx[2], *dvy[2], *dppx[2], *dppy[2];
   double *dHux[2], *dHuy[2], *dHvx[2], *dHvy[2], *dapx[2], *dapy[2], *dzbx[2], *dzby[2];
   double* wsebnd;      // [nth]
-  int* flag;           // [4] device status flags: 1 non-finite, 2 depth classes changed
+  int* flag;           // [4] device status flags: 1 non-finite, 2 depth classes changed, 3 cells in chg
+  int* chg;            // [nD] cells whose depth classes changed: row | classes << 28
 };
 
 // depth h = p/g - zb with two roundings (as the host and the reference form it)
@@ -733,8 +734,9 @@ __global__ void __launch_bounds__(TPB) kf_check(FlowDev G, FlowState S) {
 // ---- wetting and drying --------------------------------------------------
 
 // Depth classes of every cell from the water level (the inputs of the wet/dry
-// rules, flow.F90:1259-1271 and 1363-1416); sets flag[2] and stores the new
-// classes when any cell's classes differ from the stored ones.
+// rules, flow.F90:1259-1271 and 1363-1416); a cell whose classes differ from
+// the stored ones stores the new ones, raises flag[2] and appends itself to
+// S.chg (count in flag[3]; at most one entry per cell per launch).
 __global__ void __launch_bounds__(TPB) kf_wet_codes(FlowDev G, FlowState S, unsigned char* code) {
   const int r = blockIdx.x * TPB + threadIdx.x;
   if (r >= G.nD) return;
@@ -743,6 +745,26 @@ __global__ void __launch_bounds__(TPB) kf_wet_codes(FlowDev G, FlowState S, unsi
   if (c != code[r]) {
     code[r] = c;
     S.flag[2] = 1;
+    S.chg[atomicAdd(&S.flag[3], 1)] = r | ((int)c << 28);
+  }
+}
+
+// Zero flux and viscosity on the faces of the listed cells that have a dry
+// side (flow.F90:1501-1524), both sides of each face.  Listing the cells that
+// became dry (and the cells of dummies that did) reaches every face the
+// reference zeroes that is not zero already: the flow step leaves flux and
+// viscosity zero on faces with a dry side.
+__global__ void __launch_bounds__(TPB) kf_wet_faces_list(FlowDev G, FlowState S, const int* list, int m) {
+  const int j = blockIdx.x * TPB + threadIdx.x;
+  if (j >= m) return;
+  const int r = list[j];
+  const int nf = G.ncface[r];
+  for (int k = 0; k < nf; ++k) {
+    const int f = fidx(G, k, r), nck = G.nb[f];
+    if (G.iwet[r] * G.iwet[nck] != 0) continue;
+    const int fb = fidx(G, G.back[f], nck);
+    S.flux[f] = 0.0; S.visk[f] = 0.0;
+    S.flux[fb] = 0.0; S.visk[fb] = 0.0;
   }
 }
 
@@ -864,6 +886,87 @@ __global__ void kf_scatter_uvv(const int* idx, int m, const double* buf, double*
   if (j >= m) return;
   const int c = idx[j];
   u[c] = buf[3 * j]; v[c] = buf[3 * j + 1]; vis[c] = buf[3 * j + 2];
+}
+
+// a[idx[j]] = v[j] (bytes)
+__global__ void kf_scatter_u8(const int* idx, const unsigned char* v, int m, unsigned char* a) {
+  const int j = blockIdx.x * TPB + threadIdx.x;
+  if (j < m) a[idx[j]] = v[j];
+}
+
+// a[idx[j]] = v[j] (ints)
+__global__ void kf_scatter_i32(const int* idx, const int* v, int m, int* a) {
+  const int j = blockIdx.x * TPB + threadIdx.x;
+  if (j < m) a[idx[j]] = v[j];
+}
+
+// ---- flow_pond on the device (flow.F90:1807-1876): connected components of
+// the wet active cells by union-find.  A root is only ever hooked under a
+// root of smaller index (compare-and-swap), and path halving only points a
+// cell at an ancestor, so a parent always has a smaller index than its child:
+// every walk up a chain ends, and the partition does not depend on the order
+// in which threads meet.  The walks are bounded all the same.
+
+constexpr int kUfLimit = 1 << 26;
+
+__device__ __forceinline__ int uf_root(int* par, int x) {
+  for (int guard = 0; guard < kUfLimit; ++guard) {
+    const int p = par[x];
+    if (p == x) return x;
+    const int gp = par[p];
+    if (gp != p) par[x] = gp;
+    x = p;
+  }
+  return x;
+}
+
+__device__ __forceinline__ void uf_union(int* par, int a, int b) {
+  int ra = uf_root(par, a), rb = uf_root(par, b);
+  for (int guard = 0; guard < kUfLimit && ra != rb; ++guard) {
+    if (ra < rb) { const int t = ra; ra = rb; rb = t; }
+    const int old = atomicCAS(&par[ra], ra, rb);
+    if (old == ra) return;
+    ra = uf_root(par, old);
+    rb = uf_root(par, rb);
+  }
+}
+
+__global__ void __launch_bounds__(TPB) kf_pond_init(int n, int* par) {
+  const int i = blockIdx.x * TPB + threadIdx.x;
+  if (i < n) par[i] = i;
+}
+
+// union of every pair of face neighbours that are both wet active cells of pn
+__global__ void __launch_bounds__(TPB) kf_pond_hook(FlowDev G, const unsigned char* pn, int* par) {
+  const int i = blockIdx.x * TPB + threadIdx.x;
+  if (i >= G.n || !pn[i]) return;
+  const int nf = G.ncface[i];
+  for (int k = 0; k < nf; ++k) {
+    const int j = G.nb[fidx(G, k, i)];
+    if (j > i && j < G.n && pn[j]) uf_union(par, i, j);
+  }
+}
+
+// components holding a wet string cell are kept
+__global__ void kf_pond_seed(const int* seeds, int m, const unsigned char* pn, int* par, unsigned char* seeded) {
+  const int j = blockIdx.x * TPB + threadIdx.x;
+  if (j >= m) return;
+  const int s = seeds[j];
+  if (pn[s]) seeded[uf_root(par, s)] = 1;
+}
+
+// final wet flags of the active cells (pn, less the unseeded components when
+// ponding is off); cells whose flag changed are appended to chg (count in cnt)
+__global__ void __launch_bounds__(TPB) kf_pond_final(int n, const unsigned char* pn, int* par,
+                                                     const unsigned char* seeded, int ponding, int* iwet, int* chg,
+                                                     int* cnt) {
+  const int i = blockIdx.x * TPB + threadIdx.x;
+  if (i >= n) return;
+  const int w = pn[i] && (ponding || seeded[uf_root(par, i)]) ? 1 : 0;
+  if (w != iwet[i]) {
+    iwet[i] = w;
+    chg[atomicAdd(cnt, 1)] = i;
+  }
 }
 
 }  // namespace cms

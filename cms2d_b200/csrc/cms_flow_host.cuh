@@ -52,6 +52,22 @@ struct cms_flow {
   double wd_ms[3] = {0, 0, 0};      // host time of the updates: read-back, rules, application
   int* d_list = nullptr;            // [n + nD] cell lists of an update (device numbering)
   double* d_buf = nullptr;          // [3 nD] gathered (u, v, vis)
+  // host copies (natural order) the incremental update works from
+  std::vector<unsigned char> code_nat, w0, pn;  // depth classes, depth set, narrow-channel set
+  cms::NarrowScratch nsc;
+  std::vector<unsigned char> wall_mem;          // [n] wet cells with a face to a dry cell or a dummy
+  std::vector<int> wall_list, corner_list;      // eddy-viscosity recurrence cells, cell order
+  std::vector<int> vpos, vlast;                 // [n] schedule-builder scratch, -1 between uses
+  // device side of the update: narrow-channel set, flow_pond's union-find
+  unsigned char* d_pn = nullptr;                // [nD] (device order)
+  int* d_par = nullptr;                         // [n] union-find parents
+  unsigned char* d_seeded = nullptr;            // [n] component holds a wet string cell
+  int* d_seedc = nullptr;                       // string cells (device rows)
+  int nseedc = 0;
+  int* d_fchg = nullptr;                        // [n] active cells whose final flag changed
+  int* d_cnt = nullptr;                         // [1] their count
+  int* d_chg = nullptr;                         // [nD] cells whose depth classes changed (kf_wet_codes)
+  int nchg_pending = 0;
   signed char* d_fslot_dev = nullptr;  // [nmf][n] ELL slot of face k of device row r
   // gradient copies: index of the current one
   int cur_dppx = 0, cur_duv = 0, cur_dH = 0, cur_dap = 0;
@@ -137,62 +153,86 @@ static int solve_core64(Solver* S, int nsolv, int nswp, cms_solve_info* info) {
   return info->status;
 }
 
-// Level schedule of an in-place natural-order recurrence over a cell list:
-// cell c reads cells reads[c]; a read of an earlier list cell must see its
-// updated value (next level), any other read sees the value before the pass.
-static void level_schedule(const std::vector<int>& list_nat, const std::vector<std::vector<std::pair<int, int>>>& reads,
-                           const std::vector<int>& n2d, std::vector<int>& lvl_start, std::vector<int>& cells_dev,
-                           std::vector<unsigned char>& rd_cur) {
-  const int m = (int)list_nat.size();
-  std::vector<int> pos_of(n2d.size(), -1), level(m, 0);
-  for (int j = 0; j < m; ++j) pos_of[list_nat[j]] = j;
-  std::vector<unsigned char> mask(m, 0);
-  for (int j = 0; j < m; ++j) {
-    int l = 0;
-    for (auto& rk : reads[j]) {  // (face k, natural cell read)
-      const int q = pos_of[rk.second];
-      if (q >= 0 && q < j) {  // an earlier list cell: read its update
-        l = std::max(l, level[q] + 1);
-        mask[j] |= (unsigned char)(1u << rk.first);
-      }
-    }
-    level[j] = l;
+// Eddy-viscosity recurrence lists (flow_eddyvis.f90:169-209): wet cells with
+// a face to a dry cell or a dummy (wall cells), and corner cells.
+static bool wall_cell(const FlowGeom& g, int i) {
+  if (g.iwet[i] != 1) return false;
+  for (int k = 0; k < g.ncface[i]; ++k) {
+    const int c = g.nb[(size_t)i * g.nmf + k];
+    if (c >= g.n || g.iwet[c] == 0) return true;
   }
-  int L = 0;
-  for (int j = 0; j < m; ++j) L = std::max(L, level[j] + 1);
-  lvl_start.assign(L + 1, 0);
-  for (int j = 0; j < m; ++j) lvl_start[level[j] + 1]++;
-  for (int l = 0; l < L; ++l) lvl_start[l + 1] += lvl_start[l];
-  cells_dev.assign(m, 0);
-  rd_cur.assign(m, 0);
-  std::vector<int> fill(lvl_start.begin(), lvl_start.end() - 1);
-  for (int j = 0; j < m; ++j) {
-    const int at = fill[level[j]]++;
-    cells_dev[at] = n2d[list_nat[j]];
-    rd_cur[at] = mask[j];
-  }
+  return false;
 }
 
-// Eddy-viscosity recurrence lists from the current wet set: wet cells next to
-// a dry or dummy neighbour, and corner cells (flow_eddyvis.f90:169-209), each
-// in level order.
-static int vis_lists(Flow* F) {
+static void vis_membership_full(Flow* F) {
+  FlowGeom& g = F->geom;
+  const int n = F->n;
+  F->wall_mem.assign(n, 0);
+  F->wall_list.clear();
+  F->corner_list.clear();
+  for (int i = 0; i < n; ++i) {
+    if (wall_cell(g, i)) { F->wall_mem[i] = 1; F->wall_list.push_back(i); }
+    if (g.icorner[i]) F->corner_list.push_back(i);
+  }
+  F->vpos.assign(n, -1);
+  F->vlast.assign(n, -1);
+}
+
+// Corner flags and list membership of the touched active cells (natural ids).
+static void vis_membership_update(Flow* F, const std::vector<int>& touched) {
+  FlowGeom& g = F->geom;
+  const int nmf = F->nmf;
+  std::vector<int> wadd, wdel, cadd, cdel;
+  for (int i : touched) {
+    int nd = 0;
+    if (g.iwet[i] == 1)
+      for (int k = 0; k < g.ncface[i]; ++k) nd += (g.iwet[g.nb[(size_t)i * nmf + k]] == 0);
+    const int corner = (g.iwet[i] == 1 && nd > 1) ? 1 : 0;
+    if (corner != g.icorner[i]) { (corner ? cadd : cdel).push_back(i); g.icorner[i] = corner; }
+    const unsigned char w = wall_cell(g, i) ? 1 : 0;
+    if (w != F->wall_mem[i]) { (w ? wadd : wdel).push_back(i); F->wall_mem[i] = w; }
+  }
+  auto merge = [](std::vector<int>& list, std::vector<int>& add, std::vector<int>& del) {
+    if (add.empty() && del.empty()) return;
+    std::sort(add.begin(), add.end());
+    std::sort(del.begin(), del.end());
+    std::vector<int> out;
+    out.reserve(list.size() + add.size());
+    size_t a = 0, d = 0;
+    for (int x : list) {
+      while (a < add.size() && add[a] < x) out.push_back(add[a++]);
+      while (d < del.size() && del[d] < x) ++d;
+      if (d < del.size() && del[d] == x) { ++d; continue; }
+      out.push_back(x);
+    }
+    while (a < add.size()) out.push_back(add[a++]);
+    list.swap(out);
+  };
+  merge(F->wall_list, wadd, wdel);
+  merge(F->corner_list, cadd, cdel);
+}
+
+// Level schedules of the two recurrences from the lists (work in the list
+// sizes): a cell is placed after every earlier list cell whose update it reads.
+// Wall cells (kf_vis_wall): reads of earlier list cells are marked in rd_cur;
+// a read of a dry active cell takes the value of the last earlier list cell
+// that wrote it (src, a face of d_wallv), and the dry cells written get their
+// last writer's value afterwards (kf_vis_wall_final).  Corner cells
+// (kf_vis_corner): reads of earlier corner cells are marked in rd_cur.
+static int vis_schedules(Flow* F) {
   const FlowGeom& g = F->geom;
   const int n = F->n, nD = F->nD, nmf = F->nmf;
   static const int kk_of[5] = {0, 3, 4, 1, 2};
   auto nbf = [&](int i, int k) { return g.nb[(size_t)i * nmf + k]; };
   auto drf = [&](int i, int k) { return g.dir[(size_t)i * nmf + k]; };
   auto wallface = [&](int i, int k) { const int c = nbf(i, k); return c >= n || g.iwet[c] == 0; };
-  // wall cells in cell order; walk them as the reference loop does, noting for
-  // every read of a dry active cell which earlier list cell wrote it last
-  std::vector<int> wl;
-  for (int i = 0; i < n; ++i) {
-    if (g.iwet[i] != 1) continue;
-    for (int k = 0; k < g.ncface[i]; ++k)
-      if (wallface(i, k)) { wl.push_back(i); break; }
-  }
+  std::vector<int>& pos = F->vpos;
+  std::vector<int>& lastw = F->vlast;
+  cudaStream_t s = F->S->stream;
+  // wall cells
+  const std::vector<int>& wl = F->wall_list;
   const int m = (int)wl.size();
-  std::vector<int> pos(n, -1), level(m, 0), lastw(n, -1), src((size_t)m * nmf, -1);
+  std::vector<int> level(m, 0), src((size_t)m * nmf, -1), written;
   std::vector<unsigned char> cur(m, 0);
   for (int p = 0; p < m; ++p) pos[wl[p]] = p;
   for (int p = 0; p < m; ++p) {
@@ -218,7 +258,10 @@ static int vis_lists(Flow* F) {
     level[p] = l;
     for (int k = 0; k < g.ncface[i]; ++k) {
       const int c = nbf(i, k);
-      if (c < n && g.iwet[c] == 0) lastw[c] = p * nmf + k;
+      if (c < n && g.iwet[c] == 0) {
+        if (lastw[c] < 0) written.push_back(c);
+        lastw[c] = p * nmf + k;
+      }
     }
   }
   int L = 0;
@@ -239,10 +282,10 @@ static int vis_lists(Flow* F) {
     }
   }
   std::vector<int> fin_c, fin_f;
-  for (int c = 0; c < n; ++c)
-    if (lastw[c] >= 0) { fin_c.push_back(F->n2d[c]); fin_f.push_back(face_dev(lastw[c])); }
+  std::sort(written.begin(), written.end());
+  for (int c : written) { fin_c.push_back(F->n2d[c]); fin_f.push_back(face_dev(lastw[c])); lastw[c] = -1; }
+  for (int p = 0; p < m; ++p) pos[wl[p]] = -1;
   F->nwall_fin = (int)fin_c.size();
-  cudaStream_t s = F->S->stream;
   if (m > 0) {
     CMS_CUDA(cudaMemcpyAsync(F->d_wall_cells, cells.data(), m * sizeof(int), cudaMemcpyHostToDevice, s));
     CMS_CUDA(cudaMemcpyAsync(F->d_wall_rd, rd.data(), m, cudaMemcpyHostToDevice, s));
@@ -254,22 +297,42 @@ static int vis_lists(Flow* F) {
     CMS_CUDA(cudaMemcpyAsync(F->d_wall_fin_faces, fin_f.data(), fin_f.size() * sizeof(int), cudaMemcpyHostToDevice,
                              s));
   }
+  // corner cells
+  const std::vector<int>& cl = F->corner_list;
+  const int mc = (int)cl.size();
+  std::vector<int> clev(mc, 0);
+  std::vector<unsigned char> ccur(mc, 0);
+  for (int p = 0; p < mc; ++p) pos[cl[p]] = p;
+  int LC = 0;
+  for (int p = 0; p < mc; ++p) {
+    const int i = cl[p];
+    int l = 0;
+    for (int k = 0; k < g.ncface[i]; ++k) {
+      const int c = nbf(i, k);
+      if (c < n && pos[c] >= 0 && pos[c] < p) {
+        ccur[p] |= (unsigned char)(1u << k);
+        l = std::max(l, clev[pos[c]] + 1);
+      }
+    }
+    clev[p] = l;
+    LC = std::max(LC, l + 1);
+  }
+  for (int p = 0; p < mc; ++p) pos[cl[p]] = -1;
+  F->corner_lvl.assign(LC + 1, 0);
+  for (int p = 0; p < mc; ++p) F->corner_lvl[clev[p] + 1]++;
+  for (int l = 0; l < LC; ++l) F->corner_lvl[l + 1] += F->corner_lvl[l];
+  std::vector<int> cfill(F->corner_lvl.begin(), F->corner_lvl.end() - 1), ccells(mc);
+  std::vector<unsigned char> crd(mc);
+  for (int p = 0; p < mc; ++p) {
+    const int q = cfill[clev[p]]++;
+    ccells[q] = F->n2d[cl[p]];
+    crd[q] = ccur[p];
+  }
+  if (mc > 0) {
+    CMS_CUDA(cudaMemcpyAsync(F->d_corner_cells, ccells.data(), mc * sizeof(int), cudaMemcpyHostToDevice, s));
+    CMS_CUDA(cudaMemcpyAsync(F->d_corner_rd, crd.data(), mc, cudaMemcpyHostToDevice, s));
+  }
   CMS_CUDA(cudaStreamSynchronize(s));  // the host vectors go out of scope
-  std::vector<int> cl;
-  std::vector<std::vector<std::pair<int, int>>> cr;
-  for (int i = 0; i < n; ++i) {
-    if (!g.icorner[i]) continue;
-    std::vector<std::pair<int, int>> reads;
-    for (int k = 0; k < g.ncface[i]; ++k) reads.push_back({k, g.nb[(size_t)i * nmf + k]});
-    cl.push_back(i);
-    cr.push_back(reads);
-  }
-  level_schedule(cl, cr, F->n2d, F->corner_lvl, cells, rd);
-  if (!cells.empty()) {
-    CMS_CUDA(cudaMemcpyAsync(F->d_corner_cells, cells.data(), cells.size() * sizeof(int), cudaMemcpyHostToDevice, s));
-    CMS_CUDA(cudaMemcpyAsync(F->d_corner_rd, rd.data(), rd.size(), cudaMemcpyHostToDevice, s));
-    CMS_CUDA(cudaStreamSynchronize(s));
-  }
   return CMS_OK;
 }
 
@@ -421,8 +484,14 @@ static int flow_create(int ncells, int ncellsD, int nmf, const int* c2c, const i
     R.ponding = F->opts.ponding != 0;
     R.narrowchannels = F->opts.narrowchannels != 0;
     if ((rc = F->alloc(&F->d_code, nD)) || (rc = F->alloc(&F->d_list, (size_t)n + nD)) ||
-        (rc = F->alloc(&F->d_buf, (size_t)3 * nD)))
+        (rc = F->alloc(&F->d_buf, (size_t)3 * nD)) || (rc = F->alloc(&F->d_pn, nD)) || (rc = F->alloc(&F->d_par, n)) ||
+        (rc = F->alloc(&F->d_seeded, n)) || (rc = F->alloc(&F->d_fchg, n)) || (rc = F->alloc(&F->d_cnt, 1)) ||
+        (rc = F->alloc(&F->d_chg, nD)))
       return fail(rc);
+    std::vector<int> sd;
+    for (int c : R.seed_cells) sd.push_back(F->n2d[c]);
+    F->nseedc = (int)sd.size();
+    if ((rc = F->upload(&F->d_seedc, sd))) return fail(rc);
   }
   // parameters (flow.F90:21-168, 684-694, friction.F90:44-49)
   const double hdry = F->opts.hdry > 0.0 ? F->opts.hdry : 0.05;
@@ -447,6 +516,7 @@ static int flow_create(int ncells, int ncellsD, int nmf, const int* c2c, const i
       if ((rc = F->alloc(a, nD))) return fail(rc);
   }
   if ((rc = F->alloc(&T.wsebnd, std::max(nth, 1))) || (rc = F->alloc(&T.flag, 4))) return fail(rc);
+  T.chg = F->d_chg;
   if ((rc = F->alloc(&F->d_wse_cell, nD))) return fail(rc);
   F->d_wse = T.wsebnd;
   if (cudaMallocHost((void**)&F->h_flag, 4 * sizeof(int)) != cudaSuccess) return fail(CMS_DEVICE_ERROR);
@@ -473,8 +543,10 @@ static int flow_create(int ncells, int ncellsD, int nmf, const int* c2c, const i
   if ((rc = F->alloc(&F->d_wall_cells, n)) || (rc = F->alloc(&F->d_wall_rd, n)) ||
       (rc = F->alloc(&F->d_wall_src, (size_t)n * nmf)) || (rc = F->alloc(&F->d_wallv, (size_t)nmf * nD)) ||
       (rc = F->alloc(&F->d_wall_fin_cells, n)) || (rc = F->alloc(&F->d_wall_fin_faces, n)) ||
-      (rc = F->alloc(&F->d_corner_cells, n)) || (rc = F->alloc(&F->d_corner_rd, n)) || (rc = vis_lists(F)))
+      (rc = F->alloc(&F->d_corner_cells, n)) || (rc = F->alloc(&F->d_corner_rd, n)))
     return fail(rc);
+  vis_membership_full(F);
+  if ((rc = vis_schedules(F))) return fail(rc);
   for (int i = 0; i < n; ++i) F->nfaces += g.ncface[i];
   if (cudaStreamSynchronize(S->stream) != cudaSuccess) return fail(CMS_DEVICE_ERROR);
   *out = F;
@@ -587,45 +659,100 @@ static int gw_rows(Flow* F, const std::vector<int>* cells) {
   return CMS_OK;
 }
 
-// Applies a new wet set (natural order, all nD cells): device flags, corner
-// cells and eddy-viscosity lists; then, except at the cold start, the rest of
-// flow_wetdry(0) and der_update (flow.F90:1473-1524, derivatives.f90:204-296):
-// dry-to-wet initialisation of u, v, vis (5 passes in cell order over the
-// newly wet cells), zero flux and viscosity on faces with a dry side, and the
-// gradient operator of every active cell whose state changed and of its
-// neighbours.  At the cold start the whole operator is built from the new set
-// (der_init).
-static int wetdry_apply(Flow* F, const std::vector<int>& neww, bool cold) {
+// Cold-start wet set (natural order, all nD cells): device flags, corner
+// flags, eddy-viscosity lists and the whole wet-cell gradient operator
+// (der_init builds it from the wet set of flow_init's flow_wetdry call).
+static int wetdry_cold(Flow* F, const std::vector<int>& neww) {
   FlowGeom& g = F->geom;
-  const int n = F->n, nD = F->nD, nmf = F->nmf;
-  cudaStream_t s = F->S->stream;
-  std::vector<int> old = g.iwet;
   g.iwet = neww;
-  int changed = 0, changed_all = 0, nwet = 0;
-  for (int i = 0; i < nD; ++i) {
-    const int d = old[i] != neww[i];
-    changed_all += d;
-    if (i < n) { changed += d; nwet += neww[i]; }
-  }
+  int nwet = 0;
+  for (int i = 0; i < F->n; ++i) nwet += neww[i];
   F->nwet = nwet;
-  F->last_changed = changed;
-  if (!cold && changed_all == 0) return CMS_OK;
+  F->last_changed = 0;
   corner_flags(g);
+  vis_membership_full(F);
+  FCHK(vis_schedules(F));
   FCHK(wet_upload(F));
-  FCHK(vis_lists(F));
-  if (cold) return gw_rows(F, nullptr);
-  if (changed == 0) return CMS_OK;  // only dummies changed: der_update looks at active cells
+  return gw_rows(F, nullptr);
+}
+
+// The rest of flow_wetdry(0) and der_update after the final wet flags of the
+// active cells in act (natural ids; the device flags already hold them) and
+// of the dummies in dum (natural ids, new flags in pn) changed
+// (flow.F90:1460-1524, derivatives.f90:204-296): corner flags and recurrence
+// lists around the changes, dry-to-wet initialisation of u, v, vis (5 passes
+// in cell order over the newly wet cells, on a gathered neighbourhood), zero
+// flux and viscosity on the faces of cells that became dry, and the gradient
+// operator rows of every changed active cell and its neighbours.
+static int wetdry_apply(Flow* F, std::vector<int>& act, const std::vector<int>& dum) {
+  FlowGeom& g = F->geom;
+  const int n = F->n, nmf = F->nmf;
+  cudaStream_t s = F->S->stream;
+  if ((int)F->nsc.mark.size() != F->nD) F->nsc.mark.assign(F->nD, 0);
+  std::sort(act.begin(), act.end());
+  std::vector<int> newly, dried;
+  for (int x : act) {
+    g.iwet[x] ^= 1;
+    (g.iwet[x] ? newly : dried).push_back(x);
+    F->nwet += g.iwet[x] ? 1 : -1;
+  }
+  F->last_changed = (int)act.size();
+  std::vector<int> parents;  // cells of changed dummies
+  if (!dum.empty()) {
+    std::vector<int> idx, val;
+    for (int x : dum) {
+      g.iwet[x] = F->pn[x];
+      idx.push_back(F->n2d[x]);
+      val.push_back(g.iwet[x]);
+      for (int k = 0; k < g.ncface[x]; ++k) {
+        const int c = g.nb[(size_t)x * nmf + k];
+        if (c >= 0 && c < n) parents.push_back(c);
+      }
+    }
+    const int m = (int)idx.size();
+    CMS_CUDA(cudaMemcpyAsync(F->d_list, idx.data(), m * sizeof(int), cudaMemcpyHostToDevice, s));
+    CMS_CUDA(cudaMemcpyAsync(F->d_list + m, val.data(), m * sizeof(int), cudaMemcpyHostToDevice, s));
+    FLAUNCH(F, (kf_scatter_i32<<<fblk(m), TPB, 0, s>>>(F->d_list, F->d_list + m, m, F->d_iwet)));
+    CMS_CUDA(cudaStreamSynchronize(s));
+  }
+  if (act.empty() && dum.empty()) return CMS_OK;
+  // corner flags and recurrence lists of the cells within one face of a change
+  {
+    std::vector<int> touched;
+    std::vector<unsigned char>& mk = F->nsc.mark;
+    auto touch = [&](int c) { if (c >= 0 && c < n && !mk[c]) { mk[c] = 1; touched.push_back(c); } };
+    for (int x : act) {
+      touch(x);
+      for (int k = 0; k < g.ncface[x]; ++k) touch(g.nb[(size_t)x * nmf + k]);
+    }
+    for (int c : parents) touch(c);
+    for (int c : touched) mk[c] = 0;
+    vis_membership_update(F, touched);
+    FCHK(vis_schedules(F));
+  }
   // dry-to-wet initialisation on the host from the gathered neighbourhood
-  std::vector<int> newly;
-  for (int i = 0; i < n; ++i)
-    if (neww[i] == 1 && old[i] == 0) newly.push_back(i);
   if (!newly.empty()) {
-    std::vector<int> pos(nD, -1), gat;
-    auto add = [&](int c) { if (pos[c] < 0) { pos[c] = (int)gat.size(); gat.push_back(c); } };
+    std::vector<int> pos_list, gat;
+    std::vector<int>& pos = F->vpos;
+    auto add = [&](int c) {
+      if (c < n) {
+        if (pos[c] < 0) { pos[c] = (int)gat.size(); gat.push_back(c); }
+      } else {
+        for (size_t q = 0; q < gat.size(); ++q)
+          if (gat[q] == c) return;
+        gat.push_back(c);
+      }
+    };
     for (int i : newly) {
       add(i);
       for (int k = 0; k < g.ncface[i]; ++k) add(g.nb[(size_t)i * nmf + k]);
     }
+    auto where = [&](int c) -> int {
+      if (c < n) return pos[c];
+      for (size_t q = 0; q < gat.size(); ++q)
+        if (gat[q] == c) return (int)q;
+      return -1;
+    };
     const int m = (int)gat.size();
     std::vector<int> gdev(m);
     for (int q = 0; q < m; ++q) gdev[q] = F->n2d[gat[q]];
@@ -640,9 +767,9 @@ static int wetdry_apply(Flow* F, const std::vector<int>& neww, bool cold) {
         double us = 0.0, vs = 0.0, viss = 0.0;
         int ns = 0;
         for (int k = 0; k < g.ncface[i]; ++k) {
-          const int c = g.nb[(size_t)i * nmf + k], q = pos[c];
+          const int c = g.nb[(size_t)i * nmf + k], q = where(c);
           us = us + buf[3 * q]; vs = vs + buf[3 * q + 1]; viss = viss + buf[3 * q + 2];
-          ns += neww[c];
+          ns += g.iwet[c];
         }
         const int q = pos[i];
         buf[3 * q] = us / ((double)ns + small) / 1.25;
@@ -656,42 +783,103 @@ static int wetdry_apply(Flow* F, const std::vector<int>& neww, bool cold) {
       gdev[j] = F->n2d[newly[j]];
       for (int c = 0; c < 3; ++c) out[3 * j + c] = buf[3 * q + c];
     }
+    for (int c : gat)
+      if (c < n) pos[c] = -1;
     CMS_CUDA(cudaMemcpyAsync(F->d_list, gdev.data(), mn * sizeof(int), cudaMemcpyHostToDevice, s));
     CMS_CUDA(cudaMemcpyAsync(F->d_buf, out.data(), out.size() * sizeof(double), cudaMemcpyHostToDevice, s));
     FLAUNCH(F, (kf_scatter_uvv<<<fblk(mn), TPB, 0, s>>>(F->d_list, mn, F->d_buf, F->st.u, F->st.v, F->st.vis)));
     CMS_CUDA(cudaStreamSynchronize(s));
   }
-  FLAUNCHB(F, fbytes(F, 1, 4), (kf_wet_faces<<<fblk(n), TPB, 0, s>>>(F->G, F->st)));
-  // der_update's list: changed active cells and their neighbours, active ones only
-  std::vector<unsigned char> chg(nD, 0);
-  for (int i = 0; i < n; ++i)
-    if (neww[i] != old[i]) {
-      chg[i] = 1;
-      for (int k = 0; k < g.ncface[i]; ++k) chg[g.nb[(size_t)i * nmf + k]] = 1;
+  // faces of the cells that became dry, and of the cells of dummies that did
+  {
+    std::vector<int> zl;
+    for (int x : dried) zl.push_back(F->n2d[x]);
+    for (int c : parents) zl.push_back(F->n2d[c]);
+    if (!zl.empty()) {
+      const int m = (int)zl.size();
+      CMS_CUDA(cudaMemcpyAsync(F->d_list, zl.data(), m * sizeof(int), cudaMemcpyHostToDevice, s));
+      FLAUNCH(F, (kf_wet_faces_list<<<fblk(m), TPB, 0, s>>>(F->G, F->st, F->d_list, m)));
+      CMS_CUDA(cudaStreamSynchronize(s));
     }
+  }
+  // der_update's list: changed active cells and their active neighbours
+  if (act.empty()) return CMS_OK;
   std::vector<int> list;
-  for (int i = 0; i < n; ++i)
-    if (chg[i]) list.push_back(F->n2d[i]);
+  std::vector<unsigned char>& mk = F->nsc.mark;
+  auto mark = [&](int c) { if (c >= 0 && c < n && !mk[c]) { mk[c] = 1; list.push_back(c); } };
+  for (int x : act) {
+    mark(x);
+    for (int k = 0; k < g.ncface[x]; ++k) mark(g.nb[(size_t)x * nmf + k]);
+  }
+  for (int& c : list) { mk[c] = 0; c = F->n2d[c]; }
   return gw_rows(F, &list);
 }
 
 // Wet/dry update at the start of a step whose depth classes changed: the
-// rules on the classes the last step ended with, then wetdry_apply.
-static int wetdry_update(Flow* F) {
+// changed classes come back as a list, the narrow-channel set is updated
+// incrementally on the host, flow_pond runs on the device (union-find over
+// the new narrow-channel set), and the changes of the final flags are
+// applied (wetdry_apply).
+static int wetdry_update(Flow* F, int nchg) {
   using clk = std::chrono::steady_clock;
   auto ms = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
   const auto t0 = clk::now();
-  const int nD = F->nD;
-  std::vector<unsigned char> cd(nD), cn(nD);
-  CMS_CUDA(cudaMemcpyAsync(cd.data(), F->d_code, nD, cudaMemcpyDeviceToHost, F->S->stream));
-  CMS_CUDA(cudaStreamSynchronize(F->S->stream));
-  for (int r = 0; r < nD; ++r) cn[F->d2n[r]] = cd[r];
+  const int n = F->n;
+  cudaStream_t s = F->S->stream;
+  std::vector<int> enc(nchg), changed;
+  if (nchg > 0) {
+    CMS_CUDA(cudaMemcpyAsync(enc.data(), F->d_chg, nchg * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CMS_CUDA(cudaStreamSynchronize(s));
+  }
+  for (int e : enc) {
+    const int x = F->d2n[e & 0x0fffffff];
+    F->code_nat[x] = (unsigned char)((unsigned)e >> 28);
+    changed.push_back(x);
+  }
   const auto t1 = clk::now();
-  std::vector<int> neww;
-  wetdry_rules(F->geom, cn.data(), F->wd, neww);
+  std::vector<int> pch;
+  narrow_update(F->geom, F->code_nat.data(), F->wd, changed, F->w0, F->pn, F->nsc, pch);
   const auto t2 = clk::now();
   F->wd_updates++;
-  const int rc = wetdry_apply(F, neww, false);
+  std::vector<int> act, dum;
+  std::vector<int> idx;
+  std::vector<unsigned char> val;
+  for (int x : pch) {
+    if (x >= n) {
+      if (F->geom.iwet[x] != F->pn[x]) dum.push_back(x);
+      continue;
+    }
+    idx.push_back(F->n2d[x]);
+    val.push_back(F->pn[x]);
+  }
+  if (!idx.empty()) {  // the active part of the narrow-channel set changed: flow_pond again
+    const int m = (int)idx.size();
+    CMS_CUDA(cudaMemcpyAsync(F->d_list, idx.data(), m * sizeof(int), cudaMemcpyHostToDevice, s));
+    CMS_CUDA(cudaMemcpyAsync(F->d_buf, val.data(), m, cudaMemcpyHostToDevice, s));
+    FLAUNCH(F, (kf_scatter_u8<<<fblk(m), TPB, 0, s>>>(F->d_list, (const unsigned char*)F->d_buf, m, F->d_pn)));
+    CMS_CUDA(cudaMemsetAsync(F->d_cnt, 0, sizeof(int), s));
+    const int ponding = F->wd.ponding ? 1 : 0;
+    if (!ponding) {
+      FLAUNCH(F, (kf_pond_init<<<fblk(n), TPB, 0, s>>>(n, F->d_par)));
+      FLAUNCH(F, (kf_pond_hook<<<fblk(n), TPB, 0, s>>>(F->G, F->d_pn, F->d_par)));
+      CMS_CUDA(cudaMemsetAsync(F->d_seeded, 0, n, s));
+      if (F->nseedc)
+        FLAUNCH(F, (kf_pond_seed<<<fblk(F->nseedc), TPB, 0, s>>>(F->d_seedc, F->nseedc, F->d_pn, F->d_par,
+                                                               F->d_seeded)));
+    }
+    FLAUNCH(F, (kf_pond_final<<<fblk(n), TPB, 0, s>>>(n, F->d_pn, F->d_par, F->d_seeded, ponding, F->d_iwet,
+                                                      F->d_fchg, F->d_cnt)));
+    int m2 = 0;
+    CMS_CUDA(cudaMemcpyAsync(&m2, F->d_cnt, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CMS_CUDA(cudaStreamSynchronize(s));
+    if (m2 > 0) {
+      act.resize(m2);
+      CMS_CUDA(cudaMemcpyAsync(act.data(), F->d_fchg, m2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+      CMS_CUDA(cudaStreamSynchronize(s));
+      for (int& r : act) r = F->d2n[r];
+    }
+  }
+  const int rc = wetdry_apply(F, act, dum);
   const auto t3 = clk::now();
   F->wd_ms[0] += ms(t0, t1); F->wd_ms[1] += ms(t1, t2); F->wd_ms[2] += ms(t2, t3);
   return rc;
@@ -704,7 +892,8 @@ static int flow_init(Flow* F, const double* eta0_nat) {
   // wet set of the cold start (prestart.f90:308-315): flow_wetdry(0), again
   // with ponding on when every cell is dry
   {
-    std::vector<unsigned char> cn(nD), cd(nD);
+    std::vector<unsigned char>& cn = F->code_nat;
+    cn.assign(nD, 0);
     for (int i = 0; i < nD; ++i) {
       const double pi = eta0_nat[i] * F->G.grav;
       const double hh = pi * F->G.gravinv - F->geom.zb[i];
@@ -712,18 +901,24 @@ static int flow_init(Flow* F, const double* eta0_nat) {
                               (hh < F->G.hdry2 ? WD_LT2 : 0));
     }
     std::vector<int> neww;
-    wetdry_rules(F->geom, cn.data(), F->wd, neww);
+    depth_set(F->geom, cn.data(), F->wd, F->w0);
+    narrow_full(F->geom, cn.data(), F->wd, F->w0, F->pn);
+    pond_host(F->geom, F->wd, F->pn, neww);
     int nwet = 0;
     for (int i = 0; i < F->n; ++i) nwet += neww[i];
     if (nwet == 0 && !F->wd.ponding) {
       F->wd.ponding = true;
-      wetdry_rules(F->geom, cn.data(), F->wd, neww);
+      pond_host(F->geom, F->wd, F->pn, neww);
     }
-    FCHK(wetdry_apply(F, neww, true));
-    for (int r = 0; r < nD; ++r) cd[r] = cn[F->d2n[r]];
+    F->nsc = NarrowScratch();
+    FCHK(wetdry_cold(F, neww));
+    std::vector<unsigned char> cd(nD), pd(nD);
+    for (int r = 0; r < nD; ++r) { cd[r] = cn[F->d2n[r]]; pd[r] = F->pn[F->d2n[r]]; }
     CMS_CUDA(cudaMemcpyAsync(F->d_code, cd.data(), nD, cudaMemcpyHostToDevice, s));
+    CMS_CUDA(cudaMemcpyAsync(F->d_pn, pd.data(), nD, cudaMemcpyHostToDevice, s));
     CMS_CUDA(cudaStreamSynchronize(s));
     F->wd_pending = 0;
+    F->nchg_pending = 0;
   }
   std::vector<double> p(nD), h(nD), eta(nD);
   for (int r = 0; r < nD; ++r) {
@@ -810,8 +1005,9 @@ static int step_begin(Flow* F, double dt, const double* wsebnd) {
   cudaStream_t s = F->S->stream;
   F->last_changed = 0;
   if (F->wd_pending) {  // flow_wetdry(0) and der_update (flow_imp.F90:73-79)
-    FCHK(wetdry_update(F));
+    FCHK(wetdry_update(F, F->nchg_pending));
     F->wd_pending = 0;
+    F->nchg_pending = 0;
   }
   if (F->nth) {  // water levels of the string, placed on the string's dummies
     CMS_CUDA(cudaMemcpyAsync(F->d_wse, wsebnd, F->nth * sizeof(double), cudaMemcpyHostToDevice, s));
@@ -887,7 +1083,8 @@ static int step_end(Flow* F, double dt, int niter, int iconv, cms_flow_info* inf
   CMS_CUDA(cudaStreamSynchronize(s));
   if (F->h_flag[2]) {
     F->wd_pending = 1;
-    CMS_CUDA(cudaMemsetAsync(T.flag + 2, 0, sizeof(int), s));
+    F->nchg_pending = F->h_flag[3];
+    CMS_CUDA(cudaMemsetAsync(T.flag + 2, 0, 2 * sizeof(int), s));
   }
   F->t_sim += dt;
   std::memset(info, 0, sizeof(*info));

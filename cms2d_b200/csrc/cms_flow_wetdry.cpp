@@ -11,7 +11,8 @@ namespace {
 // direct neighbour on one side plus the cells beyond the neighbour on the
 // other side; the north-north count of the reference is formed but its test
 // reads the south count again (flow.F90:1384-1396), so it adds no rule.
-bool removal_fires(const FlowGeom& g, const std::vector<int>& w, const unsigned char* code, int i, bool narrow) {
+template <typename W>
+bool removal_fires(const FlowGeom& g, const W& w, const unsigned char* code, int i, bool narrow) {
   const int nmf = g.nmf, nf = g.ncface[i];
   const int* nb = &g.nb[(size_t)i * nmf];
   const int* dr = &g.dir[(size_t)i * nmf];
@@ -43,41 +44,66 @@ bool removal_fires(const FlowGeom& g, const std::vector<int>& w, const unsigned 
   return pair_count(1, 3) == 0 || pair_count(2, 4) == 0 || pair_count(4, 2) == 0;
 }
 
-}  // namespace
+// calls f(c) for the active cells within two faces of active cell i (i included)
+template <typename Fn>
+void within_two(const FlowGeom& g, int i, Fn f) {
+  const int n = g.n, nmf = g.nmf;
+  f(i);
+  for (int k = 0; k < g.ncface[i]; ++k) {
+    const int c = g.nb[(size_t)i * nmf + k];
+    if (c < 0 || c >= n) continue;
+    f(c);
+    for (int kk = 0; kk < g.ncface[c]; ++kk) {
+      const int c2 = g.nb[(size_t)c * nmf + kk];
+      if (c2 >= 0 && c2 < n) f(c2);
+    }
+  }
+}
 
-void wetdry_rules(const FlowGeom& g, const unsigned char* code, const WetDryRules& R, std::vector<int>& iwet) {
-  const int n = g.n, nD = g.nD, nmf = g.nmf;
-  iwet.assign(nD, 0);
-  for (int i = 0; i < nD; ++i) iwet[i] = (code[i] & WD_WET) ? 1 : 0;
-  for (int i = 0; i < nD; ++i)
-    if (R.closed[i]) iwet[i] = 0;
-  // narrow channels: worklist to the fixed point
-  std::vector<int> stack;
-  std::vector<unsigned char> queued(n, 0);
-  stack.reserve(n);
-  for (int i = n - 1; i >= 0; --i)
-    if (iwet[i]) { stack.push_back(i); queued[i] = 1; }
-  auto requeue = [&](int c) {
-    if (c >= 0 && c < n && iwet[c] && !queued[c]) { queued[c] = 1; stack.push_back(c); }
-  };
+// removals to the fixed point from the queued cells (worklist)
+void remove_to_fixed_point(const FlowGeom& g, const unsigned char* code, bool narrow, std::vector<unsigned char>& pn,
+                           std::vector<int>& stack, std::vector<unsigned char>& queued, std::vector<int>* removed) {
   while (!stack.empty()) {
     const int i = stack.back();
     stack.pop_back();
     queued[i] = 0;
-    if (!iwet[i] || !removal_fires(g, iwet, code, i, R.narrowchannels)) continue;
-    iwet[i] = 0;
+    if (!pn[i] || !removal_fires(g, pn, code, i, narrow)) continue;
+    pn[i] = 0;
+    if (removed) removed->push_back(i);
     // every cell whose counts include i lies within two faces of it
-    for (int k = 0; k < g.ncface[i]; ++k) {
-      const int c = g.nb[(size_t)i * nmf + k];
-      requeue(c);
-      if (c >= 0 && c < n)
-        for (int kk = 0; kk < g.ncface[c]; ++kk) requeue(g.nb[(size_t)c * nmf + kk]);
-    }
+    within_two(g, i, [&](int c) {
+      if (pn[c] && !queued[c]) { queued[c] = 1; stack.push_back(c); }
+    });
   }
+}
+
+}  // namespace
+
+void depth_set(const FlowGeom& g, const unsigned char* code, const WetDryRules& R, std::vector<unsigned char>& w0) {
+  w0.assign(g.nD, 0);
+  for (int i = 0; i < g.nD; ++i) w0[i] = (!R.closed[i] && (code[i] & WD_WET)) ? 1 : 0;
+}
+
+void narrow_full(const FlowGeom& g, const unsigned char* code, const WetDryRules& R,
+                 const std::vector<unsigned char>& w0, std::vector<unsigned char>& pn) {
+  const int n = g.n;
+  pn = w0;
+  std::vector<int> stack;
+  std::vector<unsigned char> queued(g.nD, 0);
+  stack.reserve(n);
+  for (int i = n - 1; i >= 0; --i)
+    if (pn[i]) { stack.push_back(i); queued[i] = 1; }
+  remove_to_fixed_point(g, code, R.narrowchannels, pn, stack, queued, nullptr);
+}
+
+void pond_host(const FlowGeom& g, const WetDryRules& R, const std::vector<unsigned char>& pn, std::vector<int>& iwet) {
+  const int n = g.n, nD = g.nD, nmf = g.nmf;
+  iwet.assign(nD, 0);
+  for (int i = 0; i < nD; ++i) iwet[i] = pn[i];
   if (R.ponding) return;
   // flow_pond: wet cells reachable from the string seeds through wet active cells
   std::vector<unsigned char> pond(nD, 0);
-  stack.clear();
+  std::vector<int> stack;
   for (size_t j = 0; j < R.seed_cells.size(); ++j) {
     const int c = R.seed_cells[j], d = R.seed_dummies[j];
     if (iwet[d]) pond[d] = 1;
@@ -95,6 +121,85 @@ void wetdry_rules(const FlowGeom& g, const unsigned char* code, const WetDryRule
   }
   for (int i = 0; i < nD; ++i)
     if (!pond[i]) iwet[i] = 0;
+}
+
+void wetdry_rules(const FlowGeom& g, const unsigned char* code, const WetDryRules& R, std::vector<int>& iwet) {
+  std::vector<unsigned char> w0, pn;
+  depth_set(g, code, R, w0);
+  narrow_full(g, code, R, w0, pn);
+  pond_host(g, R, pn, iwet);
+}
+
+void narrow_update(const FlowGeom& g, const unsigned char* code, const WetDryRules& R,
+                   const std::vector<int>& changed, std::vector<unsigned char>& w0, std::vector<unsigned char>& pn,
+                   NarrowScratch& sc, std::vector<int>& pchanged) {
+  const int n = g.n, nD = g.nD;
+  if ((int)sc.mark.size() != nD) { sc.mark.assign(nD, 0); sc.queued.assign(nD, 0); }
+  std::vector<int>& cand = sc.list;
+  std::vector<int>& stack = sc.stack;
+  cand.clear();
+  stack.clear();
+  // new depth set; dummies take it as their final state (no rule touches
+  // them), and a dummy that changes acts on the cells within two faces of it
+  // through its cell
+  std::vector<int> leavers, wetter_dummies;
+  for (int x : changed) {
+    const unsigned char nw = (!R.closed[x] && (code[x] & WD_WET)) ? 1 : 0;
+    w0[x] = nw;
+    if (x >= n) {
+      if (pn[x] != nw) {
+        pn[x] = nw;
+        pchanged.push_back(x);
+        (nw ? wetter_dummies : leavers).push_back(x);
+      }
+      continue;
+    }
+    if (pn[x] && !nw) leavers.push_back(x);
+  }
+  auto around = [&](int x, auto f) {  // cells within two faces of x (through its cell for a dummy)
+    if (x < n) { within_two(g, x, f); return; }
+    for (int k = 0; k < g.ncface[x]; ++k) {
+      const int c = g.nb[(size_t)x * g.nmf + k];
+      if (c >= 0 && c < n) within_two(g, c, f);
+    }
+  };
+  // candidates: removed (or newly depth-wet) cells linked to a changed cell
+  // through removed cells within two faces of each other
+  auto removed_cell = [&](int c) { return w0[c] && !pn[c]; };
+  for (int x : changed)
+    if (x < n && removed_cell(x) && !sc.mark[x]) { sc.mark[x] = 1; cand.push_back(x); }
+  for (int x : wetter_dummies)
+    around(x, [&](int c) {
+      if (!sc.mark[c] && removed_cell(c)) { sc.mark[c] = 1; cand.push_back(c); }
+    });
+  for (size_t q = 0; q < cand.size(); ++q)
+    within_two(g, cand[q], [&](int c) {
+      if (!sc.mark[c] && removed_cell(c)) { sc.mark[c] = 1; cand.push_back(c); }
+    });
+  // tentative set: previous kept cells minus leavers plus candidates
+  for (int x : leavers)
+    if (x < n) { pn[x] = 0; pchanged.push_back(x); }
+  for (int c : cand) {
+    sc.mark[c] = 0;
+    pn[c] = 1;
+    if (!sc.queued[c]) { sc.queued[c] = 1; stack.push_back(c); }
+  }
+  auto enqueue = [&](int c) {
+    if (pn[c] && !sc.queued[c]) { sc.queued[c] = 1; stack.push_back(c); }
+  };
+  for (int x : changed)
+    if (x < n) enqueue(x);
+  for (int x : leavers) around(x, enqueue);
+  std::vector<int> removed;
+  remove_to_fixed_point(g, code, R.narrowchannels, pn, stack, sc.queued, &removed);
+  // net changes of the candidates: re-added ones that stayed, and removals of
+  // cells that were kept before (a candidate removed again is no change)
+  for (int c : cand) sc.mark[c] = 1;
+  for (int c : cand)
+    if (pn[c]) pchanged.push_back(c);
+  for (int x : removed)
+    if (!sc.mark[x]) pchanged.push_back(x);
+  for (int c : cand) sc.mark[c] = 0;
 }
 
 }  // namespace cms

@@ -71,3 +71,42 @@ def test_closed_dummies_dry_string_dummies_follow_depth():
     walls = np.setdiff1d(np.arange(n, g.ncellsD), th_d)
     assert np.all(w[walls] == 0)
     assert np.array_equal(w[th_d], _depth_wet(c, eta)[th_d])
+
+
+def _dump(case, code, path):
+    g = case.grid
+    with open(path, "wb") as f:
+        np.array([g.ncells, g.ncellsD, g.nmaxfaces], np.int32).tofile(f)
+        g.ncface.astype(np.int32).tofile(f)
+        (g.cell2cell.astype(np.int32) - 1).tofile(f)
+        g.idirface.astype(np.int32).tofile(f)
+        code.astype(np.uint8).tofile(f)
+        np.array([case.th_cells.size], np.int32).tofile(f)
+        d = g.cell2cell[case.th_cells - 1, case.th_faces - 1] - 1
+        np.stack([case.th_cells - 1, d], 1).astype(np.int32).tofile(f)
+
+
+@pytest.mark.parametrize("refine", [False, True])
+def test_incremental_narrow_update_equals_full(tmp_path, refine):
+    """The step's incremental update of the narrow-channel set against the full
+    recomputation, over 300 random batches of depth-class changes per mode."""
+    import os
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = str(tmp_path / "wdinc")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(root, "cms2d_b200", "csrc"), "-I",
+                    os.path.join(root, "include"), "-o", exe, os.path.join(root, "tests", "wetdry_incremental_check.cpp"),
+                    os.path.join(root, "cms2d_b200", "csrc", "cms_flow_wetdry.cpp")], check=True)
+    c = cases.tidal_flat(60, 40, seed=3, refine=refine)
+    n = c.grid.ncells
+    rng = np.random.default_rng(1)
+    zb = c.zb.copy()
+    zb[:n] = rng.uniform(-0.35, 0.25, n)
+    h = 0.0 - zb
+    code = (h >= 0.05) * 1 | (h < 0.25) * 2 | (h < 0.1) * 4
+    path = str(tmp_path / "grid.bin")
+    _dump(c, code, path)
+    for narrow in ("0", "1"):
+        out = subprocess.run([exe, path, narrow], capture_output=True, text=True)
+        assert out.returncode == 0, (narrow, out.stdout, out.stderr)
+        assert int(out.stdout.split()[3]) > 1000  # the batches did change the set
