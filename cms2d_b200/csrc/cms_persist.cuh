@@ -373,7 +373,11 @@ __device__ __forceinline__ void spmv_rows(const PersistArgs<T>& A, T (&y)[NR], c
 // the backward phase of group 0 also forms the following SpMV for its rows
 // (MODE 0: u = A z and u.r0 into dots[0]; MODE 1: v = A z, v.r and v.v into
 // dots[0..1]): those rows couple only to later groups, whose z is final, and
-// the gathered neighbour values serve both sums.
+// the gathered neighbour values serve both sums.  Group-0 rows have no lower
+// couplings, so ILU(0) leaves them as they are in A (both k_ilu0 and
+// k_ilu0_relax): u_rk = -aoff and u_rr = diag, and that phase reads aoff and
+// diag only (w + aoff z rounds exactly as w - luoff z, and 1/diag is the
+// stored invd).
 template <typename T, int MODE>
 __device__ __forceinline__ void pc_apply(const PersistArgs<T>& A, PhaseState& ph, const int* s_lo, const int* s_pre,
                                          double omg_d, double alf_d, double gam_d, bool pending,
@@ -447,12 +451,11 @@ __device__ __forceinline__ void pc_apply(const PersistArgs<T>& A, PhaseState& ph
     if (rr.y > rr.x) wait_neighbours(A, ph);
     if (g == 0 && A.spmv0) {
       for_rows<NR>(rr.x, rr.y, [&](const int (&r)[NR], const bool (&ok)[NR]) {
-        T w[NR], iv[NR], dg[NR], d1[NR], sa[NR], r0v[NR];
+        T w[NR], dg[NR], d1[NR], sa[NR], r0v[NR];
         int ku[NR];
 #pragma unroll
         for (int q = 0; q < NR; ++q) {
           w[q] = ldm(&A.z[r[q]]);
-          iv[q] = __ldg(&A.invd[r[q]]);
           dg[q] = __ldg(&A.diag[r[q]]);
           d1[q] = MODE == 0 ? ldm(&A.r0[r[q]]) : ldm(&A.r[r[q]]);
           if (MODE == 1 && A.fuse_upd) r0v[q] = ldm(&A.r0[r[q]]);
@@ -467,8 +470,9 @@ __device__ __forceinline__ void pc_apply(const PersistArgs<T>& A, PhaseState& ph
               const size_t e = (size_t)(A.KL + t) * A.n + r[q];
               if (t < ku[q]) {
                 const T zk = __ldcg(&A.z[__ldg(&A.col[e])]);
-                w[q] = w[q] - __ldg(&A.luoff[e]) * zk;
-                sa[q] = sa[q] + __ldg(&A.aoff[e]) * zk;
+                const T a = __ldg(&A.aoff[e]);
+                w[q] = w[q] + a * zk;
+                sa[q] = sa[q] + a * zk;
               }
             }
           }
@@ -476,7 +480,7 @@ __device__ __forceinline__ void pc_apply(const PersistArgs<T>& A, PhaseState& ph
 #pragma unroll
         for (int q = 0; q < NR; ++q) {
           if (!ok[q]) continue;
-          const T zr = iv[q] * w[q];
+          const T zr = (T(1) / dg[q]) * w[q];
           const T y = dg[q] * zr - sa[q];
           A.z[r[q]] = zr;
           if (MODE == 0) {

@@ -505,11 +505,16 @@ static double persist_bytes(const Solver* S, int iters, bool xzero, bool relax, 
     fwd += El * (s + 4) + (El > 0 ? R * s : 0.0);  // factor entries, columns, gathered values
     const bool last = fuse && (g == P.G - 1 || (relax && g >= 1));
     if (last) fwd += R * s;                         // invd
-    else bwd += R * s * 3 + Eu * (s + 4) + (Eu > 0 ? R * s : 0.0);
+    if (g == 0 && spmv0) {
+      // backward step of group 0 fused with its SpMV rows: z, diag, dot
+      // operand in; z, output out; A's entries (the factor's rows of group 0
+      // are A's), columns, gathered values
+      bwd += R * s * 5 + Eu * (s + 4) + (Eu > 0 ? R * s : 0.0);
+      continue;
+    }
+    if (!last) bwd += R * s * 3 + Eu * (s + 4) + (Eu > 0 ? R * s : 0.0);
     // SpMV: diag, own value, output, dot operand, matrix entries, columns, gathers
-    const double sp = R * s * 4 + (El + Eu) * (s + 4) + (El + Eu > 0 ? R * s : 0.0);
-    if (g == 0 && spmv0) bwd += R * s * 3 + Eu * s;  // diag, output, dot operand, A's entries
-    else spmv_rest += sp;
+    spmv_rest += R * s * 4 + (El + Eu) * (s + 4) + (El + Eu > 0 ? R * s : 0.0);
   }
   // forward right-hand sides: p-update reads r, p, u, writes p, z (5); x/r
   // update reads z, x, r, u, writes x, r, z (7)
