@@ -153,7 +153,7 @@ static int refine_batched(Ens* E, const std::vector<int>& act, const std::vector
       KLAUNCH(S, P_VEC, (double)n * 12,
               (k_ir_scale<<<gsz(n), TPB, 0, S->stream>>>(n, S->W64.r, S->W32.b, S->d_st)));
       CMS_CUDA(cudaMemsetAsync(&S->d_st->bar, 0, sizeof(GridBar), S->stream));
-      CMS_CUDA(cudaMemsetAsync(S->d_progress, 0, sizeof(unsigned int) * E->tiles[i], S->stream));
+      CMS_CUDA(cudaMemsetAsync(S->d_progress, 0, sizeof(unsigned int) * E->tiles[i] * kProgressStride, S->stream));
       E->h_args[c] = make_args<float>(S, S->A32, S->W32, E->tiles[i], R[j].imax, 2, R[j].itol, 1);
       for (int t = 0; t < E->tiles[i]; ++t) E->h_bmap[blocks++] = make_int2(c, t);
       CMS_CUDA(cudaEventRecord(E->ev_m[i], S->stream));

@@ -11,7 +11,9 @@
 // Ordering between phases.  Rows of a tile are coupled only to rows of a few
 // neighbouring tiles (dep lists, built on the host from the pattern, and
 // symmetric).  Each block publishes how many phases it has completed
-// (progress[t], a release store after every phase); before a phase in which
+// (progress[t * kProgressStride], a release store after every phase; one
+// counter per 128-byte line, so that a tile's stores do not disturb the line
+// other tiles are polling for their neighbours); before a phase in which
 // it has rows, it waits until every neighbour has completed all earlier
 // phases (acquire loads).  So a block reads neighbour values only after they
 // are written, and a neighbour never writes its rows of a phase while this
@@ -45,6 +47,7 @@
 namespace cms {
 
 constexpr unsigned int kSpinLimit = 1u << 22;
+constexpr int kProgressStride = 32;  // unsigned ints between two tiles' progress counters (128 bytes)
 constexpr int NSMAX = 6;  // sums per reduction (partial-sum buffer stride)
 
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
@@ -80,7 +83,7 @@ struct PersistArgs {
   const int* toff;         // [G][ntiles+1] tile row ranges per group
   const int* dep_ptr;      // [ntiles+1]
   const int* dep_idx;      // neighbour tiles of each tile
-  unsigned int* progress;  // [ntiles] phases completed per tile (zero at launch)
+  unsigned int* progress;  // [ntiles * kProgressStride] phases completed per tile (zero at launch)
   const int* col;
   const signed char* nlo;
   const signed char* nup;
@@ -122,7 +125,7 @@ __device__ __forceinline__ void wait_neighbours(const PersistArgs<T>& A, PhaseSt
     int fail = 0;
     const int d0 = A.dep_ptr[A.tile], d1 = A.dep_ptr[A.tile + 1];
     for (int i = d0 + (int)threadIdx.x; i < d1 && !fail; i += 32) {
-      const unsigned int* f = A.progress + A.dep_idx[i];
+      const unsigned int* f = A.progress + (size_t)A.dep_idx[i] * kProgressStride;
       unsigned int spins = 0;
       while (ld_acquire(f) < ph.done) {
         if (++spins > kSpinLimit) { atomicExch(&A.bar->err, 1); fail = 1; break; }
@@ -142,7 +145,7 @@ __device__ __forceinline__ void end_phase(const PersistArgs<T>& A, PhaseState& p
   __syncthreads();
   ++ph.done;
   ph.fresh = false;
-  if (threadIdx.x == 0) st_release(A.progress + A.tile, ph.done);
+  if (threadIdx.x == 0) st_release(A.progress + (size_t)A.tile * kProgressStride, ph.done);
 }
 
 // Grid-wide barrier on a monotone arrival counter.

@@ -475,7 +475,7 @@ static int build_tiles(Solver* S, int nt) {
     if (S->alloc(&S->d_dep_idx, didx.size() + 1)) return 0;
     S->cap_dep = didx.size() + 1;
   }
-  if (!S->d_dep_ptr && (S->alloc(&S->d_dep_ptr, GRID_CAP + 1) || S->alloc(&S->d_progress, GRID_CAP))) return 0;
+  if (!S->d_dep_ptr && (S->alloc(&S->d_dep_ptr, GRID_CAP + 1) || S->alloc(&S->d_progress, (size_t)GRID_CAP * kProgressStride))) return 0;
   cudaStream_t s = S->stream;
   if (cudaMemcpyAsync(S->d_toff, toff.data(), toff.size() * sizeof(int), cudaMemcpyHostToDevice, s) ||
       cudaMemcpyAsync(S->d_dep_ptr, dptr.data(), dptr.size() * sizeof(int), cudaMemcpyHostToDevice, s) ||
@@ -560,7 +560,7 @@ static int run_bicgstab_persistent(Solver* S, Mat<T>& A, Work<T>& W, int tiles, 
                                    int xzero) {
   PersistArgs<T> a = make_args<T>(S, A, W, tiles, maxit, norm, tol, xzero);
   CMS_CUDA(cudaMemsetAsync(&S->d_st->bar, 0, sizeof(GridBar), S->stream));
-  CMS_CUDA(cudaMemsetAsync(S->d_progress, 0, sizeof(unsigned int) * tiles, S->stream));
+  CMS_CUDA(cudaMemsetAsync(S->d_progress, 0, sizeof(unsigned int) * tiles * kProgressStride, S->stream));
   void* args[] = {&a};
   prof_begin(S);
   const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_bicg_persistent<T>, dim3(tiles), dim3(TPB), args,
