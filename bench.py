@@ -306,10 +306,10 @@ FLOW_SOLVER = dict(nsolv=3, tol=1e-6, norm=2)
 
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the
 # persistent FP32 BiCGStab kernel per Krylov iteration on a 1M-unknown system,
-# from one ncu capture of its two launches in a 1M solve (733.3 MB over 23
+# from one ncu capture of its two launches in a 1M solve (746.2 MB over 23
 # iterations; profiles/bicgstab_persistent_solve_1M.md).  The roofline's
 # traffic is this figure times the iterations of an average launch.
-PERSIST_DRAM_BYTES_PER_ITER = 733.29e6 / 23
+PERSIST_DRAM_BYTES_PER_ITER = 746.17e6 / 23
 
 
 PERSIST_CAPTURE_UNKNOWNS = 1_000_405
