@@ -1290,13 +1290,17 @@ long long orcf_get(void* h, int which, double* out) {
     for (int i = 1; i <= f->nD; ++i) out[i - 1] = a[i];
     return f->nD;
   }
+  if (which == 202) {  // cell area (geo_def areap)
+    for (int i = 1; i <= f->nD; ++i) out[i - 1] = f->areap[i];
+    return f->nD;
+  }
   const V* cell[] = {&f->p, &f->h, &f->u, &f->v, &f->eta, &f->vis, &f->cfrict, &f->dpx, &f->dpy};
-  const V* face[] = {&f->flux, &f->visk, &f->hk, &f->acoef, &f->fintp, &f->zbk};
+  const V* face[] = {&f->flux, &f->visk, &f->hk, &f->acoef, &f->fintp, &f->zbk, &f->dsxy};
   if (which >= 0 && which < 9) {
     for (int i = 1; i <= f->nD; ++i) out[i - 1] = (*cell[which])[i];
     return f->nD;
   }
-  if (which >= 100 && which < 106) {
+  if (which >= 100 && which < 107) {
     const V& a = *face[which - 100];
     for (int i = 1; i <= f->nD; ++i)
       for (int k = 1; k <= f->nmf; ++k) out[(size_t)(i - 1) * f->nmf + k - 1] = a[(size_t)i * f->NF + k];
