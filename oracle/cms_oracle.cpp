@@ -543,17 +543,238 @@ SolveStats pgmres(Pattern& p, Work<R>& wk, int nmaxiter, const R* acoef, const R
   return st;
 }
 
+// ---------------------------------------------------------------------------
+// The MATRIX_SOLVER options other than BiCGStab and GMRES, as the serial loops
+// the reference runs with its default single OpenMP thread.
+
+// One Gauss-Seidel pass over cells i0, i0+step, ... up to i1 (inclusive):
+// gauss_seidel / gauss_seidel_SOR, gauss-seidel.f90:2-75 (sor: relaxsor blend).
+template <typename R>
+void gs_pass(Pattern& p, const R* acoef, const R* ap, const R* su, R* phi, int i0, int i1, int step, bool sor,
+             R relaxsor) {
+  const int nmf = p.nmaxfaces;
+  const R com = R(1.0) - relaxsor;
+  for (int i = i0; step > 0 ? i <= i1 : i >= i1; i += step) {
+    R term = R(0);
+    for (int k = 1; k <= p.ncface[i - 1]; ++k) term = term + acoef[(size_t)(i - 1) * nmf + k - 1] * phi[c2c(p, k, i) - 1];
+    if (sor) phi[i - 1] = relaxsor * (term + su[i - 1]) / ap[i - 1] + com * phi[i - 1];
+    else phi[i - 1] = (term + su[i - 1]) / ap[i - 1];
+  }
+}
+
+// nsweeps forward passes (gauss_seidel, gauss_seidel_SOR), or nsweeps/2
+// forward+backward pairs (solv_sgs, solv_ssor, gauss-seidel.f90:191-262).
+template <typename R>
+SolveStats gauss_seidel(Pattern& p, int nsweeps, bool symmetric, bool sor, R relaxsor, const R* acoef, const R* ap,
+                        const R* su, R* phi) {
+  const int n = p.ncells;
+  SolveStats st{0, 0, 0.0};
+  const int reps = symmetric ? nsweeps / 2 : nsweeps;
+  for (int it = 0; it < reps; ++it) {
+    gs_pass(p, acoef, ap, su, phi, 1, n, 1, sor, relaxsor);
+    if (symmetric) gs_pass(p, acoef, ap, su, phi, n, 1, -1, sor, relaxsor);
+  }
+  st.iters = st.inner = reps;
+  return st;
+}
+
+// The 5-point solvers read exactly the four compass slots (1 N, 2 E, 3 S, 4 W)
+// of every cell; the reference runs them on Cartesian grids only (flow.F90:
+// 749-751 switches to GMRES when the grid has refinement joints).
+inline bool five_point(Pattern& p) {
+  if (p.nmaxfaces < 4) return false;
+  for (int i = 1; i <= p.ncells; ++i) {
+    if (p.ncface[i - 1] != 4) return false;
+    for (int k = 1; k <= 4; ++k)
+      if (c2c(p, k, i) < 1 || c2c(p, k, i) > p.ncellsD) return false;
+  }
+  return true;
+}
+
+template <typename R>
+R sum4(Pattern& p, const R* acoef, const R* v, int i) {
+  R t = R(0);
+  for (int k = 1; k <= 4; ++k) t = t + acoef[(size_t)(i - 1) * p.nmaxfaces + k - 1] * v[c2c(p, k, i) - 1];
+  return t;
+}
+
+// sip5: source/solvers/sip.f90:2-174 (Stone's strongly implicit procedure,
+// alpha 0.92; stops after more than nmaxiter/2 iterations once the RMS
+// residual fell below 1e-3 of the first, or when it grew tenfold).
+template <typename R>
+SolveStats sip5(Pattern& p, int nmaxiter, const R* acoef, const R* ap, const R* b, R* phi) {
+  const int n = p.ncells, nD = p.ncellsD, nmf = p.nmaxfaces;
+  SolveStats st{0, 0, 0.0};
+  const R alpha = R(0.92), resmax = R(0.001);
+  const int nitermin = nmaxiter / 2;
+  std::vector<R> Lw(nD, R(0)), Ls(nD, R(0)), Lpr(nD, R(0)), r(nD, R(0)), Un(nD, R(0)), Ue(nD, R(0)), res(nD, R(0));
+  auto a = [&](int k, int i) { return acoef[(size_t)(i - 1) * nmf + k - 1]; };
+  for (int i = 1; i <= n; ++i) {
+    const int ncs = c2c(p, 3, i), ncw = c2c(p, 4, i);
+    Lw[i - 1] = -a(3, i) / (R(1.0) + alpha * Un[ncs - 1]);
+    Ls[i - 1] = -a(4, i) / (R(1.0) + alpha * Ue[ncw - 1]);
+    const R term1 = alpha * Lw[i - 1] * Un[ncs - 1];
+    const R term2 = alpha * Ls[i - 1] * Ue[ncw - 1];
+    Lpr[i - 1] = R(1.0) / (ap[i - 1] + term1 + term2 - (Ls[i - 1] * Un[ncw - 1] + Lw[i - 1] * Ue[ncs - 1]));
+    Un[i - 1] = -(a(2, i) + term1) * Lpr[i - 1];
+    Ue[i - 1] = -(a(1, i) + term2) * Lpr[i - 1];
+  }
+  R res0 = R(0);
+  for (int niter = 1; niter <= nmaxiter; ++niter) {
+    R ressum = R(0);
+    for (int i = 1; i <= n; ++i) {
+      res[i - 1] = b[i - 1] + sum4(p, acoef, phi, i) - ap[i - 1] * phi[i - 1];
+      ressum = ressum + res[i - 1] * res[i - 1];
+    }
+    const R resn = std::sqrt(ressum / R(n));
+    if (niter == 1) res0 = resn;
+    for (int i = 1; i <= n; ++i)
+      r[i - 1] = Lpr[i - 1] * (res[i - 1] - Lw[i - 1] * r[c2c(p, 3, i) - 1] - Ls[i - 1] * r[c2c(p, 4, i) - 1]);
+    for (int i = n; i >= 1; --i)
+      r[i - 1] = r[i - 1] - Ue[i - 1] * r[c2c(p, 1, i) - 1] - Un[i - 1] * r[c2c(p, 2, i) - 1];
+    for (int i = 1; i <= n; ++i) phi[i - 1] = phi[i - 1] + r[i - 1];
+    const R rsm = resn / std::max(res0, R(1.0e-6));
+    st.iters = st.inner = niter;
+    st.relres = (double)rsm;
+    if (niter > nitermin && rsm < resmax) return st;
+    if (rsm > R(10.0)) return st;
+  }
+  return st;
+}
+
+// iccg5: source/solvers/iccg.f90:2-184 (conjugate gradients preconditioned by
+// the diagonal incomplete Cholesky factor of the 5-point matrix; stopping test
+// as sip5 on the L1 residual ratio).
+template <typename R>
+SolveStats iccg5(Pattern& p, int nmaxiter, const R* acoef, const R* ap, const R* b, R* phi) {
+  const int n = p.ncells, nD = p.ncellsD, nmf = p.nmaxfaces;
+  SolveStats st{0, 0, 0.0};
+  const int nitermin = nmaxiter / 2;
+  const R resmax = R(0.001);
+  std::vector<R> res(nD, R(0)), d(nD, R(0)), zk(nD, R(0)), pk(nD, R(0));
+  auto a = [&](int k, int i) { return acoef[(size_t)(i - 1) * nmf + k - 1]; };
+  R res0 = R(0);
+  for (int i = 1; i <= n; ++i) {
+    res[i - 1] = b[i - 1] + sum4(p, acoef, phi, i) - ap[i - 1] * phi[i - 1];
+    res0 = res0 + std::abs(res[i - 1]);
+  }
+  for (int i = 1; i <= n; ++i) {
+    const R aw = a(4, i), as = a(3, i);
+    const R dr = ap[i - 1] - d[c2c(p, 4, i) - 1] * aw * aw - d[c2c(p, 3, i) - 1] * as * as;
+    d[i - 1] = R(1.0) / std::max(dr, R(1.0e-3));
+  }
+  R s0 = R(1.0e20);
+  for (int niter = 1; niter <= nmaxiter; ++niter) {
+    for (int i = 1; i <= n; ++i)
+      zk[i - 1] = (res[i - 1] + a(4, i) * zk[c2c(p, 4, i) - 1] + a(3, i) * zk[c2c(p, 3, i) - 1]) * d[i - 1];
+    for (int i = 1; i <= n; ++i) zk[i - 1] = zk[i - 1] / d[i - 1];
+    for (int i = n; i >= 1; --i)
+      zk[i - 1] = (zk[i - 1] + a(2, i) * zk[c2c(p, 2, i) - 1] + a(1, i) * zk[c2c(p, 1, i) - 1]) * d[i - 1];
+    R sk = R(0), s2 = R(0), resn = R(0);
+    for (int i = 1; i <= n; ++i) sk = sk + res[i - 1] * zk[i - 1];
+    const R beta = sk / std::max(s0, R(1.0e-10));
+    for (int i = 1; i <= n; ++i) pk[i - 1] = zk[i - 1] + beta * pk[i - 1];
+    for (int i = 1; i <= n; ++i) {
+      zk[i - 1] = ap[i - 1] * pk[i - 1] - sum4(p, acoef, pk.data(), i);
+      s2 = s2 + pk[i - 1] * zk[i - 1];
+    }
+    const R alpha = sk / std::max(s2, R(1.0e-10));
+    for (int i = 1; i <= n; ++i) {
+      phi[i - 1] = phi[i - 1] + alpha * pk[i - 1];
+      res[i - 1] = res[i - 1] - alpha * zk[i - 1];
+      resn = resn + std::abs(res[i - 1]);
+    }
+    s0 = sk;
+    const R resm = resn / std::max(res0, R(1.0e-10));
+    st.iters = st.inner = niter;
+    st.relres = (double)resm;
+    if (niter > nitermin && resm < resmax) return st;
+    if (resm > R(10.0)) return st;
+  }
+  return st;
+}
+
+// iccgstab5: source/solvers/iccgstab.f90:2-163 (BiCGStab preconditioned by the
+// same diagonal incomplete factor, without the 1e-3 pivot floor).
+template <typename R>
+SolveStats iccgstab5(Pattern& p, int nmaxiter, const R* acoef, const R* ap, const R* b, R* phi) {
+  const int n = p.ncells, nD = p.ncellsD, nmf = p.nmaxfaces;
+  SolveStats st{0, 0, 0.0};
+  const R resmax = R(0.001), tiny = R(1.0e-20);
+  std::vector<R> res(nD, R(0)), d(nD, R(0)), zk(nD, R(0)), pk(nD, R(0)), uk(nD, R(0)), vk(nD, R(0)), reso(nD, R(0));
+  auto a = [&](int k, int i) { return acoef[(size_t)(i - 1) * nmf + k - 1]; };
+  R res0 = R(0);
+  for (int i = 1; i <= n; ++i) {
+    res[i - 1] = b[i - 1] + sum4(p, acoef, phi, i) - ap[i - 1] * phi[i - 1];
+    res0 = res0 + std::abs(res[i - 1]);
+  }
+  for (int i = 1; i <= n; ++i) {
+    const R aw = a(4, i), as = a(3, i);
+    d[i - 1] = R(1.0) / (ap[i - 1] - d[c2c(p, 4, i) - 1] * aw * aw - d[c2c(p, 3, i) - 1] * as * as);
+    d[i - 1] = d[i - 1] + tiny;
+  }
+  for (int i = 0; i < n; ++i) reso[i] = res[i];
+  auto precond = [&](const std::vector<R>& y) {
+    for (int i = 1; i <= n; ++i)
+      zk[i - 1] = (y[i - 1] + a(4, i) * zk[c2c(p, 4, i) - 1] + a(3, i) * zk[c2c(p, 3, i) - 1]) * d[i - 1];
+    for (int i = 1; i <= n; ++i) zk[i - 1] = zk[i - 1] / (d[i - 1] + tiny);
+    for (int i = n; i >= 1; --i)
+      zk[i - 1] = (zk[i - 1] + a(2, i) * zk[c2c(p, 2, i) - 1] + a(1, i) * zk[c2c(p, 1, i) - 1]) * d[i - 1];
+  };
+  R alf = R(1.0), beto = R(1.0), gam = R(1.0);
+  for (int niter = 1; niter <= nmaxiter; ++niter) {
+    R bet = R(0);
+    for (int i = 0; i < n; ++i) bet = bet + res[i] * reso[i];
+    const R om = bet * gam / (alf * beto + tiny);
+    beto = bet;
+    for (int i = 0; i < n; ++i) pk[i] = res[i] + om * (pk[i] - alf * uk[i]);
+    precond(pk);
+    for (int i = 1; i <= n; ++i) uk[i - 1] = ap[i - 1] * zk[i - 1] - sum4(p, acoef, zk.data(), i);
+    R ukreso = R(0);
+    for (int i = 0; i < n; ++i) ukreso = ukreso + uk[i] * reso[i];
+    gam = bet / (ukreso + tiny);
+    for (int i = 0; i < n; ++i) {
+      phi[i] = phi[i] + gam * zk[i];
+      res[i] = res[i] - gam * uk[i];
+    }
+    precond(res);
+    for (int i = 1; i <= n; ++i) vk[i - 1] = ap[i - 1] * zk[i - 1] - sum4(p, acoef, zk.data(), i);
+    R vres = R(0), vv = R(0);
+    for (int i = 0; i < n; ++i) {
+      vres = vres + vk[i] * res[i];
+      vv = vv + vk[i] * vk[i];
+    }
+    alf = vres / (vv + tiny);
+    R resn = R(0);
+    for (int i = 0; i < n; ++i) {
+      phi[i] = phi[i] + alf * zk[i];
+      res[i] = res[i] - alf * vk[i];
+      resn = resn + std::abs(res[i]);
+    }
+    const R resm = resn / std::max(res0, R(1.0e-10));
+    st.iters = st.inner = niter;
+    st.relres = (double)resm;
+    if (resm < resmax) return st;
+  }
+  return st;
+}
+
 struct OracleHandle {
   Pattern p;
   Work<double> wd;
   Work<float> wf;
 };
 
-// solve: source/solvers/solvers.f90:205-304 (nsolv 3 = BiCGStab, 4 = GMRES).
+// solve: source/solvers/solvers.f90:205-304.  nsolv: 1 Gauss-Seidel, 2 SGS /
+// SSOR, 3 BiCGStab, 4 GMRES, 5 hybrid BiCGStab / Gauss-Seidel, 6 SIP, 7 ICCG
+// (pressure) / SIP, 8 ICCG (pressure) / ICCGSTAB (solvers.f90:242-289).  n is
+// the variable index (1 pressure correction, 2-3 velocity, 4 sediment, 5
+// salinity or heat; 0 none), relaxsor the SOR constant and nswp0_vel the
+// velocity iteration count the hybrid solver scales for n = 4, 5.
 template <typename R>
 int solve_impl(OracleHandle* h, Work<R>& wk, const R* acoef, R* ss, const R* sp, R* res, R* phi, R relax, int nswp,
                int nsolv, int precond, R tol, int lfil, R droptol, R permtol, R* rmom, int* iters, int* inner,
-               double* relres, int norm) {
+               double* relres, int norm, int n_var = 0, R relaxsor = R(1.8), int nswp0_vel = 5) {
   Pattern& p = h->p;
   const int n = p.ncells, nmf = p.nmaxfaces;
   std::vector<R> ap(n);
@@ -571,9 +792,27 @@ int solve_impl(OracleHandle* h, Work<R>& wk, const R* acoef, R* ss, const R* sp,
   }
   *rmom = std::sqrt(adak(n, res) / R(n));
   SolveStats st{0, 0, 0.0};
-  if (nsolv == 3) st = pbicgstab(p, wk, nswp, acoef, ap.data(), ss, phi, precond, tol, lfil, droptol, permtol, norm);
-  else if (nsolv == 4) st = pgmres(p, wk, nswp, acoef, ap.data(), ss, phi, precond, tol, lfil, droptol, permtol);
-  else return -1;
+  const R rm = *rmom;  // rmom(n); the pressure tests below read rmom(1) only when n == 1
+  if (nsolv == 1) {
+    st = gauss_seidel(p, nswp, false, false, relaxsor, acoef, ap.data(), ss, phi);
+  } else if (nsolv == 2) {
+    st = gauss_seidel(p, nswp, true, n_var == 1 && rm < R(1.0e-3), relaxsor, acoef, ap.data(), ss, phi);
+  } else if (nsolv == 3 || (nsolv == 5 && n_var == 1 && rm > R(1.0e-4))) {
+    st = pbicgstab(p, wk, nswp, acoef, ap.data(), ss, phi, precond, tol, lfil, droptol, permtol, norm);
+  } else if (nsolv == 4) {
+    st = pgmres(p, wk, nswp, acoef, ap.data(), ss, phi, precond, tol, lfil, droptol, permtol);
+  } else if (nsolv == 5) {
+    // nswp(1:3) = 4 nswp0(1:3), nswp(4:5) = 3 nswp0(2:3) for the Gauss-Seidel branch
+    const int sweeps = n_var >= 4 ? 3 * nswp0_vel : 4 * nswp;
+    st = gauss_seidel(p, sweeps, false, n_var == 1 && rm < R(1.0e-3), relaxsor, acoef, ap.data(), ss, phi);
+  } else if (nsolv >= 6 && nsolv <= 8) {
+    if (!five_point(p)) return -1;
+    if (nsolv == 6 || (nsolv == 7 && n_var != 1)) st = sip5(p, nswp, acoef, ap.data(), ss, phi);
+    else if (n_var == 1) st = iccg5(p, nswp, acoef, ap.data(), ss, phi);
+    else st = iccgstab5(p, nswp, acoef, ap.data(), ss, phi);
+  } else {
+    return -1;
+  }
   *iters = st.iters;
   *inner = st.inner;
   *relres = st.relres;
@@ -661,6 +900,26 @@ int orc_solve_f(void* hv, const float* acoef, float* ss, const float* sp, float*
 
 // Applies the factor built by the last orc_solve_* call: x = (LU)^-1 y (lusol,
 // sparse.f90:237-264).  y, x: 0-based arrays of length ncells.
+// solve() with the variable index and the settings the nsolv = 1, 2, 5-8
+// branches read (relaxsor: flow.F90:131; nswp0_vel: nswp0(2)).
+int orc_solve_n_d(void* hv, int n, const double* acoef, double* ss, const double* sp, double* res, double* phi,
+                  double relax, int nswp, int nsolv, double relaxsor, int nswp0_vel, int precond, double tol,
+                  double* rmom, int* iters, int* inner, double* relres, int norm) {
+  auto* h = static_cast<OracleHandle*>(hv);
+  const int lfil = nsolv == 4 ? 8 : 35;
+  return solve_impl<double>(h, h->wd, acoef, ss, sp, res, phi, relax, nswp, nsolv, precond, tol, lfil, 1e-3, 0.5,
+                            rmom, iters, inner, relres, norm, n, relaxsor, nswp0_vel);
+}
+
+int orc_solve_n_f(void* hv, int n, const float* acoef, float* ss, const float* sp, float* res, float* phi,
+                  float relax, int nswp, int nsolv, float relaxsor, int nswp0_vel, int precond, float tol,
+                  float* rmom, int* iters, int* inner, double* relres, int norm) {
+  auto* h = static_cast<OracleHandle*>(hv);
+  const int lfil = nsolv == 4 ? 8 : 35;
+  return solve_impl<float>(h, h->wf, acoef, ss, sp, res, phi, relax, nswp, nsolv, precond, tol, lfil, 1e-3f, 0.5f,
+                           rmom, iters, inner, relres, norm, n, relaxsor, nswp0_vel);
+}
+
 void orc_lusol_d(void* hv, const double* y, double* x) {
   auto* h = static_cast<OracleHandle*>(hv);
   int n = h->p.ncells;

@@ -54,6 +54,12 @@ def lib():
         L.orc_solve_f.argtypes = [P, f32p, f32p, f32p, f32p, f32p, C.c_float, C.c_int, C.c_int, C.c_int, C.c_float,
                                   C.c_int, C.c_float, C.c_float, fp, ip, ip, dp, C.c_int]
         L.orc_solve_f.restype = C.c_int
+        L.orc_solve_n_d.argtypes = [P, C.c_int, f64p, f64p, f64p, f64p, f64p, C.c_double, C.c_int, C.c_int,
+                                    C.c_double, C.c_int, C.c_int, C.c_double, dp, ip, ip, dp, C.c_int]
+        L.orc_solve_n_d.restype = C.c_int
+        L.orc_solve_n_f.argtypes = [P, C.c_int, f32p, f32p, f32p, f32p, f32p, C.c_float, C.c_int, C.c_int,
+                                    C.c_float, C.c_int, C.c_int, C.c_float, fp, ip, ip, dp, C.c_int]
+        L.orc_solve_n_f.restype = C.c_int
         L.orc_lusol_d.argtypes = [P, f64p, f64p]
         _LIB = L
     return _LIB
@@ -89,12 +95,25 @@ class OracleSolver:
         return ia, ja
 
     def solve(self, acoef, ss, sp, res, phi, relax=1.0, nswp=15, nsolv=3, precond=PC_ILU0, tol=1e-3, lfil=None,
-              droptol=1e-3, permtol=0.5, norm=1):
+              droptol=1e-3, permtol=0.5, norm=1, n=None, relaxsor=1.8, nswp0_vel=5):
         """Arguments mirror solve(acoef,ss,sp,res,phi,n): ss, res and phi are updated in place.
 
+        n (the variable index), relaxsor and nswp0_vel select the branches of
+        nsolv = 1, 2, 5, 6, 7, 8 (solvers.f90:242-289); nsolv 3 and 4 ignore them.
         Returns dict(status, rmom, iters, inner, relres).
         """
         L = lib()
+        if n is not None or nsolv not in (3, 4):
+            dt = acoef.dtype
+            rm = (C.c_double if dt == np.float64 else C.c_float)()
+            it = C.c_int(); inner = C.c_int(); rr = C.c_double()
+            fn = L.orc_solve_n_d if dt == np.float64 else L.orc_solve_n_f
+            for a in (acoef, ss, sp, res, phi):
+                assert a.dtype == dt and a.flags.c_contiguous
+            st = fn(self._h, int(n or 0), acoef, ss, sp, res, phi, relax, int(nswp), int(nsolv), relaxsor,
+                    int(nswp0_vel), int(precond), tol, C.byref(rm), C.byref(it), C.byref(inner), C.byref(rr),
+                    int(norm))
+            return dict(status=st, rmom=rm.value, iters=it.value, inner=inner.value, relres=rr.value)
         if lfil is None:
             lfil = 8 if nsolv == 4 else 35  # solvers.f90:195-199
         dt = acoef.dtype
@@ -117,8 +136,8 @@ class FlowOracle:
     """CPU restatement of one implicit flow step (flow_imp, flow_imp.F90:29-312)."""
 
     CELL = {"p": 0, "h": 1, "u": 2, "v": 3, "eta": 4, "vis": 5, "cfrict": 6, "dpx": 7, "dpy": 8, "iwet": 200,
-            "icorner": 201}
-    FACE = {"flux": 100, "visk": 101, "hk": 102, "acoef": 103, "fintp": 104, "zbk": 105}
+            "icorner": 201, "areap": 202}
+    FACE = {"flux": 100, "visk": 101, "hk": 102, "acoef": 103, "fintp": 104, "zbk": 105, "dsxy": 106}
 
     def __init__(self, case, skewcor: bool = True):
         L = lib()
