@@ -11,6 +11,10 @@ implicit time step (all SIMPLEC outer iterations until check_conv).  The
 headline runs the solves in FP32 inside FP64 iterative refinement; the plain
 FP64 drop-in runs the same steps in the same process for comparison.
 
+Workload "solvers": one solve() call per MATRIX_SOLVER option (Gauss-Seidel,
+SGS, BiCGStab, GMRES, SIP, ICCG, ICCGSTAB) on a symmetric Cartesian system of
+--cells unknowns, FP64, at the reference's default nswp(n); ms per call.
+
 Workload "solve": the pressure-correction system of the solver sweep at 1M
 unknowns (telescoping 5-point stencil with up to two extra neighbours per face
 at refinement interfaces, seeded off-diagonals in [-1,-0.1], diagonal 1.02 x
@@ -277,6 +281,103 @@ def cpu_baseline(args, g, acoef, ss, sp, phi, threads=None):
             "sample": f"1 full solve of the same {g.ncells}-unknown system, natural-order ILU0-BiCGStab "
                       f"(serial factor/sweeps as in the reference), {out['iters']} iterations",
             "iters": out["iters"]}
+
+
+# MATRIX_SOLVER options timed by the "solvers" workload: (nsolv, n, ordering),
+# nswp(n) at the reference's defaults for that solver (flow.F90:752-821)
+SOLVER_OPTIONS = [(3, 1, "multicolor"), (4, 1, "multicolor"), (1, 1, "multicolor"), (1, 1, "natural"),
+                  (2, 2, "multicolor"), (2, 2, "natural"), (6, 1, "natural"), (7, 1, "multicolor"),
+                  (7, 1, "natural"), (8, 2, "multicolor"), (8, 2, "natural")]
+SOLVER_LABEL = {1: "Gauss-Seidel", 2: "SGS", 3: "BiCGStab", 4: "GMRES", 6: "SIP", 7: "ICCG", 8: "ICCGSTAB"}
+
+
+def symmetric_cartesian_system(nx: int, ny: int, seed: int):
+    """Cartesian grid with the solver-sweep values made symmetric (the face
+    coefficient of a cell pair is shared), so that every option, ICCG included,
+    sees a symmetric positive definite pressure-correction-like system."""
+    from cms2d_b200 import grid as G
+    g = G.cartesian_grid(nx, ny)
+    acoef, ss, sp, phi = G.random_system(g, seed=seed)
+    n = g.ncells
+    for k, kb in ((2, 0), (3, 1)):  # south face = the south neighbour's north face; west = west's east
+        j = g.cell2cell[:n, k].astype(np.int64) - 1
+        m = j < n
+        acoef[:n, k][m] = acoef[j[m], kb]
+    sp[:n] = -0.02 * acoef[:n].sum(axis=1)
+    return g, acoef, ss, sp, phi
+
+
+def run_solvers_ours(args):
+    """ms per solve() call for each MATRIX_SOLVER option on one system."""
+    import torch
+    from cms2d_b200 import solver as S
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    side = int(round(args.cells ** 0.5))
+    g, acoef, ss, sp, phi = symmetric_cartesian_system(side, side, seed=17)
+    N = g.ncells
+    t_acoef = torch.from_numpy(acoef).to(dev)
+    t_sp = torch.from_numpy(sp).to(dev)
+    t_ss0 = torch.from_numpy(ss).to(dev)
+    t_phi0 = torch.from_numpy(phi).to(dev)
+    t_ss = t_ss0.clone(); t_phi = t_phi0.clone(); t_res = torch.zeros_like(t_ss)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    rows = []
+    with ClockSampler(local) as clk:
+        for nsolv, n, ordering in SOLVER_OPTIONS:
+            solver = S.Solver(g, ordering=ordering, precision="fp64", verify=False, nsolv=nsolv)
+            sstream = torch.cuda.ExternalStream(solver.stream_handle, device=dev)
+            nswp = S.NSWP_DEFAULT[nsolv][n]
+            ms, info = 0.0, None
+            for q in range(args.warmup + args.steps):
+                t_ss.copy_(t_ss0); t_phi.copy_(t_phi0); flush.fill_(1.0)
+                torch.cuda.synchronize(dev)
+                e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(sstream)
+                info = solver.solve(t_acoef, t_ss, t_sp, t_res, t_phi, n=n, relax=1.0, nswp=nswp, nsolv=nsolv,
+                                    raise_on_error=False)
+                e1.record(sstream)
+                e1.synchronize()
+                if q >= args.warmup:
+                    ms += e0.elapsed_time(e1)
+            solver.set_options(verify=True)
+            t_ss.copy_(t_ss0); t_phi.copy_(t_phi0)
+            chk = solver.solve(t_acoef, t_ss, t_sp, t_res, t_phi, n=n, relax=1.0, nswp=nswp, nsolv=nsolv,
+                               raise_on_error=False)
+            rows.append({"nsolv": nsolv, "solver": SOLVER_LABEL[nsolv], "n": n, "ordering": ordering,
+                         "nswp": nswp, "groups": solver.ncolors, "ms_per_solve": round(ms / args.steps, 3),
+                         "iters": info["iters"], "status": info["status"],
+                         "true_relres": chk["true_relres"]})
+            solver.close()
+    out = {"metric": "ms per solve() call by MATRIX_SOLVER option (FP64, nswp(n) of the reference defaults)",
+           "value": None, "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded symmetric solver-sweep values on a Cartesian grid)",
+           "config": {"workload": f"solve() of a {side}x{side} Cartesian system ({N} unknowns), every "
+                                  f"MATRIX_SOLVER option", "cells": N,
+                      "l2": "flushed between solves (256 MB write)"},
+           "options": rows, "clocks": clk.summary()}
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        O.set_threads(1)
+        o = O.OracleSolver(g)
+        cpu = []
+        for nsolv, n, ordering in SOLVER_OPTIONS:
+            if ordering != "natural" and nsolv not in (3, 4):
+                continue
+            a, b, c, p = [x.copy() for x in (acoef, ss, sp, phi)]
+            t0 = time.perf_counter()
+            r = o.solve(a, b, c, np.zeros_like(b), p, relax=1.0, nswp=S.NSWP_DEFAULT[nsolv][n], nsolv=nsolv, n=n,
+                        precond=O.PC_ILU0)
+            cpu.append({"nsolv": nsolv, "n": n, "ms_per_solve": round(1e3 * (time.perf_counter() - t0), 1),
+                        "iters": r["iters"]})
+        out["cpu_baseline"] = {"unit": "ms per solve", "cores": 1, "kind": "port",
+                               "sample": "one solve per option, natural order (the reference's serial loops, "
+                                         "ILU0 for BiCGStab/GMRES)", "options": cpu}
+    print(json.dumps(out), flush=True)
 
 
 def run_solve_reference(args):
@@ -706,7 +807,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="flow", choices=["flow", "solve", "ensemble"])
+    ap.add_argument("--workload", default="flow", choices=["flow", "solve", "ensemble", "solvers"])
     ap.add_argument("--members", type=int, default=64, help="ensemble: basins")
     ap.add_argument("--ens-min", type=int, default=50_000, help="ensemble: smallest basin (cells)")
     ap.add_argument("--ens-max", type=int, default=400_000, help="ensemble: largest basin (cells)")
@@ -729,7 +830,13 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.workload == "ensemble":
+    if args.workload == "solvers":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the solvers workload reports its CPU arm "
+                                                                  "in its own line (cpu_baseline)"}))
+            return
+        run_solvers_ours(args)
+    elif args.workload == "ensemble":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the ensemble workload has no CPU arm"}))
             return

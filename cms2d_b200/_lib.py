@@ -23,7 +23,7 @@ class SolverOpts(C.Structure):
     _fields_ = [("ordering", C.c_int), ("precision", C.c_int), ("norm", C.c_int), ("tol", C.c_double),
                 ("max_iters", C.c_int), ("inner_tol", C.c_double), ("inner_max", C.c_int),
                 ("max_refine", C.c_int), ("verify", C.c_int), ("multi_kernel", C.c_int),
-                ("inner_relax", C.c_int)]
+                ("inner_relax", C.c_int), ("relaxsor", C.c_double), ("nswp0_vel", C.c_int)]
 
 
 class SolveInfo(C.Structure):
@@ -71,6 +71,8 @@ def lib():
         for dev in ("", "dev_"):
             fn = getattr(L, f"cms_solver_solve_{dev}{name}")
             fn.argtypes = [vp, vp, vp, vp, vp, vp, real, i, i, C.POINTER(SolveInfo)]
+            fn = getattr(L, f"cms_solver_solve_{dev}n_{name}")
+            fn.argtypes = [vp, i, vp, vp, vp, vp, vp, real, i, i, C.POINTER(SolveInfo)]
     L.cms_solver_ncolors.argtypes = [vp]
     L.cms_solver_device_bytes.argtypes = [vp]
     L.cms_solver_device_bytes.restype = C.c_size_t

@@ -19,6 +19,7 @@
 
 #include "cms_common.cuh"
 #include "cms_krylov.cuh"
+#include "cms_legacy.cuh"
 #include "cms_order.h"
 #include "cms_persist.cuh"
 #include "cmsgpu.h"
@@ -92,6 +93,12 @@ struct cms_solver {
   size_t cap_toff = 0, cap_dep = 0;  // capacities of d_toff / d_dep_idx
   int cur_relax = 0;  // the FP32 factor in A32 is the two-phase one (k_ilu0_relax)
   int cur_fuse = 0;   // inner solves of refinement: update folded into the next iteration
+  // MATRIX_SOLVER options 1, 2, 5-8: compass table (built on first use),
+  // its properties (-1 not built) and the 5-point solvers' scratch
+  int* d_cmp = nullptr;
+  int leg_props = -1;
+  double* leg64 = nullptr;
+  float* leg32 = nullptr;
   cms::Staging<double> S64;
   cms::Staging<float> S32;
   size_t bytes = 0;
@@ -672,6 +679,10 @@ static int run_krylov(Solver* S, Mat<T>& A, Work<T>& W, int nsolv, int maxit, in
   return CMS_UNSUPPORTED;
 }
 
+}  // namespace cms
+#include "cms_legacy_host.cuh"
+namespace cms {
+
 // FP64 residual norm^2 of the device-order system into slot (A in TA, x in TX).
 template <typename TA, typename TX>
 static int resid64(Solver* S, Mat<TA>& A, const double* b, const TX* x, double* rout, float* rout32, int slot) {
@@ -750,19 +761,36 @@ static int run_refine(Solver* S, int nsolv, int maxit, double tol, cms_solve_inf
 // The whole solve() on device-resident natural-order arrays.
 template <typename T>
 static int solve_dev(Solver* S, const T* acoef, T* ss, const T* sp, T* res, T* phi, T relax, int nswp, int nsolv,
-                     cms_solve_info* info) {
+                     cms_solve_info* info, int nvar = 0) {
   const HostPattern& P = S->hp;
   cms_solve_info loc{};
   if (!info) info = &loc;
   std::memset(info, 0, sizeof(*info));
   info->ncolors = P.G;
   info->true_relres = -1.0;
-  if (nsolv != 3 && nsolv != 4) return info->status = CMS_UNSUPPORTED;
+  if (nsolv < 0 || nsolv > 8) return info->status = CMS_UNSUPPORTED;
+  const bool legacy = nsolv != 3 && nsolv != 4;
+  if (nsolv >= 6) {
+    const int props = legacy_props(S);
+    if (props < 0) return info->status = CMS_DEVICE_ERROR;
+    const int kind = legacy_plan(nsolv, nvar, 0.0, nswp, S->opts.nswp0_vel).kind;
+    if (!(props & LEG_FIVE_POINT)) {
+      std::snprintf(g_last_error, sizeof(g_last_error),
+                    "nsolv %d: the 5-point solvers need exactly four faces (N, E, S, W) per cell", nsolv);
+      return info->status = CMS_UNSUPPORTED;
+    }
+    if (kind == LK_SIP && !(props & LEG_SIP_ORDER)) {
+      std::snprintf(g_last_error, sizeof(g_last_error),
+                    "nsolv %d: SIP runs in the natural ordering of a grid numbered row by row from the south-west",
+                    nsolv);
+      return info->status = CMS_UNSUPPORTED;
+    }
+  }
   const int maxit = S->opts.max_iters > 0 ? S->opts.max_iters : nswp;
   const double tol = S->opts.tol > 0 ? S->opts.tol : 1e-3;
   const int norm = S->opts.norm == 2 ? 2 : 1;
   int prec = S->opts.precision;
-  if (sizeof(T) == 4) prec = CMS_PREC_FP32;
+  if (sizeof(T) == 4 || legacy) prec = sizeof(T) == 4 ? CMS_PREC_FP32 : CMS_PREC_FP64;
   const bool is64 = sizeof(T) == 8;
   Mat<T>& A = *reinterpret_cast<Mat<T>*>(is64 ? (void*)&S->A64 : (void*)&S->A32);
   Work<T>& W = *reinterpret_cast<Work<T>*>(is64 ? (void*)&S->W64 : (void*)&S->W32);
@@ -786,10 +814,30 @@ static int solve_dev(Solver* S, const T* acoef, T* ss, const T* sp, T* res, T* p
       CHK((resid64<float, float>(S, S->A32, S->W64.r, S->W32.x, nullptr, nullptr, S_TRUE0)));
     }
   }
-  if (is64 && prec == CMS_PREC_FP32_REFINE) {
-    CHK(run_refine(S, nsolv, maxit, tol, info));
+  LegPlan plan;
+  int leg_sweeps = 0;
+  if (legacy) {
+    double rm = 0.0;
+    if (nsolv == 2 || nsolv == 5) {  // the branch reads this call's rmom
+      CMS_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, S->stream));
+      CMS_CUDA(cudaStreamSynchronize(S->stream));
+      rm = S->h_st->s[S_RMOM];
+    }
+    plan = legacy_plan(nsolv, nvar, rm, maxit, S->opts.nswp0_vel);
+  }
+  if (plan.kind == LK_NONE) {
+  } else if (plan.kind == LK_GS) {
+    CHK(run_gauss_seidel<T>(S, A, W, plan.sweeps, plan.symmetric, plan.sor, S->opts.relaxsor, &leg_sweeps));
+  } else if (plan.kind == LK_SIP) {
+    CHK(run_sip<T>(S, A, W, acoef, maxit));
+  } else if (plan.kind == LK_ICCG) {
+    CHK(run_iccg<T>(S, A, W, maxit));
+  } else if (plan.kind == LK_ICCGSTAB) {
+    CHK(run_iccgstab<T>(S, A, W, maxit));
+  } else if (is64 && prec == CMS_PREC_FP32_REFINE) {
+    CHK(run_refine(S, legacy ? 3 : nsolv, maxit, tol, info));
   } else {
-    CHK(run_krylov<T>(S, A, W, nsolv, maxit, norm, tol, 0));
+    CHK(run_krylov<T>(S, A, W, legacy ? 3 : nsolv, maxit, norm, tol, 0));
   }
   if (S->opts.verify) {
     if (is64) CHK((resid64<double, double>(S, S->A64, S->W64.b, S->W64.x, nullptr, nullptr, S_TRUE1)));
@@ -801,7 +849,9 @@ static int solve_dev(Solver* S, const T* acoef, T* ss, const T* sp, T* res, T* p
   CMS_CUDA(cudaStreamSynchronize(S->stream));
   const DevState& h = *S->h_st;
   info->rmom = h.s[S_RMOM];
-  if (!(is64 && prec == CMS_PREC_FP32_REFINE)) {
+  if (plan.kind == LK_GS || plan.kind == LK_NONE) {
+    info->iters = info->inner = leg_sweeps;  // fixed sweep count, no stopping test
+  } else if (!(is64 && prec == CMS_PREC_FP32_REFINE)) {
     info->iters = h.iter;
     info->inner = (nsolv == 4) ? h.inner : h.iter;
     info->relres = h.s[S_RELRES];
@@ -818,7 +868,7 @@ static int solve_dev(Solver* S, const T* acoef, T* ss, const T* sp, T* res, T* p
 
 template <typename T>
 static int solve_host(Solver* S, const T* acoef, T* ss, const T* sp, T* res, T* phi, T relax, int nswp, int nsolv,
-                      cms_solve_info* info) {
+                      cms_solve_info* info, int nvar = 0) {
   const bool is64 = sizeof(T) == 8;
   Staging<T>& st = *reinterpret_cast<Staging<T>*>(is64 ? (void*)&S->S64 : (void*)&S->S32);
   CHK(alloc_staging<T>(S, st));
@@ -828,7 +878,7 @@ static int solve_host(Solver* S, const T* acoef, T* ss, const T* sp, T* res, T* 
   CMS_CUDA(cudaMemcpyAsync(st.ss, ss, nD * sizeof(T), cudaMemcpyHostToDevice, s));
   CMS_CUDA(cudaMemcpyAsync(st.sp, sp, nD * sizeof(T), cudaMemcpyHostToDevice, s));
   CMS_CUDA(cudaMemcpyAsync(st.phi, phi, nD * sizeof(T), cudaMemcpyHostToDevice, s));
-  const int rc = solve_dev<T>(S, st.acoef, st.ss, st.sp, st.res, st.phi, relax, nswp, nsolv, info);
+  const int rc = solve_dev<T>(S, st.acoef, st.ss, st.sp, st.res, st.phi, relax, nswp, nsolv, info, nvar);
   if (rc == CMS_DEVICE_ERROR || rc == CMS_BAD_ARGUMENT || rc == CMS_UNSUPPORTED) return rc;
   const size_t n = S->hp.n;
   CMS_CUDA(cudaMemcpyAsync(ss, st.ss, n * sizeof(T), cudaMemcpyDeviceToHost, s));
@@ -858,6 +908,8 @@ void cms_solver_default_opts(cms_solver_opts* o) {
   o->verify = 1;
   o->multi_kernel = 0;
   o->inner_relax = 1;
+  o->relaxsor = 1.8;   // flow.F90:131
+  o->nswp0_vel = 5;    // nswp0(2) of the hybrid solver's defaults (flow.F90:795-798)
 }
 
 int cms_solver_create(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, const int* ncface,
@@ -908,6 +960,27 @@ int cms_solver_solve_dev_f(cms_solver* s, const float* acoef, float* ss, const f
                            float relax, int nswp, int nsolv, cms_solve_info* info) {
   if (!s || !acoef || !ss || !sp || !res || !phi) return CMS_BAD_ARGUMENT;
   return cms::solve_dev<float>(s, acoef, ss, sp, res, phi, relax, nswp, nsolv, info);
+}
+
+int cms_solver_solve_n_d(cms_solver* s, int n, const double* acoef, double* ss, const double* sp, double* res,
+                         double* phi, double relax, int nswp, int nsolv, cms_solve_info* info) {
+  if (!s || !acoef || !ss || !sp || !res || !phi) return CMS_BAD_ARGUMENT;
+  return cms::solve_host<double>(s, acoef, ss, sp, res, phi, relax, nswp, nsolv, info, n);
+}
+int cms_solver_solve_n_f(cms_solver* s, int n, const float* acoef, float* ss, const float* sp, float* res, float* phi,
+                         float relax, int nswp, int nsolv, cms_solve_info* info) {
+  if (!s || !acoef || !ss || !sp || !res || !phi) return CMS_BAD_ARGUMENT;
+  return cms::solve_host<float>(s, acoef, ss, sp, res, phi, relax, nswp, nsolv, info, n);
+}
+int cms_solver_solve_dev_n_d(cms_solver* s, int n, const double* acoef, double* ss, const double* sp, double* res,
+                             double* phi, double relax, int nswp, int nsolv, cms_solve_info* info) {
+  if (!s || !acoef || !ss || !sp || !res || !phi) return CMS_BAD_ARGUMENT;
+  return cms::solve_dev<double>(s, acoef, ss, sp, res, phi, relax, nswp, nsolv, info, n);
+}
+int cms_solver_solve_dev_n_f(cms_solver* s, int n, const float* acoef, float* ss, const float* sp, float* res,
+                             float* phi, float relax, int nswp, int nsolv, cms_solve_info* info) {
+  if (!s || !acoef || !ss || !sp || !res || !phi) return CMS_BAD_ARGUMENT;
+  return cms::solve_dev<float>(s, acoef, ss, sp, res, phi, relax, nswp, nsolv, info, n);
 }
 
 int cms_solver_profile(cms_solver* s, int enable) {
@@ -985,19 +1058,17 @@ int cms_gpu_update_wet(const int* iwet) {
 }
 int cms_gpu_solve_d(int n, const double* acoef, double* ss, const double* sp, double* res, double* phi, double relax,
                     int nswp, int nsolv, double* rmom) {
-  (void)n;  // the variable index selects relax/nswp on the caller's side
   std::lock_guard<std::mutex> lk(g_mu);
   if (!g_solver) return CMS_BAD_ARGUMENT;
-  int rc = cms_solver_solve_d(g_solver, acoef, ss, sp, res, phi, relax, nswp, nsolv, &g_info);
+  int rc = cms_solver_solve_n_d(g_solver, n, acoef, ss, sp, res, phi, relax, nswp, nsolv, &g_info);
   if (rmom) *rmom = g_info.rmom;
   return rc;
 }
 int cms_gpu_solve_f(int n, const float* acoef, float* ss, const float* sp, float* res, float* phi, float relax,
                     int nswp, int nsolv, float* rmom) {
-  (void)n;
   std::lock_guard<std::mutex> lk(g_mu);
   if (!g_solver) return CMS_BAD_ARGUMENT;
-  int rc = cms_solver_solve_f(g_solver, acoef, ss, sp, res, phi, relax, nswp, nsolv, &g_info);
+  int rc = cms_solver_solve_n_f(g_solver, n, acoef, ss, sp, res, phi, relax, nswp, nsolv, &g_info);
   if (rmom) *rmom = (float)g_info.rmom;
   return rc;
 }

@@ -19,10 +19,16 @@ from . import _lib
 
 # relax(n) defaults: source/flow/flow.F90:124-130 (pp 1.0, u 0.8, v 0.8, c 0.8, s 0.8)
 RELAX_DEFAULT = {1: 1.0, 2: 0.8, 3: 0.8, 4: 0.8, 5: 0.8}
-# nswp(n) defaults per solver: source/flow/flow.F90:779-792
-NSWP_DEFAULT = {3: {1: 15, 2: 5, 3: 5, 4: 5, 5: 5}, 4: {1: 20, 2: 5, 3: 5, 4: 3, 5: 3}}
+# nswp(n) defaults per solver: source/flow/flow.F90:752-821
+NSWP_DEFAULT = {0: {1: 40, 2: 10, 3: 10, 4: 10, 5: 10}, 1: {1: 100, 2: 30, 3: 30, 4: 15, 5: 15},
+                2: {1: 80, 2: 20, 3: 20, 4: 15, 5: 15}, 3: {1: 15, 2: 5, 3: 5, 4: 5, 5: 5},
+                4: {1: 20, 2: 5, 3: 5, 4: 3, 5: 3}, 5: {1: 20, 2: 5, 3: 5, 4: 3, 5: 3},
+                6: {1: 30, 2: 7, 3: 7, 4: 5, 5: 5}, 7: {1: 30, 2: 7, 3: 7, 4: 5, 5: 5},
+                8: {1: 30, 2: 7, 3: 7, 4: 5, 5: 5}}
 NSOLV_DEFAULT = 4  # GMRES, source/solvers/solvers.f90:8
-SOLVER_NAMES = {"BICGSTAB": 3, "GMRES": 4}  # MATRIX_SOLVER card values (solvers.f90:12-13)
+# MATRIX_SOLVER card values (asolv, solvers.f90:9-17); ADI has no branch in solve()
+SOLVER_NAMES = {"ADI": 0, "GAUSS-SEIDEL": 1, "GAUSS-SEIDEL-SOR": 2, "BICGSTAB": 3, "GMRES": 4, "HYBRID": 5,
+                "SIP": 6, "ICCG": 7, "ICCGSTAB": 8}
 
 _ORDER = {"multicolor": _lib.ORDER_MULTICOLOR, "natural": _lib.ORDER_NATURAL}
 _PREC = {"fp64": _lib.PREC_FP64, "fp32_refine": _lib.PREC_FP32_REFINE, "fp32": _lib.PREC_FP32}
@@ -68,7 +74,7 @@ class Solver:
     def __init__(self, grid, iwet=None, ordering: str = "multicolor", precision: str = "fp64", tol: float = 1e-3,
                  norm: int = 1, max_iters: int = 0, inner_tol: float = 1e-3, inner_max: int = 50,
                  max_refine: int = 30, verify: bool = True, nsolv: int = NSOLV_DEFAULT,
-                 multi_kernel: bool = False, inner_relax: bool = True):
+                 multi_kernel: bool = False, inner_relax: bool = True, relaxsor: float = 1.8, nswp0_vel: int = 5):
         L = _lib.lib()
         self.grid = grid
         self.nsolv = nsolv
@@ -85,6 +91,8 @@ class Solver:
         self.opts.verify = int(verify)
         self.opts.multi_kernel = int(multi_kernel)
         self.opts.inner_relax = int(inner_relax)
+        self.opts.relaxsor = relaxsor
+        self.opts.nswp0_vel = nswp0_vel
         self._c2c = np.ascontiguousarray(grid.cell2cell, np.int32)
         self._ncf = np.ascontiguousarray(grid.ncface, np.int32)
         self._iwet = np.ones(grid.ncellsD, np.int32) if iwet is None else np.ascontiguousarray(iwet, np.int32)
@@ -189,9 +197,9 @@ class Solver:
             # the handle's own stream reads the tensors: finish the work that produced them
             import torch
             torch.cuda.current_stream(acoef.device).synchronize()
-        fn = {(True, False): L.cms_solver_solve_d, (False, False): L.cms_solver_solve_f,
-              (True, True): L.cms_solver_solve_dev_d, (False, True): L.cms_solver_solve_dev_f}[(is64, dev)]
-        rc = fn(self._h, *[_ptr(a) for a in arrs], float(relax), int(nswp), int(nsolv), C.byref(info))
+        fn = {(True, False): L.cms_solver_solve_n_d, (False, False): L.cms_solver_solve_n_f,
+              (True, True): L.cms_solver_solve_dev_n_d, (False, True): L.cms_solver_solve_dev_n_f}[(is64, dev)]
+        rc = fn(self._h, int(n), *[_ptr(a) for a in arrs], float(relax), int(nswp), int(nsolv), C.byref(info))
         if raise_on_error:
             _lib.check(rc, "solve", allow=(_lib.CMS_OK, _lib.CMS_NOT_CONVERGED, _lib.CMS_NONFINITE))
         out = info.as_dict()

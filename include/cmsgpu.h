@@ -71,6 +71,10 @@ typedef struct cms_solver_opts {
                         couplings among rows of colours >= 2, so its sweeps take two
                         phases like a red/black grid; 0: exact multicolour ILU(0).
                         The FP64 residual makes either converge to the same answer.   */
+  double relaxsor;   /* SOR constant of nsolv 2 and 5 (SUCCESSIVE_OVER_RELAXATION_CONSTANT
+                        card, default 1.8: flow.F90:131)                                */
+  int nswp0_vel;     /* nswp0(2), the velocity iteration count the hybrid solver
+                        (nsolv 5) triples for n = 4, 5 (solvers.f90:265); default 5  */
 } cms_solver_opts;
 
 typedef struct cms_solve_info {
@@ -118,6 +122,30 @@ int cms_solver_solve_dev_d(cms_solver* s, const double* acoef, double* ss, const
                            double relax, int nswp, int nsolv, cms_solve_info* info);
 int cms_solver_solve_dev_f(cms_solver* s, const float* acoef, float* ss, const float* sp, float* res, float* phi,
                            float relax, int nswp, int nsolv, cms_solve_info* info);
+
+/* solve() with the variable index n (1 pressure correction, 2-3 velocity, 4
+ * sediment, 5 salinity or heat; 0 none) for every MATRIX_SOLVER option
+ * (solvers.f90:242-289): nsolv 0 (ADI) the prologue only, as solve() has no
+ * branch for it; 1 Gauss-Seidel; 2 symmetric Gauss-Seidel, or
+ * SSOR for n = 1 once rmom < 1e-3; 3 BiCGStab; 4 GMRES; 5 BiCGStab for n = 1
+ * while rmom > 1e-4, else Gauss-Seidel with 4*nswp passes (n <= 3) or
+ * 3*opts.nswp0_vel passes (n = 4, 5), SOR for n = 1; 6 SIP; 7 ICCG for n = 1,
+ * else SIP; 8 ICCG for n = 1, else ICCGSTAB.  The Gauss-Seidel passes and the
+ * incomplete Cholesky factor follow the handle's ordering (natural: the
+ * reference's serial loops; multicolour: their multicolour form).  SIP, ICCG
+ * and ICCGSTAB need exactly four faces per cell (a Cartesian grid), and SIP
+ * the natural ordering of a grid numbered row by row from the south-west
+ * (CMS_UNSUPPORTED otherwise).  Options other than 3 and 4 run in the type of
+ * the call (CMS_PREC_FP32_REFINE is not applied to them).  The entry points
+ * without n behave as n = 0. */
+int cms_solver_solve_n_d(cms_solver* s, int n, const double* acoef, double* ss, const double* sp, double* res,
+                         double* phi, double relax, int nswp, int nsolv, cms_solve_info* info);
+int cms_solver_solve_n_f(cms_solver* s, int n, const float* acoef, float* ss, const float* sp, float* res, float* phi,
+                         float relax, int nswp, int nsolv, cms_solve_info* info);
+int cms_solver_solve_dev_n_d(cms_solver* s, int n, const double* acoef, double* ss, const double* sp, double* res,
+                             double* phi, double relax, int nswp, int nsolv, cms_solve_info* info);
+int cms_solver_solve_dev_n_f(cms_solver* s, int n, const float* acoef, float* ss, const float* sp, float* res,
+                             float* phi, float relax, int nswp, int nsolv, cms_solve_info* info);
 
 /* Number of groups the sweeps run and device bytes held by the handle. */
 int cms_solver_ncolors(const cms_solver* s);

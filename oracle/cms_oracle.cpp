@@ -793,7 +793,9 @@ int solve_impl(OracleHandle* h, Work<R>& wk, const R* acoef, R* ss, const R* sp,
   *rmom = std::sqrt(adak(n, res) / R(n));
   SolveStats st{0, 0, 0.0};
   const R rm = *rmom;  // rmom(n); the pressure tests below read rmom(1) only when n == 1
-  if (nsolv == 1) {
+  if (nsolv == 0) {
+    // ADI: solve() has no branch for it; phi is left as it is
+  } else if (nsolv == 1) {
     st = gauss_seidel(p, nswp, false, false, relaxsor, acoef, ap.data(), ss, phi);
   } else if (nsolv == 2) {
     st = gauss_seidel(p, nswp, true, n_var == 1 && rm < R(1.0e-3), relaxsor, acoef, ap.data(), ss, phi);
