@@ -664,6 +664,29 @@ __global__ void __launch_bounds__(TPB) kf_velface_eta(FlowDev G, FlowState S) {
   }
 }
 
+// flow_convflux (flow.F90:1879-1909), for a hot start: face fluxes from the
+// cell velocities on each cell's no-repeat faces, copied with the opposite
+// sign to the neighbour's face.  Correctly rounded steps in the reference's
+// order: from the same inputs the result equals the host computation's.
+__global__ void __launch_bounds__(TPB) kf_convflux(FlowDev G, FlowState S) {
+  const int r = blockIdx.x * TPB + threadIdx.x;
+  if (r >= G.n) return;
+  const unsigned char own = G.owned[r];
+  for (int k = 0; k < G.ncface[r]; ++k) {
+    if (!((own >> k) & 1)) continue;
+    const int f = fidx(G, k, r), nck = G.nb[f], d = G.dir[f];
+    const double fx = fnxd(d), fy = fnyd(d);
+    const double uni = __dadd_rn(__dmul_rn(fx, S.u[r]), __dmul_rn(fy, S.v[r]));
+    const double unk = __dadd_rn(__dmul_rn(fx, S.u[nck]), __dmul_rn(fy, S.v[nck]));
+    const double fk = G.fintp[f];
+    const double w = (double)(G.iwet[r] * G.iwet[nck]);
+    const double fl = __dmul_rn(__dmul_rn(__dmul_rn(w, G.ds[f]), S.hk[f]),
+                                __dadd_rn(__dmul_rn(fk, unk), __dmul_rn(__dsub_rn(1.0, fk), uni)));
+    S.flux[f] = fl;
+    S.flux[fidx(G, G.back[f], nck)] = -fl;
+  }
+}
+
 // flow_update (CMS_Flow.f90:243-300): time levels; pp and its gradient reset
 __global__ void __launch_bounds__(TPB) kf_update(FlowDev G, FlowState S, double* dppx0, double* dppy0, double* dppx1,
                                                  double* dppy1) {

@@ -26,6 +26,7 @@ struct cms_flow {
   // water-level string (device numbering)
   int nth = 0;
   int *d_th_cell = nullptr, *d_th_dummy = nullptr;
+  std::vector<int> th_cell_nat, th_dummy_nat;  // the same, natural numbering (0-based)
   double* d_wse = nullptr;       // [nth] values of the current step
   double* d_wse_cell = nullptr;  // [nD] the same, at the dummy cells
   // wall string
@@ -528,6 +529,8 @@ static int flow_create(int ncells, int ncellsD, int nmf, const int* c2c, const i
       const int i = th_cells[j] - 1, k = th_faces[j] - 1;
       tc[j] = F->n2d[i];
       tg[j] = F->n2d[c2c[(size_t)i * nmf + k] - 1];
+      F->th_cell_nat.push_back(i);
+      F->th_dummy_nat.push_back(c2c[(size_t)i * nmf + k] - 1);
     }
     if ((rc = F->upload(&F->d_th_cell, tc)) || (rc = F->upload(&F->d_th_dummy, tg))) return fail(rc);
     std::vector<int> wc, wg;
@@ -885,17 +888,39 @@ static int wetdry_update(Flow* F, int nchg) {
   return rc;
 }
 
-static int flow_init(Flow* F, const double* eta0_nat) {
+// Cold start (u_nat == nullptr: at rest) or hot start from the water pressure
+// p_nat and velocities u_nat, v_nat of all nD cells (natural order), and the
+// face fluxes flux_nat ([nD][nmf]) when the hot-start file holds them.
+static int flow_start(Flow* F, std::vector<double> p_nat, const double* u_nat, const double* v_nat,
+                      const double* flux_nat = nullptr) {
   FlowState& T = F->st;
   cudaStream_t s = F->S->stream;
   const int nD = F->nD;
+  const bool hot = u_nat != nullptr;
+  std::vector<double> u0, v0;
+  std::vector<int> wet_hot;
+  if (hot) {
+    // hot_init (hot_start.F90:1164-1200): cells with h < hmin + 1e-5 are dry
+    // and at rest; each water-level string dummy takes its cell's values
+    u0.assign(u_nat, u_nat + nD);
+    v0.assign(v_nat, v_nat + nD);
+    wet_hot.assign(nD, 1);
+    for (int i = 0; i < nD; ++i) {
+      const double hh = p_nat[i] * F->G.gravinv - F->geom.zb[i];
+      if (hh < F->G.hmin + 1.0e-5) { wet_hot[i] = 0; u0[i] = v0[i] = 0.0; }
+    }
+    for (size_t j = 0; j < F->th_cell_nat.size(); ++j) {
+      const int i = F->th_cell_nat[j], d = F->th_dummy_nat[j];
+      u0[d] = u0[i]; v0[d] = v0[i]; p_nat[d] = p_nat[i];
+    }
+  }
   // wet set of the cold start (prestart.f90:308-315): flow_wetdry(0), again
   // with ponding on when every cell is dry
   {
     std::vector<unsigned char>& cn = F->code_nat;
     cn.assign(nD, 0);
     for (int i = 0; i < nD; ++i) {
-      const double pi = eta0_nat[i] * F->G.grav;
+      const double pi = p_nat[i];
       const double hh = pi * F->G.gravinv - F->geom.zb[i];
       cn[i] = (unsigned char)((hh >= F->G.hdry ? WD_WET : 0) | (hh < F->G.hdry1 ? WD_LT1 : 0) |
                               (hh < F->G.hdry2 ? WD_LT2 : 0));
@@ -920,10 +945,28 @@ static int flow_init(Flow* F, const double* eta0_nat) {
     F->wd_pending = 0;
     F->nchg_pending = 0;
   }
+  if (hot) {
+    // flow_wetdry(0) against hot_init's wet set: the dry-to-wet initialisation
+    // of the cells it wets (flow.F90:1476-1491, five passes in cell order; the
+    // viscosities are all zero at this point)
+    const FlowGeom& g = F->geom;
+    for (int pass = 0; pass < 5; ++pass)
+      for (int i = 0; i < F->n; ++i) {
+        if (!(g.iwet[i] == 1 && wet_hot[i] == 0)) continue;
+        double us = 0.0, vs = 0.0;
+        int ns = 0;
+        for (int k = 0; k < g.ncface[i]; ++k) {
+          const int j = g.nb[(size_t)i * g.nmf + k];
+          us = us + u0[j]; vs = vs + v0[j]; ns += g.iwet[j];
+        }
+        u0[i] = us / ((double)ns + 1.0e-15) / 1.25;
+        v0[i] = vs / ((double)ns + 1.0e-15) / 1.25;
+      }
+  }
   std::vector<double> p(nD), h(nD), eta(nD);
   for (int r = 0; r < nD; ++r) {
     const int i = F->d2n[r];
-    p[r] = eta0_nat[i] * F->G.grav;
+    p[r] = p_nat[i];
     double hh = p[r] * F->G.gravinv - F->geom.zb[i];
     if (hh < F->G.hdry) hh = std::max(hh, F->G.hmin);
     h[r] = hh;
@@ -935,6 +978,13 @@ static int flow_init(Flow* F, const double* eta0_nat) {
   const size_t cb = nD * sizeof(double), fb = (size_t)F->nmf * nD * sizeof(double);
   for (double* a : {T.u, T.v, T.pp, T.vis, T.cfrict, T.uv, T.bsvel})
     CMS_CUDA(cudaMemsetAsync(a, 0, cb, s));
+  std::vector<double> ud, vd;
+  if (hot) {
+    ud.resize(nD); vd.resize(nD);
+    for (int r = 0; r < nD; ++r) { ud[r] = u0[F->d2n[r]]; vd[r] = v0[F->d2n[r]]; }
+    CMS_CUDA(cudaMemcpyAsync(T.u, ud.data(), cb, cudaMemcpyHostToDevice, s));
+    CMS_CUDA(cudaMemcpyAsync(T.v, vd.data(), cb, cudaMemcpyHostToDevice, s));
+  }
   for (double* a : {T.flux, T.visk, T.hk, T.pk, T.acoef, T.zbk}) CMS_CUDA(cudaMemsetAsync(a, 0, fb, s));
   for (int c = 0; c < 2; ++c)
     for (double* a : {T.dpx[c], T.dpy[c], T.dux[c], T.duy[c], T.dvx[c], T.dvy[c], T.dppx[c], T.dppy[c], T.dHux[c],
@@ -961,7 +1011,29 @@ static int flow_init(Flow* F, const double* eta0_nat) {
                                                   F->opts.skewcor ? T.dzby[0] : nullptr)));
   }
   FCHK(flow_grad_interp(F));
+  std::vector<double> fd;
+  if (hot && flux_nat) {
+    // the file's fluxes, zero across faces flow_wetdry(0) left with a dry side
+    // (flow.F90:1497-1512); flow_convflux is skipped (prestart.f90:319)
+    const FlowGeom& g = F->geom;
+    const int nmf = F->nmf;
+    std::vector<double> fn(flux_nat, flux_nat + (size_t)nD * nmf);
+    for (int i = 0; i < F->n; ++i)
+      for (int k = 0; k < g.ncface[i]; ++k) {
+        const size_t f = (size_t)i * nmf + k;
+        if (!g.owned[f]) continue;
+        const int j = g.nb[f];
+        if (g.iwet[i] * g.iwet[j] == 0) { fn[f] = 0.0; fn[(size_t)j * nmf + g.back[f]] = 0.0; }
+      }
+    fd.assign((size_t)nmf * nD, 0.0);
+    for (int i = 0; i < nD; ++i)
+      for (int k = 0; k < nmf; ++k) fd[(size_t)k * nD + F->n2d[i]] = fn[(size_t)i * nmf + k];
+    CMS_CUDA(cudaMemcpyAsync(T.flux, fd.data(), fb, cudaMemcpyHostToDevice, s));
+  } else if (hot) {
+    FLAUNCH(F, (kf_convflux<<<fblk(F->n), TPB, 0, s>>>(F->G, T)));
+  }
   FCHK(flow_vis(F, T.dux[F->cur_duv], T.duy[F->cur_duv], T.dvx[F->cur_duv], T.dvy[F->cur_duv]));
+  CMS_CUDA(cudaStreamSynchronize(s));  // ud, vd are read by the copies above
   // time levels
   FLAUNCH(F, (kf_update<<<fblk(nD), TPB, 0, s>>>(F->G, T, T.dppx[0], T.dppy[0], T.dppx[1], T.dppy[1])));
   CMS_CUDA(cudaStreamSynchronize(s));
@@ -1161,7 +1233,14 @@ int cms_flow_create(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell
 
 int cms_flow_init(cms_flow* f, const double* eta0) {
   if (!f || !eta0) return CMS_BAD_ARGUMENT;
-  return cms::flow_init(f, eta0);
+  std::vector<double> p(f->nD);
+  for (int i = 0; i < f->nD; ++i) p[i] = eta0[i] * f->G.grav;
+  return cms::flow_start(f, std::move(p), nullptr, nullptr);
+}
+
+int cms_flow_init_hot(cms_flow* f, const double* p, const double* u, const double* v, const double* flux) {
+  if (!f || !p || !u || !v) return CMS_BAD_ARGUMENT;
+  return cms::flow_start(f, std::vector<double>(p, p + f->nD), u, v, flux);
 }
 
 int cms_flow_step(cms_flow* f, double dt, const double* wsebnd, cms_flow_info* info) {

@@ -44,6 +44,7 @@ def _bind(L):
     L.cms_flow_default_opts.argtypes = [C.POINTER(FlowOpts)]
     L.cms_flow_create.argtypes = [i, i, i] + [vp] * 9 + [i, vp, vp, C.POINTER(FlowOpts), C.POINTER(vp)]
     L.cms_flow_init.argtypes = [vp, vp]
+    L.cms_flow_init_hot.argtypes = [vp, vp, vp, vp, vp]
     L.cms_flow_step.argtypes = [vp, d, vp, C.POINTER(FlowInfo)]
     L.cms_flow_get.argtypes = [vp, i, vp]
     L.cms_flow_launches.argtypes = [vp]
@@ -126,6 +127,23 @@ class FlowModel:
         eta0 = np.ascontiguousarray(eta0, np.float64)
         _lib.check(_lib.lib().cms_flow_init(self._h, _p(eta0)), "cms_flow_init")
         self.t = 0.0
+
+    def init_hot(self, p, u, v, t=0.0, flux=None):
+        """Hot start from the water pressure and velocities of all ncellsD cells
+        (natural order) and, when the hot-start file holds them, the face fluxes
+        [ncellsD, nmaxfaces]; t is the simulation time the state belongs to."""
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (p, u, v)]
+        for a in arrs:
+            if a.shape != (self.g.ncellsD,):
+                raise ValueError("p, u, v must have ncellsD entries")
+        fl = None
+        if flux is not None:
+            fl = np.ascontiguousarray(flux, np.float64)
+            if fl.shape != (self.g.ncellsD, self.g.nmaxfaces):
+                raise ValueError("flux must be [ncellsD, nmaxfaces]")
+        _lib.check(_lib.lib().cms_flow_init_hot(self._h, *[_p(a) for a in arrs], None if fl is None else _p(fl)),
+                   "cms_flow_init_hot")
+        self.t = float(t)
 
     def step(self, dt=None, wsebnd=None):
         dt = self.case.dt if dt is None else dt

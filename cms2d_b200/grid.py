@@ -83,19 +83,15 @@ def _lookup(owner, xx, yy):
     return out
 
 
-def telescoping_grid(level: np.ndarray, dx0: float, active=None, nmaxfaces: int | None = None) -> Grid:
-    """Builds a telescoping grid from a parent-level map.
-
-    level:  int array [nby, nbx] of refinement levels (0 = parent size dx0).
-    active: optional callable (xc, yc, size) -> bool array selecting active leaves
-            (inactive leaves are land: depth -999 in a .tel file).
-    """
+def _leaves(level: np.ndarray):
+    """All leaves of a parent-level map on the finest lattice, row-major by
+    lower-left corner (y, then x): corners fx, fy, size fs (lattice units)."""
     level = np.asarray(level, dtype=np.int64)
     nby, nbx = level.shape
-    lmax = int(level.max())
     # 2:1 balance between edge-adjacent parents
     if np.any(np.abs(np.diff(level, axis=0)) > 1) or np.any(np.abs(np.diff(level, axis=1)) > 1):
         raise ValueError("adjacent parent cells differ by more than one refinement level")
+    lmax = int(level.max())
     R = 1 << lmax  # fine lattice points per parent side
     fxl, fyl, fsl = [], [], []
     for L in range(lmax + 1):
@@ -110,27 +106,16 @@ def telescoping_grid(level: np.ndarray, dx0: float, active=None, nmaxfaces: int 
         fyl.append((jj[:, None] * R + b[None, :] * s).ravel())
         fsl.append(np.full(ii.size * n * n, s, dtype=np.int64))
     fx = np.concatenate(fxl); fy = np.concatenate(fyl); fs = np.concatenate(fsl)
-    h = dx0 / R  # fine lattice spacing
-    xc = (fx + 0.5 * fs) * h
-    yc = (fy + 0.5 * fs) * h
-    keep = np.ones(fx.size, dtype=bool)
-    if active is not None:
-        keep = np.asarray(active(xc, yc, fs * h), dtype=bool)
-    # inactive (land) leaves are painted -1 so that their sides get dummies
-    owner = _owner_lookup(fx[~keep], fy[~keep], fs[~keep], np.full(int((~keep).sum()), -1, dtype=np.int64),
-                          nbx * R, nby * R)
-    fx, fy, fs, xc, yc = fx[keep], fy[keep], fs[keep], xc[keep], yc[keep]
     order = np.lexsort((fx, fy))  # row-major: y then x
-    fx, fy, fs, xc, yc = fx[order], fy[order], fs[order], xc[order], yc[order]
-    ncells = fx.size
-    ids = np.arange(1, ncells + 1, dtype=np.int64)
-    act = _owner_lookup(fx, fy, fs, ids, nbx * R, nby * R)
-    owner = np.where(act > 0, act, owner)
-    del act
-    # .tel neighbour slots n1,n2,e1,e2,s1,s2,w1,w2 (second of a pair 0 unless
-    # the side is split between two finer neighbours)
+    return fx[order], fy[order], fs[order], lmax, R, nbx * R, nby * R
+
+
+def _neighbour_slots(owner, fx, fy, fs):
+    """The .tel neighbour slots n1,n2,e1,e2,s1,s2,w1,w2 of each leaf from the
+    lattice owner map (the second of a pair is 0 unless the side is split
+    between two finer neighbours)."""
     x0, y0, s = fx, fy, fs
-    loc = np.zeros((ncells, 8), dtype=np.int64)
+    loc = np.zeros((fx.size, 8), dtype=np.int64)
     pairs = [
         ((x0, y0 + s), (x0 + s - 1, y0 + s)),          # north: west half, east half
         ((x0 + s, y0 + s - 1), (x0 + s, y0)),          # east: north half, south half
@@ -143,9 +128,22 @@ def telescoping_grid(level: np.ndarray, dx0: float, active=None, nmaxfaces: int 
         n2 = np.where(n2 == n1, 0, n2)
         loc[:, 2 * side] = n1
         loc[:, 2 * side + 1] = n2
-    # slot kinds (read_tel, geospatial.F90:472-494): a side with no active
-    # neighbour gets one dummy in its first slot; an inactive half of a split
-    # side gets its own dummy; active neighbours are internal faces.
+    return loc
+
+
+def assemble(loc, xc, yc, dxc, dyc, nmaxfaces: int | None = None, level=None, telescoping: bool = False,
+             fx=None, fy=None, fs=None) -> Grid:
+    """read_tel's second pass (source/geospatial/geospatial.F90:540-741) for the
+    active cells of a grid: loc[i, j] is the neighbour of active cell i in .tel
+    slot j (n1,n2,e1,e2,s1,s2,w1,w2) as an active id (1-based), -1 for an
+    inactive (land) cell, 0 for none.  xc, yc, dxc, dyc: cell centres and
+    sizes.  A side with no active neighbour gets one dummy in its first slot,
+    an inactive half of a split side its own dummy, active neighbours internal
+    faces; dummies are numbered in cell order then slot order, with ncface 4,
+    a back link on the opposite face and the position and size read_tel gives
+    them (half size when the side is split)."""
+    loc = np.asarray(loc, dtype=np.int64)
+    ncells = loc.shape[0]
     slot_kind = np.zeros((ncells, 8), dtype=np.int8)  # 0 none, 1 internal, 2 dummy
     for q in range(4):
         a1, a2 = loc[:, 2 * q], loc[:, 2 * q + 1]
@@ -153,9 +151,9 @@ def telescoping_grid(level: np.ndarray, dx0: float, active=None, nmaxfaces: int 
         slot_kind[:, 2 * q] = np.where(has, np.where(a1 > 0, 1, np.where(a1 < 0, 2, 0)), 2)
         slot_kind[:, 2 * q + 1] = np.where(has, np.where(a2 > 0, 1, np.where(a2 < 0, 2, 0)), 0)
     nf = (slot_kind > 0).sum(axis=1)
-    nmf_needed = int(nf.max())
+    nmf_needed = int(nf.max()) if ncells else 4
     if nmaxfaces is None:
-        nmaxfaces = 4 if (nmf_needed <= 4 and lmax == 0) else 6
+        nmaxfaces = 4 if (nmf_needed <= 4 and not telescoping) else 6
     if nmf_needed > nmaxfaces:
         raise ValueError(f"a cell has {nmf_needed} faces > nmaxfaces={nmaxfaces}")
     ndummy = int((slot_kind == 2).sum())
@@ -164,7 +162,6 @@ def telescoping_grid(level: np.ndarray, dx0: float, active=None, nmaxfaces: int 
     idirface = np.zeros((ncellsD, nmaxfaces), dtype=np.int32)
     ncface = np.zeros(ncellsD, dtype=np.int32)
     ncface[:ncells] = nf
-    # dummy ids in cell order then slot order (read_tel's ndum counter)
     dmask = slot_kind == 2
     dnum = np.cumsum(dmask.ravel()).reshape(dmask.shape) + ncells  # 1-based id for dummy slots
     present = slot_kind > 0
@@ -174,13 +171,11 @@ def telescoping_grid(level: np.ndarray, dx0: float, active=None, nmaxfaces: int 
     vals = np.where(slot_kind[rows, slots] == 2, dnum[rows, slots], loc[rows, slots])
     cell2cell[rows, kk] = vals
     idirface[rows, kk] = slots // 2 + 1
-    # dummies: ncface 4, back link on the opposite face, position and size as
-    # in read_tel (geospatial.F90:573-716; half-size when the side is split)
     X = np.zeros(ncellsD); Y = np.zeros(ncellsD); DX = np.zeros(ncellsD); DY = np.zeros(ncellsD)
     LEV = np.zeros(ncellsD, dtype=np.int8)
-    size = fs * h
-    X[:ncells] = xc; Y[:ncells] = yc; DX[:ncells] = size; DY[:ncells] = size
-    LEV[:ncells] = (lmax - np.log2(fs).astype(np.int64)).astype(np.int8)
+    X[:ncells] = xc; Y[:ncells] = yc; DX[:ncells] = dxc; DY[:ncells] = dyc
+    if level is not None:
+        LEV[:ncells] = level
     dr, dsl = np.nonzero(dmask)
     did = dnum[dr, dsl] - 1  # 0-based row of the dummy
     side = dsl // 2 + 1
@@ -191,24 +186,53 @@ def telescoping_grid(level: np.ndarray, dx0: float, active=None, nmaxfaces: int 
         cell2cell[did[m], back[q] - 1] = dr[m] + 1
     partner = loc[dr, dsl ^ 1]  # the other slot of the pair
     split = partner > 0
-    # full-size offsets (x, y) in units of the parent size, and half-size
-    # offsets per slot j = 1..8
+    # full-size offsets per side and half-size offsets per slot, in units of
+    # the cell's own dx (x) and dy (y)
     full = {1: (0.0, 1.0), 2: (1.0, 0.0), 3: (0.0, -1.0), 4: (-1.0, 0.0)}
     half = {0: (-0.25, 0.75), 1: (0.25, 0.75), 2: (0.75, 0.25), 3: (0.75, -0.25),
             4: (0.25, -0.75), 5: (-0.25, -0.75), 6: (-0.75, -0.25), 7: (-0.75, 0.25)}
-    sz = size[dr]
     ofx = np.array([full[q][0] for q in side]) if side.size else np.zeros(0)
     ofy = np.array([full[q][1] for q in side]) if side.size else np.zeros(0)
     hfx = np.array([half[j][0] for j in dsl]) if dsl.size else np.zeros(0)
     hfy = np.array([half[j][1] for j in dsl]) if dsl.size else np.zeros(0)
-    X[did] = xc[dr] + np.where(split, hfx, ofx) * sz
-    Y[did] = yc[dr] + np.where(split, hfy, ofy) * sz
-    DX[did] = np.where(split, 0.5, 1.0) * sz
-    DY[did] = DX[did]
+    sx, sy = np.asarray(dxc)[dr], np.asarray(dyc)[dr]
+    X[did] = np.asarray(xc)[dr] + np.where(split, hfx, ofx) * sx
+    Y[did] = np.asarray(yc)[dr] + np.where(split, hfy, ofy) * sy
+    DX[did] = np.where(split, 0.5, 1.0) * sx
+    DY[did] = np.where(split, 0.5, 1.0) * sy
     LEV[did] = LEV[dr] + split.astype(np.int8)
     return Grid(ncells=ncells, ncellsD=ncellsD, nmaxfaces=nmaxfaces, cell2cell=cell2cell, ncface=ncface,
                 idirface=idirface, x=X, y=Y, dx=DX, dy=DY, level=LEV, fx=fx, fy=fy, fs=fs,
-                telescoping=lmax > 0)
+                telescoping=telescoping)
+
+
+def telescoping_grid(level: np.ndarray, dx0: float, active=None, nmaxfaces: int | None = None) -> Grid:
+    """Builds a telescoping grid from a parent-level map.
+
+    level:  int array [nby, nbx] of refinement levels (0 = parent size dx0).
+    active: optional callable (xc, yc, size) -> bool array selecting active leaves
+            (inactive leaves are land: depth -999 in a .tel file).
+    """
+    fx, fy, fs, lmax, R, W, H = _leaves(level)
+    h = dx0 / R  # fine lattice spacing
+    xc = (fx + 0.5 * fs) * h
+    yc = (fy + 0.5 * fs) * h
+    keep = np.ones(fx.size, dtype=bool)
+    if active is not None:
+        keep = np.asarray(active(xc, yc, fs * h), dtype=bool)
+    # inactive (land) leaves are painted -1 so that their sides get dummies
+    owner = _owner_lookup(fx[~keep], fy[~keep], fs[~keep], np.full(int((~keep).sum()), -1, dtype=np.int64), W, H)
+    fx, fy, fs, xc, yc = fx[keep], fy[keep], fs[keep], xc[keep], yc[keep]
+    ncells = fx.size
+    ids = np.arange(1, ncells + 1, dtype=np.int64)
+    act = _owner_lookup(fx, fy, fs, ids, W, H)
+    owner = np.where(act > 0, act, owner)
+    del act
+    loc = _neighbour_slots(owner, fx, fy, fs)
+    size = fs * h
+    lev = (lmax - np.log2(fs).astype(np.int64)).astype(np.int8)
+    return assemble(loc, xc, yc, size, size, nmaxfaces=nmaxfaces, level=lev, telescoping=lmax > 0, fx=fx, fy=fy,
+                    fs=fs)
 
 
 def cartesian_grid(nx: int, ny: int, dx: float = 20.0, active=None) -> Grid:

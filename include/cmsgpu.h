@@ -256,6 +256,18 @@ int cms_flow_create(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell
 /* Cold start at rest from the water level eta0 (ncellsD values, natural
  * order), as prestart does (prestart.f90:302-325). */
 int cms_flow_init(cms_flow* f, const double* eta0);
+/* Hot start from the water pressure p (= g * water level) and velocities u, v
+ * of all ncellsD cells, natural order, as a hot-start file holds them
+ * (hot_read): hot_init (hot_start.F90:1125-1215: cells with h < hmin + 1e-5
+ * dry and at rest, water-level string dummies copy their cell), then the rest
+ * of prestart (prestart.f90:298-325): flow_wetdry(0) against hot_init's wet
+ * set (dry-to-wet initialisation of the cells it wets), the wet-cell gradient
+ * operator of the resulting wet set, bed slope, face values, face fluxes from
+ * the velocities (flow_convflux, flow.F90:1879-1909) unless flux gives the
+ * file's face fluxes ([ncellsD][nmaxfaces] like CMS_FLOW_FLUX; NULL: none),
+ * friction, eddy viscosity.  Replaces cms_flow_init; stepping continues with
+ * cms_flow_step. */
+int cms_flow_init_hot(cms_flow* f, const double* p, const double* u, const double* v, const double* flux);
 /* One time step of length dt; wsebnd holds the string's water levels at the
  * new time level (one per string entry).  The step starts with wetting and
  * drying (flow_wetdry(0), flow.F90:1231-1539, and der_update,

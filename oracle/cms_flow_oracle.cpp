@@ -1269,6 +1269,91 @@ int orcf_init(void* h, const double* eta0) {
   return 0;
 }
 
+// flow_convflux (flow.F90:1879-1909): face fluxes from the cell velocities on
+// each cell's no-repeat faces, copied with the opposite sign to the
+// neighbour's face (bndflux adds nothing without flux or cross-shore strings).
+void flow_convflux(Flow& f) {
+  for (int i = 1; i <= f.n; ++i)
+    for (int j = 1; j <= f.nxyface[i]; ++j) {
+      const int k = f.FI(f.kxyface, j, i), nck = f.C(k, i), jcn = f.FI(f.llec, k, i);
+      const double uni = f.F(f.fnx, k, i) * f.u[i] + f.F(f.fny, k, i) * f.v[i];
+      const double unk = f.F(f.fnx, k, i) * f.u[nck] + f.F(f.fny, k, i) * f.v[nck];
+      const double fk = f.F(f.fintp, k, i);
+      f.F(f.flux, k, i) = (double)(f.iwet[i] * f.iwet[nck]) * f.F(f.ds, k, i) * f.F(f.hk, k, i) *
+                          (fk * unk + (1.0 - fk) * uni);
+      f.F(f.flux, jcn, nck) = -f.F(f.flux, k, i);
+    }
+}
+
+// Hot start from the water pressure p and the velocities u, v of all ncellsD
+// cells (what a hot-start file holds): hot_init (hot_start.F90:1125-1215) --
+// h = p/g - zb; a cell with h < hmin + 1e-5 is dry (h = hmin, u = v = 0,
+// eta = -999; p is kept, as when the file gave the pressure), else wet (eta =
+// p/g); the dummy of each water-level string face takes its cell's u, v, p,
+// eta and h; flow_update's time levels -- then the rest of prestart
+// (prestart.f90:298-325): flow_wetdry(0) against hot_init's wet set (it wets
+// cells with the dry-to-wet initialisation and zeroes the fluxes of dry
+// faces), again with ponding on when every cell is dry; iwet1 = iwet; eta;
+// bed slope and face beds; flow_grad_interp; flow_convflux unless the file
+// held the face fluxes (flux != NULL, [ncellsD][nmaxfaces]); fric_eval;
+// flow_eddyvis.  The wet-cell gradient operator is built from the wet set
+// this start ends with (the reference builds it in der_init, before the hot
+// start is read, from the wet set of the cold initial condition).
+int orcf_init_hot(void* h, const double* p, const double* u, const double* v, const double* flux) {
+  auto* f = static_cast<Flow*>(h);
+  const double g = f->P.grav, gravinv = 1.0 / g;
+  for (int i = 1; i <= f->nD; ++i) {
+    f->p[i] = p[i - 1];
+    f->u[i] = u[i - 1];
+    f->v[i] = v[i - 1];
+    f->vis[i] = 0.0;
+    f->h[i] = f->p[i] * gravinv - f->zb[i];
+    if (f->h[i] < f->P.hmin + 1.0e-5) {
+      f->h[i] = f->P.hmin;
+      f->iwet[i] = 0;
+      f->u[i] = f->v[i] = 0.0;
+      f->eta[i] = -999.0;
+    } else {
+      f->iwet[i] = 1;
+      f->eta[i] = f->p[i] * gravinv;
+    }
+  }
+  for (size_t j = 0; j < f->th_cells.size(); ++j) {
+    const int i = f->th_cells[j], k = f->th_faces[j], nck = f->C(k, i);
+    f->u[nck] = f->u[i]; f->v[nck] = f->v[i]; f->p[nck] = f->p[i]; f->eta[nck] = f->eta[i];
+    f->zb[nck] = f->zb[i];
+    f->h[i] = std::max(f->P.hmin, f->p[i] * gravinv - f->zb[i]);
+    f->h[nck] = f->h[i];
+  }
+  for (int i = 1; i <= f->nD; ++i) f->iwet1[i] = f->iwet[i];
+  std::fill(f->flux.begin(), f->flux.end(), 0.0);
+  std::fill(f->visk.begin(), f->visk.end(), 0.0);
+  if (flux)
+    for (int i = 1; i <= f->nD; ++i)
+      for (int k = 1; k <= f->nmf; ++k) f->F(f->flux, k, i) = flux[(size_t)(i - 1) * f->nmf + k - 1];
+  flow_wetdry(*f);
+  int nwet = 0;
+  for (int i = 1; i <= f->n; ++i) nwet += f->iwet[i];
+  if (nwet == 0) {
+    f->P.ponding = true;
+    flow_wetdry(*f);
+  }
+  for (int i = 1; i <= f->nD; ++i) {
+    f->iwet1[i] = f->iwet[i];
+    f->eta[i] = f->iwet[i] ? f->p[i] * gravinv : -999.0;
+  }
+  build_go(*f, f->gow, 1);
+  solver_set_wet(*f);
+  grad_eval(*f, f->goa, f->zb, f->dzbx, f->dzby);
+  interp_c2f(*f, f->zb, 0, f->zbk, &f->dzbx, &f->dzby);
+  flow_grad_interp(*f);
+  if (!flux) flow_convflux(*f);
+  fric_eval(*f);
+  flow_eddyvis(*f);
+  for (int i = 1; i <= f->nD; ++i) { f->u1[i] = f->u[i]; f->v1[i] = f->v[i]; f->p1[i] = f->p[i]; f->h1[i] = f->h[i]; }
+  return 0;
+}
+
 // One implicit time step (flow_imp + flow_update).  wsebnd: water level of each
 // TH-string cell.  Returns 0 ok, 2 divergent/non-finite.
 int orcf_step(void* h, double dt, const double* wsebnd, int maxit, int* niter, double* rmom3) {

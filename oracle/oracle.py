@@ -151,6 +151,7 @@ class FlowOracle:
             L.orcf_destroy.argtypes = [P]
             L.orcf_set_solver.argtypes = [P, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int]
             L.orcf_init.argtypes = [P, f64]
+            L.orcf_init_hot.argtypes = [P, f64, f64, f64, C.c_void_p]
             L.orcf_step.argtypes = [P, C.c_double, f64, C.c_int, C.POINTER(C.c_int), f64]
             L.orcf_step.restype = C.c_int
             L.orcf_get.argtypes = [P, C.c_int, f64]
@@ -196,6 +197,14 @@ class FlowOracle:
         if eta0 is None:
             eta0 = np.full(self.g.ncellsD, self.case.wse(0.0))
         lib().orcf_init(self._h, np.ascontiguousarray(eta0, np.float64))
+
+    def init_hot(self, p, u, v, t=0.0, flux=None):
+        """Hot start from the water pressure and velocities of all ncellsD cells
+        (and the face fluxes [ncellsD, nmaxfaces] when the file holds them)."""
+        fl = None if flux is None else np.ascontiguousarray(flux, np.float64)
+        lib().orcf_init_hot(self._h, *[np.ascontiguousarray(a, np.float64) for a in (p, u, v)],
+                            None if fl is None else fl.ctypes.data)
+        self.t = t
 
     def step(self, maxit=None, dt=None):
         dt = self.case.dt if dt is None else dt
