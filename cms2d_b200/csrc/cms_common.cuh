@@ -137,4 +137,24 @@ __device__ __forceinline__ bool grid_sum(double (&v)[NS], double* partials, unsi
 
 template <typename T> __device__ __forceinline__ T ldg(const T* p) { return __ldg(p); }
 
+// Polls of a device-side wait before it gives up and reports an error.
+constexpr unsigned int kSpinLimit = 1u << 22;
+
+// gpu-scope acquire load / release store of a progress flag
+__device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(unsigned int* p, unsigned int v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// relaxed load of a flag; a fence_acquire after the last one orders the loads that follow
+__device__ __forceinline__ unsigned int ld_relaxed(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void fence_acquire() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
 }  // namespace cms

@@ -5,10 +5,13 @@
 //
 // All work in device order on the ELL matrix of cms_krylov.cuh (A = diag - O,
 // aoff = O >= 0, right-hand side b with the dummy-cell terms folded in).
-// Recurrences run one group per launch: the rows of a group are not coupled,
-// and every coupling of a row to an earlier group is a lower slot.  In the
+// Recurrences follow the groups: the rows of a group are not coupled, and
+// every coupling of a row to an earlier group is a lower slot.  In the
 // natural (level-scheduled) ordering this is the reference's serial loop; in
 // the multicolour ordering it is the multicolour form of the same method.
+// With few groups (colours) each group is one launch; with many (the natural
+// ordering's level sets) the passes run pipelined inside one launch
+// (k_gs_pipe, k_tri_pipe below).
 //
 // Every iteration kernel starts with `if (st->done) return;`, so the host can
 // issue a whole solve's launches ahead and let the device stopping test end it.
@@ -363,5 +366,243 @@ __global__ void k_stab_start(DevState* st) {
   st->s[S_BET0] = 1.0;
   st->s[S_GAM] = 1.0;
 }
+
+// ----------------------------------------------------------------------------
+// Pipelined passes, for orderings with many groups (the natural ordering's
+// level sets, one launch each above).  One launch runs one pass, or many
+// Gauss-Seidel passes, over all rows.  The work unit is a chunk of at most TPB
+// rows of one group, claimed in order through a ticket (pass-major; a
+// backward pass takes the chunks in reverse order).  A row waits until each
+// coupling on the pass's new side (lower slots forward, upper slots backward)
+// has completed this pass, and each coupling on the old side and the row
+// itself the previous one (done[j] counts the passes row j completed),
+// computes, and publishes its count with a release store.  A unit waits only on rows of units with
+// earlier tickets, which blocks that are already running hold, so the
+// pipeline always advances.  Every wait is bounded: one that runs out sets
+// *err (the host reports a device error) and the row goes on with what it
+// has, so that the launch drains.  Values written in the launch are read
+// through L2 (ld.global.cg): L1 is not coherent across SMs.
+
+struct PipeSched {
+  const int* cstart;     // [nchunk + 1] first device row of each chunk
+  int nchunk;
+  unsigned int* done;    // [n] passes completed per row
+  unsigned int* ticket;  // work-unit counter of the launch (zero at launch)
+  int* err;              // [8] err[0]: a wait ran out; err[1..5]: where (pipe_ready)
+};
+
+// Waits until every row js[q] (bit q of vmask set) has completed needs[q]
+// passes (the arrays are indexed by compile-time positions): all the
+// flags are read together (relaxed), then one acquire fence orders the data
+// loads that follow.  The first wait that runs out records where: err[1..5] =
+// row waiting, a row not ready, its need, the count seen, unit.
+template <int M>
+__device__ __forceinline__ bool pipe_ready(const PipeSched& ps, const int (&js)[M], const unsigned int (&needs)[M],
+                                           unsigned int vmask, int r, int unit) {
+  unsigned int spins = 0;
+  for (;;) {
+    int badj = -1;
+    unsigned int seen = 0, badneed = 0;
+#pragma unroll
+    for (int q = 0; q < M; ++q)
+      if ((vmask >> q) & 1u) {
+        const unsigned int v = ld_relaxed(&ps.done[js[q]]);
+        if (v < needs[q]) { badj = js[q]; badneed = needs[q]; seen = v; }
+      }
+    if (badj < 0) break;
+    if (++spins > kSpinLimit) {
+      if (atomicCAS(ps.err, 0, 1) == 0) {
+        ps.err[1] = r; ps.err[2] = badj; ps.err[3] = (int)badneed; ps.err[4] = (int)seen; ps.err[5] = unit;
+      }
+      fence_acquire();
+      return false;
+    }
+    if ((spins & 1023u) == 0 && *(volatile int*)ps.err) break;
+  }
+  fence_acquire();
+  return true;
+}
+
+// Claims the next unit for the block; -1 when none is left.
+__device__ __forceinline__ int pipe_claim(const PipeSched& ps, int total) {
+  __shared__ int s_unit;
+  __syncthreads();
+  if (threadIdx.x == 0) s_unit = (int)atomicAdd(ps.ticket, 1u);
+  __syncthreads();
+  const int t = s_unit;
+  return t < total ? t : -1;
+}
+
+// npass Gauss-Seidel passes (sym: alternately forward and backward) in one
+// launch; base = passes the rows completed before it.  units (forward passes
+// only; nullptr: pass-major order) lists the work units as (pass, chunk) in
+// wavefront order: chunk c of level L in pass h comes with the others of
+// wave L + 2h, after every unit it waits on, so that consecutive passes
+// overlap instead of following each other.
+template <typename T, bool SOR>
+__global__ void __launch_bounds__(TPB) k_gs_pipe(int n, int KL, const int* __restrict__ col,
+                                                 const signed char* __restrict__ nlo,
+                                                 const signed char* __restrict__ nup, const T* __restrict__ aoff,
+                                                 const T* __restrict__ diag, const T* __restrict__ b, T* x, T w,
+                                                 PipeSched ps, int npass, int sym, unsigned int base,
+                                                 const int2* __restrict__ units) {
+  const int total = npass * ps.nchunk;
+  for (int t; (t = pipe_claim(ps, total)) >= 0;) {
+    int h, c;
+    if (units) {
+      const int2 u = units[t];
+      h = u.x; c = u.y;
+    } else {
+      h = t / ps.nchunk;
+      const int c0 = t - h * ps.nchunk;
+      c = (sym && (h & 1)) ? ps.nchunk - 1 - c0 : c0;
+    }
+    const bool bwd = sym && (h & 1);
+    const int r = ps.cstart[c] + threadIdx.x;
+    if (r >= ps.cstart[c + 1]) continue;
+    const unsigned int mine = base + (unsigned int)h + 1u;
+    const int kl = nlo[r], ku = nup[r];
+    // positions: 0 the row itself, 1..KMAX lower slots, KMAX+1..2 KMAX upper
+    int js[1 + 2 * KMAX];
+    unsigned int needs[1 + 2 * KMAX];
+    T av[2 * KMAX];
+    // the row itself: where the direction turns, its neighbours alone do not
+    // order it (a row with couplings on the old side only could otherwise
+    // start this pass before finishing the last one)
+    js[0] = r; needs[0] = mine - 1u;
+    unsigned int vmask = 1u;
+#pragma unroll
+    for (int s = 0; s < KMAX; ++s) {
+      const bool lo = s < kl, up = s < ku;
+      js[1 + s] = lo ? __ldg(&col[(size_t)s * n + r]) : r;
+      av[s] = lo ? __ldg(&aoff[(size_t)s * n + r]) : T(0);
+      needs[1 + s] = bwd ? mine - 1u : mine;
+      js[1 + KMAX + s] = up ? __ldg(&col[(size_t)(KL + s) * n + r]) : r;
+      av[KMAX + s] = up ? __ldg(&aoff[(size_t)(KL + s) * n + r]) : T(0);
+      needs[1 + KMAX + s] = bwd ? mine : mine - 1u;
+      vmask |= (lo ? 1u << (1 + s) : 0u) | (up ? 1u << (1 + KMAX + s) : 0u);
+    }
+    pipe_ready(ps, js, needs, vmask, r, t);
+    T term = T(0);
+#pragma unroll
+    for (int s = 0; s < KMAX; ++s)
+      if (s < kl) term = term + av[s] * __ldcg(&x[js[1 + s]]);
+#pragma unroll
+    for (int s = 0; s < KMAX; ++s)
+      if (s < ku) term = term + av[KMAX + s] * __ldcg(&x[js[1 + KMAX + s]]);
+    const T br = __ldg(&b[r]), dr = __ldg(&diag[r]);
+    if (SOR) x[r] = w * (term + br) / dr + (T(1) - w) * __ldcg(&x[r]);
+    else x[r] = (term + br) / dr;
+    st_release(&ps.done[r], mine);
+  }
+}
+
+// One pipelined pass of a triangular recurrence: Op::row(r) reads only rows
+// on the pass's new side (through L2) and rows of earlier launches.
+template <class Op>
+__global__ void __launch_bounds__(TPB) k_tri_pipe(Op op, int n, int KL, const int* __restrict__ col,
+                                                  const signed char* __restrict__ nlo,
+                                                  const signed char* __restrict__ nup, PipeSched ps, int bwd,
+                                                  unsigned int epoch, const DevState* st) {
+  if (st && st->done) return;  // every block sees the same flag (set by an earlier launch)
+  for (int t; (t = pipe_claim(ps, ps.nchunk)) >= 0;) {
+    const int c = bwd ? ps.nchunk - 1 - t : t;
+    const int r = ps.cstart[c] + threadIdx.x;
+    if (r >= ps.cstart[c + 1]) continue;
+    int js[KMAX];
+    unsigned int needs[KMAX];
+    const int m = bwd ? nup[r] : nlo[r];
+    const size_t off = bwd ? (size_t)KL * n : 0;
+    unsigned int vmask = 0u;
+#pragma unroll
+    for (int s = 0; s < KMAX; ++s) {
+      js[s] = s < m ? __ldg(&col[off + (size_t)s * n + r]) : r;
+      needs[s] = epoch;
+      vmask |= s < m ? 1u << s : 0u;
+    }
+    pipe_ready(ps, js, needs, vmask, r, t);
+    op.row(r);
+    st_release(&ps.done[r], epoch);
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T cg_or0(const T* v, int j) { return j >= 0 ? __ldcg(&v[j]) : T(0); }
+
+// The recurrences of k_dic, k_dic_fwd, k_dic_bwd, k_sip_factor, k_sip_fwd and
+// k_sip_bwd, one row each, for k_tri_pipe.
+template <typename T, bool STAB>
+struct OpDicFactor {
+  int n; const int* col; const signed char* nlo; const T* aoff; const T* diag; T* d;
+  __device__ void row(int r) const {
+    const int kl = nlo[r];
+    T dr = diag[r];
+    for (int s = 0; s < kl; ++s) {
+      const T a = aoff[(size_t)s * n + r];
+      dr = dr - __ldcg(&d[col[(size_t)s * n + r]]) * (a * a);
+    }
+    d[r] = STAB ? T(1) / dr + T(1.0e-20) : T(1) / fmax(dr, T(1.0e-3));
+  }
+};
+
+template <typename T>
+struct OpDicFwd {
+  int n; const int* col; const signed char* nlo; const T* aoff; const T* d; const T* y; T* z;
+  __device__ void row(int r) const {
+    const int kl = nlo[r];
+    T acc = y[r];
+    for (int s = 0; s < kl; ++s) acc = acc + aoff[(size_t)s * n + r] * __ldcg(&z[col[(size_t)s * n + r]]);
+    z[r] = acc * d[r];
+  }
+};
+
+template <typename T>
+struct OpDicBwd {
+  int n, KL; const int* col; const signed char* nup; const T* aoff; const T* d; T* z; T eps;
+  __device__ void row(int r) const {
+    const int ku = nup[r];
+    T acc = __ldcg(&z[r]) / (d[r] + eps);
+    for (int s = 0; s < ku; ++s)
+      acc = acc + aoff[(size_t)(KL + s) * n + r] * __ldcg(&z[col[(size_t)(KL + s) * n + r]]);
+    z[r] = acc * d[r];
+  }
+};
+
+template <typename T>
+struct OpSipFactor {
+  int n; const int* cmp; const T* cf; const T* diag; SipFactor<T> f; T alpha;
+  __device__ void row(int r) const {
+    const int s = cmp[(size_t)2 * n + r], w = cmp[(size_t)3 * n + r];
+    const T un_s = cg_or0(f.un, s), ue_s = cg_or0(f.ue, s), un_w = cg_or0(f.un, w), ue_w = cg_or0(f.ue, w);
+    const T lw = -cf[(size_t)2 * n + r] / (T(1) + alpha * un_s);
+    const T ls = -cf[(size_t)3 * n + r] / (T(1) + alpha * ue_w);
+    const T term1 = alpha * lw * un_s;
+    const T term2 = alpha * ls * ue_w;
+    const T lpr = T(1) / (diag[r] + term1 + term2 - (ls * un_w + lw * ue_s));
+    f.lw[r] = lw;
+    f.ls[r] = ls;
+    f.lpr[r] = lpr;
+    f.un[r] = -(cf[(size_t)1 * n + r] + term1) * lpr;
+    f.ue[r] = -(cf[(size_t)0 * n + r] + term2) * lpr;
+  }
+};
+
+template <typename T>
+struct OpSipFwd {
+  int n; const int* cmp; SipFactor<T> f; const T* res; T* v;
+  __device__ void row(int r) const {
+    const int s = cmp[(size_t)2 * n + r], w = cmp[(size_t)3 * n + r];
+    v[r] = f.lpr[r] * (res[r] - f.lw[r] * cg_or0(v, s) - f.ls[r] * cg_or0(v, w));
+  }
+};
+
+template <typename T>
+struct OpSipBwd {
+  int n; const int* cmp; SipFactor<T> f; T* v;
+  __device__ void row(int r) const {
+    const int nn = cmp[r], e = cmp[(size_t)1 * n + r];
+    v[r] = __ldcg(&v[r]) - f.ue[r] * cg_or0(v, nn) - f.un[r] * cg_or0(v, e);
+  }
+};
 
 }  // namespace cms

@@ -46,18 +46,9 @@
 
 namespace cms {
 
-constexpr unsigned int kSpinLimit = 1u << 22;
 constexpr int kProgressStride = 32;  // unsigned ints between two tiles' progress counters (128 bytes)
 constexpr int NSMAX = 6;  // sums per reduction (partial-sum buffer stride)
 
-__device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
-  unsigned int v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_release(unsigned int* p, unsigned int v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
 __device__ __forceinline__ void red_release_add(unsigned int* p, unsigned int v) {
   asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }

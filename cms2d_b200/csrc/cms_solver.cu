@@ -97,6 +97,19 @@ struct cms_solver {
   // its properties (-1 not built) and the 5-point solvers' scratch
   int* d_cmp = nullptr;
   int leg_props = -1;
+  // pipelined passes (orderings with many groups): chunk table, per-row pass
+  // counts, work-unit ticket, error flag, passes issued in the current solve
+  int* d_pipe_cstart = nullptr;
+  int pipe_nchunk = 0;
+  unsigned int* d_pipe_done = nullptr;
+  unsigned int* d_pipe_ticket = nullptr;
+  int* d_pipe_err = nullptr;
+  unsigned int pipe_epoch = 0;
+  std::vector<int> pipe_gchunk;  // [G + 1] first chunk of each group
+  int pipe_wave = 0;             // 1 + the largest group step to an upper neighbour
+  int2* d_pipe_units = nullptr;  // wavefront order of the units of forward passes
+  size_t pipe_units_cap = 0;
+  int pipe_units_npass = 0;
   double* leg64 = nullptr;
   float* leg32 = nullptr;
   cms::Staging<double> S64;
