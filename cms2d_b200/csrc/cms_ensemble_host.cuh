@@ -228,7 +228,9 @@ static int ensemble_solve(Ens* E, const std::vector<int>& act, int which) {
     CHK(refine_batched(E, act, nswp, infos));
   } else {
     for (size_t j = 0; j < act.size(); ++j) {
-      const int rc = solve_core64(E->m[act[j]]->S, E->m[act[j]]->opts.nsolv, nswp[j], infos[j]);
+      Flow* F = E->m[act[j]];
+      const int nvar = which == ES_U ? 2 : which == ES_V ? 3 : 1;
+      const int rc = solve_core64(F->S, F->opts.nsolv, nswp[j], infos[j], nvar, F->st.acoef, F->nD);
       if (rc == CMS_DEVICE_ERROR || rc == CMS_UNSUPPORTED || rc == CMS_BAD_ARGUMENT) return rc;
     }
   }

@@ -129,22 +129,66 @@ using Flow = ::cms_flow;
 
 // Krylov solve of the system a flow prologue wrote into the FP64 buffers
 // (A64, W64.b, W64.x; A32 too for refinement); the solution stays in W64.x.
-static int solve_core64(Solver* S, int nsolv, int nswp, cms_solve_info* info) {
+// The solve of a system the flow kernels assembled into the solver's device
+// buffers.  nvar: the variable index of solve(..., n) (1 pp, 2 u, 3 v), read
+// by the MATRIX_SOLVER options other than BiCGStab and GMRES; face: the flow's
+// face coefficients ([nmf][nD], device rows), from which SIP takes its compass
+// coefficients.
+static int solve_core64(Solver* S, int nsolv, int nswp, cms_solve_info* info, int nvar = 0,
+                        const double* face = nullptr, int nD = 0) {
   std::memset(info, 0, sizeof(*info));
   info->ncolors = S->hp.G;
   info->true_relres = -1.0;
-  if (nsolv != 3 && nsolv != 4) return info->status = CMS_UNSUPPORTED;
+  if (nsolv < 0 || nsolv > 8) return info->status = CMS_UNSUPPORTED;
   const int maxit = S->opts.max_iters > 0 ? S->opts.max_iters : nswp;
   const double tol = S->opts.tol > 0 ? S->opts.tol : 1e-3;
   const int norm = S->opts.norm == 2 ? 2 : 1;
-  const bool refine = S->opts.precision == CMS_PREC_FP32_REFINE;
-  if (refine) CHK(run_refine(S, nsolv, maxit, tol, info));
-  else CHK(run_krylov<double>(S, S->A64, S->W64, nsolv, maxit, norm, tol, 0));
+  const bool legacy = nsolv != 3 && nsolv != 4;
+  bool refine = S->opts.precision == CMS_PREC_FP32_REFINE;
+  LegPlan plan;
+  int leg_sweeps = 0;
+  if (legacy) {
+    if (nsolv >= 6) {
+      const int props = legacy_props(S);
+      const int kind = legacy_plan(nsolv, nvar, 0.0, maxit, S->opts.nswp0_vel).kind;
+      if (!(props & LEG_FIVE_POINT) || (kind == LK_SIP && (!(props & LEG_SIP_ORDER) || !face))) {
+        std::snprintf(g_last_error, sizeof(g_last_error),
+                      "nsolv %d: SIP, ICCG and ICCGSTAB need four faces per cell, SIP also the natural ordering",
+                      nsolv);
+        return info->status = CMS_UNSUPPORTED;
+      }
+    }
+    double rm = 0.0;
+    if (nsolv == 2 || nsolv == 5) {  // the branch reads this call's rmom
+      CMS_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, S->stream));
+      CMS_CUDA(cudaStreamSynchronize(S->stream));
+      rm = S->h_st->s[S_RMOM];
+    }
+    plan = legacy_plan(nsolv, nvar, rm, maxit, S->opts.nswp0_vel);
+    refine = refine && plan.kind == LK_KRYLOV;  // the hybrid's BiCGStab branch keeps the refinement
+  }
+  if (plan.kind == LK_NONE) {
+  } else if (plan.kind == LK_GS) {
+    CHK(run_gauss_seidel<double>(S, S->A64, S->W64, plan.sweeps, plan.symmetric, plan.sor, S->opts.relaxsor,
+                                 &leg_sweeps));
+  } else if (plan.kind == LK_SIP) {
+    CHK(run_sip<double>(S, S->A64, S->W64, face, maxit, nD));
+  } else if (plan.kind == LK_ICCG) {
+    CHK(run_iccg<double>(S, S->A64, S->W64, maxit));
+  } else if (plan.kind == LK_ICCGSTAB) {
+    CHK(run_iccgstab<double>(S, S->A64, S->W64, maxit));
+  } else if (refine) {
+    CHK(run_refine(S, legacy ? 3 : nsolv, maxit, tol, info));
+  } else {
+    CHK(run_krylov<double>(S, S->A64, S->W64, legacy ? 3 : nsolv, maxit, norm, tol, 0));
+  }
   CMS_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, S->stream));
   CMS_CUDA(cudaStreamSynchronize(S->stream));
   const DevState& h = *S->h_st;
   info->rmom = h.s[S_RMOM];
-  if (!refine) {
+  if (plan.kind == LK_GS || plan.kind == LK_NONE) {
+    info->iters = info->inner = leg_sweeps;
+  } else if (!refine) {
     info->iters = h.iter;
     info->inner = (nsolv == 4) ? h.inner : h.iter;
     info->relres = h.s[S_RELRES];
@@ -391,6 +435,7 @@ static int flow_create(int ncells, int ncellsD, int nmf, const int* c2c, const i
   so.inner_tol = F->opts.inner_tol;
   so.inner_max = F->opts.inner_max;
   so.multi_kernel = F->opts.multi_kernel;
+  if (F->opts.relaxsor > 0.0) so.relaxsor = F->opts.relaxsor;
   int rc = cms_solver_create(ncells, ncellsD, nmf, c2c, ncface, iwet.data(), &so, &F->S);
   if (rc) return fail(rc);
   Solver* S = F->S;
@@ -605,7 +650,8 @@ static int flow_solve_end(Flow* F, double* phi, double* rmom, const cms_solve_in
 static int flow_solve(Flow* F, double* ss, const double* sp, double* phi, double relax, int nswp, double* rmom,
                       cms_solve_info* info) {
   CHK(flow_solve_begin(F, ss, sp, phi, relax));
-  const int rc = solve_core64(F->S, F->opts.nsolv, nswp, info);
+  const int nvar = phi == F->st.u ? 2 : phi == F->st.v ? 3 : 1;
+  const int rc = solve_core64(F->S, F->opts.nsolv, nswp, info, nvar, F->st.acoef, F->nD);
   if (rc == CMS_DEVICE_ERROR || rc == CMS_UNSUPPORTED || rc == CMS_BAD_ARGUMENT) return rc;
   return flow_solve_end(F, phi, rmom, info);
 }
@@ -1221,6 +1267,7 @@ void cms_flow_default_opts(cms_flow_opts* o) {
   o->hdry = 0.05;
   o->ponding = 0;
   o->narrowchannels = 0;
+  o->relaxsor = 1.8;
 }
 
 int cms_flow_create(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, const int* ncface,

@@ -121,6 +121,15 @@ __global__ void __launch_bounds__(TPB) k_sip_coef(int n, int nmf, const int* __r
   }
 }
 
+// cf[k*n + r] = face coefficient k of device row r in a [nmf][nD] device-row array
+template <typename T>
+__global__ void __launch_bounds__(TPB) k_sip_coef_dev(int n, int nD, const T* __restrict__ face, T* cf) {
+  for (int r = blockIdx.x * TPB + threadIdx.x; r < n; r += gridDim.x * TPB) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) cf[(size_t)k * n + r] = face[(size_t)k * nD + r];
+  }
+}
+
 template <typename T>
 struct SipFactor {
   T *lw, *ls, *lpr, *un, *ue;

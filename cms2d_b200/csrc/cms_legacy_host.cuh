@@ -369,9 +369,10 @@ static int run_iccgstab(Solver* S, Mat<T>& A, Work<T>& W, int maxit) {
   return use_pipe(S) ? pipe_end(S) : CMS_OK;
 }
 
-// SIP (sip.f90:2-174); acoef is the caller's natural-order array.
+// SIP (sip.f90:2-174).  acoef: the caller's natural-order array, or with
+// face_nD > 0 the flow's face coefficients ([nmf][face_nD], device rows).
 template <typename T>
-static int run_sip(Solver* S, Mat<T>& A, Work<T>& W, const T* acoef, int maxit) {
+static int run_sip(Solver* S, Mat<T>& A, Work<T>& W, const T* acoef, int maxit, int face_nD = 0) {
   const HostPattern& P = S->hp;
   const int n = P.n, nb_all = S->tab.blk[S->tab.ng];
   T* base = legacy_scratch<T>(S);
@@ -380,8 +381,12 @@ static int run_sip(Solver* S, Mat<T>& A, Work<T>& W, const T* acoef, int maxit) 
   SipFactor<T> f{base + (size_t)4 * n, base + (size_t)5 * n, base + (size_t)6 * n, base + (size_t)7 * n,
                  base + (size_t)8 * n};
   const double s = sizeof(T);
-  KLAUNCH(S, P_VEC, (double)n * (4 + 8 * s),
-          (k_sip_coef<T><<<gsz(n), TPB, 0, S->stream>>>(n, P.nmf, S->d_perm, acoef, cf)));
+  if (face_nD > 0)
+    KLAUNCH(S, P_VEC, (double)n * 8 * s,
+            (k_sip_coef_dev<T><<<gsz(n), TPB, 0, S->stream>>>(n, face_nD, acoef, cf)));
+  else
+    KLAUNCH(S, P_VEC, (double)n * (4 + 8 * s),
+            (k_sip_coef<T><<<gsz(n), TPB, 0, S->stream>>>(n, P.nmf, S->d_perm, acoef, cf)));
   const bool pipe = use_pipe(S);
   // counters first: the pipelined factor pass below skips itself while the
   // previous solve's stop flag is still set

@@ -13,6 +13,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
+from . import solver as _solver
 
 _ORDER = {"multicolor": _lib.ORDER_MULTICOLOR, "natural": _lib.ORDER_NATURAL}
 _PREC = {"fp64": _lib.PREC_FP64, "fp32_refine": _lib.PREC_FP32_REFINE}
@@ -25,7 +26,8 @@ class FlowOpts(C.Structure):
     _fields_ = [("nsolv", C.c_int), ("ordering", C.c_int), ("precision", C.c_int), ("norm", C.c_int),
                 ("tol", C.c_double), ("nswp_pp", C.c_int), ("nswp_uv", C.c_int), ("maxit", C.c_int),
                 ("skewcor", C.c_int), ("inner_tol", C.c_double), ("inner_max", C.c_int),
-                ("multi_kernel", C.c_int), ("hdry", C.c_double), ("ponding", C.c_int), ("narrowchannels", C.c_int)]
+                ("multi_kernel", C.c_int), ("hdry", C.c_double), ("ponding", C.c_int), ("narrowchannels", C.c_int),
+                ("relaxsor", C.c_double)]
 
 
 class FlowInfo(C.Structure):
@@ -70,7 +72,7 @@ class FlowModel:
                  tol: float = 1e-3, norm: int = 1, nswp_pp: int | None = None, nswp_uv: int | None = None,
                  maxit: int = 0, skewcor: bool = True, inner_tol: float = 1e-3, inner_max: int = 50,
                  multi_kernel: bool = False, hdry: float = 0.05, ponding: bool = False,
-                 narrowchannels: bool = False):
+                 narrowchannels: bool = False, relaxsor: float = 1.8):
         L = _lib.lib()
         _bind(L)
         self.case = case
@@ -83,9 +85,9 @@ class FlowModel:
         o.precision = _PREC[precision]
         o.tol = tol
         o.norm = norm
-        # nswp defaults per solver (flow.F90:779-792)
-        o.nswp_pp = nswp_pp if nswp_pp is not None else (15 if nsolv == 3 else 20)
-        o.nswp_uv = nswp_uv if nswp_uv is not None else 5
+        # nswp defaults per solver (flow.F90:752-821)
+        o.nswp_pp = nswp_pp if nswp_pp is not None else _solver.NSWP_DEFAULT[nsolv][1]
+        o.nswp_uv = nswp_uv if nswp_uv is not None else _solver.NSWP_DEFAULT[nsolv][2]
         o.maxit = maxit
         o.skewcor = int(skewcor)
         o.inner_tol = inner_tol
@@ -94,6 +96,7 @@ class FlowModel:
         o.hdry = hdry
         o.ponding = int(ponding)
         o.narrowchannels = int(narrowchannels)
+        o.relaxsor = relaxsor
         self.opts = o
         self._keep = [np.ascontiguousarray(a) for a in (
             g.cell2cell.astype(np.int32), g.ncface.astype(np.int32), g.idirface.astype(np.int32),

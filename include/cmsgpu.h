@@ -208,7 +208,8 @@ int cms_order_build(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell
 typedef struct cms_flow cms_flow;
 
 typedef struct cms_flow_opts {
-  int nsolv;         /* 3 BiCGStab, 4 GMRES (solvers.f90:8)                        */
+  int nsolv;         /* MATRIX_SOLVER 0-8 as in solve() (cms_solver_solve_n_d);
+                        4 GMRES by default (solvers.f90:8)                          */
   int ordering;      /* CMS_ORDER_*                                                */
   int precision;     /* CMS_PREC_FP64 or CMS_PREC_FP32_REFINE (the solves)         */
   int norm;          /* BiCGStab stopping norm (1 = L1 as the reference)           */
@@ -223,6 +224,7 @@ typedef struct cms_flow_opts {
   double hdry;       /* drying depth (flow.F90:51, hmin = hdry); 0: 0.05 m          */
   int ponding;       /* keep isolated water bodies (flow.F90:54; default 0)         */
   int narrowchannels; /* keep one-cell-wide channels (flow.F90:55; default 0)       */
+  double relaxsor;   /* SOR constant of nsolv 2 and 5 (flow.F90:131; default 1.8)   */
 } cms_flow_opts;
 
 typedef struct cms_flow_info {

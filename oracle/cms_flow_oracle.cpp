@@ -26,6 +26,9 @@ void orc_set_wet(void* h, const int* iwet);
 int orc_solve_d(void* hv, const double* acoef, double* ss, const double* sp, double* res, double* phi, double relax,
                 int nswp, int nsolv, int precond, double tol, int lfil, double droptol, double permtol, double* rmom,
                 int* iters, int* inner, double* relres, int norm);
+int orc_solve_n_d(void* hv, int n, const double* acoef, double* ss, const double* sp, double* res, double* phi,
+                  double relax, int nswp, int nsolv, double relaxsor, int nswp0_vel, int precond, double tol,
+                  double* rmom, int* iters, int* inner, double* relres, int norm);
 }
 
 namespace {
@@ -90,6 +93,7 @@ struct Flow {
   void* solver_perm = nullptr;
   // solver settings
   int nsolv = 4, precond = 1, nswp_pp = 20, nswp_uv = 5, norm = 1;
+  double relaxsor = 1.8;  // SOR constant of nsolv 2 and 5 (flow.F90:131)
   double tol = 1e-3;
   int last_niter = 0, last_iconv = 1;
   long long solve_iters = 0;
@@ -1024,9 +1028,16 @@ int solve(Flow& f, V& ss, V& sp, V& res, V& phi, int var, double* rmom_out) {
   int nswp = var == 1 ? f.nswp_pp : f.nswp_uv;
   double rm = 0, rr = 0;
   int it = 0, inner = 0;
-  int lfil = f.nsolv == 4 ? 8 : 35;
-  int st = orc_solve_d(pm ? f.solver_perm : f.solver, a.data(), s0.data(), p0.data(), r0.data(), x0.data(), relax,
-                       nswp, f.nsolv, f.precond, f.tol, lfil, 1.0e-3, 0.5, &rm, &it, &inner, &rr, f.norm);
+  int st;
+  if (f.nsolv == 3 || f.nsolv == 4) {
+    const int lfil = f.nsolv == 4 ? 8 : 35;
+    st = orc_solve_d(pm ? f.solver_perm : f.solver, a.data(), s0.data(), p0.data(), r0.data(), x0.data(), relax,
+                     nswp, f.nsolv, f.precond, f.tol, lfil, 1.0e-3, 0.5, &rm, &it, &inner, &rr, f.norm);
+  } else {  // the other MATRIX_SOLVER options read the variable index (solvers.f90:242-289)
+    st = orc_solve_n_d(pm ? f.solver_perm : f.solver, var, a.data(), s0.data(), p0.data(), r0.data(), x0.data(),
+                       relax, nswp, f.nsolv, f.relaxsor, f.nswp_uv, f.precond, f.tol, &rm, &it, &inner, &rr,
+                       f.norm);
+  }
   f.solve_iters += it;
   for (int r = 0; r < nD; ++r) {
     const int i = row_of(r) + 1;

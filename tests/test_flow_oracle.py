@@ -59,3 +59,30 @@ def test_telescoping_joint_cells_present():
     r = f.step()
     assert r["status"] == 0
     assert np.all(np.isfinite(f.get("u")[: c.grid.ncells]))
+
+
+def test_every_matrix_solver_option_steps_the_basin():
+    """The oracle's flow step with each MATRIX_SOLVER option at the reference's
+    default nswp(n) (flow.F90:752-821): steps finish and follow the tide like
+    GMRES does (the water level differs only by the solvers' truncation).
+    ADI (0), which solve() has no branch for, leaves the corrections at zero,
+    and check_conv reports the outer loop divergent."""
+    from cms2d_b200 import solver as S
+    c = cases.tidal_basin(40, 20, seed=0)
+    n = c.grid.ncells
+    ref = O.FlowOracle(c)
+    ref.set_solver(nsolv=4, tol=1e-3)
+    ref.init()
+    for _ in range(3):
+        ref.step()
+    for nsolv in (0, 1, 2, 3, 5, 6, 7, 8):
+        d = S.NSWP_DEFAULT[nsolv]
+        f = O.FlowOracle(c)
+        f.set_solver(nsolv=nsolv, tol=1e-3, nswp_pp=d[1], nswp_uv=d[2])
+        f.init()
+        status = [f.step()["status"] for _ in range(3)]
+        if nsolv == 0:
+            assert status == [2, 2, 2]
+            continue
+        assert status == [0, 0, 0], nsolv
+        assert np.abs(f.get("eta")[:n] - ref.get("eta")[:n]).max() < 1e-6, nsolv
