@@ -398,6 +398,7 @@ struct PipeSched {
   unsigned int* done;    // [n] passes completed per row
   unsigned int* ticket;  // work-unit counter of the launch (zero at launch)
   int* err;              // [8] err[0]: a wait ran out; err[1..5]: where (pipe_ready)
+  unsigned int spin_limit;  // polls before a wait gives up (kSpinLimit)
 };
 
 // Waits until every row js[q] (bit q of vmask set) has completed needs[q]
@@ -419,7 +420,7 @@ __device__ __forceinline__ bool pipe_ready(const PipeSched& ps, const int (&js)[
         if (v < needs[q]) { badj = js[q]; badneed = needs[q]; seen = v; }
       }
     if (badj < 0) break;
-    if (++spins > kSpinLimit) {
+    if (++spins > ps.spin_limit) {
       if (atomicCAS(ps.err, 0, 1) == 0) {
         ps.err[1] = r; ps.err[2] = badj; ps.err[3] = (int)badneed; ps.err[4] = (int)seen; ps.err[5] = unit;
       }
@@ -504,6 +505,15 @@ __global__ void __launch_bounds__(TPB) k_gs_pipe(int n, int KL, const int* __res
     else x[r] = (term + br) / dr;
     st_release(&ps.done[r], mine);
   }
+}
+
+// The wait of the pipelined passes on rows that never complete (test of the
+// bounded wait: every thread of one block waits on row j of a done array
+// nobody writes, gives up after ps.spin_limit polls and records it).
+__global__ void k_pipe_wait_probe(PipeSched ps, int j) {
+  int js[1] = {j};
+  unsigned int needs[1] = {1u};
+  pipe_ready(ps, js, needs, 1u, (int)threadIdx.x, 0);
 }
 
 // One pipelined pass of a triangular recurrence: Op::row(r) reads only rows

@@ -133,8 +133,9 @@ static int pipe_units(Solver* S, int npass) {
 }
 
 static PipeSched pipe_sched(Solver* S) {
-  return PipeSched{S->d_pipe_cstart, S->pipe_nchunk, S->d_pipe_done, S->d_pipe_ticket, S->d_pipe_err};
+  return PipeSched{S->d_pipe_cstart, S->pipe_nchunk, S->d_pipe_done, S->d_pipe_ticket, S->d_pipe_err, kSpinLimit};
 }
+
 
 // End of such a solve: a wait that ran out is a device error.
 static int pipe_end(Solver* S) {
@@ -148,6 +149,20 @@ static int pipe_end(Solver* S) {
     return CMS_DEVICE_ERROR;
   }
   return CMS_OK;
+}
+
+// Runs the pipelined passes' wait on a row that never completes, with a
+// limit of spin_limit polls: the wait must give up, record where, and leave
+// the device usable.  CMS_DEVICE_ERROR (with the message) is the expected
+// result; anything else means the bounded wait failed.
+static int pipe_wait_selftest(Solver* S, unsigned int spin_limit) {
+  CHK(pipe_begin(S));
+  PipeSched ps = pipe_sched(S);
+  ps.spin_limit = spin_limit;
+  KLAUNCH(S, P_SCALAR, 0, (k_pipe_wait_probe<<<1, 32, 0, S->stream>>>(ps, 0)));
+  const int rc = pipe_end(S);
+  CMS_CUDA(cudaGetLastError());
+  return rc;
 }
 
 // One pipelined pass of a triangular recurrence (forward: lower slots first).

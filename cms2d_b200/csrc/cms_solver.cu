@@ -1114,6 +1114,11 @@ int cms_order_build(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell
 
 const char* cms_gpu_version(void) { return "cmsgpu 0.1 (sm_100a)"; }
 
+int cms_solver_wait_selftest(cms_solver* s, unsigned int spin_limit) {
+  if (!s || spin_limit == 0) return CMS_BAD_ARGUMENT;
+  return cms::pipe_wait_selftest(s, spin_limit);
+}
+
 const char* cms_gpu_last_error(void) { return g_last_error; }
 
 }  // extern "C"

@@ -370,6 +370,13 @@ int cms_solve_residual_noalloc_d(int ncells, int ncellsD, int nmaxfaces, const i
                                  const double* phi, double relax, double* rmom, void* stream);
 const char* cms_noalloc_last_error(void);
 
+/* Failure-detection check of the bounded device waits: one block waits on a
+ * progress flag that nothing sets, as the pipelined sweeps wait on a
+ * neighbour row, and gives up after spin_limit polls.  Returns
+ * CMS_DEVICE_ERROR with the wait's position in cms_gpu_last_error() -- the
+ * expected result -- and leaves the handle usable. */
+int cms_solver_wait_selftest(cms_solver* s, unsigned int spin_limit);
+
 /* Library version string. */
 const char* cms_gpu_version(void);
 /* Text of the last error a call reported (device or argument errors). */
