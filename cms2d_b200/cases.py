@@ -18,6 +18,10 @@ tidal_flat:   intertidal flat that wets and dries over the tide: bed from 1 m
               M2 tide of 1 m.  Cartesian, or telescoping with a refined zone
               around the creek.
 
+from_grid_file: a case on a grid read from a .tel or .cart file
+              (cms2d_b200.gridio), with a water-level string on its open north
+              edge, a tide and a uniform Manning n.
+
 A case carries the grid (cms2d_b200.grid.Grid), bed elevation zb (= -depth,
 ncellsD values; dummies copy their parent cell), coefman (ncells), the
 water-level string (1-based cells and faces of the open edge) and the tide.
@@ -108,6 +112,16 @@ def tidal_basin(nx: int = 200, ny: int = 100, dx: float = 20.0, seed: int = 0, a
     th_cells, th_faces = _north_string(g)
     return Case("tidal_basin", g, zb, np.full(n, manning), th_cells, th_faces, [(amp, M2_HOURS)], dt,
                 int(round(hours * 3600.0 / dt)))
+
+
+def from_grid_file(gf, tide=((0.5, M2_HOURS),), manning: float = 0.025, dt: float = 600.0, hours: float = 24.0,
+                   name: str = "grid_file") -> Case:
+    """A case on a grid read by gridio.read_tel / read_cart: the bed from the
+    file, the water-level string on every north face that leads to a dummy."""
+    g = gf.grid
+    th_cells, th_faces = _north_string(g)
+    return Case(name, g, np.asarray(gf.zb, dtype=np.float64), np.full(g.ncells, manning), th_cells, th_faces,
+                [tuple(t) for t in tide], dt, int(round(hours * 3600.0 / dt)))
 
 
 def ensemble_basins(nmembers: int = 64, seed: int = 0, nmin: int = 50_000, nmax: int = 400_000,

@@ -163,3 +163,28 @@ def test_reference_test_grids(path):
                 assert len(kk) == 1 and int(g.idirface[j, kk[0]]) == back[d]
             else:  # dummy: its back link on the opposite face
                 assert int(g.cell2cell[j, back[d] - 1]) - 1 == i and int(g.ncface[j]) == 4
+
+
+def test_case_from_grid_file_steps(tmp_path):
+    """A telescoping file read back and run: the oracle's flow steps finish and
+    follow the tide, identical to the same case built from the level map."""
+    from cms2d_b200 import cases
+    from oracle import oracle as O
+    lev = G.refinement_rectangles(10, 8, [(1, 3, 2, 7, 6)])
+    depth = lambda x, y: 2.0 + 0.02 * y  # noqa: E731
+    p = tmp_path / "basin.tel"
+    gridio.write_tel(p, lev, 20.0, depth)
+    c = cases.from_grid_file(gridio.read_tel(p), dt=300.0)
+    g2 = G.telescoping_grid(lev, 20.0, nmaxfaces=6)
+    zb2 = cases._fill_dummies(g2, -(2.0 + 0.02 * g2.y[: g2.ncells]))
+    c2 = cases.Case("ref", g2, zb2, np.full(g2.ncells, 0.025), *cases._north_string(g2), [(0.5, cases.M2_HOURS)],
+                    300.0, 10)
+    runs = []
+    for case in (c, c2):
+        f = O.FlowOracle(case)
+        f.init()
+        for _ in range(3):
+            assert f.step()["status"] == 0
+        runs.append(f.get("eta")[: g2.ncells])
+    np.testing.assert_allclose(runs[0], runs[1], rtol=0, atol=1e-12)
+    assert abs(runs[0].mean() - c.wse(900.0)) < 0.02
