@@ -1,0 +1,55 @@
+"""Card files (*.cmcards): the cards the implicit flow step serves, read as
+flow_cards reads them, and a case run from the reference's own test inputs
+(grid and cards, read in place where the reference tree is present)."""
+import glob
+import os
+
+import pytest
+
+from cms2d_b200 import cards, cases, gridio
+from cms2d_b200 import solver as S
+from oracle import oracle as O
+
+REF_CARDS = sorted(glob.glob("/root/reference/testing/tests_flow/L05*/*.cmcards"))
+
+
+def test_flow_settings(tmp_path):
+    p = tmp_path / "a.cmcards"
+    p.write_text("""! comment line
+CMS_VERSION        5.3
+TELESCOPING        "grid one.tel"
+SOLUTION_SCHEME    IMPLICIT
+MATRIX_SOLVER      GAUSS-SEIDEL-SOR   ! trailing comment
+SOR_CONSTANT       1.6
+PRESSURE_ITERATIONS 60
+VEL_ITER           12
+HYDRO_MAX_ITER     25
+DRYING_DEPTH       5 'cm'
+WATER_PONDING      ON
+NARROW_CHANNELS    OFF
+SKEWNESS_CORRECTION OFF
+HYDRO_TIMESTEP     10 'min'
+MATRIX_SOLVER      HYBRID
+""")
+    kw, dt, grid = cards.flow_settings(cards.read_cards(p), str(tmp_path))
+    assert kw == dict(nsolv=5, nswp_pp=60, nswp_uv=12, maxit=25, relaxsor=1.6, hdry=0.05, ponding=True,
+                      narrowchannels=False, skewcor=False)
+    assert dt == 600.0 and grid == os.path.join(str(tmp_path), "grid one.tel")
+    p.write_text("SOLUTION_SCHEME EXPLICIT\n")
+    with pytest.raises(ValueError, match="implicit"):
+        cards.flow_settings(cards.read_cards(p))
+
+
+@pytest.mark.skipif(not REF_CARDS, reason="reference test inputs not present")
+def test_reference_test_case_runs_from_its_cards():
+    path = REF_CARDS[0]
+    kw, dt, grid = cards.flow_settings(cards.read_cards(path), os.path.dirname(path))
+    assert kw["nsolv"] == S.SOLVER_NAMES["GMRES"] and kw["hdry"] == 0.05 and kw["skewcor"] is True
+    assert dt == 60.0 and os.path.exists(grid)
+    case = cases.from_grid_file(gridio.read_tel(grid), tide=((0.02, cases.M2_HOURS),), dt=dt)
+    d = S.NSWP_DEFAULT[kw["nsolv"]]
+    f = O.FlowOracle(case)
+    f.set_solver(nsolv=kw["nsolv"], precond=O.PC_ILU0, tol=1e-3, nswp_pp=d[1], nswp_uv=d[2])
+    f.init()
+    for _ in range(3):
+        assert f.step()["status"] == 0
