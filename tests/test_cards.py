@@ -10,7 +10,7 @@ from cms2d_b200 import cards, cases, gridio
 from cms2d_b200 import solver as S
 from oracle import oracle as O
 
-REF_CARDS = sorted(glob.glob("/root/reference/testing/tests_flow/L05*/*.cmcards"))
+REF_CARDS = sorted(glob.glob("/root/reference/testing/tests_flow/*/*.cmcards"))
 
 
 def test_flow_settings(tmp_path):
@@ -41,8 +41,16 @@ MATRIX_SOLVER      HYBRID
 
 
 @pytest.mark.skipif(not REF_CARDS, reason="reference test inputs not present")
+@pytest.mark.parametrize("path", REF_CARDS, ids=[os.path.basename(p) for p in REF_CARDS])
+def test_reference_cards_parse(path):
+    kw, dt, grid = cards.flow_settings(cards.read_cards(path), os.path.dirname(path))
+    assert kw["nsolv"] in S.SOLVER_NAMES.values() and 0 < kw["hdry"] < 1 and dt > 0
+    assert gridio.read_tel(grid).grid.ncells > 0
+
+
+@pytest.mark.skipif(not REF_CARDS, reason="reference test inputs not present")
 def test_reference_test_case_runs_from_its_cards():
-    path = REF_CARDS[0]
+    path = [p for p in REF_CARDS if "L05" in os.path.basename(p)][0]
     kw, dt, grid = cards.flow_settings(cards.read_cards(path), os.path.dirname(path))
     assert kw["nsolv"] == S.SOLVER_NAMES["GMRES"] and kw["hdry"] == 0.05 and kw["skewcor"] is True
     assert dt == 60.0 and os.path.exists(grid)
