@@ -1415,5 +1415,10 @@ void orcf_set_wetdry(void* h, int ponding, int narrowchannels) {
   f->P.narrowchannels = narrowchannels != 0;
 }
 int orcf_njoint(void* h) { return (int)static_cast<Flow*>(h)->idjoint.size(); }
+// DRYING_DEPTH card: hmin = hdry, hdry1 = 5 hdry, hdry2 = 2 hdry (flow.F90:686-693)
+void orcf_set_hdry(void* h, double hdry) {
+  auto* f = static_cast<Flow*>(h);
+  f->P.hmin = hdry; f->P.hdry = hdry; f->P.hdry1 = 5.0 * hdry; f->P.hdry2 = 2.0 * hdry;
+}
 
 }  // extern "C"

@@ -162,6 +162,7 @@ class FlowOracle:
             L.orcf_set_order.argtypes = [P, i32]
             L.orcf_last_nlist.argtypes = [P]
             L.orcf_set_wetdry.argtypes = [P, C.c_int, C.c_int]
+            L.orcf_set_hdry.argtypes = [P, C.c_double]
             L._flow_bound = True
         g = case.grid
         self.case = case
@@ -189,9 +190,13 @@ class FlowOracle:
         """Solve in another unknown order (perm[r] = natural 0-based cell of solver row r)."""
         lib().orcf_set_order(self._h, np.ascontiguousarray(perm, np.int32))
 
-    def set_wetdry(self, ponding=False, narrowchannels=False):
-        """The ponding and narrow-channel switches of the wetting and drying rules."""
+    def set_wetdry(self, ponding=False, narrowchannels=False, hdry=None):
+        """The ponding and narrow-channel switches of the wetting and drying
+        rules, and the drying depth (hmin = hdry, the one- and two-cell depths
+        5 and 2 hdry)."""
         lib().orcf_set_wetdry(self._h, int(ponding), int(narrowchannels))
+        if hdry is not None:
+            lib().orcf_set_hdry(self._h, float(hdry))
 
     def init(self, eta0=None):
         if eta0 is None:

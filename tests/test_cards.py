@@ -49,15 +49,17 @@ def test_reference_cards_parse(path):
 
 
 @pytest.mark.skipif(not REF_CARDS, reason="reference test inputs not present")
-def test_reference_test_case_runs_from_its_cards():
-    path = [p for p in REF_CARDS if "L05" in os.path.basename(p)][0]
+@pytest.mark.parametrize("path", REF_CARDS, ids=[os.path.basename(p) for p in REF_CARDS])
+def test_reference_test_case_runs_from_its_cards(path):
     kw, dt, grid = cards.flow_settings(cards.read_cards(path), os.path.dirname(path))
-    assert kw["nsolv"] == S.SOLVER_NAMES["GMRES"] and kw["hdry"] == 0.05 and kw["skewcor"] is True
+    assert kw["nsolv"] == S.SOLVER_NAMES["GMRES"] and kw["skewcor"] is True
     assert dt == 60.0 and os.path.exists(grid)
     case = cases.from_grid_file(gridio.read_tel(grid), tide=((0.02, cases.M2_HOURS),), dt=dt)
     d = S.NSWP_DEFAULT[kw["nsolv"]]
     f = O.FlowOracle(case)
     f.set_solver(nsolv=kw["nsolv"], precond=O.PC_ILU0, tol=1e-3, nswp_pp=d[1], nswp_uv=d[2])
+    f.set_wetdry(ponding=kw.get("ponding", False), narrowchannels=kw.get("narrowchannels", False),
+                 hdry=kw["hdry"])
     f.init()
     for _ in range(3):
         assert f.step()["status"] == 0
