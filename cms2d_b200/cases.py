@@ -18,6 +18,9 @@ tidal_flat:   intertidal flat that wets and dries over the tide: bed from 1 m
               M2 tide of 1 m.  Cartesian, or telescoping with a refined zone
               around the creek.
 
+gauges:       seeded water-level gauge cells of a case (the misfit of the
+              adjoint gradient and the fixtures of the parity tests).
+
 from_grid_file: a case on a grid read from a .tel or .cart file
               (cms2d_b200.gridio), with a water-level string on its open north
               edge, a tide and a uniform Manning n.
@@ -230,3 +233,13 @@ def tidal_flat(nx: int = 60, ny: int = 40, dx: float = 20.0, seed: int = 0, amp:
     th_cells, th_faces = _north_string(g)
     return Case("tidal_flat", g, zb, np.full(n, manning), th_cells, th_faces, [(amp, M2_HOURS)], dt,
                 int(round(hours * 3600.0 / dt)), t0=t0_hours * 3600.0)
+
+
+def gauges(case: Case, count: int = 200, seed: int = 5, min_depth: float = 1.0) -> np.ndarray:
+    """count seeded gauge cells (0-based active cell numbers, ascending):
+    cells at least min_depth below mean sea level, away from the drying depth,
+    so that a water-level gauge there stays wet."""
+    n = case.grid.ncells
+    ok = np.nonzero(-case.zb[:n] >= min_depth)[0]
+    rng = np.random.default_rng(seed)
+    return np.sort(rng.choice(ok, size=min(count, ok.size), replace=False)).astype(np.int64)

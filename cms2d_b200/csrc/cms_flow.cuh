@@ -14,6 +14,7 @@ namespace cms {
 
 struct FlowDev {
   int n, nD, nmf, nsc, ider;
+  int ndsch;  // advection scheme of the momentum coefficients (0 none, 1 upwind, 2 hybrid, 3 power law, 4 exponential)
   // connectivity (device numbering)
   const int* ncface;          // [nD]
   const int* nb;              // [nmf][nD] neighbour (dummies >= n), -1 none
@@ -51,7 +52,28 @@ __device__ __forceinline__ double expcoef(double dk, double fk) {  // comp_lib.f
   const double peck = absfk / fmax(fmax(dk, 1.0e-6), absfk);
   return dk * peck / fmax(exp(peck) - 1.0, 1.0e-6) + fmax(0.0, -fk);
 }
-__device__ __forceinline__ double upwcoef(double dk, double fk) { return dk + fmax(0.0, -fk); }
+__device__ __forceinline__ double upwcoef(double dk, double fk) { return dk + fmax(0.0, -fk); }  // comp_lib.f90:54-64
+__device__ __forceinline__ double hybcoef(double dk, double fk) {  // comp_lib.f90:67-78
+  const double peck = fabs(fk) / fmax(dk, 1.0e-6);
+  return dk * fmax(0.0, 1.0 - 0.5 * peck) + fmax(0.0, -fk);
+}
+__device__ __forceinline__ double powcoef(double dk, double fk) {  // comp_lib.f90:81-93
+  const double absfk = fabs(fk);
+  const double peck = absfk / fmax(fmax(dk, absfk), 1.0e-6);
+  const double p2 = peck * peck;
+  return dk * (1.0 - p2 * p2 * peck) + fmax(0.0, -fk);
+}
+// the momentum face coefficient of the selected scheme (the coefficient
+// function coeffsourcesink_uv is called with, flow_imp.F90:120-126)
+__device__ __forceinline__ double schemecoef(int ndsch, double dk, double fk) {
+  switch (ndsch) {
+    case 0: return 0.0;  // zerocoef, comp_lib.f90:40-51
+    case 2: return hybcoef(dk, fk);
+    case 3: return powcoef(dk, fk);
+    case 4: return expcoef(dk, fk);
+    default: return upwcoef(dk, fk);
+  }
+}
 __device__ __forceinline__ double wallcoef(double yp, double y0) {  // fric_lib.f90:162-194
   const double y0lim = fmin(fmax(y0, 1.0e-6), yp * 0.9999);
   const double c = 0.4 / log(yp / y0lim);
@@ -110,7 +132,7 @@ __device__ __forceinline__ void defcor_face(const FlowDev& G, const FlowState& S
   const double rpk = xface ? G.rpy[f] : G.rpx[f];
   const double rpn = xface ? G.rpy[fb] : G.rpx[fb];
   // acoef of the face from its own inputs (the momentum coefficient of (ko, o))
-  const double a = expcoef(S.visk[f] * S.hk[f] * G.dsxy[f], S.flux[f]);
+  const double a = schemecoef(G.ndsch, S.visk[f] * S.hk[f] * G.dsxy[f], S.flux[f]);
   if (fabs(rpk) > 1.0e-6) {
     const double val = (a + S.flux[f]) * rpk;
     us = val * (xface ? duy[o] : dux[o]);
@@ -122,7 +144,7 @@ __device__ __forceinline__ void defcor_face(const FlowDev& G, const FlowState& S
   }
 }
 
-// coeffsourcesink_uv(exponentialcoef) (flow_imp.F90:409-466), the skewness
+// coeffsourcesink_uv(schemecoef) (flow_imp.F90:409-466), the skewness
 // deferred correction of joint cells (defcorparagradvec), and bound_uv
 // (boundaries.F90:3310-3490): water-level string faces (bnd_vel_openwse,
 // bnd_vel.f90:35-95) then wall friction (wallfric) or dry-cell rows.
@@ -140,9 +162,11 @@ __global__ void __launch_bounds__(TPB) kf_coef_uv(FlowDev G, FlowState S, const 
   const int nf = G.ncface[r];
   for (int k = 0; k < nf; ++k) {
     const int f = fidx(G, k, r);
-    S.acoef[f] = expcoef(S.visk[f] * S.hk[f] * G.dsxy[f], S.flux[f]);
+    S.acoef[f] = schemecoef(G.ndsch, S.visk[f] * S.hk[f] * G.dsxy[f], S.flux[f]);
   }
-  if (G.ider == 2 && G.joint[r]) {
+  // deferred skewness correction of joint cells: every first-order scheme
+  // but NONE (flow_imp.F90:127-138)
+  if (G.ider == 2 && G.joint[r] && G.ndsch != 0) {
     double ssu = 0.0, ssv = 0.0;
     for (int k = 0; k < nf; ++k) {
       double us = 0.0, vs = 0.0;

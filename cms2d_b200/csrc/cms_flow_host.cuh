@@ -402,6 +402,12 @@ static int flow_create(int ncells, int ncellsD, int nmf, const int* c2c, const i
   if (opts) F->opts = *opts;
   F->n = ncells; F->nD = ncellsD; F->nmf = nmf;
   auto fail = [&](int rc) { cms_flow_destroy(F); return rc; };
+  if (F->opts.ndsch < 0 || F->opts.ndsch > 4) {
+    std::snprintf(g_last_error, sizeof(g_last_error),
+                  "ADVECTION_SCHEME %d: only the first-order schemes 0-4 (NONE, UPWIND, HYBRID, POWERLAW, "
+                  "EXPONENTIAL) are served", F->opts.ndsch);
+    return fail(CMS_UNSUPPORTED);
+  }
   // wet set: active cells and string dummies wet, other dummies are walls
   std::vector<int> iwet(ncellsD, 0);
   for (int i = 0; i < ncells; ++i) iwet[i] = 1;
@@ -478,6 +484,10 @@ static int flow_create(int ncells, int ncellsD, int nmf, const int* c2c, const i
   }
   FlowDev& D = F->G;
   D.n = n; D.nD = nD; D.nmf = nmf; D.nsc = g.nsc; D.ider = g.ider;
+  // upwind when there is neither turbulent nor constant viscosity
+  // (flow.F90:744-746): mturbul is 5 and cviscon 1e-6 here, so the rule never
+  // fires and the scheme is the option's
+  D.ndsch = F->opts.ndsch;
   int *p_ncf, *p_nb;
   signed char *p_back, *p_dir;
   unsigned char *p_owned, *p_thm, *p_joint, *p_crm;
@@ -539,7 +549,12 @@ static int flow_create(int ncells, int ncellsD, int nmf, const int* c2c, const i
     F->nseedc = (int)sd.size();
     if ((rc = F->upload(&F->d_seedc, sd))) return fail(rc);
   }
-  // parameters (flow.F90:21-168, 684-694, friction.F90:44-49)
+  // parameters (flow.F90:21-168, 684-694, friction.F90:44-49).  hdry1 and
+  // hdry2 are read only by the narrow-channel removal rules
+  // (flow.F90:1340-1424), which run with narrow channels off, and then
+  // flow.F90:686-689 has set them to 5 and 2 hdry whatever the
+  // DRYING_DEPTH_ONE_CELL/TWO_CELL cards said; with narrow channels on they
+  // are not read (flow.F90:1324-1338).
   const double hdry = F->opts.hdry > 0.0 ? F->opts.hdry : 0.05;
   D.grav = 9.81; D.gravinv = 1.0 / 9.81; D.hmin = hdry; D.hdry = hdry; D.hdry1 = 5.0 * hdry; D.hdry2 = 2.0 * hdry;
   D.relax_uv = 0.8; D.relax_p = 1.0;
@@ -1268,6 +1283,7 @@ void cms_flow_default_opts(cms_flow_opts* o) {
   o->ponding = 0;
   o->narrowchannels = 0;
   o->relaxsor = 1.8;
+  o->ndsch = 4;
 }
 
 int cms_flow_create(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, const int* ncface,

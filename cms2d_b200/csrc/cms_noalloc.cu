@@ -11,8 +11,8 @@
 // when the library is loaded and held by every GPU that loads it until exit.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdio>
-#include <mutex>
 
 #include "cms_common.cuh"
 #include "cmsgpu.h"
@@ -26,10 +26,8 @@ static_assert(CMS_NOALLOC_MAX_CELLS % cms::TPB == 0, "max cells must be a multip
 
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mu;
-double* g_scratch_addr[kMaxDevices] = {nullptr};
-char g_err[256] = "";
+// Message of the last failed call of this thread.
+thread_local char g_err[256] = "";
 
 // ap = (sum_k acoef - sp)/relax; ss += (1-relax)*phi*ap;
 // res = iwet*(sum_k acoef*phi_nb + ss - ap*phi)/ap; rmom = sqrt(sum res^2 / ncells)
@@ -63,28 +61,25 @@ __global__ void __launch_bounds__(cms::TPB) k_residual_noalloc(int n, int nmf, c
   if (cms::grid_sum<1>(v, scratch, ticket)) scratch[kMaxBlocks] = sqrt(v[0] / (double)n);
 }
 
-// Resolves the device address of the scratch array for the current device,
-// once per device.
+// Resolves the device address of the scratch array in the current device's
+// context.  Done on every call: it allocates nothing and costs a lookup, and a
+// cached address would go stale after cudaDeviceReset (the module is loaded
+// again in the new context).
 double* scratch_for_current_device(int* rc) {
-  int dev = -1;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
-    std::snprintf(g_err, sizeof(g_err), "no usable current CUDA device");
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) {
+    std::snprintf(g_err, sizeof(g_err), "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
     *rc = CMS_DEVICE_ERROR;
     return nullptr;
   }
-  std::lock_guard<std::mutex> lk(g_setup_mu);
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) {
-      std::snprintf(g_err, sizeof(g_err), "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
-      *rc = CMS_DEVICE_ERROR;
-      return nullptr;
-    }
-    g_scratch_addr[dev] = static_cast<double*>(p);
-  }
   *rc = CMS_OK;
-  return g_scratch_addr[dev];
+  return static_cast<double*>(p);
+}
+
+int device_error(const char* what, cudaError_t e) {
+  std::snprintf(g_err, sizeof(g_err), "%s: %s", what, cudaGetErrorString(e));
+  return CMS_DEVICE_ERROR;
 }
 
 }  // namespace
@@ -108,15 +103,21 @@ extern "C" int cms_solve_residual_noalloc_d(int ncells, int ncellsD, int nmaxfac
   if (!scratch) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   // the ticket must start at zero; the partials are overwritten by every block
-  if (cudaMemsetAsync(scratch + kMaxBlocks + 1, 0, sizeof(double), s) != cudaSuccess) return CMS_DEVICE_ERROR;
+  cudaError_t e = cudaMemsetAsync(scratch + kMaxBlocks + 1, 0, sizeof(double), s);
+  if (e != cudaSuccess) return device_error("cudaMemsetAsync", e);
   const int nb = (ncells + cms::TPB - 1) / cms::TPB;
   k_residual_noalloc<<<nb, cms::TPB, 0, s>>>(ncells, nmaxfaces, cell2cell, ncface, iwet, acoef, ss, sp, res, phi,
                                              relax, scratch);
-  if (cudaGetLastError() != cudaSuccess) return CMS_DEVICE_ERROR;
-  if (cudaMemcpyAsync(rmom, scratch + kMaxBlocks, sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-      cudaStreamSynchronize(s) != cudaSuccess)
-    return CMS_DEVICE_ERROR;
-  return (*rmom == *rmom) ? CMS_OK : CMS_NONFINITE;
+  if ((e = cudaGetLastError()) != cudaSuccess) return device_error("kernel launch", e);
+  if ((e = cudaMemcpyAsync(rmom, scratch + kMaxBlocks, sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+    return device_error("cudaMemcpyAsync", e);
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return device_error("cudaStreamSynchronize", e);
+  if (!std::isfinite(*rmom)) {
+    std::snprintf(g_err, sizeof(g_err), "rmom is not finite");
+    return CMS_NONFINITE;
+  }
+  g_err[0] = '\0';
+  return CMS_OK;
 }
 
 extern "C" const char* cms_noalloc_last_error(void) { return g_err; }

@@ -95,6 +95,7 @@ struct PersistArgs {
   DevState* st;
   int maxit, norm, xzero;
   double tol;
+  unsigned int spin_limit;  // polls before a wait gives up (kSpinLimit; smaller in the wait self-test)
 };
 
 // Per-block phase state (uniform across the block).
@@ -119,7 +120,7 @@ __device__ __forceinline__ void wait_neighbours(const PersistArgs<T>& A, PhaseSt
       const unsigned int* f = A.progress + (size_t)A.dep_idx[i] * kProgressStride;
       unsigned int spins = 0;
       while (ld_acquire(f) < ph.done) {
-        if (++spins > kSpinLimit) { atomicExch(&A.bar->err, 1); fail = 1; break; }
+        if (++spins > A.spin_limit) { atomicExch(&A.bar->err, 1); fail = 1; break; }
         if ((spins & 255u) == 0 && bar_failed(A.bar)) { fail = 1; break; }
       }
     }
@@ -153,7 +154,7 @@ __device__ __forceinline__ void grid_barrier(const PersistArgs<T>& A, PhaseState
       red_release_add(&A.bar->count, 1u);
       unsigned int spins = 0;
       while (ld_acquire(&A.bar->count) < ph.target) {
-        if (++spins > kSpinLimit) { atomicExch(&A.bar->err, 1); fail = 1; break; }
+        if (++spins > A.spin_limit) { atomicExch(&A.bar->err, 1); fail = 1; break; }
         if ((spins & 255u) == 0 && bar_failed(A.bar)) { fail = 1; break; }
       }
     }
@@ -761,6 +762,30 @@ __global__ void __launch_bounds__(TPB, 4) k_bicg_batched(const PersistArgs<T>* _
   }
   __syncthreads();
   bicg_body<T>(sA);
+}
+
+// Failure-detection check of the waits above: one block runs tile 0 of a
+// two-tile system whose tile 1 never runs, so tile 1 never publishes a phase
+// and never arrives at a grid barrier.  which = 0: the neighbour wait
+// (phase 1 of tile 1); 1: the grid barrier (2 arrivals needed).  The wait
+// must give up after A.spin_limit polls and set A.bar->err; out[0] = 1 when
+// the block saw it fail, out[1] the barrier arrivals it saw.
+template <typename T>
+__global__ void __launch_bounds__(TPB) k_persist_wait_probe(PersistArgs<T> A, int which, int* out) {
+  __shared__ PersistArgs<T> sA;
+  if (threadIdx.x == 0) {
+    sA = A;
+    sA.tile = 0;
+    sA.ntiles = 2;
+  }
+  __syncthreads();
+  PhaseState ph{1u, 0u, false, true};
+  if (which == 0) wait_neighbours(sA, ph);
+  else grid_barrier(sA, ph);
+  if (threadIdx.x == 0) {
+    out[0] = ph.ok ? 0 : 1;
+    out[1] = (int)ld_acquire(&sA.bar->count);
+  }
 }
 
 // Factor of the two-phase preconditioner: ILU(0) of A without the couplings

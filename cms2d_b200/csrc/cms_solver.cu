@@ -565,11 +565,57 @@ static PersistArgs<T> make_args(Solver* S, Mat<T>& A, Work<T>& W, int tiles, int
   a.b = W.b; a.x = W.x; a.r = W.r; a.r0 = W.r0; a.p = W.p; a.u = W.u; a.v = W.v; a.z = W.z;
   a.part = S->d_ppart; a.bar = &S->d_st->bar; a.st = S->d_st;
   a.maxit = maxit; a.norm = norm; a.xzero = xzero; a.tol = tol;
+  a.spin_limit = kSpinLimit;
   a.relax = S->cur_relax;
   a.fuse_upd = (S->cur_fuse && norm == 2) ? 1 : 0;
   a.g1 = P.G > 1 ? P.gstart[1] : P.n;
   a.spmv0 = (P.gkl[0] == 0 && ((a.relax || a.gku_last == 0) ? P.G >= 2 : P.G >= 1)) ? 1 : 0;
   return a;
+}
+
+// Runs one of the persistent kernel's waits (which = 0 neighbour wait, 1
+// grid barrier) on a two-tile table whose second tile never runs, with a
+// limit of spin_limit polls, on scratch of its own (the handle's tables are
+// untouched).  CMS_DEVICE_ERROR with the message is the expected result.
+static int persist_wait_selftest(Solver* S, unsigned int spin_limit, int which) {
+  // one buffer: progress [2 * stride], dep_ptr [3], dep_idx [2], GridBar, out [2]
+  const size_t nprog = 2 * kProgressStride;
+  const size_t words = nprog + 3 + 2 + sizeof(GridBar) / sizeof(unsigned int) + 2;
+  unsigned int* buf = nullptr;
+  CMS_CUDA(cudaMalloc((void**)&buf, words * sizeof(unsigned int)));
+  struct Free { unsigned int* p; ~Free() { cudaFree(p); } } fr{buf};
+  int* dep_ptr = reinterpret_cast<int*>(buf + nprog);
+  int* dep_idx = dep_ptr + 3;
+  GridBar* bar = reinterpret_cast<GridBar*>(dep_idx + 2);
+  int* out = reinterpret_cast<int*>(bar + 1);
+  const int h_dep[5] = {0, 1, 2, 1, 0};  // tile 0 depends on tile 1 and tile 1 on tile 0
+  CMS_CUDA(cudaMemsetAsync(buf, 0, words * sizeof(unsigned int), S->stream));
+  CMS_CUDA(cudaMemcpyAsync(dep_ptr, h_dep, sizeof(h_dep), cudaMemcpyHostToDevice, S->stream));
+  PersistArgs<float> a;
+  std::memset(&a, 0, sizeof(a));
+  a.dep_ptr = dep_ptr; a.dep_idx = dep_idx; a.progress = buf; a.bar = bar; a.st = S->d_st;
+  a.spin_limit = spin_limit;
+  k_persist_wait_probe<float><<<1, TPB, 0, S->stream>>>(a, which, out);
+  CMS_CUDA(cudaGetLastError());
+  S->launches++;
+  int h_out[2] = {0, 0};
+  GridBar h_bar{};
+  CMS_CUDA(cudaMemcpyAsync(h_out, out, sizeof(h_out), cudaMemcpyDeviceToHost, S->stream));
+  CMS_CUDA(cudaMemcpyAsync(&h_bar, bar, sizeof(GridBar), cudaMemcpyDeviceToHost, S->stream));
+  CMS_CUDA(cudaStreamSynchronize(S->stream));
+  if (h_out[0] == 1 && h_bar.err == 1) {
+    if (which == 0)
+      std::snprintf(g_last_error, sizeof(g_last_error),
+                    "persistent kernel: the neighbour wait gave up after %u polls (tile 1 never completed phase 1)",
+                    spin_limit);
+    else
+      std::snprintf(g_last_error, sizeof(g_last_error),
+                    "persistent kernel: the grid barrier gave up after %u polls (%d of 2 blocks arrived)", spin_limit,
+                    h_out[1]);
+    return CMS_DEVICE_ERROR;
+  }
+  std::snprintf(g_last_error, sizeof(g_last_error), "persistent kernel wait self-test: the wait did not give up");
+  return CMS_OK;
 }
 
 // The whole BiCGStab solve as one cooperative launch.  Returns 1 (nothing
@@ -1113,6 +1159,11 @@ int cms_order_build(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell
 }
 
 const char* cms_gpu_version(void) { return "cmsgpu 0.1 (sm_100a)"; }
+
+int cms_solver_persist_wait_selftest(cms_solver* s, unsigned int spin_limit, int which) {
+  if (!s || spin_limit == 0 || (which != 0 && which != 1)) return CMS_BAD_ARGUMENT;
+  return cms::persist_wait_selftest(s, spin_limit, which);
+}
 
 int cms_solver_wait_selftest(cms_solver* s, unsigned int spin_limit) {
   if (!s || spin_limit == 0) return CMS_BAD_ARGUMENT;

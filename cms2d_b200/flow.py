@@ -27,7 +27,7 @@ class FlowOpts(C.Structure):
                 ("tol", C.c_double), ("nswp_pp", C.c_int), ("nswp_uv", C.c_int), ("maxit", C.c_int),
                 ("skewcor", C.c_int), ("inner_tol", C.c_double), ("inner_max", C.c_int),
                 ("multi_kernel", C.c_int), ("hdry", C.c_double), ("ponding", C.c_int), ("narrowchannels", C.c_int),
-                ("relaxsor", C.c_double)]
+                ("relaxsor", C.c_double), ("ndsch", C.c_int)]
 
 
 class FlowInfo(C.Structure):
@@ -72,7 +72,7 @@ class FlowModel:
                  tol: float = 1e-3, norm: int = 1, nswp_pp: int | None = None, nswp_uv: int | None = None,
                  maxit: int = 0, skewcor: bool = True, inner_tol: float = 1e-3, inner_max: int = 50,
                  multi_kernel: bool = False, hdry: float = 0.05, ponding: bool = False,
-                 narrowchannels: bool = False, relaxsor: float = 1.8):
+                 narrowchannels: bool = False, relaxsor: float = 1.8, ndsch: int = 4):
         L = _lib.lib()
         _bind(L)
         self.case = case
@@ -97,6 +97,7 @@ class FlowModel:
         o.ponding = int(ponding)
         o.narrowchannels = int(narrowchannels)
         o.relaxsor = relaxsor
+        o.ndsch = ndsch
         self.opts = o
         self._keep = [np.ascontiguousarray(a) for a in (
             g.cell2cell.astype(np.int32), g.ncface.astype(np.int32), g.idirface.astype(np.int32),

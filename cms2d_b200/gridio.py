@@ -42,7 +42,9 @@ class GridFile:
     mapid: np.ndarray     # [ncells] file row (1-based) of each active cell
 
 
-def read_tel(path) -> GridFile:
+def parse_tel(path):
+    """(angle, x0, y0, rows) of a .tel file: rows[ncellsfull][14] holds each
+    cell's ``id x y dx dy n1 n2 e1 e2 s1 s2 w1 w2 depth`` as read."""
     with open(path) as f:
         lines = f.read().splitlines()
     if len(lines) < 2:
@@ -63,6 +65,18 @@ def read_tel(path) -> GridFile:
             vals.extend(lines[q].replace(",", " ").split())
             q += 1
         rows[r] = [float(v) for v in vals[:14]]
+    return angle, x0, y0, rows
+
+
+def read_tel(path) -> GridFile:
+    angle, x0, y0, rows = parse_tel(path)
+    return tel_grid(rows, angle, x0, y0, str(path))
+
+
+def tel_grid(rows: np.ndarray, angle: float = 0.0, x0: float = 0.0, y0: float = 0.0, name: str = "grid") -> GridFile:
+    """The grid of a .tel file's cell rows (parse_tel), as read_tel builds it."""
+    path = name
+    nfull = rows.shape[0]
     xt, yt, dxt, dyt = rows[:, 1], rows[:, 2], rows[:, 3], rows[:, 4]
     loct = rows[:, 5:13].astype(np.int64)
     zt = rows[:, 13]

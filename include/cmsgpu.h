@@ -225,6 +225,10 @@ typedef struct cms_flow_opts {
   int ponding;       /* keep isolated water bodies (flow.F90:54; default 0)         */
   int narrowchannels; /* keep one-cell-wide channels (flow.F90:55; default 0)       */
   double relaxsor;   /* SOR constant of nsolv 2 and 5 (flow.F90:131; default 1.8)   */
+  int ndsch;         /* ADVECTION_SCHEME (flow.F90:533-545, definitions.F90:166-171):
+                        0 NONE, 1 UPWIND, 2 HYBRID, 3 POWERLAW, 4 EXPONENTIAL
+                        (default, flow.F90:111); the higher-order deferred-
+                        correction schemes 5-18 give CMS_UNSUPPORTED             */
 } cms_flow_opts;
 
 typedef struct cms_flow_info {
@@ -360,10 +364,13 @@ int cms_gpu_finalize(void);
  * default stream); the call returns after the result is on the host.
  * Scratch is a fixed device array inside the library (about 0.5 MB per GPU,
  * held from load to exit); ncells above CMS_NOALLOC_MAX_CELLS is rejected with
- * CMS_BAD_ARGUMENT.  The first call on each device resolves the array's
- * address (cudaGetSymbolAddress) with that device current; make that first
- * call before any stream capture.  Every call shares the one array, so calls
- * that overlap on the GPU (other streams or threads) race: serialise them. */
+ * CMS_BAD_ARGUMENT.  Every call resolves the array's address in the current
+ * device's context (cudaGetSymbolAddress, no allocation), so the call works on
+ * whichever device is current.  The call synchronises its stream and copies
+ * rmom to the host, so it cannot be made during stream capture.  Every call
+ * shares the one array, so calls that overlap on the GPU (other streams or
+ * threads) race: serialise them.  cms_noalloc_last_error() gives the message of
+ * the calling thread's last failed call. */
 #define CMS_NOALLOC_MAX_CELLS 16777216
 int cms_solve_residual_noalloc_d(int ncells, int ncellsD, int nmaxfaces, const int* cell2cell, const int* ncface,
                                  const int* iwet, const double* acoef, double* ss, const double* sp, double* res,
@@ -376,6 +383,12 @@ const char* cms_noalloc_last_error(void);
  * CMS_DEVICE_ERROR with the wait's position in cms_gpu_last_error() -- the
  * expected result -- and leaves the handle usable. */
 int cms_solver_wait_selftest(cms_solver* s, unsigned int spin_limit);
+/* The same check for the persistent BiCGStab kernel's waits: which = 0 its
+ * wait on a neighbour tile's progress counter, 1 its grid barrier, each run
+ * by one block of a two-tile table whose other tile never runs, giving up
+ * after spin_limit polls.  Returns CMS_DEVICE_ERROR with the message (the
+ * expected result); the handle stays usable. */
+int cms_solver_persist_wait_selftest(cms_solver* s, unsigned int spin_limit, int which);
 
 /* Library version string. */
 const char* cms_gpu_version(void);

@@ -49,6 +49,7 @@ struct Params {
   double rmommaxp = 1e-3, rmomtargetp = 1e-4, rmomminp = 1e-8, rmomratiop = 0.5;      // flow.F90:135-150
   double rmommaxuv = 1e-2, rmomtargetuv = 1e-3, rmomminuv = 1e-7, rmomratiouv = 1.0;
   int dtvar = 0;                  // fixed time step in this build
+  int ndsch = 4;                  // advection scheme, exponential (flow.F90:111)
 };
 
 struct Flow {
@@ -109,6 +110,26 @@ double exponentialcoef(double dk, double fk) {  // comp_lib.f90:96-109
   return dk * peck / std::max(std::exp(peck) - 1.0, 1.0e-6) + std::max(0.0, -fk);
 }
 double upwindcoef(double dk, double fk) { return dk + std::max(0.0, -fk); }  // comp_lib.f90:54-64
+double hybridcoef(double dk, double fk) {  // comp_lib.f90:67-78
+  double peck = std::fabs(fk) / std::max(dk, 1.0e-6);
+  return dk * std::max(0.0, 1.0 - 0.5 * peck) + std::max(0.0, -fk);
+}
+double powerlawcoef(double dk, double fk) {  // comp_lib.f90:81-93
+  double absfk = std::fabs(fk);
+  double peck = absfk / std::max(std::max(dk, absfk), 1.0e-6);
+  double p2 = peck * peck;
+  return dk * (1.0 - p2 * p2 * peck) + std::max(0.0, -fk);
+}
+// the coefficient function flow_imp passes to coeffsourcesink_uv (flow_imp.F90:120-126)
+double schemecoef(int ndsch, double dk, double fk) {
+  switch (ndsch) {
+    case 0: return 0.0;  // zerocoef (comp_lib.f90:40-51)
+    case 2: return hybridcoef(dk, fk);
+    case 3: return powerlawcoef(dk, fk);
+    case 4: return exponentialcoef(dk, fk);
+    default: return upwindcoef(dk, fk);
+  }
+}
 double wall_coef(double yp, double y0) {  // fric_lib.f90:162-194
   double y0lim = std::min(std::max(y0, 1.0e-6), yp * 0.9999);
   double c = 0.4 / std::log(yp / y0lim);
@@ -679,7 +700,7 @@ void srcsnk_static(Flow& f, double dt) {
   }
 }
 
-// coeffsourcesink_uv(exponentialcoef) (flow_imp.F90:409-466)
+// coeffsourcesink_uv(schemecoef) (flow_imp.F90:409-466)
 void coef_uv(Flow& f) {
   for (int i = 1; i <= f.n; ++i) {
     f.su[i] = f.ssu0[i] + (f.fc[i] * f.v[i] - f.dpx[i]) * f.h[i] * f.areap[i];
@@ -688,7 +709,7 @@ void coef_uv(Flow& f) {
     f.sp[i] = f.spuv0[i] - f.cbcfuwcap[i];
     for (int k = 1; k <= f.ncface[i]; ++k) {
       double ddk = f.F(f.visk, k, i) * f.F(f.hk, k, i) * f.F(f.dsxy, k, i);
-      f.F(f.acoef, k, i) = exponentialcoef(ddk, f.F(f.flux, k, i));
+      f.F(f.acoef, k, i) = schemecoef(f.P.ndsch, ddk, f.F(f.flux, k, i));
     }
   }
 }
@@ -1110,7 +1131,7 @@ int flow_step(Flow& f, double dt, int maxit, int* niter_out) {
   int iconv = 1, niter = 0;
   for (niter = 1; niter <= maxit; ++niter) {
     coef_uv(f);
-    if (!f.idjoint.empty()) defcor(f);
+    if (!f.idjoint.empty() && f.P.ndsch != 0) defcor(f);  // flow_imp.F90:127-138
     bound_uv(f);
     double rm = 0;
     int st = solve(f, f.su, f.spu, f.rsu, f.u, 2, &rm);
@@ -1415,7 +1436,11 @@ void orcf_set_wetdry(void* h, int ponding, int narrowchannels) {
   f->P.narrowchannels = narrowchannels != 0;
 }
 int orcf_njoint(void* h) { return (int)static_cast<Flow*>(h)->idjoint.size(); }
-// DRYING_DEPTH card: hmin = hdry, hdry1 = 5 hdry, hdry2 = 2 hdry (flow.F90:686-693)
+// DRYING_DEPTH card: hmin = hdry, hdry1 = 5 hdry, hdry2 = 2 hdry (flow.F90:686-693).
+// The one- and two-cell depths only matter with narrow channels off, when
+// flow.F90:686-689 overwrites the DRYING_DEPTH_ONE_CELL/TWO_CELL cards.
+// ADVECTION_SCHEME card (flow.F90:533-545): 0 none .. 4 exponential
+void orcf_set_scheme(void* h, int ndsch) { static_cast<Flow*>(h)->P.ndsch = ndsch; }
 void orcf_set_hdry(void* h, double hdry) {
   auto* f = static_cast<Flow*>(h);
   f->P.hmin = hdry; f->P.hdry = hdry; f->P.hdry1 = 5.0 * hdry; f->P.hdry2 = 2.0 * hdry;

@@ -163,6 +163,7 @@ class FlowOracle:
             L.orcf_last_nlist.argtypes = [P]
             L.orcf_set_wetdry.argtypes = [P, C.c_int, C.c_int]
             L.orcf_set_hdry.argtypes = [P, C.c_double]
+            L.orcf_set_scheme.argtypes = [P, C.c_int]
             L._flow_bound = True
         g = case.grid
         self.case = case
@@ -197,6 +198,10 @@ class FlowOracle:
         lib().orcf_set_wetdry(self._h, int(ponding), int(narrowchannels))
         if hdry is not None:
             lib().orcf_set_hdry(self._h, float(hdry))
+
+    def set_scheme(self, ndsch):
+        """ADVECTION_SCHEME: 0 none, 1 upwind, 2 hybrid, 3 power law, 4 exponential."""
+        lib().orcf_set_scheme(self._h, int(ndsch))
 
     def init(self, eta0=None):
         if eta0 is None:

@@ -27,10 +27,11 @@ FIXED = {"inlet": dict(nsolv=3, tol=1e-30, nswp_pp=12, nswp_uv=8),
          "basin": dict(nsolv=3, tol=1e-30, nswp_pp=8, nswp_uv=4)}
 
 
-def _pair(case, steps, maxit=4, precision="fp64", ordering="multicolor", same_order=True, **solver):
-    m = FlowModel(case, precision=precision, maxit=maxit, ordering=ordering, **solver)
+def _pair(case, steps, maxit=4, precision="fp64", ordering="multicolor", same_order=True, ndsch=4, **solver):
+    m = FlowModel(case, precision=precision, maxit=maxit, ordering=ordering, ndsch=ndsch, **solver)
     m.init()
     o = O.FlowOracle(case)
+    o.set_scheme(ndsch)
     o.set_solver(nsolv=solver["nsolv"], precond=O.PC_ILU0, tol=solver["tol"], nswp_pp=solver["nswp_pp"],
                  nswp_uv=solver["nswp_uv"], norm=solver.get("norm", 1))
     if same_order:
@@ -80,6 +81,26 @@ def test_flow_step_matches_oracle(kind, ordering):
     assert e["eta_m"] <= 1e-9
     for k in ("u", "v", "h", "vis", "flux"):
         assert e[k] <= 1e-6, (k, e)
+
+
+@pytest.mark.parametrize("ndsch", [0, 1, 2, 3])
+def test_flow_step_advection_schemes(ndsch):
+    """ADVECTION_SCHEME NONE, UPWIND, HYBRID and POWERLAW (EXPONENTIAL is the
+    default of the other tests) on the telescoping inlet, joint cells
+    included."""
+    c = cases.tidal_inlet(12000, seed=3)
+    o, m = _pair(c, steps=2, ndsch=ndsch, **FIXED["inlet"])
+    e = _errors(o, m, c.grid)
+    print("ndsch", ndsch, e)
+    assert e["eta_m"] <= 1e-9
+    for k in ("u", "v", "h", "vis", "flux"):
+        assert e[k] <= 1e-6, (k, e)
+
+
+def test_unsupported_advection_scheme_rejected():
+    from cms2d_b200 import _lib
+    with pytest.raises(_lib.CmsError, match="ADVECTION_SCHEME"):
+        FlowModel(cases.tidal_basin(20, 10, seed=1), ndsch=5)
 
 
 @pytest.mark.parametrize("nsolv", [3, 4])

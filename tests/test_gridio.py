@@ -6,10 +6,11 @@
 * Cartesian files (resolution and coordinate blocks, land, rectilinear
   spacing) read back to the generator's Cartesian grid, numbering
   id = i + (j-1)*maxcol, dummies N, E, S, W per cell.
-* The reference's own test grids (testing/tests_flow/*/*.tel), read where the
-  reference tree is present: structural checks (every internal face has its
-  back face, every dummy its back link, no isolated cells) and the header's
-  cell count.
+* The reference's own test grids (testing/tests_flow/*/*.tel), from the
+  committed fixture: structural checks (every internal face has its back
+  face, every dummy its back link, no isolated cells); where the reference
+  tree is present ($CMS_REFERENCE_DIR), read in place and compared with the
+  fixture.
 """
 import glob
 import os
@@ -19,8 +20,9 @@ import pytest
 
 from cms2d_b200 import grid as G
 from cms2d_b200 import gridio
+from tests import reference_cases as RC
 
-REF_TEL = sorted(glob.glob("/root/reference/testing/tests_flow/*/*.tel"))
+REF_TEL = sorted(glob.glob(os.path.join(RC.REF_DIR, "testing/tests_flow/*/*.tel"))) if RC.REF_DIR else []
 
 
 def _same_grid(a, b, xy_tol=1e-12):
@@ -142,16 +144,25 @@ def test_cart_without_activity_block_follows_the_last_depth(tmp_path):
             assert gridio.read_cart(p).grid.ncells == expect
 
 
-@pytest.mark.skipif(not REF_TEL, reason="reference test grids not present")
+@pytest.mark.skipif(not REF_TEL, reason="reference tree not present (set CMS_REFERENCE_DIR)")
 @pytest.mark.parametrize("path", REF_TEL, ids=[os.path.basename(p) for p in REF_TEL])
-def test_reference_test_grids(path):
+def test_reference_test_grids_match_fixture(path):
     gf = gridio.read_tel(path)
-    g = gf.grid
-    n = g.ncells
     with open(path) as f:
         f.readline()
         nfull = int(float(f.readline().split()[3]))
-    assert 0 < n <= nfull and g.ncellsD > n
+    assert 0 < gf.grid.ncells <= nfull and gf.grid.ncellsD > gf.grid.ncells
+    name = os.path.basename(os.path.dirname(path))
+    fx, _, _ = RC.load(name)
+    _same_grid(gf.grid, fx.grid, xy_tol=0.0)
+    np.testing.assert_array_equal(gf.zb, fx.zb)
+
+
+@pytest.mark.parametrize("name", RC.names())
+def test_reference_test_grids(name):
+    g = RC.load(name)[0].grid
+    n = g.ncells
+    assert 0 < n and g.ncellsD > n
     back = {1: 3, 2: 4, 3: 1, 4: 2}
     for i in range(n):
         for k in range(int(g.ncface[i])):
