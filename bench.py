@@ -380,6 +380,93 @@ def run_solvers_ours(args):
     print(json.dumps(out), flush=True)
 
 
+def inlet_systems(cells: int, seed: int = 11):
+    """The u, v and pressure-correction systems of the tidal inlet as the
+    oracle's flow step assembles them (natural order): two time steps of one
+    outer iteration each from the cold start, then the u system of the next
+    step's first outer iteration, the v system of the one after, and the pp
+    system of the third."""
+    from cms2d_b200 import cases
+    from oracle import oracle as O
+    case = cases.tidal_inlet(cells, seed=seed)
+    f = O.FlowOracle(case)
+    f.set_solver(nsolv=3, precond=O.PC_ILU0, tol=1e-6, nswp_pp=200, nswp_uv=200, norm=2)
+    f.init()
+    for _ in range(2):
+        f.step(maxit=1)
+    out = {}
+    for var, name in ((2, "u"), (3, "v"), (1, "pp")):
+        f.capture(var)
+        f.step(maxit=1)
+        out[name] = (f.captured(), 1.0 if var == 1 else 0.8)
+    return case.grid, out
+
+
+def run_iterations(args):
+    """Krylov iteration counts of one solve() per system and preconditioner
+    (the report of ILU(0) orderings against the reference's ordering and its
+    actual preconditioner): BiCGStab to the reference's stopping test (L1
+    ratio 1e-3, pbicgstab.f90:95) and to a 1e-6 relative L2 residual with
+    multicolour ILU(0) (GPU), natural-order ILU(0) (GPU and oracle) and ILUTP
+    (lfil 35, droptol 1e-3, permtol 0.5: solvers.f90:26-28,195-199, oracle);
+    GMRES(3) restarts with ILUTP(lfil 8) at the reference default 1e-3 (oracle);
+    and the inner iterations of FP32 + FP64 refinement (reduced inner form) to
+    1e-6 L2.  Systems: the solver sweep at 0.25M and 1M unknowns and the
+    1M-cell inlet's u, v and pp systems."""
+    from cms2d_b200 import grid as G
+    from cms2d_b200 import solver as S
+    from oracle import oracle as O
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return
+    O.set_threads(os.cpu_count())
+    systems = []
+    for cells in (250_000, 1_000_000):
+        g, acoef, ss, sp, phi = build_solve_case(cells, seed=17)
+        systems.append((f"sweep {g.ncells}", g, (acoef, ss, sp, phi), 1.0))
+    g_in, sy = inlet_systems(args.cells)
+    for name in ("u", "v", "pp"):
+        (a, b, c, p), relax = sy[name]
+        systems.append((f"inlet {g_in.ncells} {name}", g_in, (a, b, c, p), relax))
+    rows = []
+    for label, g, arrs, relax in systems:
+        row = {"system": label, "unknowns": g.ncells, "relax": relax}
+
+        def gpu(ordering, tol, norm, precision="fp64"):
+            s = S.Solver(g, ordering=ordering, precision=precision, tol=tol, norm=norm, verify=True, nsolv=3)
+            a, b, c, p = [np.array(x, copy=True) for x in arrs]
+            info = s.solve(a, b, c, np.zeros_like(b), p, relax=relax, nswp=5000, nsolv=3)
+            s.close()
+            return info
+
+        def orc(precond, tol, norm, nsolv=3, lfil=None):
+            o = O.OracleSolver(g)
+            a, b, c, p = [np.array(x, copy=True) for x in arrs]
+            t0 = time.perf_counter()
+            r = o.solve(a, b, c, np.zeros_like(b), p, relax=relax, nswp=5000, nsolv=nsolv, precond=precond, tol=tol,
+                        norm=norm, lfil=lfil)
+            return r, time.perf_counter() - t0
+
+        for tag, tol, norm in (("1e-3_L1", 1e-3, 1), ("1e-6_L2", 1e-6, 2)):
+            i_mc = gpu("multicolor", tol, norm)
+            i_nat = gpu("natural", tol, norm)
+            o_nat, t_nat = orc(O.PC_ILU0, tol, norm)
+            o_tp, t_tp = orc(O.PC_ILUTP, tol, norm, lfil=35)
+            row[tag] = {"gpu_multicolour_ilu0": i_mc["iters"], "colours": i_mc["ncolors"],
+                        "gpu_natural_ilu0": i_nat["iters"], "levels": i_nat["ncolors"],
+                        "oracle_natural_ilu0": o_nat["iters"], "oracle_ilutp35": o_tp["iters"],
+                        "oracle_s": {"ilu0": round(t_nat, 2), "ilutp35": round(t_tp, 2)}}
+        o_gm, t_gm = orc(O.PC_ILUTP, 1e-3, 1, nsolv=4, lfil=8)
+        row["gmres3_ilutp8_1e-3_restarts"] = o_gm["iters"]
+        i_ref = gpu("multicolor", 1e-6, 2, precision="fp32_refine")
+        row["fp32_refine_reduced_1e-6_L2"] = {"inner_iters": i_ref["iters"], "refine_steps": i_ref["refine_steps"],
+                                              "true_relres": i_ref["true_relres"]}
+        rows.append(row)
+        print(json.dumps(row), flush=True)
+    print(json.dumps({"metric": "Krylov iterations per solve by preconditioner and ordering", "value": None,
+                      "unit": "iterations", "rows": rows}), flush=True)
+
+
 def run_solve_reference(args):
     world, rank, local = dist_setup()
     if rank != 0:
@@ -451,6 +538,50 @@ def case_label(case):
         return (f"Cartesian intertidal flat {g.ncells} cells (20 m), dt={case.dt:g} s, falling tide "
                 f"(wetting and drying every step)")
     return f"telescoping tidal inlet {g.ncells} cells (40/20/10 m), dt={case.dt:g} s"
+
+
+PARITY_FIXTURE = os.path.join(ROOT, "tests", "golden", "inlet_1m_oracle.npz")
+
+
+def flow_parity(case, seed, settings, precs):
+    """Error of the first steps of this workload against the FP64 oracle:
+    the committed fixture holds the oracle's water level and velocities
+    (natural order, every solve to a 1e-9 relative residual) at seeded
+    sample cells after each of its first steps on the same case.  Each
+    precision re-runs those steps from the cold start with the bench's own
+    settings; errors are the largest difference over the sample cells and
+    steps relative to the largest oracle value (|eta| and |(u, v)|), plus the
+    relative difference of the fixture's whole-grid statistics."""
+    if not os.path.exists(PARITY_FIXTURE):
+        return None
+    from cms2d_b200.flow import FlowModel
+    z = np.load(PARITY_FIXTURE)
+    if int(z["cells"]) != case.grid.ncells or int(z["seed"]) != seed:
+        return None
+    idx, steps, n = z["sample"], z["eta"].shape[0], case.grid.ncells
+    out = {"vs": "FP64 oracle, natural order, solves to 1e-9 (committed fixture of the same case)",
+           "steps": int(steps), "sample_cells": int(idx.size)}
+    for prec in precs:
+        m = FlowModel(case, precision=prec, **settings)
+        m.init()
+        e_eta = e_vel = e_stat = 0.0
+        niter = []
+        for s in range(steps):
+            info = m.step()
+            niter.append(int(info["niter"]))
+            eta, u, v, h = (m.get(k)[:n] for k in ("eta", "u", "v", "h"))
+            eo, uo, vo = z["eta"][s], z["u"][s], z["v"][s]
+            e_eta = max(e_eta, float(np.abs(eta[idx] - eo).max() / np.abs(eo).max()))
+            e_vel = max(e_vel, float(np.hypot(u[idx] - uo, v[idx] - vo).max() / np.hypot(uo, vo).max()))
+            st = np.array([eta.mean(), eta.min(), eta.max(), np.sqrt(np.mean(eta * eta)), np.abs(u).max(),
+                           np.abs(v).max(), h.sum()])
+            so = z["stats"][s]
+            e_stat = max(e_stat, float(np.max(np.abs(st - so) / np.maximum(np.abs(so), 1e-30))))
+        m.close()
+        out[prec] = {"eta_max_rel": e_eta, "vel_max_rel": e_vel, "stats_max_rel": e_stat,
+                     "eta_max_abs_m": e_eta * float(np.abs(z["eta"]).max()),
+                     "outer_iters": niter, "oracle_outer_iters": [int(q) for q in z["niter"]]}
+    return out
 
 
 def _profile_read(L, h):
@@ -614,6 +745,8 @@ def run_flow_ours(args):
                             "ms_per_step": round(c["ms_per_step"], 3), "outer_iters_per_step": c["outer_iters"],
                             "krylov_iters_per_step": c["krylov_iters_per_step"], "status": c["status"],
                             "speedup_of_headline": round(head["value"] / c["value"], 4)}
+    if rank == 0 and not args.no_parity:
+        out["parity"] = flow_parity(case, 11 + rank, settings, precs)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = flow_cpu_sample(case, head["outer_iters"], args.cpu_outer)
     if world > 1:
@@ -644,15 +777,13 @@ def flow_cpu_sample(case, outer_per_step, n_outer, threads=None):
             "s_per_outer_iter": round(per_outer, 3)}
 
 
-# Outer SIMPLEC iterations per time step of the timed steps of the flow
-# workload (steps 4-6 of the 1M inlet after 3 warm-up steps; both precisions
-# of the GPU run take 16).  The CPU arm times a bounded number of outer
-# iterations and scales its per-iteration time by this count, since a CPU
-# step takes minutes.
-FLOW_OUTER_PER_STEP = 16
-
-
 def run_flow_reference(args):
+    """The oracle (the reference's algorithm restated: natural-order ILU(0),
+    serial factor and sweeps as in the reference, other loops OpenMP on all
+    host cores) on the same case.  Warm-up: W bounded samples of one outer
+    iteration each.  Timed: whole time steps, every outer iteration until
+    check_conv ends the step, as many as fit in --ref-budget seconds (at least
+    one; a step of the 1M inlet takes minutes), reported in "steps"."""
     world, rank, local = dist_setup()
     if rank != 0:
         return
@@ -663,51 +794,65 @@ def run_flow_reference(args):
     f = O.FlowOracle(case)
     f.set_solver(nsolv=3, precond=O.PC_ILU0, tol=1e-6, nswp_pp=200, nswp_uv=200, norm=2)
     f.init()
-    if case.grid.ncells <= 100_000:  # small cases: whole steps, as the GPU arm
-        for _ in range(args.warmup):
-            f.step()
-        times = []
-        for _ in range(args.steps):
-            t0 = time.perf_counter()
-            f.step()
-            times.append(time.perf_counter() - t0)
-        t_step = float(np.mean(times))
-        sample = f"{args.warmup} warm-up steps, then {args.steps} whole timed steps"
-    else:
-        # warm-up steps: one outer iteration each (untimed)
-        for _ in range(args.warmup):
-            f.step(maxit=1)
-        per_outer = []
-        for _ in range(args.steps):
-            t0 = time.perf_counter()
-            rr = f.step(maxit=args.cpu_outer)
-            per_outer.append((time.perf_counter() - t0) / max(rr["niter"], 1))
-        t_step = float(np.mean(per_outer)) * FLOW_OUTER_PER_STEP
-        sample = (f"{args.warmup} warm-up steps of one outer iteration, then {args.steps} steps of "
-                  f"{args.cpu_outer} outer iterations each; mean time per outer iteration "
-                  f"{np.mean(per_outer):.2f} s scaled to {FLOW_OUTER_PER_STEP} outer iterations per step")
+    small = case.grid.ncells <= 100_000
+    for _ in range(args.warmup):
+        f.step() if small else f.step(maxit=1)
+    times, outer = [], []
+    t_all = time.perf_counter()
+    while True:
+        t0 = time.perf_counter()
+        r = f.step()
+        times.append(time.perf_counter() - t0)
+        outer.append(r["niter"])
+        elapsed = time.perf_counter() - t_all
+        if len(times) >= args.steps or elapsed + np.mean(times) > args.ref_budget:
+            break
+    t_step = float(np.mean(times))
     v = 1.0 / t_step
+    # the reference's default thread count is one (NUM_THREADS, flow.F90:98):
+    # a bounded sample of outer iterations of the next step on one thread
+    O.set_threads(1)
+    n1 = 2 if not small else 0
+    one = None
+    if n1:
+        t0 = time.perf_counter()
+        r1 = f.step(maxit=n1)
+        per = (time.perf_counter() - t0) / max(r1["niter"], 1)
+        one = {"value": round(1.0 / (per * np.mean(outer)), 6), "unit": "timesteps/s", "cores": 1,
+               "s_per_outer_iter": round(per, 3),
+               "sample": f"{r1['niter']} outer iterations of the step after the timed steps on one thread, "
+                         f"scaled by the {np.mean(outer):.1f} outer iterations per step measured above (estimate)"}
+    O.set_threads(threads)
+    warm = "whole steps" if small else "steps of one outer iteration (untimed)"
+    sample = (f"{args.warmup} warm-up {warm}, then {len(times)} whole timed steps (every outer iteration until "
+              f"check_conv; {np.mean(outer):.1f} outer iterations per step), {sum(times):.1f} s")
     out = {"impl": "reference", "metric": METRIC, "value": round(v, 6), "unit": "timesteps/s",
-           "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+           "n_gpus": world, "steps": len(times), "requested_steps": args.steps, "warmup": args.warmup,
            "ms_per_step": round(1e3 * t_step, 1), "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": f"synthetic (seeded {case.name.replace('_', ' ')})",
            "config": {"workload": f"implicit flow step, {case_label(case)}, ILU0-BiCGStab solves to 1e-6 "
                                   f"rel. L2 residual",
                       "cells": case.grid.ncells, "precision": "fp64", "ordering": "natural",
                       "implementation": "CPU restatement of the reference path (oracle), OpenMP"},
+           "outer_iters_per_step": float(np.mean(outer)),
            "cpu_baseline": {"value": round(v, 6), "unit": "timesteps/s", "cores": threads, "kind": "port",
                             "sample": sample},
+           "cpu_1thread": one,
            "e2e": {"value": round(v, 6), "unit": "timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
 
 def run_ensemble_ours(args):
     """Config 4: independent basins of uneven size stepped together, the
-    solves of every outer iteration batched into one persistent launch each."""
+    solves of every outer iteration batched into one persistent launch each.
+    With N ranks the members are partitioned by LPT on their cell counts
+    (each rank builds and steps its share only; no collective until the
+    final gather of per-member records)."""
     import torch
     import torch.distributed as dist
     from cms2d_b200 import _lib, cases
     from cms2d_b200.ensemble import EnsembleModel
+    from cms2d_b200.partition import gather_results, lpt
 
     world, rank, local = dist_setup()
     if world > 1:
@@ -717,7 +862,11 @@ def run_ensemble_ours(args):
     torch.cuda.set_device(dev)
     L = _lib.lib()
     t_setup = time.perf_counter()
-    cs = cases.ensemble_basins(args.members, seed=23 + rank, nmin=args.ens_min, nmax=args.ens_max)
+    if args.members < world:
+        raise SystemExit(f"--members {args.members} is smaller than the {world} ranks")
+    specs = cases.ensemble_specs(args.members, seed=23, nmin=args.ens_min, nmax=args.ens_max)
+    mine = lpt([s["nx"] * s["ny"] for s in specs], world)[rank]
+    cs = cases.ensemble_basins(args.members, seed=23, nmin=args.ens_min, nmax=args.ens_max, members=mine)
     e = EnsembleModel(cs, **dict(FLOW_SOLVER, nswp_pp=args.nswp, nswp_uv=args.nswp, inner_tol=args.inner_tol,
                                  inner_max=args.inner_max))
     e.init()
@@ -762,29 +911,38 @@ def run_ensemble_ours(args):
     outer = float(np.mean([np.mean([i["niter"] for i in step]) for step in infos]))
     status = sorted({i["status"] for step in infos for i in step})
     steps_per_s = args.steps / (ms_total / 1e3)
+    # per-member records of this rank's share, gathered on every rank
+    recs = {k: {"rank": rank, "cells": c.grid.ncells,
+                "krylov_iters": int(sum(step[j]["krylov_iters"] for step in infos)),
+                "eta_mean": float(np.mean(e.members[j].get("eta")[: c.grid.ncells]))}
+            for j, (k, c) in enumerate(zip(mine, cs))}
+    allrecs = gather_results(recs)
+    tot_cells = int(sum(s["nx"] * s["ny"] for s in specs))
     out = {
         "metric": "member-timesteps/s of a 64-basin ensemble (FP32+refine, batched persistent solves)",
-        "value": round(world * args.members * steps_per_s, 4), "unit": "member-timesteps/s",
+        "value": round(args.members * steps_per_s, 4), "unit": "member-timesteps/s",
         "n_gpus": world, "steps": args.steps, "warmup": nwarm, "ms_per_step": round(ms_total / args.steps, 2),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 refine",
-        "data": "synthetic (seeded uneven tidal basins)",
-        "config": {"workload": f"ensemble of {args.members} tidal basins, {ncells} cells in all "
-                               f"({min(c.grid.ncells for c in cs)}-{max(c.grid.ncells for c in cs)} each), "
+        "higher_is_better": True, "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
+        "dtype": "f32+f64 refine", "data": "synthetic (seeded uneven tidal basins)",
+        "config": {"workload": f"ensemble of {args.members} tidal basins, {tot_cells} cells in all, "
                                f"dt=600 s, ILU0-BiCGStab solves to 1e-6",
-                   "members": args.members, "cells": ncells, "layout_blocks": int(e.tiles()[0]),
-                   "autotuner": e.tuning, "parallelism": f"replicas x{world}",
+                   "members": args.members, "cells": tot_cells, "layout_blocks": int(e.tiles()[0]),
+                   "autotuner": e.tuning,
+                   "parallelism": f"members partitioned over {world} ranks by LPT on cells (rank 0: "
+                                  f"{len(mine)} members, {ncells} cells)" if world > 1 else "one GPU",
                    "l2": "flushed between steps (256 MB write)"},
-        "cells_steps_per_s": round(world * ncells * steps_per_s, 1),
+        "cells_steps_per_s": round(tot_cells * steps_per_s, 1),
         "krylov_iters_per_step": kry, "outer_iters_per_step": outer, "step_status": status,
+        "members_gathered": len(allrecs),
         "batched_launches_per_step": (e.launches - launches0) / args.steps,
-        "e2e": {"value": round(world * args.members * args.steps / t_wall, 4), "unit": "member-timesteps/s",
+        "e2e": {"value": round(args.members * args.steps / t_wall, 4), "unit": "member-timesteps/s",
                 "h2d_bytes_per_step": int(sum(c.th_cells.size for c in cs) * 8), "d2h_bytes_per_step": 0},
         "gpu_launches": int(sum(m.launches for m in e.members)),
         "setup_s": round(t_setup, 1),
         "device_gb": round(sum(m.device_bytes for m in e.members) / 1e9, 2),
         "clocks": clk.summary(),
     }
-    if args.ens_sequential and rank == 0:
+    if args.ens_sequential and world == 1:
         # the same members stepped one after another with their own solver launches
         for m in e.members:  # each member's solver on the whole GPU again
             L.cms_solver_set_tiles(m.solver_handle, 0)
@@ -807,7 +965,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="flow", choices=["flow", "solve", "ensemble", "solvers"])
+    ap.add_argument("--workload", default="flow", choices=["flow", "solve", "ensemble", "solvers", "iterations"])
     ap.add_argument("--members", type=int, default=64, help="ensemble: basins")
     ap.add_argument("--ens-min", type=int, default=50_000, help="ensemble: smallest basin (cells)")
     ap.add_argument("--ens-max", type=int, default=400_000, help="ensemble: largest basin (cells)")
@@ -824,12 +982,19 @@ def main():
                     help="refinement: relative residual reduction asked of each FP32 inner solve")
     ap.add_argument("--inner-max", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="flow: skip the error check against the oracle fixture")
+    ap.add_argument("--ref-budget", type=float, default=400.0,
+                    help="reference arm: seconds of whole timed CPU steps (at least one step)")
     ap.add_argument("--ncu", action="store_true", help="warm-up and timed steps only (profiler runs)")
     ap.add_argument("--multi-kernel", action="store_true",
                     help="BiCGStab as one launch per phase instead of one persistent launch per solve")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload == "iterations":
+        if args.impl != "reference":
+            run_iterations(args)
+        return
     if args.workload == "solvers":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the solvers workload reports its CPU arm "

@@ -17,7 +17,7 @@ LIB = os.path.join(HERE, "libcmsgpu.so")
 OBJDIR = os.path.join(HERE, "_build")
 
 SOURCES = ["cms_order.cpp", "cms_flow_geom.cpp", "cms_flow_wetdry.cpp", "cms_solver.cu", "cms_noalloc.cu"]
-HEADERS = ["cms_common.cuh", "cms_krylov.cuh", "cms_persist.cuh", "cms_order.h", "cms_flow.cuh", "cms_flow_host.cuh", "cms_ensemble_host.cuh", "cms_adjoint_host.cuh", "cms_flow_geom.h", "cms_flow_wetdry.h"]
+HEADERS = sorted(f for f in os.listdir(CSRC) if f.endswith((".cuh", ".h")))
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

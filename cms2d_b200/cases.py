@@ -53,13 +53,15 @@ class Case:
     dt: float
     nsteps: int
     t0: float = 0.0  # tide phase: the water level at time t is the tide at t0 + t (seconds)
+    th_offset: np.ndarray = None  # per string cell: a constant added to the tide (a head difference)
 
     def wse(self, t_seconds: float) -> float:
         th = (t_seconds + self.t0) / 3600.0
         return float(sum(a * np.cos(2.0 * np.pi * th / T) for a, T in self.tide))
 
     def wsebnd(self, t_seconds: float) -> np.ndarray:
-        return np.full(self.th_cells.size, self.wse(t_seconds))
+        out = np.full(self.th_cells.size, self.wse(t_seconds))
+        return out if self.th_offset is None else out + self.th_offset
 
 
 def _smooth_field(shape, corr_cells: float, rng) -> np.ndarray:
@@ -76,11 +78,17 @@ def _smooth_field(shape, corr_cells: float, rng) -> np.ndarray:
 
 def _north_string(g: G.Grid):
     """Active cells whose north face leads to a dummy, with that face (1-based)."""
+    return _edge_string(g, G.N_)
+
+
+def _edge_string(g: G.Grid, direction: int):
+    """Active cells whose face of the given direction (1-4 = N, E, S, W)
+    leads to a dummy, with that face (1-based)."""
     n = g.ncells
     cells, faces = [], []
     for k in range(g.nmaxfaces):
         c = g.cell2cell[:n, k]
-        m = (k < g.ncface[:n]) & (c > n) & (g.idirface[:n, k] == G.N_)
+        m = (k < g.ncface[:n]) & (c > n) & (g.idirface[:n, k] == direction)
         idx = np.nonzero(m)[0]
         cells.append(idx + 1); faces.append(np.full(idx.size, k + 1))
     cells = np.concatenate(cells); faces = np.concatenate(faces)
@@ -127,12 +135,26 @@ def from_grid_file(gf, tide=((0.5, M2_HOURS),), manning: float = 0.025, dt: floa
                 [tuple(t) for t in tide], dt, int(round(hours * 3600.0 / dt)))
 
 
-def ensemble_basins(nmembers: int = 64, seed: int = 0, nmin: int = 50_000, nmax: int = 400_000,
-                    dt: float = 600.0, steps: int = 24) -> list:
-    """Independent tidal basins of uneven size: uniform Cartesian grids at
-    20 m with nmin..nmax cells and aspect ratios 1:1 to 4:1, each with its own
-    M2 amplitude (0.3-1.0 m), Manning n (0.015-0.035) and depth profile
-    (shore 1.5-3 m, offshore 6-14 m, its own seeded bumps)."""
+def through_flow(gf, head: float, manning: float = 0.025, dt: float = 60.0, steps: int = 10,
+                 name: str = "through_flow") -> Case:
+    """A case on a grid file (a flume or basin) driven by a water-level
+    difference: strings on the west (level +head/2) and east (-head/2) edges,
+    walls elsewhere, cold start at level 0 -- a steady through-flow after a few
+    steps, as the reference's flume test cases carry an inflow."""
+    g = gf.grid
+    wc, wf = _edge_string(g, G.W_)
+    ec, ef = _edge_string(g, G.E_)
+    cells = np.concatenate([wc, ec]); faces = np.concatenate([wf, ef])
+    off = np.concatenate([np.full(wc.size, 0.5 * head), np.full(ec.size, -0.5 * head)])
+    o = np.argsort(cells, kind="stable")
+    return Case(name, g, np.asarray(gf.zb, dtype=np.float64), np.full(g.ncells, manning), cells[o].astype(np.int32),
+                faces[o].astype(np.int32), [(0.0, M2_HOURS)], dt, steps, th_offset=off[o])
+
+
+def ensemble_specs(nmembers: int = 64, seed: int = 0, nmin: int = 50_000, nmax: int = 400_000) -> list:
+    """The members of ensemble_basins without building them: one dict of
+    tidal_basin arguments per member (nx, ny and the member's seed, M2
+    amplitude, Manning n and depth profile), drawn in member order."""
     rng = np.random.default_rng(seed)
     out = []
     for k in range(nmembers):
@@ -141,12 +163,29 @@ def ensemble_basins(nmembers: int = 64, seed: int = 0, nmin: int = 50_000, nmax:
         long_side = int(round(np.sqrt(ncell * aspect)))
         short_side = max(4, int(round(ncell / long_side)))
         nx, ny = (long_side, short_side) if rng.random() < 0.5 else (short_side, long_side)
-        c = tidal_basin(nx, ny, 20.0, seed=int(rng.integers(1 << 30)), amp=float(rng.uniform(0.3, 1.0)),
-                        manning=float(rng.uniform(0.015, 0.035)), dt=dt, hours=steps * dt / 3600.0,
-                        depth_shore=float(rng.uniform(1.5, 3.0)), depth_off=float(rng.uniform(6.0, 14.0)))
-        c.name = f"basin{k:02d}"
-        out.append(c)
+        out.append(dict(nx=nx, ny=ny, seed=int(rng.integers(1 << 30)), amp=float(rng.uniform(0.3, 1.0)),
+                        manning=float(rng.uniform(0.015, 0.035)), depth_shore=float(rng.uniform(1.5, 3.0)),
+                        depth_off=float(rng.uniform(6.0, 14.0)), name=f"basin{k:02d}"))
     return out
+
+
+def basin_from_spec(spec: dict, dt: float = 600.0, steps: int = 24) -> Case:
+    c = tidal_basin(spec["nx"], spec["ny"], 20.0, seed=spec["seed"], amp=spec["amp"], manning=spec["manning"], dt=dt,
+                    hours=steps * dt / 3600.0, depth_shore=spec["depth_shore"], depth_off=spec["depth_off"])
+    c.name = spec["name"]
+    return c
+
+
+def ensemble_basins(nmembers: int = 64, seed: int = 0, nmin: int = 50_000, nmax: int = 400_000,
+                    dt: float = 600.0, steps: int = 24, members=None) -> list:
+    """Independent tidal basins of uneven size: uniform Cartesian grids at
+    20 m with nmin..nmax cells and aspect ratios 1:1 to 4:1, each with its own
+    M2 amplitude (0.3-1.0 m), Manning n (0.015-0.035) and depth profile
+    (shore 1.5-3 m, offshore 6-14 m, its own seeded bumps).  members: the
+    indices to build (default all), e.g. one rank's share of the ensemble."""
+    specs = ensemble_specs(nmembers, seed, nmin, nmax)
+    idx = range(nmembers) if members is None else members
+    return [basin_from_spec(specs[k], dt, steps) for k in idx]
 
 
 def tidal_inlet(target_cells: int = 1_000_000, seed: int = 0, dt: float = 300.0, nsteps: int = 48) -> Case:

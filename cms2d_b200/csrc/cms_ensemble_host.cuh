@@ -26,6 +26,8 @@ struct cms_ensemble {
   int batched = 0;  // 1: the solves run as batched persistent launches
   cms::PersistArgs<float>* d_args = nullptr;
   cms::PersistArgs<float>* h_args = nullptr;  // pinned
+  cms::SchurArgs* d_sargs = nullptr;           // reduced inner solves (every member in reduced form)
+  cms::SchurArgs* h_sargs = nullptr;           // pinned
   int2* d_bmap = nullptr;
   int2* h_bmap = nullptr;  // pinned
   long long launches = 0;
@@ -95,6 +97,14 @@ static int refine_batched(Ens* E, const std::vector<int>& act, const std::vector
       }
     }
   } reset{E, act};
+  // the reduced inner form when every member's solver takes it (as each
+  // member's own step does), else the two-phase or exact factor
+  bool schur = true;
+  for (int j = 0; j < A_ && schur; ++j) {
+    Solver* S = E->m[act[j]]->S;
+    schur = S->opts.inner_relax == 2 && S->opts.ordering == CMS_ORDER_MULTICOLOR &&
+            schur_pattern(S, E->tiles[act[j]]) == CMS_OK;
+  }
   for (int j = 0; j < A_; ++j) {
     Solver* S = E->m[act[j]]->S;
     const HostPattern& P = S->hp;
@@ -108,7 +118,9 @@ static int refine_batched(Ens* E, const std::vector<int>& act, const std::vector
     rm.rmax = S->opts.max_refine > 0 ? S->opts.max_refine : 30;
     const bool relax = S->opts.inner_relax && S->opts.ordering == CMS_ORDER_MULTICOLOR && P.G > 2;
     S->cur_fuse = 1;
-    if (relax) {
+    if (schur) {
+      CHK(schur_numeric(S));
+    } else if (relax) {
       KLAUNCH(S, P_ILU0, (double)n * (3 * 4 + 2) + (double)(P.nnz_off) * (2 * 4 + 4),
               (k_ilu0_relax<float><<<gsz(n), TPB, 0, S->stream>>>(n, P.KL, P.gstart[1], S->d_col, S->d_nlo,
                                                                    S->d_nup, S->A32.aoff, S->A32.diag, S->A32.luoff,
@@ -154,17 +166,28 @@ static int refine_batched(Ens* E, const std::vector<int>& act, const std::vector
               (k_ir_scale<<<gsz(n), TPB, 0, S->stream>>>(n, S->W64.r, S->W32.b, S->d_st)));
       CMS_CUDA(cudaMemsetAsync(&S->d_st->bar, 0, sizeof(GridBar), S->stream));
       CMS_CUDA(cudaMemsetAsync(S->d_progress, 0, sizeof(unsigned int) * E->tiles[i] * kProgressStride, S->stream));
-      E->h_args[c] = make_args<float>(S, S->A32, S->W32, E->tiles[i], R[j].imax, 2, R[j].itol, 1);
+      if (schur) E->h_sargs[c] = make_schur_args(S, E->tiles[i], R[j].imax, R[j].itol);
+      else E->h_args[c] = make_args<float>(S, S->A32, S->W32, E->tiles[i], R[j].imax, 2, R[j].itol, 1);
       for (int t = 0; t < E->tiles[i]; ++t) E->h_bmap[blocks++] = make_int2(c, t);
       CMS_CUDA(cudaEventRecord(E->ev_m[i], S->stream));
       CMS_CUDA(cudaStreamWaitEvent(E->stream, E->ev_m[i], 0));
     }
-    CMS_CUDA(cudaMemcpyAsync(E->d_args, E->h_args, cont.size() * sizeof(PersistArgs<float>), cudaMemcpyHostToDevice,
-                             E->stream));
+    if (schur)
+      CMS_CUDA(cudaMemcpyAsync(E->d_sargs, E->h_sargs, cont.size() * sizeof(SchurArgs), cudaMemcpyHostToDevice,
+                               E->stream));
+    else
+      CMS_CUDA(cudaMemcpyAsync(E->d_args, E->h_args, cont.size() * sizeof(PersistArgs<float>),
+                               cudaMemcpyHostToDevice, E->stream));
     CMS_CUDA(cudaMemcpyAsync(E->d_bmap, E->h_bmap, blocks * sizeof(int2), cudaMemcpyHostToDevice, E->stream));
-    void* kargs[] = {&E->d_args, &E->d_bmap};
-    CMS_CUDA(cudaLaunchCooperativeKernel((const void*)k_bicg_batched<float>, dim3(blocks), dim3(TPB), kargs, 0,
-                                         E->stream));
+    if (schur) {
+      void* kargs[] = {&E->d_sargs, &E->d_bmap};
+      CMS_CUDA(cudaLaunchCooperativeKernel((const void*)k_schur_batched, dim3(blocks), dim3(TPB), kargs, 0,
+                                           E->stream));
+    } else {
+      void* kargs[] = {&E->d_args, &E->d_bmap};
+      CMS_CUDA(cudaLaunchCooperativeKernel((const void*)k_bicg_batched<float>, dim3(blocks), dim3(TPB), kargs, 0,
+                                           E->stream));
+    }
     E->launches++;
     CMS_CUDA(cudaEventRecord(E->ev_done, E->stream));
     for (int j : cont) {
@@ -301,6 +324,7 @@ int cms_ensemble_create(int nmembers, cms_flow* const* members, cms_ensemble** o
     if (!members[i]) return CMS_BAD_ARGUMENT;
   auto* E = new cms_ensemble();
   E->m.assign(members, members + nmembers);
+  for (auto* F : E->m) F->use_graphs = 1;  // stage kernel sequences replayed as CUDA graphs
   auto fail = [&](int rc) { cms_ensemble_destroy(E); return rc; };
   if (cudaGetDevice(&E->dev) != cudaSuccess || cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking) ||
       cudaEventCreateWithFlags(&E->ev_done, cudaEventDisableTiming))
@@ -317,6 +341,8 @@ int cms_ensemble_create(int nmembers, cms_flow* const* members, cms_ensemble** o
   if (ok && nmembers <= cms::GRID_CAP && cms::ensemble_layout(E, 0) == CMS_OK) {
     if (cudaMalloc((void**)&E->d_args, nmembers * sizeof(cms::PersistArgs<float>)) ||
         cudaMallocHost((void**)&E->h_args, nmembers * sizeof(cms::PersistArgs<float>)) ||
+        cudaMalloc((void**)&E->d_sargs, nmembers * sizeof(cms::SchurArgs)) ||
+        cudaMallocHost((void**)&E->h_sargs, nmembers * sizeof(cms::SchurArgs)) ||
         cudaMalloc((void**)&E->d_bmap, cms::GRID_CAP * sizeof(int2)) ||
         cudaMallocHost((void**)&E->h_bmap, cms::GRID_CAP * sizeof(int2)))
       return fail(CMS_DEVICE_ERROR);
@@ -356,6 +382,8 @@ void cms_ensemble_destroy(cms_ensemble* e) {
   if (!e) return;
   if (e->d_args) cudaFree(e->d_args);
   if (e->h_args) cudaFreeHost(e->h_args);
+  if (e->d_sargs) cudaFree(e->d_sargs);
+  if (e->h_sargs) cudaFreeHost(e->h_sargs);
   if (e->d_bmap) cudaFree(e->d_bmap);
   if (e->h_bmap) cudaFreeHost(e->h_bmap);
   for (auto ev : e->ev_m)

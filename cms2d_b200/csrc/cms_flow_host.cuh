@@ -72,6 +72,19 @@ struct cms_flow {
   signed char* d_fslot_dev = nullptr;  // [nmf][n] ELL slot of face k of device row r
   // gradient copies: index of the current one
   int cur_dppx = 0, cur_duv = 0, cur_dH = 0, cur_dap = 0;
+  // CUDA graphs of the stage kernel sequences (pressure-correction assembly,
+  // corrections), one per stage and gradient-copy state: a stage's kernels
+  // and arguments are fixed for a given state until the wet set changes
+  // (graph_gen counts those changes).  use_graphs: replay them (ensembles).
+  struct StageGraph {
+    cudaGraphExec_t exec = nullptr;
+    long long gen = -1;
+    int key_after = 0;
+    long long nlaunch = 0;
+  };
+  StageGraph sgraph[2][16];
+  int use_graphs = 0;
+  long long graph_gen = 0, graph_launches = 0, graph_captures = 0;
   int* h_flag = nullptr;
   cms_flow_info last{};
   cms_solve_info last_solve[3]{};  // u, v, pp of the last outer iteration
@@ -958,6 +971,7 @@ static int flow_start(Flow* F, std::vector<double> p_nat, const double* u_nat, c
   cudaStream_t s = F->S->stream;
   const int nD = F->nD;
   const bool hot = u_nat != nullptr;
+  ++F->graph_gen;  // a new wet set and its recurrence lists
   std::vector<double> u0, v0;
   std::vector<int> wet_hot;
   if (hot) {
@@ -1138,6 +1152,7 @@ static int step_begin(Flow* F, double dt, const double* wsebnd) {
   cudaStream_t s = F->S->stream;
   F->last_changed = 0;
   if (F->wd_pending) {  // flow_wetdry(0) and der_update (flow_imp.F90:73-79)
+    ++F->graph_gen;     // the recurrence lists may change: stage graphs are captured again
     FCHK(wetdry_update(F, F->nchg_pending));
     F->wd_pending = 0;
     F->nchg_pending = 0;
@@ -1165,8 +1180,64 @@ static int stage_uv(Flow* F) {
   return CMS_OK;
 }
 
+// Gradient-copy state of a flow model (the key of its stage graphs).
+static inline int stage_key(const Flow* F) { return F->cur_duv | F->cur_dH << 1 | F->cur_dap << 2 | F->cur_dppx << 3; }
+static inline void set_stage_key(Flow* F, int k) {
+  F->cur_duv = k & 1; F->cur_dH = (k >> 1) & 1; F->cur_dap = (k >> 2) & 1; F->cur_dppx = (k >> 3) & 1;
+}
+
+// Runs the kernel sequence fn issues on the solver stream, through a CUDA
+// graph when the handle replays graphs: captured on first use for the
+// current gradient-copy state (fn's host side -- the copy flips -- runs
+// during the capture, so the state after it is recorded and restored on
+// every replay), re-captured after a wet-set change.  A capture that fails
+// turns graphs off for this handle and runs fn directly.
+template <class Fn>
+static int run_stage(Flow* F, int which, Fn&& fn) {
+  if (!F->use_graphs || F->S->prof_on) return fn();
+  cudaStream_t s = F->S->stream;
+  const int key = stage_key(F);
+  Flow::StageGraph& g = F->sgraph[which][key];
+  if (!g.exec || g.gen != F->graph_gen) {
+    if (g.exec) {
+      cudaGraphExecDestroy(g.exec);
+      g.exec = nullptr;
+    }
+    const long long l0 = F->launches;
+    cudaGraph_t graph = nullptr;
+    int rc = CMS_DEVICE_ERROR;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      rc = fn();
+      const cudaError_t e = cudaStreamEndCapture(s, &graph);
+      if (e != cudaSuccess) rc = CMS_DEVICE_ERROR;
+    }
+    if (rc == CMS_OK && graph && cudaGraphInstantiate(&g.exec, graph, 0) != cudaSuccess) {
+      g.exec = nullptr;
+      rc = CMS_DEVICE_ERROR;
+    }
+    if (graph) cudaGraphDestroy(graph);
+    if (rc != CMS_OK || !g.exec) {  // nothing ran: undo the host side, launch directly from now on
+      cudaGetLastError();
+      F->use_graphs = 0;
+      F->launches = l0;
+      set_stage_key(F, key);
+      return fn();
+    }
+    g.gen = F->graph_gen;
+    g.key_after = stage_key(F);
+    g.nlaunch = F->launches - l0;
+    F->launches = l0;
+    ++F->graph_captures;
+  }
+  CMS_CUDA(cudaGraphLaunch(g.exec, s));
+  set_stage_key(F, g.key_after);
+  F->launches += g.nlaunch;
+  ++F->graph_launches;
+  return CMS_OK;
+}
+
 // pressure-correction system (after the u and v solves)
-static int stage_pp(Flow* F) {
+static int stage_pp_kernels(Flow* F) {
   FlowState& T = F->st;
   cudaStream_t s = F->S->stream;
   const bool skew = F->opts.skewcor != 0;
@@ -1183,8 +1254,10 @@ static int stage_pp(Flow* F) {
   return CMS_OK;
 }
 
-// corrections after the pressure-correction solve, then check_conv
-static int stage_corr(Flow* F, int niter, int maxit, int* iconv) {
+static int stage_pp(Flow* F) { return run_stage(F, 0, [&] { return stage_pp_kernels(F); }); }
+
+// corrections after the pressure-correction solve
+static int stage_corr_kernels(Flow* F) {
   FlowState& T = F->st;
   cudaStream_t s = F->S->stream;
   const bool skew = F->opts.skewcor != 0;
@@ -1197,6 +1270,12 @@ static int stage_corr(Flow* F, int niter, int maxit, int* iconv) {
   CHK(flow_grad_interp(F));
   const int c2 = F->cur_duv;
   CHK(flow_vis(F, T.dux[c2], T.duy[c2], T.dvx[c2], T.dvy[c2]));
+  return CMS_OK;
+}
+
+// corrections, then check_conv
+static int stage_corr(Flow* F, int niter, int maxit, int* iconv) {
+  CHK(run_stage(F, 1, [&] { return stage_corr_kernels(F); }));
   *iconv = check_conv(F->it_rm, F->it_rmom0, F->it_rmom1, niter, maxit);
   return CMS_OK;
 }
@@ -1381,9 +1460,25 @@ int cms_flow_wetdry_stats(const cms_flow* f, long long* updates, double* ms3) {
   return CMS_OK;
 }
 
+int cms_flow_set_graphs(cms_flow* f, int on) {
+  if (!f) return CMS_BAD_ARGUMENT;
+  f->use_graphs = on ? 1 : 0;
+  return CMS_OK;
+}
+
+int cms_flow_graph_stats(const cms_flow* f, long long* replays, long long* captures) {
+  if (!f) return CMS_BAD_ARGUMENT;
+  if (replays) *replays = f->graph_launches;
+  if (captures) *captures = f->graph_captures;
+  return CMS_OK;
+}
+
 void cms_flow_destroy(cms_flow* f) {
   if (!f) return;
   if (f->S) cudaStreamSynchronize(f->S->stream);
+  for (auto& row : f->sgraph)
+    for (auto& g : row)
+      if (g.exec) cudaGraphExecDestroy(g.exec);
   for (void* p : f->allocs) cudaFree(p);
   if (f->h_flag) cudaFreeHost(f->h_flag);
   if (f->S) cms_solver_destroy(f->S);

@@ -108,9 +108,11 @@ struct PhaseState {
 
 __device__ __forceinline__ bool bar_failed(GridBar* b) { return *(volatile int*)&b->err != 0; }
 
-// Waits until every neighbour tile has completed ph.done phases.
-template <typename T>
-__device__ __forceinline__ void wait_neighbours(const PersistArgs<T>& A, PhaseState& ph) {
+// Waits until every neighbour tile has completed ph.done phases.  (These
+// helpers take any argument struct with the tile, dependency, progress,
+// barrier and partial-sum fields of PersistArgs.)
+template <class Args>
+__device__ __forceinline__ void wait_neighbours(const Args& A, PhaseState& ph) {
   __shared__ int s_fail;
   if (ph.fresh) { ph.fresh = false; return; }
   if (threadIdx.x < 32) {
@@ -132,8 +134,8 @@ __device__ __forceinline__ void wait_neighbours(const PersistArgs<T>& A, PhaseSt
 }
 
 // Ends a phase: publishes the completed count.
-template <typename T>
-__device__ __forceinline__ void end_phase(const PersistArgs<T>& A, PhaseState& ph) {
+template <class Args>
+__device__ __forceinline__ void end_phase(const Args& A, PhaseState& ph) {
   __syncthreads();
   ++ph.done;
   ph.fresh = false;
@@ -141,8 +143,8 @@ __device__ __forceinline__ void end_phase(const PersistArgs<T>& A, PhaseState& p
 }
 
 // Grid-wide barrier on a monotone arrival counter.
-template <typename T>
-__device__ __forceinline__ void grid_barrier(const PersistArgs<T>& A, PhaseState& ph) {
+template <class Args>
+__device__ __forceinline__ void grid_barrier(const Args& A, PhaseState& ph) {
   __shared__ int s_fail;
   __syncthreads();
   ph.target += A.ntiles;
@@ -166,8 +168,8 @@ __device__ __forceinline__ void grid_barrier(const PersistArgs<T>& A, PhaseState
 }
 
 // Writes this block's partial sums of NS values into buffer buf.
-template <int NS, typename T>
-__device__ __forceinline__ void put_partials(const PersistArgs<T>& A, double (&v)[NS], int buf) {
+template <int NS, class Args>
+__device__ __forceinline__ void put_partials(const Args& A, double (&v)[NS], int buf) {
   block_sum<NS>(v);
   if (threadIdx.x == 0) {
 #pragma unroll
@@ -176,8 +178,8 @@ __device__ __forceinline__ void put_partials(const PersistArgs<T>& A, double (&v
 }
 
 // After a grid barrier: every thread of every block gets the grid totals.
-template <int NS, typename T>
-__device__ __forceinline__ void get_totals(const PersistArgs<T>& A, double (&tot)[NS], int buf) {
+template <int NS, class Args>
+__device__ __forceinline__ void get_totals(const Args& A, double (&tot)[NS], int buf) {
   __shared__ double bc[NS];
   double acc[NS];
 #pragma unroll

@@ -1,0 +1,435 @@
+// FP32 inner BiCGStab of iterative refinement in reduced form.
+//
+// On a multicolour ordering group 0 is an independent set placed first: its
+// rows couple only to rows of the later groups (set B).  With
+// A = [D0 A0B; AB0 ABB] the ILU(0) preconditioner of a two-group split is
+// M = (D~ + L) D~^-1 (D~ + U) with D~ = diag(D0, S), S the diagonal of the
+// Schur complement C = ABB - AB0 D0^-1 A0B, and a short calculation gives
+//
+//   (I + L D~^-1)^-1 A (D~ + U)^-1 = diag(I, C S^-1),
+//
+// so right-preconditioned BiCGStab on A M^-1 runs on an operator similar to
+// diag(I, C S^-1): the group-0 block is the identity.  This file solves the
+// reduced system instead, C S^-1 y = b_B - AB0 D0^-1 b_0 on the B rows with
+// x_B = S^-1 y and x_0 = D0^-1 (b_0 - A0B x_B): half the unknowns, one
+// unit-diagonal gather per operator application and no triangular sweep.
+// Couplings among B rows (telescoping interfaces) stay in C exactly.  The
+// reduced residual equals the full system's residual on B, and the FP64
+// residual of the refinement makes the answer independent of the inner
+// operator's rounding.
+//
+// Storage.  C S^-1 = I - Chat: Chat's off-diagonals in ELL slot-major order
+// over the reduced rows i = r - g1 (ccol: device column, coff: value, ccnt:
+// count per row), built per solve by k_schur_diag and k_schur_off from the
+// FP32 matrix; sinv[r] = 1/d_r for group-0 rows and 1/s_r (s_r = C_rr) for B
+// rows.  Vectors are indexed by device row (the B rows of the refinement's
+// FP32 work arrays).
+//
+// The persistent kernel.  One block per tile (the tiles of the persistent
+// ILU(0) kernel: tile t's B rows are toff[g][t]..toff[g][t+1] for g >= 1), a
+// BiCGStab iteration is three phases:
+//   P0  the previous iteration's y/r update and the new search direction p
+//       (own rows, no neighbour values);
+//   A   nu = Chat p (after the neighbour tiles have finished P0) and r0.nu,
+//       reduced at a grid barrier;
+//   B   t = Chat s with s = r - alpha nu formed on the fly for each gathered
+//       neighbour, and t.s, t.t, r0.t, s.s, r0.s, reduced at a grid barrier;
+// the next residual norm comes from ||r||^2 = s.s - 2 w t.s + w^2 t.t and the
+// next r0.r from r0.s - w r0.t.  Waits and barriers are those of the
+// persistent ILU(0) kernel (bounded, cms_persist.cuh).
+#pragma once
+#include "cms_persist.cuh"
+
+namespace cms {
+
+constexpr int KSC = 16;  // largest off-diagonal count of a reduced row the kernels take
+
+struct SchurArgs {
+  int n, g1, nB, KL, G;
+  int KC;                  // slots of Chat (largest count)
+  int ntiles, tile;
+  const int* toff;         // [G][ntiles+1] tile row ranges per group
+  const int* dep_ptr;      // neighbour tiles under Chat's couplings
+  const int* dep_idx;
+  unsigned int* progress;  // [ntiles * kProgressStride] (zero at launch)
+  const int* ccol;         // [KC][nB]
+  const float* coff;       // [KC][nB]
+  const signed char* ccnt; // [nB]
+  const int* col;          // A's ELL (device order)
+  const signed char* nlo;
+  const signed char* nup;
+  const float* aoff;
+  const float* sinv;       // [n]
+  const float* b;
+  float* x;
+  float *r, *r0, *p, *nu, *t, *y;
+  double* part;            // [2][NSMAX][ntiles]
+  GridBar* bar;
+  DevState* st;
+  int maxit;
+  double tol;
+  unsigned int spin_limit;
+};
+
+// sinv: 1/d_r for group-0 rows, 1/s_r for B rows with
+// s_r = d_r - sum_{j in group 0} a_rj a_jr / d_j (A's off-diagonals are
+// -aoff; products accumulated in FP64).
+__global__ void __launch_bounds__(TPB) k_schur_diag(int n, int g1, int KL, const int* __restrict__ col,
+                                                    const signed char* __restrict__ nlo,
+                                                    const signed char* __restrict__ nup,
+                                                    const float* __restrict__ aoff, const float* __restrict__ diag,
+                                                    float* __restrict__ sinv) {
+  for (int r = blockIdx.x * TPB + threadIdx.x; r < n; r += gridDim.x * TPB) {
+    const float dr = diag[r];
+    if (r < g1) {
+      sinv[r] = 1.0f / dr;
+      continue;
+    }
+    double c = dr;
+    const int kl = nlo[r];
+    for (int s = 0; s < kl; ++s) {
+      const size_t e = (size_t)s * n + r;
+      const int j = col[e];
+      if (j >= g1) continue;
+      const int nuj = nup[j];
+      for (int t2 = 0; t2 < nuj; ++t2) {
+        const size_t e2 = (size_t)(KL + t2) * n + j;
+        if (col[e2] == r) c -= (double)aoff[e] * (double)aoff[e2] / (double)diag[j];
+      }
+    }
+    sinv[r] = (float)(1.0 / c);
+  }
+}
+
+// Chat's off-diagonals of reduced row i (r = g1 + i):
+// coff_rk = (aoff_rk [k in B] + sum_{j in group 0} aoff_rj aoff_jk / d_j) / s_k.
+__global__ void __launch_bounds__(TPB) k_schur_off(int n, int g1, int nB, int KL, int KC,
+                                                   const int* __restrict__ col, const signed char* __restrict__ nlo,
+                                                   const signed char* __restrict__ nup,
+                                                   const float* __restrict__ aoff, const float* __restrict__ diag,
+                                                   const float* __restrict__ sinv, const int* __restrict__ ccol,
+                                                   const signed char* __restrict__ ccnt, float* __restrict__ coff) {
+  for (int i = blockIdx.x * TPB + threadIdx.x; i < nB; i += gridDim.x * TPB) {
+    const int r = g1 + i;
+    const int kc = ccnt[i];
+    int cc[KSC];
+    double acc[KSC];
+#pragma unroll
+    for (int q = 0; q < KSC; ++q) {
+      cc[q] = q < kc ? ccol[(size_t)q * nB + i] : -1;
+      acc[q] = 0.0;
+    }
+    auto add = [&](int k, double v) {
+#pragma unroll
+      for (int q = 0; q < KSC; ++q)
+        if (cc[q] == k) acc[q] += v;
+    };
+    const int kl = nlo[r], ku = nup[r];
+    for (int s = 0; s < kl + ku; ++s) {
+      const size_t e = (size_t)(s < kl ? s : KL + (s - kl)) * n + r;
+      const int k = col[e];
+      const double a = aoff[e];
+      if (k >= g1) {
+        add(k, a);
+        continue;
+      }
+      const double w = a / (double)diag[k];  // k is a group-0 row j
+      const int nuj = nup[k];
+      for (int t2 = 0; t2 < nuj; ++t2) {
+        const size_t e2 = (size_t)(KL + t2) * n + k;
+        const int k2 = col[e2];
+        if (k2 != r) add(k2, w * (double)aoff[e2]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < KSC; ++q)
+      if (q < KC) coff[(size_t)q * nB + i] = q < kc ? (float)(acc[q] * (double)sinv[cc[q]]) : 0.0f;
+  }
+}
+
+// Rows of this tile in groups ga..gb as one index space (ranges in shared
+// memory: s_lo first row of each group's range, s_pre prefix counts).
+template <int NR, typename F>
+__device__ __forceinline__ void for_tile_rows(const int* s_lo, const int* s_pre, int ga, int gb, F&& f) {
+  const int k0 = s_pre[ga], k1 = s_pre[gb + 1];
+  for (int base = k0 + (int)threadIdx.x; base < k1; base += NR * (int)blockDim.x) {
+    int r[NR];
+    bool ok[NR];
+#pragma unroll
+    for (int q = 0; q < NR; ++q) {
+      int k = base + q * (int)blockDim.x;
+      ok[q] = k < k1;
+      if (!ok[q]) k = base;
+      int g = ga;
+      while (g < gb && k >= s_pre[g + 1]) ++g;
+      r[q] = s_lo[g] + (k - s_pre[g]);
+    }
+    f(r, ok);
+  }
+}
+
+// acc[q] - sum_s coff[s] * w(col) over the reduced row's slots, w(k) given
+// by a functor of the gathered column.
+template <int NR, typename W>
+__device__ __forceinline__ void chat_sub(const SchurArgs& A, float (&acc)[NR], const int (&r)[NR], W&& w) {
+  int kc[NR];
+#pragma unroll
+  for (int q = 0; q < NR; ++q) kc[q] = __ldg(&A.ccnt[r[q] - A.g1]);
+#pragma unroll
+  for (int s = 0; s < KSC; ++s) {
+    if (s < A.KC) {
+#pragma unroll
+      for (int q = 0; q < NR; ++q) {
+        if (s < kc[q]) {
+          const size_t e = (size_t)s * A.nB + (r[q] - A.g1);
+          acc[q] = acc[q] - __ldg(&A.coff[e]) * w(__ldg(&A.ccol[e]));
+        }
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void schur_body(const SchurArgs& A) {
+  constexpr int NR = 2;
+  const int G = A.G;
+  PhaseState ph{0u, 0u, true, true};
+  __shared__ int s_lo[GFLAT], s_pre[GFLAT + 1];
+  if (threadIdx.x == 0) {
+    int acc = 0;
+    for (int g = 0; g < G; ++g) {
+      const int* o = A.toff + (size_t)g * (A.ntiles + 1) + A.tile;
+      s_lo[g] = __ldg(o);
+      s_pre[g] = acc;
+      acc += __ldg(o + 1) - __ldg(o);
+    }
+    s_pre[G] = acc;
+  }
+  __syncthreads();
+  const int n = A.n, g1 = A.g1;
+  // start: r = r0 = b_B - AB0 D0^-1 b_0, p = nu = t = y = 0
+  double res0 = 0.0, rho = 0.0;
+  {
+    double s1[1] = {0.0};
+    for_tile_rows<NR>(s_lo, s_pre, 1, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR]) {
+      float acc[NR];
+      int kl[NR];
+#pragma unroll
+      for (int q = 0; q < NR; ++q) {
+        acc[q] = __ldg(&A.b[r[q]]);
+        kl[q] = __ldg(&A.nlo[r[q]]);
+      }
+#pragma unroll
+      for (int s = 0; s < KMAX; ++s) {
+        if (s < A.KL) {
+#pragma unroll
+          for (int q = 0; q < NR; ++q) {
+            if (s < kl[q]) {
+              const size_t e = (size_t)s * n + r[q];
+              const int j = __ldg(&A.col[e]);
+              if (j < g1) acc[q] = acc[q] + __ldg(&A.aoff[e]) * (__ldg(&A.b[j]) * __ldg(&A.sinv[j]));
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < NR; ++q) {
+        if (!ok[q]) continue;
+        A.r[r[q]] = acc[q]; A.r0[r[q]] = acc[q];
+        A.p[r[q]] = 0.0f; A.nu[r[q]] = 0.0f; A.t[r[q]] = 0.0f; A.y[r[q]] = 0.0f;
+        s1[0] += (double)acc[q] * (double)acc[q];
+      }
+    });
+    put_partials<1>(A, s1, 0);
+    end_phase(A, ph);
+    grid_barrier(A, ph);
+    if (ph.ok) {
+      get_totals<1>(A, s1, 0);
+      res0 = sqrt(s1[0]);
+      rho = s1[0];
+    }
+  }
+  double alf = 1.0, omg = 1.0, bet = 0.0, rel = res0 > 0.0 ? 1.0 : 0.0;
+  int it = 0, converged = res0 > 0.0 ? 0 : 1, nonfinite = 0, buf = 1;
+  bool pending = false;  // an iteration's y/r update not yet applied
+  while (ph.ok && !converged && it < A.maxit) {
+    ++it;
+    // P0: the pending update, then p = r + bet (p - omg nu)
+    {
+      const float a = (float)alf, w = (float)omg, be = (float)bet;
+      for_tile_rows<NR>(s_lo, s_pre, 1, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR]) {
+        float rr[NR], pv[NR], nv[NR], tv[NR], yv[NR];
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+          rr[q] = ldm(&A.r[r[q]]);
+          pv[q] = ldm(&A.p[r[q]]);
+          nv[q] = ldm(&A.nu[r[q]]);
+          if (pending) {
+            tv[q] = ldm(&A.t[r[q]]);
+            yv[q] = ldm(&A.y[r[q]]);
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+          if (!ok[q]) continue;
+          float rn = rr[q];
+          if (pending) {
+            const float sv = rr[q] - a * nv[q];
+            A.y[r[q]] = yv[q] + a * pv[q] + w * sv;
+            rn = sv - w * tv[q];
+            A.r[r[q]] = rn;
+          }
+          A.p[r[q]] = rn + be * (pv[q] - w * nv[q]);
+        }
+      });
+      pending = false;
+      end_phase(A, ph);
+    }
+    // A: nu = Chat p, r0.nu
+    {
+      double s1[1] = {0.0};
+      wait_neighbours(A, ph);
+      for_tile_rows<NR>(s_lo, s_pre, 1, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR]) {
+        float acc[NR], r0v[NR];
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+          acc[q] = ldm(&A.p[r[q]]);
+          r0v[q] = ldm(&A.r0[r[q]]);
+        }
+        chat_sub(A, acc, r, [&](int k) { return ldm(&A.p[k]); });
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+          if (!ok[q]) continue;
+          A.nu[r[q]] = acc[q];
+          s1[0] += (double)r0v[q] * (double)acc[q];
+        }
+      });
+      put_partials<1>(A, s1, buf);
+      end_phase(A, ph);
+      grid_barrier(A, ph);
+      if (!ph.ok) break;
+      get_totals<1>(A, s1, buf);
+      buf ^= 1;
+      alf = rho / s1[0];
+    }
+    // B: t = Chat s, s = r - alf nu; t.s, t.t, r0.t, s.s, r0.s
+    {
+      double s5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+      const float a = (float)alf;
+      for_tile_rows<NR>(s_lo, s_pre, 1, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR]) {
+        float acc[NR], sv[NR], r0v[NR];
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+          sv[q] = ldm(&A.r[r[q]]) - a * ldm(&A.nu[r[q]]);
+          r0v[q] = ldm(&A.r0[r[q]]);
+          acc[q] = sv[q];
+        }
+        chat_sub(A, acc, r, [&](int k) { return ldm(&A.r[k]) - a * ldm(&A.nu[k]); });
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+          if (!ok[q]) continue;
+          A.t[r[q]] = acc[q];
+          const double tq = acc[q], sq = sv[q], oq = r0v[q];
+          s5[0] += tq * sq;
+          s5[1] += tq * tq;
+          s5[2] += oq * tq;
+          s5[3] += sq * sq;
+          s5[4] += oq * sq;
+        }
+      });
+      put_partials<5>(A, s5, buf);
+      end_phase(A, ph);
+      grid_barrier(A, ph);
+      if (!ph.ok) break;
+      get_totals<5>(A, s5, buf);
+      buf ^= 1;
+      omg = s5[0] / fmax(s5[1], SMALL);
+      const double rr = fmax(s5[3] - 2.0 * omg * s5[0] + omg * omg * s5[1], 0.0);
+      const double rho1 = s5[4] - omg * s5[2];
+      bet = (rho1 / rho) * (alf / omg);
+      rho = rho1;
+      rel = sqrt(rr) / res0;
+      pending = true;
+      if (!isfinite(rel) || !isfinite(bet)) { nonfinite = 1; break; }
+      if (rel < A.tol) converged = 1;
+    }
+  }
+  // the last update (y only), x_B = S^-1 y, then x_0 = D0^-1 (b_0 + sum aoff x_B)
+  if (ph.ok && !nonfinite) {
+    const float a = (float)alf, w = (float)omg;
+    for_tile_rows<NR>(s_lo, s_pre, 1, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR]) {
+      float yv[NR], si[NR];
+#pragma unroll
+      for (int q = 0; q < NR; ++q) {
+        yv[q] = ldm(&A.y[r[q]]);
+        if (pending) yv[q] = yv[q] + a * ldm(&A.p[r[q]]) + w * (ldm(&A.r[r[q]]) - a * ldm(&A.nu[r[q]]));
+        si[q] = __ldg(&A.sinv[r[q]]);
+      }
+#pragma unroll
+      for (int q = 0; q < NR; ++q)
+        if (ok[q]) A.x[r[q]] = yv[q] * si[q];
+    });
+    end_phase(A, ph);
+    grid_barrier(A, ph);
+    if (ph.ok) {
+      for_tile_rows<NR>(s_lo, s_pre, 0, 0, [&](const int (&r)[NR], const bool (&ok)[NR]) {
+        float acc[NR], si[NR];
+        int ku[NR];
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+          acc[q] = __ldg(&A.b[r[q]]);
+          si[q] = __ldg(&A.sinv[r[q]]);
+          ku[q] = __ldg(&A.nup[r[q]]);
+        }
+#pragma unroll
+        for (int t2 = 0; t2 < KMAX; ++t2) {
+#pragma unroll
+          for (int q = 0; q < NR; ++q) {
+            if (t2 < ku[q]) {
+              const size_t e = (size_t)(A.KL + t2) * n + r[q];
+              acc[q] = acc[q] + __ldg(&A.aoff[e]) * ldm(&A.x[__ldg(&A.col[e])]);
+            }
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < NR; ++q)
+          if (ok[q]) A.x[r[q]] = acc[q] * si[q];
+      });
+    }
+  }
+  if (A.tile == 0 && threadIdx.x == 0) {
+    A.st->iter = it;
+    A.st->s[S_RELRES] = rel;
+    A.st->s[S_RES0] = res0;
+    A.st->converged = converged;
+    A.st->nonfinite = nonfinite;
+    A.st->done = 1;
+  }
+}
+
+// Several independent systems (an ensemble) in one launch: bmap[b] = (member,
+// tile) of block b; members share nothing but the launch.
+__global__ void __launch_bounds__(TPB, 4) k_schur_batched(const SchurArgs* __restrict__ members,
+                                                          const int2* __restrict__ bmap) {
+  __shared__ SchurArgs sA;
+  if (threadIdx.x == 0) {
+    const int2 mt = bmap[blockIdx.x];
+    sA = members[mt.x];
+    sA.tile = mt.y;
+  }
+  __syncthreads();
+  schur_body(sA);
+}
+
+// One system: block b works on tile b.
+__global__ void __launch_bounds__(TPB, 4) k_schur_bicg(SchurArgs A) {
+  __shared__ SchurArgs sA;
+  if (threadIdx.x == 0) {
+    sA = A;
+    sA.ntiles = gridDim.x;
+    sA.tile = blockIdx.x;
+  }
+  __syncthreads();
+  schur_body(sA);
+}
+
+}  // namespace cms

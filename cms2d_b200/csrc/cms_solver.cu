@@ -22,6 +22,7 @@
 #include "cms_legacy.cuh"
 #include "cms_order.h"
 #include "cms_persist.cuh"
+#include "cms_schur.cuh"
 #include "cmsgpu.h"
 
 static char g_last_error[512] = "";
@@ -91,6 +92,15 @@ struct cms_solver {
   double* d_ppart = nullptr;
   int ptiles = 0;  // tiles (= blocks) of the persistent kernel; 0 not built, -1 not launchable
   size_t cap_toff = 0, cap_dep = 0;  // capacities of d_toff / d_dep_idx
+  // reduced (Schur complement) inner solve of refinement (cms_schur.cuh):
+  // Chat's pattern and values, 1/d and 1/s, neighbour tiles under Chat
+  int sc_state = 0;  // 0 not built, 1 built, -1 not possible on this pattern
+  int sc_KC = 0, sc_tiles = 0;
+  long long sc_nnz = 0, sc_e0b = 0;  // stored entries of Chat; couplings between group 0 and B
+  int *d_sccol = nullptr, *d_sdep_ptr = nullptr, *d_sdep_idx = nullptr;
+  float *d_scoff = nullptr, *d_ssinv = nullptr;
+  signed char* d_sccnt = nullptr;
+  size_t cap_sdep = 0;
   int cur_relax = 0;  // the FP32 factor in A32 is the two-phase one (k_ilu0_relax)
   int cur_fuse = 0;   // inner solves of refinement: update folded into the next iteration
   // MATRIX_SOLVER options 1, 2, 5-8: compass table (built on first use),
@@ -168,7 +178,7 @@ static inline int gsz(int rows) { return std::max(1, std::min(nblk(rows), GRID_C
 // Kernel classes timed by the profiler (cms_solver_profile_*).
 enum ProfCat : int {
   P_PROLOGUE = 0, P_ILU0 = 1, P_FWD = 2, P_BWD = 3, P_SPMV = 4, P_VEC = 5, P_RESID64 = 6, P_SCALAR = 7,
-  P_FLOW = 8, P_PERSIST = 9, P_NCAT = 10
+  P_FLOW = 8, P_PERSIST = 9, P_SCHUR_BUILD = 10, P_SCHUR = 11, P_NCAT = 12
 };
 
 static void prof_begin(Solver* S) {
@@ -414,17 +424,19 @@ static int bicg_iter(Solver* S, Mat<T>& A, Work<T>& W) {
 // Blocks of the persistent kernels that can be resident at once on the
 // device (cooperative launch limit); 0 when it cannot be launched.
 static int persist_capacity(int dev) {
-  int coop = 0, nsm = 0, per32 = 0, per64 = 0, perb = 0;
+  int coop = 0, nsm = 0, per32 = 0, per64 = 0, perb = 0, pers = 0, persb = 0;
   if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop ||
       cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per32, k_bicg_persistent<float>, TPB, 0) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per64, k_bicg_persistent<double>, TPB, 0) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perb, k_bicg_batched<float>, TPB, 0) != cudaSuccess ||
-      std::min(std::min(per32, per64), perb) <= 0) {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pers, k_schur_bicg, TPB, 0) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&persb, k_schur_batched, TPB, 0) != cudaSuccess ||
+      std::min(std::min(std::min(std::min(per32, per64), perb), pers), persb) <= 0) {
     cudaGetLastError();
     return 0;
   }
-  return std::min(std::min(std::min(per32, per64), perb) * nsm, GRID_CAP);
+  return std::min(std::min(std::min(std::min(std::min(per32, per64), perb), pers), persb) * nsm, GRID_CAP);
 }
 
 static int build_tiles(Solver* S, int nt);
@@ -755,20 +767,206 @@ static int resid64(Solver* S, Mat<TA>& A, const double* b, const TX* x, double* 
   return CMS_OK;
 }
 
+// Pattern of the reduced inner system (cms_schur.cuh): Chat's columns per B
+// row (direct couplings to B rows and the B neighbours of each group-0
+// neighbour, the row itself excluded), once per handle; the neighbour-tile
+// lists under Chat for the persistent tiles, rebuilt when the tile count
+// changes.  CMS_UNSUPPORTED when the ordering has no independent first group
+// or a reduced row has more than KSC entries.
+static int schur_pattern(Solver* S, int tiles) {
+  const HostPattern& P = S->hp;
+  const int n = P.n;
+  if (S->sc_state < 0) return CMS_UNSUPPORTED;
+  if (S->sc_state == 0) {
+    S->sc_state = -1;
+    if (P.G < 2 || P.G > GFLAT || P.gkl[0] != 0) return CMS_UNSUPPORTED;
+    const int g1 = P.gstart[1], nB = n - g1;
+    if (g1 <= 0 || nB <= 0) return CMS_UNSUPPORTED;
+    std::vector<int> tmp((size_t)nB * KSC);
+    std::vector<signed char> cnt(nB);
+    int KC = 0;
+    long long nnz = 0, e0b = 0;
+    for (int j = 0; j < g1; ++j) e0b += P.nup[j];
+    for (int i = 0; i < nB; ++i) {
+      const int r = g1 + i;
+      int loc[8 * KMAX];
+      int m = 0;
+      const int kl = P.nlo[r], ku = P.nup[r];
+      for (int s = 0; s < kl + ku; ++s) {
+        const int k = P.col[(size_t)(s < kl ? s : P.KL + (s - kl)) * n + r];
+        if (k >= g1) {
+          loc[m++] = k;
+          continue;
+        }
+        for (int t = 0; t < P.nup[k]; ++t) {
+          const int k2 = P.col[(size_t)(P.KL + t) * n + k];
+          if (k2 != r && m < 8 * KMAX) loc[m++] = k2;
+        }
+      }
+      std::sort(loc, loc + m);
+      const int mc = (int)(std::unique(loc, loc + m) - loc);
+      if (mc > KSC) return CMS_UNSUPPORTED;
+      std::copy(loc, loc + mc, tmp.begin() + (size_t)i * KSC);
+      cnt[i] = (signed char)mc;
+      KC = std::max(KC, mc);
+      nnz += mc;
+    }
+    KC = std::max(KC, 1);
+    std::vector<int> ccol((size_t)KC * nB);
+    for (int i = 0; i < nB; ++i)
+      for (int q = 0; q < KC; ++q) ccol[(size_t)q * nB + i] = q < cnt[i] ? tmp[(size_t)i * KSC + q] : g1 + i;
+    CHK(S->alloc(&S->d_sccol, ccol.size()));
+    CHK(S->alloc(&S->d_scoff, ccol.size()));
+    CHK(S->alloc(&S->d_sccnt, (size_t)nB));
+    CHK(S->alloc(&S->d_ssinv, (size_t)n));
+    CHK(S->alloc(&S->d_sdep_ptr, (size_t)GRID_CAP + 1));
+    CMS_CUDA(cudaMemcpyAsync(S->d_sccol, ccol.data(), ccol.size() * sizeof(int), cudaMemcpyHostToDevice, S->stream));
+    CMS_CUDA(cudaMemcpyAsync(S->d_sccnt, cnt.data(), cnt.size(), cudaMemcpyHostToDevice, S->stream));
+    CMS_CUDA(cudaStreamSynchronize(S->stream));
+    S->sc_KC = KC;
+    S->sc_nnz = nnz;
+    S->sc_e0b = e0b;
+    S->sc_tiles = 0;
+    S->sc_state = 1;
+  }
+  if (S->sc_tiles == tiles) return CMS_OK;
+  // neighbour tiles under Chat (tile t = natural cells [t n / nt, (t+1) n / nt))
+  const int g1 = P.gstart[1], nB = n - g1;
+  std::vector<int> ccol((size_t)S->sc_KC * nB);
+  std::vector<signed char> cnt(nB);
+  CMS_CUDA(cudaMemcpyAsync(ccol.data(), S->d_sccol, ccol.size() * sizeof(int), cudaMemcpyDeviceToHost, S->stream));
+  CMS_CUDA(cudaMemcpyAsync(cnt.data(), S->d_sccnt, cnt.size(), cudaMemcpyDeviceToHost, S->stream));
+  CMS_CUDA(cudaStreamSynchronize(S->stream));
+  std::vector<int> tstart(tiles + 1);
+  for (int t = 0; t <= tiles; ++t) tstart[t] = (int)((long long)t * n / tiles);
+  std::vector<int> tile_nat(n);
+  for (int t = 0; t < tiles; ++t)
+    for (int c = tstart[t]; c < tstart[t + 1]; ++c) tile_nat[c] = t;
+  std::vector<std::vector<int>> dep(tiles);
+  auto add = [&](int a, int b) {
+    for (int q : dep[a]) if (q == b) return;
+    dep[a].push_back(b);
+  };
+  for (int i = 0; i < nB; ++i) {
+    const int ti = tile_nat[P.perm[g1 + i]];
+    for (int q = 0; q < cnt[i]; ++q) {
+      const int tj = tile_nat[P.perm[ccol[(size_t)q * nB + i]]];
+      if (tj != ti) { add(ti, tj); add(tj, ti); }
+    }
+  }
+  std::vector<int> dptr(tiles + 1, 0), didx;
+  for (int t = 0; t < tiles; ++t) {
+    std::sort(dep[t].begin(), dep[t].end());
+    didx.insert(didx.end(), dep[t].begin(), dep[t].end());
+    dptr[t + 1] = (int)didx.size();
+  }
+  if (didx.size() + 1 > S->cap_sdep) {
+    CHK(S->alloc(&S->d_sdep_idx, didx.size() + 1));
+    S->cap_sdep = didx.size() + 1;
+  }
+  CMS_CUDA(cudaMemcpyAsync(S->d_sdep_ptr, dptr.data(), dptr.size() * sizeof(int), cudaMemcpyHostToDevice, S->stream));
+  if (!didx.empty())
+    CMS_CUDA(cudaMemcpyAsync(S->d_sdep_idx, didx.data(), didx.size() * sizeof(int), cudaMemcpyHostToDevice,
+                             S->stream));
+  CMS_CUDA(cudaStreamSynchronize(S->stream));
+  S->sc_tiles = tiles;
+  return CMS_OK;
+}
+
+// Chat's values and sinv from the FP32 matrix (once per solve).
+static int schur_numeric(Solver* S) {
+  const HostPattern& P = S->hp;
+  const int n = P.n, g1 = P.gstart[1], nB = n - g1;
+  const double nnz = (double)P.nnz_off;
+  KLAUNCH(S, P_SCHUR_BUILD, 8.0 * nnz + 10.0 * n,
+          (k_schur_diag<<<gsz(n), TPB, 0, S->stream>>>(n, g1, P.KL, S->d_col, S->d_nlo, S->d_nup, S->A32.aoff,
+                                                         S->A32.diag, S->d_ssinv)));
+  KLAUNCH(S, P_SCHUR_BUILD, 8.0 * nnz + 10.0 * n + 4.0 * n + 8.0 * (double)S->sc_nnz + nB,
+          (k_schur_off<<<gsz(nB), TPB, 0, S->stream>>>(n, g1, nB, P.KL, S->sc_KC, S->d_col, S->d_nlo, S->d_nup,
+                                                        S->A32.aoff, S->A32.diag, S->d_ssinv, S->d_sccol,
+                                                        S->d_sccnt, S->d_scoff)));
+  return CMS_OK;
+}
+
+// Algorithmic bytes of one reduced-system launch: the start (reduced
+// right-hand side), per iteration P0 (8 vector accesses per row), A (p, r0,
+// count, Chat, nu) and B (r, nu, r0, count, Chat, t), and the end (y update,
+// x_B, then x_0 from b, 1/d and the group-0 rows' couplings).
+static double schur_bytes(const Solver* S, int iters) {
+  const HostPattern& P = S->hp;
+  const double n = P.n, g1 = P.gstart[1], nB = n - g1, C = 8.0 * (double)S->sc_nnz, E = 8.0 * (double)S->sc_e0b;
+  const double start = 4.0 * n + 4.0 * g1 + E + nB + 24.0 * nB;
+  const double it = 32.0 * nB + (13.0 * nB + C) + (17.0 * nB + C);
+  const double end = 24.0 * nB + 9.0 * g1 + E + 4.0 * nB + 4.0 * g1;
+  return start + iters * it + end;
+}
+
+// Arguments of the reduced-system kernel for one system on `tiles` tiles.
+static SchurArgs make_schur_args(Solver* S, int tiles, int maxit, double tol) {
+  const HostPattern& P = S->hp;
+  SchurArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.n = P.n; a.g1 = P.gstart[1]; a.nB = P.n - a.g1; a.KL = P.KL; a.G = P.G; a.KC = S->sc_KC;
+  a.ntiles = tiles;
+  a.toff = S->d_toff; a.dep_ptr = S->d_sdep_ptr; a.dep_idx = S->d_sdep_idx; a.progress = S->d_progress;
+  a.ccol = S->d_sccol; a.coff = S->d_scoff; a.ccnt = S->d_sccnt;
+  a.col = S->d_col; a.nlo = S->d_nlo; a.nup = S->d_nup; a.aoff = S->A32.aoff; a.sinv = S->d_ssinv;
+  a.b = S->W32.b; a.x = S->W32.x;
+  a.r = S->W32.r; a.r0 = S->W32.r0; a.p = S->W32.p; a.nu = S->W32.u; a.t = S->W32.v; a.y = S->W32.z;
+  a.part = S->d_ppart; a.bar = &S->d_st->bar; a.st = S->d_st;
+  a.maxit = maxit; a.tol = tol; a.spin_limit = kSpinLimit;
+  return a;
+}
+
+// The reduced FP32 inner solve (W32.b -> W32.x) as one cooperative launch.
+static int run_schur_bicgstab(Solver* S, int tiles, int maxit, double tol) {
+  SchurArgs a = make_schur_args(S, tiles, maxit, tol);
+  CMS_CUDA(cudaMemsetAsync(&S->d_st->bar, 0, sizeof(GridBar), S->stream));
+  CMS_CUDA(cudaMemsetAsync(S->d_progress, 0, sizeof(unsigned int) * tiles * kProgressStride, S->stream));
+  void* args[] = {&a};
+  prof_begin(S);
+  const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_schur_bicg, dim3(tiles), dim3(TPB), args, 0,
+                                                    S->stream);
+  if (e != cudaSuccess) {
+    std::snprintf(g_last_error, sizeof(g_last_error), "cooperative launch (reduced BiCGStab): %s",
+                  cudaGetErrorString(e));
+    return CMS_DEVICE_ERROR;
+  }
+  S->launches++;
+  const size_t nrec = S->prof_recs.size();
+  prof_end(S, P_SCHUR, 0.0);
+  const bool recorded = S->prof_recs.size() > nrec;
+  CMS_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, S->stream));
+  CMS_CUDA(cudaStreamSynchronize(S->stream));
+  if (S->h_st->bar.err) {
+    std::snprintf(g_last_error, sizeof(g_last_error), "reduced BiCGStab: a grid barrier wait timed out");
+    return CMS_DEVICE_ERROR;
+  }
+  if (recorded) S->prof_recs.back().bytes = schur_bytes(S, S->h_st->iter);
+  return CMS_OK;
+}
+
 // Iterative refinement: FP64 residual/correction, FP32 matrix + factor + Krylov.
 static int run_refine(Solver* S, int nsolv, int maxit, double tol, cms_solve_info* info) {
   const HostPattern& P = S->hp;
   const int n = P.n;
   // A32 was written by the prologue; b64/x64 live in W64.b / W64.x.  The FP32
   // factor is the two-phase one when the persistent BiCGStab will run it.
-  const bool relax = nsolv == 3 && S->opts.inner_relax && S->opts.ordering == CMS_ORDER_MULTICOLOR && P.G > 2 &&
-                     !S->opts.multi_kernel && persist_tiles(S) > 0;
+  // inner_relax 2: the reduced system of cms_schur.cuh (any multicolour
+  // ordering with an independent first group); 1: the two-phase factor
+  // (more than two colours); 0: the exact multicolour ILU(0)
+  const bool mc_persist = nsolv == 3 && S->opts.ordering == CMS_ORDER_MULTICOLOR && !S->opts.multi_kernel &&
+                          persist_tiles(S) > 0;
+  const bool schur = mc_persist && S->opts.inner_relax == 2 && schur_pattern(S, S->ptiles) == CMS_OK;
+  const bool relax = !schur && mc_persist && S->opts.inner_relax && P.G > 2;
   struct RelaxScope {  // the flags describe A32's factor and its solves only while this solve runs
     Solver* s;
     ~RelaxScope() { s->cur_relax = 0; s->cur_fuse = 0; }
   } relax_scope{S};
   S->cur_fuse = 1;
-  if (relax) {
+  if (schur) {
+    CHK(schur_numeric(S));
+  } else if (relax) {
     KLAUNCH(S, P_ILU0, (double)n * (3 * 4 + 2) + (double)(P.nnz_off) * (2 * 4 + 4),
             (k_ilu0_relax<float><<<gsz(n), TPB, 0, S->stream>>>(n, P.KL, P.gstart[1], S->d_col, S->d_nlo,
                                                                  S->d_nup, S->A32.aoff, S->A32.diag, S->A32.luoff,
@@ -796,7 +994,9 @@ static int run_refine(Solver* S, int nsolv, int maxit, double tol, cms_solve_inf
     if (rel <= tol || steps >= rmax || inner_total >= maxit) break;
     // inner FP32 solve A32 d = r/||r|| from d = 0 (factor already built)
     KLAUNCH(S, P_VEC, (double)n * 12, (k_ir_scale<<<gsz(n), TPB, 0, S->stream>>>(n, S->W64.r, S->W32.b, S->d_st)));
-    if (nsolv == 3) {
+    if (schur) {
+      CHK(run_schur_bicgstab(S, S->ptiles, imax, itol));
+    } else if (nsolv == 3) {
       CHK(run_bicgstab<float>(S, S->A32, S->W32, imax, 2, itol, 1, false));
     } else {
       CMS_CUDA(cudaMemsetAsync(S->W32.x, 0, sizeof(float) * n, S->stream));
@@ -966,7 +1166,7 @@ void cms_solver_default_opts(cms_solver_opts* o) {
   o->max_refine = 30;
   o->verify = 1;
   o->multi_kernel = 0;
-  o->inner_relax = 1;
+  o->inner_relax = 2;
   o->relaxsor = 1.8;   // flow.F90:131
   o->nswp0_vel = 5;    // nswp0(2) of the hybrid solver's defaults (flow.F90:795-798)
 }

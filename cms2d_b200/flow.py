@@ -54,6 +54,8 @@ def _bind(L):
     L.cms_flow_device_bytes.argtypes = [vp]
     L.cms_flow_device_bytes.restype = C.c_size_t
     L.cms_flow_njoint.argtypes = [vp]
+    L.cms_flow_set_graphs.argtypes = [vp, i]
+    L.cms_flow_graph_stats.argtypes = [vp, vp, vp]
     L.cms_flow_solver.argtypes = [vp]
     L.cms_flow_solver.restype = vp
     L.cms_flow_last_solves.argtypes = [vp, C.POINTER(_lib.SolveInfo * 3)]
@@ -160,6 +162,16 @@ class FlowModel:
         self.t += dt
         self.last = info.as_dict()
         return self.last
+
+    def set_graphs(self, on: bool = True):
+        """Replay the stage kernel sequences as CUDA graphs (cms_flow_set_graphs)."""
+        _lib.check(_lib.lib().cms_flow_set_graphs(self._h, int(on)), "cms_flow_set_graphs")
+
+    def graph_stats(self):
+        """(graph replays, graph captures) so far."""
+        r, c = C.c_longlong(), C.c_longlong()
+        _lib.lib().cms_flow_graph_stats(self._h, C.byref(r), C.byref(c))
+        return r.value, c.value
 
     def get(self, name):
         g = self.g

@@ -69,12 +69,15 @@ class Solver:
                refinement; applies to float64 arrays) or "fp32".
     tol/norm:  stopping test; the reference uses 1e-3 on the L1 ratio
                (BiCGStab) or on the GMRES residual estimate.
+    inner_relax: FP32 inner BiCGStab of refinement on a multicolour ordering:
+               2 the reduced (Schur complement) system, 1 the two-phase
+               factor, 0 the exact multicolour ILU(0) (True/False mean 1/0).
     """
 
     def __init__(self, grid, iwet=None, ordering: str = "multicolor", precision: str = "fp64", tol: float = 1e-3,
                  norm: int = 1, max_iters: int = 0, inner_tol: float = 1e-3, inner_max: int = 50,
                  max_refine: int = 30, verify: bool = True, nsolv: int = NSOLV_DEFAULT,
-                 multi_kernel: bool = False, inner_relax: bool = True, relaxsor: float = 1.8, nswp0_vel: int = 5):
+                 multi_kernel: bool = False, inner_relax: int = 2, relaxsor: float = 1.8, nswp0_vel: int = 5):
         L = _lib.lib()
         self.grid = grid
         self.nsolv = nsolv
@@ -145,7 +148,7 @@ class Solver:
         return _lib.lib().cms_solver_stream(self._h) or 0
 
     PROFILE_CLASSES = ("prologue", "ilu0", "fwd_sweep", "bwd_sweep", "spmv", "vector", "resid64", "scalar", "flow",
-                       "bicgstab_persistent")
+                       "bicgstab_persistent", "reduced_build", "bicgstab_reduced")
 
     def profile(self, enable: bool = True):
         _lib.check(_lib.lib().cms_solver_profile(self._h, int(enable)), "cms_solver_profile")

@@ -66,11 +66,15 @@ typedef struct cms_solver_opts {
                         (grid barriers between colour phases, dot products reduced
                         in the kernel); 1: one launch per phase with host polling.
                         Both run the same arithmetic.                                  */
-  int inner_relax;   /* refinement with BiCGStab on a grid that needs more than two
-                        colours: 1 (default) factors the FP32 inner system without the
+  int inner_relax;   /* FP32 inner BiCGStab of refinement on a multicolour ordering:
+                        2 (default) solves the reduced system on the rows of colours
+                        >= 1 (Schur complement of the independent colour-0 block,
+                        right-scaled by its diagonal), which is red/black ILU(0)
+                        preconditioning in reduced form: no triangular sweeps, half
+                        the unknowns; 1 factors the FP32 system without the
                         couplings among rows of colours >= 2, so its sweeps take two
                         phases like a red/black grid; 0: exact multicolour ILU(0).
-                        The FP64 residual makes either converge to the same answer.   */
+                        The FP64 residual makes each converge to the same answer.   */
   double relaxsor;   /* SOR constant of nsolv 2 and 5 (SUCCESSIVE_OVER_RELAXATION_CONSTANT
                         card, default 1.8: flow.F90:131)                                */
   int nswp0_vel;     /* nswp0(2), the velocity iteration count the hybrid solver
@@ -158,11 +162,12 @@ long long cms_solver_launches(const cms_solver* s);
  * 0 prologue, 1 ILU(0) factor, 2 forward sweep, 3 backward sweep, 4 SpMV,
  * 5 vector/reduction kernels, 6 FP64 residual, 7 scalar kernels, 8 flow-step
  * assembly/correction kernels (a flow handle's solver), 9 persistent
- * BiCGStab (factor + every iteration in one launch).
+ * BiCGStab (every iteration in one launch), 10 reduced-system build (the
+ * inner solve's Schur complement), 11 persistent reduced BiCGStab.
  * profile_read fills ms[CMS_PROF_CLASSES], bytes[..] (algorithmic bytes:
  * every array a kernel touches counted once) and count[..] (launches);
  * reset=1 clears. */
-#define CMS_PROF_CLASSES 10
+#define CMS_PROF_CLASSES 12
 int cms_solver_profile(cms_solver* s, int enable);
 int cms_solver_profile_read(cms_solver* s, int reset, double* ms, double* bytes, long long* count);
 /* Adjoint of solve() (no counterpart in the reference), FP64, device
@@ -304,6 +309,14 @@ int cms_flow_njoint(const cms_flow* f);
  * rules, ms3[2] application (flags, lists, dry-to-wet initialisation,
  * gradient-operator rows).  No counterpart in the reference. */
 int cms_flow_wetdry_stats(const cms_flow* f, long long* updates, double* ms3);
+/* Replay of the step's stage kernel sequences (pressure-correction assembly,
+ * corrections and gradients) as CUDA graphs, captured per gradient-copy
+ * state and again after every wet-set change: on = 1 turns it on (ensembles
+ * do so for their members), 0 off (default: direct launches).  Graphs are
+ * not used while the solver's profiling is on.  graph_stats gives the
+ * replays and captures so far.  No counterpart in the reference. */
+int cms_flow_set_graphs(cms_flow* f, int on);
+int cms_flow_graph_stats(const cms_flow* f, long long* replays, long long* captures);
 void cms_flow_destroy(cms_flow* f);
 
 /* ---- Ensembles of independent flow models --------------------------------

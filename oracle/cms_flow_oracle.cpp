@@ -98,6 +98,10 @@ struct Flow {
   double tol = 1e-3;
   int last_niter = 0, last_iconv = 1;
   long long solve_iters = 0;
+  // capture of one assembled system (the iteration-count report): the next
+  // solve of variable cap_var is copied, natural order, before it runs
+  int cap_var = 0, cap_done = 0;
+  V cap_acoef, cap_ss, cap_sp, cap_phi;
 
   inline int& C(int k, int i) { return c2c[(size_t)i * NF + k]; }
   inline double& F(V& a, int k, int i) { return a[(size_t)i * NF + k]; }
@@ -1045,6 +1049,15 @@ int solve(Flow& f, V& ss, V& sp, V& res, V& phi, int var, double* rmom_out) {
     for (int k = 1; k <= nmf; ++k) a[(size_t)r * nmf + k - 1] = f.F(f.acoef, k, i);
     s0[r] = ss[i]; p0[r] = sp[i]; x0[r] = phi[i];
   }
+  if (f.cap_var == var && !f.cap_done) {
+    f.cap_acoef.assign((size_t)nD * nmf, 0.0);
+    f.cap_ss.assign(nD, 0.0); f.cap_sp.assign(nD, 0.0); f.cap_phi.assign(nD, 0.0);
+    for (int i = 1; i <= nD; ++i) {
+      for (int k = 1; k <= nmf; ++k) f.cap_acoef[(size_t)(i - 1) * nmf + k - 1] = f.F(f.acoef, k, i);
+      f.cap_ss[i - 1] = ss[i]; f.cap_sp[i - 1] = sp[i]; f.cap_phi[i - 1] = phi[i];
+    }
+    f.cap_done = 1;
+  }
   double relax = var == 1 ? f.P.relax_pp : f.P.relax_uv;
   int nswp = var == 1 ? f.nswp_pp : f.nswp_uv;
   double rm = 0, rr = 0;
@@ -1427,6 +1440,22 @@ long long orcf_get(void* h, int which, double* out) {
 }
 
 long long orcf_solve_iters(void* h) { return static_cast<Flow*>(h)->solve_iters; }
+// Arms the capture of the next solve() of variable var (1 pp, 2 u, 3 v).
+void orcf_capture(void* h, int var) {
+  Flow* f = static_cast<Flow*>(h);
+  f->cap_var = var;
+  f->cap_done = 0;
+}
+// The captured system (natural order, acoef [ncellsD][nmaxfaces]); 0 if none.
+int orcf_captured(void* h, double* acoef, double* ss, double* sp, double* phi) {
+  Flow* f = static_cast<Flow*>(h);
+  if (!f->cap_done) return 0;
+  std::copy(f->cap_acoef.begin(), f->cap_acoef.end(), acoef);
+  std::copy(f->cap_ss.begin(), f->cap_ss.end(), ss);
+  std::copy(f->cap_sp.begin(), f->cap_sp.end(), sp);
+  std::copy(f->cap_phi.begin(), f->cap_phi.end(), phi);
+  return 1;
+}
 // cells der_update recomputed at the start of the last step
 int orcf_last_nlist(void* h) { return static_cast<Flow*>(h)->last_nlist; }
 // ponding and narrowchannels switches (flow.F90:54-55)

@@ -164,6 +164,9 @@ class FlowOracle:
             L.orcf_set_wetdry.argtypes = [P, C.c_int, C.c_int]
             L.orcf_set_hdry.argtypes = [P, C.c_double]
             L.orcf_set_scheme.argtypes = [P, C.c_int]
+            L.orcf_capture.argtypes = [P, C.c_int]
+            L.orcf_captured.argtypes = [P, f64, f64, f64, f64]
+            L.orcf_captured.restype = C.c_int
             L._flow_bound = True
         g = case.grid
         self.case = case
@@ -237,6 +240,20 @@ class FlowOracle:
         out = np.zeros(g.ncellsD * g.nmaxfaces)
         lib().orcf_get(self._h, self.FACE[name], out)
         return out.reshape(g.ncellsD, g.nmaxfaces)
+
+    def capture(self, var):
+        """Arms the capture of the next solve() of variable var (1 pp, 2 u, 3 v)."""
+        lib().orcf_capture(self._h, int(var))
+
+    def captured(self):
+        """(acoef [ncellsD, nmaxfaces], ss, sp, phi) of the captured system, as
+        solve() received it, natural order; None before the capture."""
+        g = self.g
+        a = np.zeros(g.ncellsD * g.nmaxfaces)
+        ss, sp, phi = np.zeros(g.ncellsD), np.zeros(g.ncellsD), np.zeros(g.ncellsD)
+        if not lib().orcf_captured(self._h, a, ss, sp, phi):
+            return None
+        return a.reshape(g.ncellsD, g.nmaxfaces), ss, sp, phi
 
     @property
     def solve_iters(self):

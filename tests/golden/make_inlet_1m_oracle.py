@@ -2,7 +2,9 @@
 workload -- the three-level telescoping tidal inlet of about 1.0M cells
 (cms2d_b200.cases.tidal_inlet(1_000_000, seed=11), dt = 300 s) -- in the
 reference's natural cell order, every solve (ILU(0)-BiCGStab) driven to a
-1e-10 relative L2 residual, the outer SIMPLEC loop ended by check_conv.
+1e-9 relative L2 residual (FP64 BiCGStab stagnates near 3e-10 on the
+pressure-correction systems, so 1e-10 is not reachable), the outer SIMPLEC
+loop ended by check_conv.
 
 The full fields (3 x 8 MB per step) are too large to commit, so the file
 holds, after each of STEPS steps: the water level and the velocities at
@@ -29,7 +31,7 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 from cms2d_b200 import cases  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 
-CELLS, SEED, STEPS, NSAMPLE, TOL = 1_000_000, 11, 6, 8192, 1e-10
+CELLS, SEED, STEPS, NSAMPLE, TOL = 1_000_000, 11, 6, 8192, 1e-9
 OUT = os.path.join(HERE, "inlet_1m_oracle.npz")
 
 
@@ -54,7 +56,7 @@ def main():
     idx = sample_cells(n)
     gauges = cases.gauges(case)
     f = O.FlowOracle(case)
-    f.set_solver(nsolv=3, precond=O.PC_ILU0, tol=TOL, nswp_pp=5000, nswp_uv=5000, norm=2)
+    f.set_solver(nsolv=3, precond=O.PC_ILU0, tol=TOL, nswp_pp=3000, nswp_uv=3000, norm=2)
     f.init()
     eta_s, u_s, v_s, eta_g, stats, niter = [], [], [], [], [], []
     for s in range(STEPS):

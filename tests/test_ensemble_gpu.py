@@ -113,3 +113,42 @@ def test_ensemble_wetting_and_drying():
         assert np.array_equal(m.get("iwet"), w)
     _compare(e, solo, cs, 1e-10, 1e-8)
     e.close()
+
+
+def test_stage_graphs_match_direct_launches():
+    """A flow model whose stage kernel sequences replay as CUDA graphs gives
+    the same bits as direct launches, through wet/dry changes on an
+    intertidal flat (each change makes the graphs be captured again)."""
+    c = cases.tidal_flat(60, 40, seed=2, t0_hours=2.0)
+    out = []
+    for graphs in (False, True):
+        m = FlowModel(c, precision="fp64", nsolv=3, tol=1e-8, norm=2, nswp_pp=400, nswp_uv=400)
+        m.set_graphs(graphs)
+        m.init()
+        changed = 0
+        for _ in range(6):
+            info = m.step()
+            assert info["status"] == 0, info
+            changed += info["nchanged"]
+        out.append((m.get("eta").copy(), m.get("u").copy(), m.get("v").copy(), m.graph_stats(), changed))
+        m.close()
+    (e0, u0, v0, s0, c0), (e1, u1, v1, s1, c1) = out
+    assert s0 == (0, 0)
+    assert c0 == c1 > 0
+    replays, captures = s1
+    assert replays > 0 and captures > 4, s1  # two stages, re-captured after wet-set changes
+    np.testing.assert_array_equal(e0, e1)
+    np.testing.assert_array_equal(u0, u1)
+    np.testing.assert_array_equal(v0, v1)
+
+
+def test_ensemble_replays_stage_graphs():
+    cs = _basins()
+    e = EnsembleModel(cs, **{k: v for k, v in SET.items() if k != "precision"})
+    e.init()
+    for _ in range(2):
+        assert all(i["status"] == 0 for i in e.step())
+    for m in e.members:
+        replays, captures = m.graph_stats()
+        assert replays > captures > 0
+    e.close()

@@ -3,18 +3,28 @@ L10_Sed_BedAggradation_SedSorting: their telescoping grids and card
 settings, from the committed fixture) stepped by the GPU flow model and by
 the oracle on the same case.
 
-The cards select GMRES (nsolv 4), skewness correction on and each case's
-drying depth; the strings and Manning fields of the cases live in HDF5
-files, so each case takes a north water-level string and a uniform n.
-FP64: the oracle solves in the GPU's unknown order, both sides drive every
-solve to a 1e-10 relative L2 residual and run 4 outer iterations per step;
-water level within 1e-9 m, velocities and fluxes within 1e-6 of their
-largest value.  FP32 + FP64 refinement against the oracle in the natural
-(reference) order at converged solves: within 1e-5.
+The cases are laboratory flumes and a small basin (0.1-0.5 m cells, 0.3-0.7
+m deep); their inflow boundaries live in HDF5 files, so each case is driven
+by a through-flow instead: water-level strings on the west (+head/2) and east
+(-head/2) edges (cases.through_flow), which gives currents of about 0.1 m/s
+in the flumes.  Each case keeps its cards' skewness correction and drying
+depth.
+
+On these systems the reference's BiCGStab cannot drive a solve to a tight
+tolerance: its absolute small = 1e-15 guards (pbicgstab.f90:44,84) dominate
+the recurrence scalars once r.r falls below ~1e-15, which the
+pressure-correction systems of a flume (continuity residuals of ~1e-5) reach
+at a relative residual of ~1e-2 (the oracle converges on the same system
+scaled by 1e6).  So, as in the other flow-step tests, every solve runs a
+fixed number of Krylov iterations (tolerance never met, residuals far above
+that floor) in the same unknown order on both sides, FP64: water level within
+1e-9 m, velocities and fluxes within 1e-6 of their largest value, wet set
+identical.  Both the cards' GMRES(3) and BiCGStab, both orderings.
 """
 import numpy as np
 import pytest
 
+from cms2d_b200 import cases
 from cms2d_b200.flow import FlowModel
 from oracle import oracle as O
 from tests import reference_cases as RC
@@ -23,44 +33,42 @@ from tests.test_flow_gpu import _errors
 pytestmark = pytest.mark.gpu
 
 NAMES = RC.names()
+HEAD = {"L05_Implicit_Test01": 0.002, "L08_Sed_LSTF": 0.004, "L10_Sed_BedAggradation_SedSorting": 0.004}
+FIXED = {3: dict(tol=1e-30, nswp_pp=6, nswp_uv=3), 4: dict(tol=1e-30, nswp_pp=3, nswp_uv=1)}
 
 
-def _run(name, precision, ordering, same_order, steps=3, maxit=4):
-    case, kw = RC.case(name)
+def _run(name, nsolv, ordering, steps=4, maxit=4):
+    gf, kw, dt = RC.load(name)
+    case = cases.through_flow(gf, HEAD[name], dt=dt)
     wd = dict(hdry=kw["hdry"], ponding=kw.get("ponding", False), narrowchannels=kw.get("narrowchannels", False))
-    solver = dict(nsolv=kw["nsolv"], tol=1e-10, norm=2, nswp_pp=400, nswp_uv=400)
-    m = FlowModel(case, precision=precision, maxit=maxit, ordering=ordering, skewcor=kw["skewcor"], **solver, **wd)
+    solver = dict(nsolv=nsolv, norm=2, **FIXED[nsolv])
+    m = FlowModel(case, precision="fp64", maxit=maxit, ordering=ordering, skewcor=kw["skewcor"], **solver, **wd)
     m.init()
-    o = O.FlowOracle(case)
-    o.set_solver(nsolv=solver["nsolv"], precond=O.PC_ILU0, tol=solver["tol"], nswp_pp=solver["nswp_pp"],
+    o = O.FlowOracle(case, skewcor=kw["skewcor"])
+    o.set_solver(nsolv=nsolv, precond=O.PC_ILU0, tol=solver["tol"], nswp_pp=solver["nswp_pp"],
                  nswp_uv=solver["nswp_uv"], norm=2)
     o.set_wetdry(**wd)
-    if same_order:
-        o.set_order(m.perm())
+    o.set_order(m.perm())
     o.init()
+    n = case.grid.ncells
     for _ in range(steps):
         r = o.step(maxit=maxit)
         i = m.step()
         assert r["status"] == 0 and i["status"] == 0, (r, i)
         assert r["niter"] == i["niter"]
-        np.testing.assert_array_equal(m.get("iwet")[: case.grid.ncells], o.get("iwet")[: case.grid.ncells])
-    return _errors(o, m, case.grid)
+        np.testing.assert_array_equal(m.get("iwet")[:n], o.get("iwet")[:n])
+    e = _errors(o, m, case.grid)
+    e["vel_max"] = float(np.hypot(o.get("u")[:n], o.get("v")[:n]).max())
+    return e
 
 
 @pytest.mark.parametrize("ordering", ["natural", "multicolor"])
+@pytest.mark.parametrize("nsolv", [4, 3], ids=["gmres", "bicgstab"])
 @pytest.mark.parametrize("name", NAMES)
-def test_reference_case_fp64_matches_oracle(name, ordering):
-    e = _run(name, "fp64", ordering, same_order=True)
-    print(name, ordering, e)
+def test_reference_case_matches_oracle(name, nsolv, ordering):
+    e = _run(name, nsolv, ordering)
+    print(name, nsolv, ordering, e)
+    assert e["vel_max"] > 1e-3  # a real current, not rounding noise
     assert e["eta_m"] <= 1e-9
     for k in ("u", "v", "h", "flux"):
         assert e[k] <= 1e-6, (k, e)
-
-
-@pytest.mark.parametrize("name", NAMES)
-def test_reference_case_fp32_refine_matches_fp64_oracle(name):
-    e = _run(name, "fp32_refine", "multicolor", same_order=False)
-    print(name, "fp32+refine", e)
-    assert e["eta_m"] <= 1e-6
-    for k in ("u", "v", "h", "flux"):
-        assert e[k] <= 1e-5, (k, e)

@@ -6,6 +6,7 @@ FP64 oracle solution (the north-star bound for the refined solver).
 """
 import numpy as np
 import pytest
+import scipy.sparse.linalg as spla
 
 from cms2d_b200 import grid as G
 from cms2d_b200 import solver as S
@@ -249,23 +250,34 @@ def test_persistent_matches_multi_kernel(precision, kind):
     assert np.abs(p0 - p1).max() <= tol * np.abs(p1).max()
 
 
-@pytest.mark.parametrize("kind", ["tel", "big"])
-def test_two_phase_inner_factor(kind):
-    """FP32 + refinement with the two-phase inner factor (couplings among the
-    rows of colours >= 2 dropped) converges to the FP64 tolerance and to the
-    same solution as the exact multicolour factor."""
-    g = G.solver_test_grid(250_000) if kind == "big" else _grids()["tel"]
+@pytest.mark.parametrize("kind", ["cart", "tel", "big"])
+def test_inner_solve_forms(kind):
+    """FP32 + refinement with each inner BiCGStab form -- the reduced
+    (Schur complement) system, the two-phase factor (couplings among the rows
+    of colours >= 2 dropped; the exact factor on a two-colour grid) and the
+    exact multicolour factor -- converges to the FP64 tolerance and to the same
+    solution, which is the direct solution of the system."""
+    g = {"big": lambda: G.solver_test_grid(250_000), "tel": lambda: _grids()["tel"],
+         "cart": lambda: G.cartesian_grid(300, 200)}[kind]()
     acoef, ss, sp, phi = G.random_system(g, seed=9)
     res = {}
-    for relax in (True, False):
+    for relax in (2, 1, 0):
         s = S.Solver(g, precision="fp32_refine", tol=1e-8, norm=2, inner_relax=relax)
         assert s.last_info is None
         a, b, c, p = _copy(acoef, ss, sp, phi)
         r = np.zeros_like(b)
         info = s.solve(a, b, c, r, p, nswp=2000, nsolv=3)
-        assert info["status"] == 0 and info["ncolors"] > 2, info
+        assert info["status"] == 0 and info["ncolors"] == (2 if kind == "cart" else info["ncolors"]), info
         assert info["true_relres"] <= 1e-8, info
         res[relax] = (info, p[: g.ncells].copy())
-    print({k: (v[0]["iters"], v[0]["refine_steps"]) for k, v in res.items()})
-    p1, p0 = res[True][1], res[False][1]
-    assert np.abs(p1 - p0).max() <= 1e-6 * np.abs(p0).max()
+    print(kind, {k: (v[0]["iters"], v[0]["refine_steps"]) for k, v in res.items()})
+    p0 = res[0][1]
+    for relax in (2, 1):
+        assert np.abs(res[relax][1] - p0).max() <= 1e-6 * np.abs(p0).max(), relax
+    if kind != "big":
+        A = interior_matrix(g, acoef, sp)
+        n = g.ncells
+        rhs = ss[:n] + np.array([sum(acoef[i, k] * phi[g.cell2cell[i, k] - 1] for k in range(g.ncface[i])
+                                     if g.cell2cell[i, k] > n) for i in range(n)])
+        x = spla.spsolve(A.tocsc(), rhs)
+        assert np.abs(res[2][1] - x).max() <= 1e-6 * np.abs(x).max()
