@@ -135,7 +135,8 @@ def run_solve_ours(args):
     g, acoef, ss, sp, phi = build_solve_case(args.cells, seed=17 + rank)
     N = g.ncells
     solver = S.Solver(g, precision=args.precision, tol=1e-6, norm=2, verify=False, inner_tol=args.inner_tol,
-                      inner_max=args.inner_max, nsolv=3, multi_kernel=args.multi_kernel)
+                      inner_max=args.inner_max, nsolv=3, multi_kernel=args.multi_kernel,
+                      reduced_layout=args.reduced_layout)
     nswp = 5000
     # device-resident inputs
     t_acoef = torch.from_numpy(acoef).to(dev)
@@ -412,9 +413,9 @@ def run_iterations(args):
     GMRES(3) restarts with ILUTP(lfil 8) at the reference default 1e-3 (oracle);
     and the inner iterations of FP32 + FP64 refinement (reduced inner form) to
     1e-6 L2.  Systems: the solver sweep at 0.25M and 1M unknowns and the
-    1M-cell inlet's u, v and pp systems."""
-    from cms2d_b200 import grid as G
-    from cms2d_b200 import solver as S
+    1M-cell inlet's u, v and pp systems.  --iter-part gpu / cpu runs only the
+    GPU or only the oracle columns (the oracle's serial factor and sweeps need
+    no GPU; the two halves merge on the system names)."""
     from oracle import oracle as O
     world, rank, local = dist_setup()
     if rank != 0:
@@ -429,10 +430,12 @@ def run_iterations(args):
         (a, b, c, p), relax = sy[name]
         systems.append((f"inlet {g_in.ncells} {name}", g_in, (a, b, c, p), relax))
     rows = []
+    do_gpu, do_cpu = args.iter_part in ("all", "gpu"), args.iter_part in ("all", "cpu")
     for label, g, arrs, relax in systems:
         row = {"system": label, "unknowns": g.ncells, "relax": relax}
 
         def gpu(ordering, tol, norm, precision="fp64"):
+            from cms2d_b200 import solver as S
             s = S.Solver(g, ordering=ordering, precision=precision, tol=tol, norm=norm, verify=True, nsolv=3)
             a, b, c, p = [np.array(x, copy=True) for x in arrs]
             info = s.solve(a, b, c, np.zeros_like(b), p, relax=relax, nswp=5000, nsolv=3)
@@ -448,19 +451,26 @@ def run_iterations(args):
             return r, time.perf_counter() - t0
 
         for tag, tol, norm in (("1e-3_L1", 1e-3, 1), ("1e-6_L2", 1e-6, 2)):
-            i_mc = gpu("multicolor", tol, norm)
-            i_nat = gpu("natural", tol, norm)
-            o_nat, t_nat = orc(O.PC_ILU0, tol, norm)
-            o_tp, t_tp = orc(O.PC_ILUTP, tol, norm, lfil=35)
-            row[tag] = {"gpu_multicolour_ilu0": i_mc["iters"], "colours": i_mc["ncolors"],
-                        "gpu_natural_ilu0": i_nat["iters"], "levels": i_nat["ncolors"],
-                        "oracle_natural_ilu0": o_nat["iters"], "oracle_ilutp35": o_tp["iters"],
-                        "oracle_s": {"ilu0": round(t_nat, 2), "ilutp35": round(t_tp, 2)}}
-        o_gm, t_gm = orc(O.PC_ILUTP, 1e-3, 1, nsolv=4, lfil=8)
-        row["gmres3_ilutp8_1e-3_restarts"] = o_gm["iters"]
-        i_ref = gpu("multicolor", 1e-6, 2, precision="fp32_refine")
-        row["fp32_refine_reduced_1e-6_L2"] = {"inner_iters": i_ref["iters"], "refine_steps": i_ref["refine_steps"],
-                                              "true_relres": i_ref["true_relres"]}
+            r = {}
+            if do_gpu:
+                i_mc = gpu("multicolor", tol, norm)
+                i_nat = gpu("natural", tol, norm)
+                r.update(gpu_multicolour_ilu0=i_mc["iters"], colours=i_mc["ncolors"],
+                         gpu_natural_ilu0=i_nat["iters"], levels=i_nat["ncolors"])
+            if do_cpu:
+                o_nat, t_nat = orc(O.PC_ILU0, tol, norm)
+                o_tp, t_tp = orc(O.PC_ILUTP, tol, norm, lfil=35)
+                r.update(oracle_natural_ilu0=o_nat["iters"], oracle_ilutp35=o_tp["iters"],
+                         oracle_s={"ilu0": round(t_nat, 2), "ilutp35": round(t_tp, 2)})
+            row[tag] = r
+        if do_cpu:
+            o_gm, t_gm = orc(O.PC_ILUTP, 1e-3, 1, nsolv=4, lfil=8)
+            row["gmres3_ilutp8_1e-3_restarts"] = o_gm["iters"]
+        if do_gpu:
+            i_ref = gpu("multicolor", 1e-6, 2, precision="fp32_refine")
+            row["fp32_refine_reduced_1e-6_L2"] = {"inner_iters": i_ref["iters"],
+                                                  "refine_steps": i_ref["refine_steps"],
+                                                  "true_relres": i_ref["true_relres"]}
         rows.append(row)
         print(json.dumps(row), flush=True)
     print(json.dumps({"metric": "Krylov iterations per solve by preconditioner and ordering", "value": None,
@@ -612,7 +622,7 @@ def run_flow_ours(args):
     g = case.grid
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
     settings = dict(FLOW_SOLVER, nswp_pp=args.nswp, nswp_uv=args.nswp, inner_tol=args.inner_tol,
-                    inner_max=args.inner_max, multi_kernel=args.multi_kernel)
+                    inner_max=args.inner_max, multi_kernel=args.multi_kernel, reduced_layout=args.reduced_layout)
     precs = [args.precision]
     if not args.no_companion:
         precs.append("fp64" if args.precision == "fp32_refine" else "fp32_refine")
@@ -983,9 +993,13 @@ def main():
     ap.add_argument("--inner-max", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-parity", action="store_true", help="flow: skip the error check against the oracle fixture")
+    ap.add_argument("--iter-part", default="all", choices=["all", "gpu", "cpu"],
+                    help="iterations workload: the GPU columns, the oracle columns, or both")
     ap.add_argument("--ref-budget", type=float, default=400.0,
                     help="reference arm: seconds of whole timed CPU steps (at least one step)")
     ap.add_argument("--ncu", action="store_true", help="warm-up and timed steps only (profiler runs)")
+    ap.add_argument("--reduced-layout", type=int, default=0,
+                    help="threads x rows layout of the reduced inner solve (0 auto, 1-4)")
     ap.add_argument("--multi-kernel", action="store_true",
                     help="BiCGStab as one launch per phase instead of one persistent launch per solve")
     args = ap.parse_args()

@@ -23,7 +23,8 @@ class SolverOpts(C.Structure):
     _fields_ = [("ordering", C.c_int), ("precision", C.c_int), ("norm", C.c_int), ("tol", C.c_double),
                 ("max_iters", C.c_int), ("inner_tol", C.c_double), ("inner_max", C.c_int),
                 ("max_refine", C.c_int), ("verify", C.c_int), ("multi_kernel", C.c_int),
-                ("inner_relax", C.c_int), ("relaxsor", C.c_double), ("nswp0_vel", C.c_int)]
+                ("inner_relax", C.c_int), ("relaxsor", C.c_double), ("nswp0_vel", C.c_int),
+                ("reduced_layout", C.c_int)]
 
 
 class SolveInfo(C.Structure):

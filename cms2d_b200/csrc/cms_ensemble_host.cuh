@@ -181,7 +181,8 @@ static int refine_batched(Ens* E, const std::vector<int>& act, const std::vector
     CMS_CUDA(cudaMemcpyAsync(E->d_bmap, E->h_bmap, blocks * sizeof(int2), cudaMemcpyHostToDevice, E->stream));
     if (schur) {
       void* kargs[] = {&E->d_sargs, &E->d_bmap};
-      CMS_CUDA(cudaLaunchCooperativeKernel((const void*)k_schur_batched, dim3(blocks), dim3(TPB), kargs, 0,
+      // the layout the ensemble's tile split was sized for (256 threads per block)
+      CMS_CUDA(cudaLaunchCooperativeKernel((const void*)k_schur_batched<TPB, 2>, dim3(blocks), dim3(TPB), kargs, 0,
                                            E->stream));
     } else {
       void* kargs[] = {&E->d_args, &E->d_bmap};

@@ -652,6 +652,21 @@ __global__ void kf_vis_corner(FlowDev G, FlowState S, const int* cells, const un
 }
 
 // a[idx[j]] = vals[j]
+// Water levels of a tidal/harmonic string (bnd_eval, boundaries.F90:4098-4124)
+// at thrs hours: wse_j = sum_k f_k amp_k cos(speed_k thrs + vu_k - phase_k +
+// psi_jk) + offset + wsevar_j, coef [ntc][5] = (f, amp, speed, vu, phase).
+__global__ void kf_tide_eval(int nth, int ntc, const double* __restrict__ coef, const double* __restrict__ psi,
+                             const double* __restrict__ wsevar, double thrs, double offset, double* __restrict__ out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nth) return;
+  double w = 0.0;
+  for (int k = 0; k < ntc; ++k) {
+    const double* c = coef + 5 * k;
+    w = w + c[0] * c[1] * cos(c[2] * thrs + c[3] - c[4] + psi[(size_t)j * ntc + k]);
+  }
+  out[j] = w + offset + wsevar[j];
+}
+
 __global__ void kf_scatter_vals(const int* idx, const double* vals, int m, double* a) {
   const int j = blockIdx.x * TPB + threadIdx.x;
   if (j < m) a[idx[j]] = vals[j];

@@ -29,6 +29,11 @@ struct cms_flow {
   std::vector<int> th_cell_nat, th_dummy_nat;  // the same, natural numbering (0-based)
   double* d_wse = nullptr;       // [nth] values of the current step
   double* d_wse_cell = nullptr;  // [nD] the same, at the dummy cells
+  // tidal/harmonic constituents of the string, evaluated on the device when
+  // a step is given no water levels (cms_flow_set_tide)
+  int ntc = 0;
+  double *d_tide = nullptr, *d_psi = nullptr, *d_wsevar = nullptr;  // [ntc][5], [nth][ntc], [nth]
+  double tide_dtj = 0.0, tide_offset = 0.0;
   // wall string
   int nw = 0;
   int *d_w_cell = nullptr, *d_w_dummy = nullptr;
@@ -455,6 +460,7 @@ static int flow_create(int ncells, int ncellsD, int nmf, const int* c2c, const i
   so.inner_max = F->opts.inner_max;
   so.multi_kernel = F->opts.multi_kernel;
   if (F->opts.relaxsor > 0.0) so.relaxsor = F->opts.relaxsor;
+  so.reduced_layout = F->opts.reduced_layout;
   int rc = cms_solver_create(ncells, ncellsD, nmf, c2c, ncface, iwet.data(), &so, &F->S);
   if (rc) return fail(rc);
   Solver* S = F->S;
@@ -1158,7 +1164,12 @@ static int step_begin(Flow* F, double dt, const double* wsebnd) {
     F->nchg_pending = 0;
   }
   if (F->nth) {  // water levels of the string, placed on the string's dummies
-    CMS_CUDA(cudaMemcpyAsync(F->d_wse, wsebnd, F->nth * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (wsebnd)
+      CMS_CUDA(cudaMemcpyAsync(F->d_wse, wsebnd, F->nth * sizeof(double), cudaMemcpyHostToDevice, s));
+    else  // bnd_eval on the device: the constituents at the new time level
+      FLAUNCH(F, (kf_tide_eval<<<fblk(F->nth), TPB, 0, s>>>(F->nth, F->ntc, F->d_tide, F->d_psi, F->d_wsevar,
+                                                            (F->t_sim + dt) / 3600.0 + F->tide_dtj, F->tide_offset,
+                                                            F->d_wse)));
     FLAUNCH(F, (kf_scatter_vals<<<fblk(F->nth), TPB, 0, s>>>(F->d_th_dummy, F->d_wse, F->nth, F->d_wse_cell)));
   }
   FLAUNCHB(F, fbytes(F, 13, 0, 3), (kf_static<<<fblk(F->nD), TPB, 0, s>>>(F->G, T, dt)));
@@ -1386,8 +1397,45 @@ int cms_flow_init_hot(cms_flow* f, const double* p, const double* u, const doubl
 }
 
 int cms_flow_step(cms_flow* f, double dt, const double* wsebnd, cms_flow_info* info) {
-  if (!f || !f->inited || dt <= 0.0 || (f->nth > 0 && !wsebnd)) return CMS_BAD_ARGUMENT;
+  if (!f || !f->inited || dt <= 0.0 || (f->nth > 0 && !wsebnd && f->ntc == 0)) return CMS_BAD_ARGUMENT;
   return cms::flow_step(f, dt, wsebnd, info);
+}
+
+int cms_flow_set_tide(cms_flow* f, int ntc, const double* amp, const double* speed, const double* phase,
+                      const double* nodal, const double* vu, const double* psi, const double* wsevar, double dtj,
+                      double offset) {
+  if (!f || ntc <= 0 || !amp || !speed || !phase || f->nth <= 0) return CMS_BAD_ARGUMENT;
+  const int nth = f->nth;
+  std::vector<double> coef((size_t)ntc * 5), ps((size_t)nth * ntc, 0.0), var(nth, 0.0);
+  for (int k = 0; k < ntc; ++k) {
+    coef[5 * k + 0] = nodal ? nodal[k] : 1.0;
+    coef[5 * k + 1] = amp[k];
+    coef[5 * k + 2] = speed[k];
+    coef[5 * k + 3] = vu ? vu[k] : 0.0;
+    coef[5 * k + 4] = phase[k];
+  }
+  if (psi) std::copy(psi, psi + (size_t)nth * ntc, ps.begin());
+  if (wsevar) std::copy(wsevar, wsevar + nth, var.begin());
+  if (f->ntc < ntc) {  // buffers for the largest constituent count set so far
+    if (f->alloc(&f->d_tide, (size_t)ntc * 5) || f->alloc(&f->d_psi, (size_t)nth * ntc)) return CMS_DEVICE_ERROR;
+  }
+  if (!f->d_wsevar && f->alloc(&f->d_wsevar, (size_t)nth)) return CMS_DEVICE_ERROR;
+  cudaStream_t s = f->S->stream;
+  if (cudaMemcpyAsync(f->d_tide, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice, s) ||
+      cudaMemcpyAsync(f->d_psi, ps.data(), ps.size() * sizeof(double), cudaMemcpyHostToDevice, s) ||
+      cudaMemcpyAsync(f->d_wsevar, var.data(), var.size() * sizeof(double), cudaMemcpyHostToDevice, s) ||
+      cudaStreamSynchronize(s))
+    return CMS_DEVICE_ERROR;
+  f->ntc = ntc;
+  f->tide_dtj = dtj;
+  f->tide_offset = offset;
+  return CMS_OK;
+}
+
+int cms_flow_set_time(cms_flow* f, double t_seconds) {
+  if (!f) return CMS_BAD_ARGUMENT;
+  f->t_sim = t_seconds;
+  return CMS_OK;
 }
 
 int cms_flow_get(cms_flow* f, int which, double* out) {

@@ -147,6 +147,60 @@ __global__ void __launch_bounds__(TPB) k_schur_off(int n, int g1, int nB, int KL
   }
 }
 
+// Block sums of NS values for blocks of BS threads (valid in thread 0).
+template <int NS, int BS>
+__device__ __forceinline__ void block_sum_bs(double (&v)[NS]) {
+  __shared__ double sm[NS][BS / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NS; ++q) v[q] = warp_sum(v[q]);
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < NS; ++q) sm[q][wid] = v[q];
+  }
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int q = 0; q < NS; ++q) v[q] = warp_sum(lane < BS / 32 ? sm[q][lane] : 0.0);
+  }
+}
+
+// This block's partial sums of NS values into buffer buf.
+template <int NS, int BS>
+__device__ __forceinline__ void put_partials_bs(const SchurArgs& A, double (&v)[NS], int buf) {
+  block_sum_bs<NS, BS>(v);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NS; ++q) A.part[((size_t)buf * NSMAX + q) * A.ntiles + A.tile] = v[q];
+  }
+}
+
+// After a grid barrier: the grid totals, summed by the first warp in a fixed
+// order (lane l adds tiles l, l + 32, ..., then a butterfly), so every block
+// forms the same bits; then shared with the block.
+template <int NS>
+__device__ __forceinline__ void get_totals_w0(const SchurArgs& A, double (&tot)[NS], int buf) {
+  __shared__ double bc[NS];
+  if (threadIdx.x < 32) {
+    double acc[NS];
+#pragma unroll
+    for (int q = 0; q < NS; ++q) acc[q] = 0.0;
+    for (int b = threadIdx.x; b < A.ntiles; b += 32) {
+#pragma unroll
+      for (int q = 0; q < NS; ++q) acc[q] += __ldcg(&A.part[((size_t)buf * NSMAX + q) * A.ntiles + b]);
+    }
+#pragma unroll
+    for (int q = 0; q < NS; ++q) acc[q] = warp_sum(acc[q]);
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int q = 0; q < NS; ++q) bc[q] = acc[q];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < NS; ++q) tot[q] = bc[q];
+}
+
 // Rows of this tile in groups ga..gb as one index space (ranges in shared
 // memory: s_lo first row of each group's range, s_pre prefix counts).
 template <int NR, typename F>
@@ -189,8 +243,8 @@ __device__ __forceinline__ void chat_sub(const SchurArgs& A, float (&acc)[NR], c
   }
 }
 
+template <int BS, int NR>
 __device__ __forceinline__ void schur_body(const SchurArgs& A) {
-  constexpr int NR = 2;
   const int G = A.G;
   PhaseState ph{0u, 0u, true, true};
   __shared__ int s_lo[GFLAT], s_pre[GFLAT + 1];
@@ -239,11 +293,11 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
         s1[0] += (double)acc[q] * (double)acc[q];
       }
     });
-    put_partials<1>(A, s1, 0);
+    put_partials_bs<1, BS>(A, s1, 0);
     end_phase(A, ph);
     grid_barrier(A, ph);
     if (ph.ok) {
-      get_totals<1>(A, s1, 0);
+      get_totals_w0<1>(A, s1, 0);
       res0 = sqrt(s1[0]);
       rho = s1[0];
     }
@@ -303,11 +357,11 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
           s1[0] += (double)r0v[q] * (double)acc[q];
         }
       });
-      put_partials<1>(A, s1, buf);
+      put_partials_bs<1, BS>(A, s1, buf);
       end_phase(A, ph);
       grid_barrier(A, ph);
       if (!ph.ok) break;
-      get_totals<1>(A, s1, buf);
+      get_totals_w0<1>(A, s1, buf);
       buf ^= 1;
       alf = rho / s1[0];
     }
@@ -336,11 +390,11 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
           s5[4] += oq * sq;
         }
       });
-      put_partials<5>(A, s5, buf);
+      put_partials_bs<5, BS>(A, s5, buf);
       end_phase(A, ph);
       grid_barrier(A, ph);
       if (!ph.ok) break;
-      get_totals<5>(A, s5, buf);
+      get_totals_w0<5>(A, s5, buf);
       buf ^= 1;
       omg = s5[0] / fmax(s5[1], SMALL);
       const double rr = fmax(s5[3] - 2.0 * omg * s5[0] + omg * omg * s5[1], 0.0);
@@ -406,10 +460,16 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
   }
 }
 
+// Block and row layouts of the reduced kernel: threads per block and rows per
+// thread per batch (cms_solver_opts.reduced_layout picks one; 0: the first).
+#define CMS_SCHUR_LAYOUTS(X) X(256, 2) X(512, 2) X(512, 4) X(1024, 2)
+constexpr int kSchurLayouts = 4;
+
 // Several independent systems (an ensemble) in one launch: bmap[b] = (member,
 // tile) of block b; members share nothing but the launch.
-__global__ void __launch_bounds__(TPB, 4) k_schur_batched(const SchurArgs* __restrict__ members,
-                                                          const int2* __restrict__ bmap) {
+template <int BS, int NR>
+__global__ void __launch_bounds__(BS, 1024 / BS) k_schur_batched(const SchurArgs* __restrict__ members,
+                                                                  const int2* __restrict__ bmap) {
   __shared__ SchurArgs sA;
   if (threadIdx.x == 0) {
     const int2 mt = bmap[blockIdx.x];
@@ -417,11 +477,12 @@ __global__ void __launch_bounds__(TPB, 4) k_schur_batched(const SchurArgs* __res
     sA.tile = mt.y;
   }
   __syncthreads();
-  schur_body(sA);
+  schur_body<BS, NR>(sA);
 }
 
 // One system: block b works on tile b.
-__global__ void __launch_bounds__(TPB, 4) k_schur_bicg(SchurArgs A) {
+template <int BS, int NR>
+__global__ void __launch_bounds__(BS, 1024 / BS) k_schur_bicg(SchurArgs A) {
   __shared__ SchurArgs sA;
   if (threadIdx.x == 0) {
     sA = A;
@@ -429,7 +490,22 @@ __global__ void __launch_bounds__(TPB, 4) k_schur_bicg(SchurArgs A) {
     sA.tile = blockIdx.x;
   }
   __syncthreads();
-  schur_body(sA);
+  schur_body<BS, NR>(sA);
+}
+
+// Kernel, block size of layout k.
+struct SchurLayout {
+  const void* single;
+  const void* batched;
+  int bs;
+};
+inline SchurLayout schur_layout(int k) {
+  int q = 0;
+#define CMS_SCHUR_PICK(B, R) \
+  if (q++ == k) return SchurLayout{(const void*)k_schur_bicg<B, R>, (const void*)k_schur_batched<B, R>, B};
+  CMS_SCHUR_LAYOUTS(CMS_SCHUR_PICK)
+#undef CMS_SCHUR_PICK
+  return SchurLayout{(const void*)k_schur_bicg<256, 2>, (const void*)k_schur_batched<256, 2>, 256};
 }
 
 }  // namespace cms

@@ -430,8 +430,8 @@ static int persist_capacity(int dev) {
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per32, k_bicg_persistent<float>, TPB, 0) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per64, k_bicg_persistent<double>, TPB, 0) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perb, k_bicg_batched<float>, TPB, 0) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pers, k_schur_bicg, TPB, 0) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&persb, k_schur_batched, TPB, 0) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pers, k_schur_bicg<TPB, 2>, TPB, 0) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&persb, k_schur_batched<TPB, 2>, TPB, 0) != cudaSuccess ||
       std::min(std::min(std::min(std::min(per32, per64), perb), pers), persb) <= 0) {
     cudaGetLastError();
     return 0;
@@ -918,15 +918,34 @@ static SchurArgs make_schur_args(Solver* S, int tiles, int maxit, double tol) {
   return a;
 }
 
+// Layout of the reduced kernel for this handle (cms_solver_opts.reduced_layout,
+// 0 = auto = 512 threads x 2 rows) and the tiles it takes: its resident blocks
+// on the device, at most one per 256 rows.  0 tiles when it cannot launch.
+static int schur_layout_index(const Solver* S) {
+  const int k = S->opts.reduced_layout;
+  return (k >= 1 && k <= kSchurLayouts) ? k - 1 : 1;
+}
+static int schur_tiles(Solver* S, int layout) {
+  const SchurLayout L = schur_layout(layout);
+  int nsm = 0, per = 0, coop = 0;
+  if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, S->dev) != cudaSuccess || !coop ||
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, S->dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, L.single, L.bs, 0) != cudaSuccess || per <= 0) {
+    cudaGetLastError();
+    return 0;
+  }
+  return std::min(std::min(per * nsm, GRID_CAP), nblk(S->hp.n));
+}
+
 // The reduced FP32 inner solve (W32.b -> W32.x) as one cooperative launch.
 static int run_schur_bicgstab(Solver* S, int tiles, int maxit, double tol) {
   SchurArgs a = make_schur_args(S, tiles, maxit, tol);
+  const SchurLayout L = schur_layout(schur_layout_index(S));
   CMS_CUDA(cudaMemsetAsync(&S->d_st->bar, 0, sizeof(GridBar), S->stream));
   CMS_CUDA(cudaMemsetAsync(S->d_progress, 0, sizeof(unsigned int) * tiles * kProgressStride, S->stream));
   void* args[] = {&a};
   prof_begin(S);
-  const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_schur_bicg, dim3(tiles), dim3(TPB), args, 0,
-                                                    S->stream);
+  const cudaError_t e = cudaLaunchCooperativeKernel(L.single, dim3(tiles), dim3(L.bs), args, 0, S->stream);
   if (e != cudaSuccess) {
     std::snprintf(g_last_error, sizeof(g_last_error), "cooperative launch (reduced BiCGStab): %s",
                   cudaGetErrorString(e));
@@ -957,7 +976,11 @@ static int run_refine(Solver* S, int nsolv, int maxit, double tol, cms_solve_inf
   // (more than two colours); 0: the exact multicolour ILU(0)
   const bool mc_persist = nsolv == 3 && S->opts.ordering == CMS_ORDER_MULTICOLOR && !S->opts.multi_kernel &&
                           persist_tiles(S) > 0;
-  const bool schur = mc_persist && S->opts.inner_relax == 2 && schur_pattern(S, S->ptiles) == CMS_OK;
+  bool schur = mc_persist && S->opts.inner_relax == 2;
+  if (schur) {  // the tiles of the reduced kernel's layout
+    const int nt = schur_tiles(S, schur_layout_index(S));
+    schur = nt > 0 && build_tiles(S, nt) == nt && schur_pattern(S, S->ptiles) == CMS_OK;
+  }
   const bool relax = !schur && mc_persist && S->opts.inner_relax && P.G > 2;
   struct RelaxScope {  // the flags describe A32's factor and its solves only while this solve runs
     Solver* s;
@@ -995,7 +1018,7 @@ static int run_refine(Solver* S, int nsolv, int maxit, double tol, cms_solve_inf
     // inner FP32 solve A32 d = r/||r|| from d = 0 (factor already built)
     KLAUNCH(S, P_VEC, (double)n * 12, (k_ir_scale<<<gsz(n), TPB, 0, S->stream>>>(n, S->W64.r, S->W32.b, S->d_st)));
     if (schur) {
-      CHK(run_schur_bicgstab(S, S->ptiles, imax, itol));
+      CHK(run_schur_bicgstab(S, S->ptiles, imax, itol));  // tiles built above for its layout
     } else if (nsolv == 3) {
       CHK(run_bicgstab<float>(S, S->A32, S->W32, imax, 2, itol, 1, false));
     } else {

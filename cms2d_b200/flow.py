@@ -27,7 +27,7 @@ class FlowOpts(C.Structure):
                 ("tol", C.c_double), ("nswp_pp", C.c_int), ("nswp_uv", C.c_int), ("maxit", C.c_int),
                 ("skewcor", C.c_int), ("inner_tol", C.c_double), ("inner_max", C.c_int),
                 ("multi_kernel", C.c_int), ("hdry", C.c_double), ("ponding", C.c_int), ("narrowchannels", C.c_int),
-                ("relaxsor", C.c_double), ("ndsch", C.c_int)]
+                ("relaxsor", C.c_double), ("ndsch", C.c_int), ("reduced_layout", C.c_int)]
 
 
 class FlowInfo(C.Structure):
@@ -55,6 +55,8 @@ def _bind(L):
     L.cms_flow_device_bytes.restype = C.c_size_t
     L.cms_flow_njoint.argtypes = [vp]
     L.cms_flow_set_graphs.argtypes = [vp, i]
+    L.cms_flow_set_tide.argtypes = [vp, i] + [vp] * 7 + [d, d]
+    L.cms_flow_set_time.argtypes = [vp, d]
     L.cms_flow_graph_stats.argtypes = [vp, vp, vp]
     L.cms_flow_solver.argtypes = [vp]
     L.cms_flow_solver.restype = vp
@@ -74,7 +76,7 @@ class FlowModel:
                  tol: float = 1e-3, norm: int = 1, nswp_pp: int | None = None, nswp_uv: int | None = None,
                  maxit: int = 0, skewcor: bool = True, inner_tol: float = 1e-3, inner_max: int = 50,
                  multi_kernel: bool = False, hdry: float = 0.05, ponding: bool = False,
-                 narrowchannels: bool = False, relaxsor: float = 1.8, ndsch: int = 4):
+                 narrowchannels: bool = False, relaxsor: float = 1.8, ndsch: int = 4, reduced_layout: int = 0):
         L = _lib.lib()
         _bind(L)
         self.case = case
@@ -100,6 +102,7 @@ class FlowModel:
         o.narrowchannels = int(narrowchannels)
         o.relaxsor = relaxsor
         o.ndsch = ndsch
+        o.reduced_layout = reduced_layout
         self.opts = o
         self._keep = [np.ascontiguousarray(a) for a in (
             g.cell2cell.astype(np.int32), g.ncface.astype(np.int32), g.idirface.astype(np.int32),
@@ -150,14 +153,32 @@ class FlowModel:
         _lib.check(_lib.lib().cms_flow_init_hot(self._h, *[_p(a) for a in arrs], None if fl is None else _p(fl)),
                    "cms_flow_init_hot")
         self.t = float(t)
+        _lib.lib().cms_flow_set_time(self._h, self.t)
+
+    def set_tide(self):
+        """Moves the case's water-level string onto the device (bnd_eval's
+        harmonic form, cms_flow_set_tide): each constituent (amp, period h)
+        becomes speed 2 pi / period and phase -speed * t0, the case's
+        per-entry offsets the level variations; steps then pass no levels."""
+        amp = np.array([a for a, _ in self.case.tide], np.float64)
+        speed = np.array([2.0 * np.pi / T for _, T in self.case.tide], np.float64)
+        phase = -speed * (self.case.t0 / 3600.0)
+        var = None if self.case.th_offset is None else np.ascontiguousarray(self.case.th_offset, np.float64)
+        self._tide = (amp, speed, phase, var)
+        _lib.check(_lib.lib().cms_flow_set_tide(self._h, amp.size, _p(amp), _p(speed), _p(phase), None, None, None,
+                                                None if var is None else _p(var), 0.0, 0.0), "cms_flow_set_tide")
+        self.device_tide = True
 
     def step(self, dt=None, wsebnd=None):
         dt = self.case.dt if dt is None else dt
-        if wsebnd is None:
+        if wsebnd is None and not getattr(self, "device_tide", False):
             wsebnd = self.case.wsebnd(self.t + dt)
-        wsebnd = np.ascontiguousarray(wsebnd, np.float64)
+        wp = None
+        if wsebnd is not None:
+            wsebnd = np.ascontiguousarray(wsebnd, np.float64)
+            wp = _p(wsebnd)
         info = FlowInfo()
-        rc = _lib.lib().cms_flow_step(self._h, float(dt), _p(wsebnd), C.byref(info))
+        rc = _lib.lib().cms_flow_step(self._h, float(dt), wp, C.byref(info))
         _lib.check(rc, "cms_flow_step", allow=(_lib.CMS_OK, _lib.CMS_NONFINITE, _lib.CMS_UNSUPPORTED))
         self.t += dt
         self.last = info.as_dict()

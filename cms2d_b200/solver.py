@@ -77,7 +77,8 @@ class Solver:
     def __init__(self, grid, iwet=None, ordering: str = "multicolor", precision: str = "fp64", tol: float = 1e-3,
                  norm: int = 1, max_iters: int = 0, inner_tol: float = 1e-3, inner_max: int = 50,
                  max_refine: int = 30, verify: bool = True, nsolv: int = NSOLV_DEFAULT,
-                 multi_kernel: bool = False, inner_relax: int = 2, relaxsor: float = 1.8, nswp0_vel: int = 5):
+                 multi_kernel: bool = False, inner_relax: int = 2, relaxsor: float = 1.8, nswp0_vel: int = 5,
+                 reduced_layout: int = 0):
         L = _lib.lib()
         self.grid = grid
         self.nsolv = nsolv
@@ -96,6 +97,7 @@ class Solver:
         self.opts.inner_relax = int(inner_relax)
         self.opts.relaxsor = relaxsor
         self.opts.nswp0_vel = nswp0_vel
+        self.opts.reduced_layout = reduced_layout
         self._c2c = np.ascontiguousarray(grid.cell2cell, np.int32)
         self._ncf = np.ascontiguousarray(grid.ncface, np.int32)
         self._iwet = np.ones(grid.ncellsD, np.int32) if iwet is None else np.ascontiguousarray(iwet, np.int32)

@@ -79,6 +79,9 @@ typedef struct cms_solver_opts {
                         card, default 1.8: flow.F90:131)                                */
   int nswp0_vel;     /* nswp0(2), the velocity iteration count the hybrid solver
                         (nsolv 5) triples for n = 4, 5 (solvers.f90:265); default 5  */
+  int reduced_layout; /* block and row layout of the reduced inner solve: 0 auto,
+                        1 256 threads x 2 rows, 2 512 x 2, 3 512 x 4, 4 1024 x 2;
+                        the tiles follow the layout's resident block count      */
 } cms_solver_opts;
 
 typedef struct cms_solve_info {
@@ -234,6 +237,7 @@ typedef struct cms_flow_opts {
                         0 NONE, 1 UPWIND, 2 HYBRID, 3 POWERLAW, 4 EXPONENTIAL
                         (default, flow.F90:111); the higher-order deferred-
                         correction schemes 5-18 give CMS_UNSUPPORTED             */
+  int reduced_layout; /* cms_solver_opts.reduced_layout of the flow's solves (0 auto) */
 } cms_flow_opts;
 
 typedef struct cms_flow_info {
@@ -280,11 +284,27 @@ int cms_flow_init(cms_flow* f, const double* eta0);
  * cms_flow_step. */
 int cms_flow_init_hot(cms_flow* f, const double* p, const double* u, const double* v, const double* flux);
 /* One time step of length dt; wsebnd holds the string's water levels at the
- * new time level (one per string entry).  The step starts with wetting and
- * drying (flow_wetdry(0), flow.F90:1231-1539, and der_update,
- * derivatives.f90:204-296) when any cell's depth class changed since the
- * last one. */
+ * new time level (one per string entry), or NULL when the string's tide was
+ * set with cms_flow_set_tide (then evaluated on the device).  The step starts
+ * with wetting and drying (flow_wetdry(0), flow.F90:1231-1539, and
+ * der_update, derivatives.f90:204-296) when any cell's depth class changed
+ * since the last one. */
 int cms_flow_step(cms_flow* f, double dt, const double* wsebnd, cms_flow_info* info);
+/* The tidal/harmonic water-level string of bnd_eval (boundaries.F90:4098-4124)
+ * evaluated on the device at the start of every step given wsebnd = NULL:
+ * wse_j(t) = sum_k f_k amp_k cos(speed_k (t/3600 + dtj) + vu_k - phase_k +
+ * psi_jk) + offset + wsevar_j, with ntc constituents (amp in m, speed in
+ * radians per hour, phase, vu and psi in radians), nodal factors f (NULL: 1),
+ * equilibrium arguments vu (NULL: 0; both NULL and dtj = 0 is the reference's
+ * harmonic, non-tidal form), per-entry phase lags psi [nth][ntc] and level
+ * variations wsevar [nth] (NULL: 0); t is the time after the step.  The
+ * reference's ramp is 1 here (a ramped start passes its levels per step). */
+int cms_flow_set_tide(cms_flow* f, int ntc, const double* amp, const double* speed, const double* phase,
+                      const double* nodal, const double* vu, const double* psi, const double* wsevar, double dtj,
+                      double offset);
+/* Simulation time of the model's state in seconds (0 after cms_flow_init and
+ * cms_flow_init_hot; the tide evaluation reads it; each step adds dt). */
+int cms_flow_set_time(cms_flow* f, double t_seconds);
 /* Wet set of flow_wetdry(0) (flow.F90:1231-1539; flow_pond 1807-1876) for the
  * water level eta (ncellsD values): depth rule, every dummy off the water-level
  * string closed (dry), narrow-channel removal (Cartesian rules; the one-cell

@@ -136,3 +136,28 @@ def test_reference_default_solver_settings_run():
         assert info["status"] == 0 and info["iconv"] in (1, 2)
     eta = m.get("eta")[: c.grid.ncells]
     assert abs(eta.mean() - c.wse(m.t)) < 0.02
+
+
+@pytest.mark.parametrize("kind", ["inlet", "through_flow"])
+def test_device_tide_matches_host_levels(kind):
+    """bnd_eval's harmonic string evaluated on the device (cms_flow_set_tide)
+    against the same levels computed on the host and passed in: the M2 + K1
+    inlet from a tide phase, and a flume driven by per-entry level offsets."""
+    if kind == "inlet":
+        c = cases.tidal_inlet(12000, seed=3)
+        c.t0 = 3600.0
+    else:
+        from tests import reference_cases as RC
+        gf, _, dt = RC.load("L10_Sed_BedAggradation_SedSorting")
+        c = cases.through_flow(gf, 0.004, dt=dt)
+    out = []
+    for device in (False, True):
+        m = FlowModel(c, precision="fp64", nsolv=3, tol=1e-10, norm=2, nswp_pp=400, nswp_uv=400)
+        m.init()
+        if device:
+            m.set_tide()
+        for _ in range(3):
+            assert m.step()["status"] == 0
+        out.append(m.get("eta")[: c.grid.ncells].copy())
+        m.close()
+    assert np.abs(out[0] - out[1]).max() <= 1e-10

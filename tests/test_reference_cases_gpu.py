@@ -19,7 +19,14 @@ scaled by 1e6).  So, as in the other flow-step tests, every solve runs a
 fixed number of Krylov iterations (tolerance never met, residuals far above
 that floor) in the same unknown order on both sides, FP64: water level within
 1e-9 m, velocities and fluxes within 1e-6 of their largest value, wet set
-identical.  Both the cards' GMRES(3) and BiCGStab, both orderings.
+identical.  The cards' GMRES(3) in both orderings; BiCGStab in the
+natural ordering.  BiCGStab in the multicolour ordering is left out here:
+with three iterations per velocity solve on these three-cell-wide flumes it
+amplifies rounding so much that the oracle disagrees with itself when only
+the summation order of its dot products changes (1 against 8 threads:
+6e-8 m on L05, 4e-7 m on L10, and L08 diverges at the third step either
+way), so no bound on the GPU's difference would mean anything; the
+multicolour BiCGStab kernels are checked on the other flow cases.
 """
 import numpy as np
 import pytest
@@ -62,8 +69,8 @@ def _run(name, nsolv, ordering, steps=4, maxit=4):
     return e
 
 
-@pytest.mark.parametrize("ordering", ["natural", "multicolor"])
-@pytest.mark.parametrize("nsolv", [4, 3], ids=["gmres", "bicgstab"])
+@pytest.mark.parametrize("nsolv,ordering", [(4, "natural"), (4, "multicolor"), (3, "natural")],
+                         ids=["gmres-natural", "gmres-multicolor", "bicgstab-natural"])
 @pytest.mark.parametrize("name", NAMES)
 def test_reference_case_matches_oracle(name, nsolv, ordering):
     e = _run(name, nsolv, ordering)
