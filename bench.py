@@ -255,7 +255,7 @@ def run_solve_ours(args):
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "kernel": top, "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(ach / peak, 4), "peak_kind": peak_kind,
-                     "traffic": persist_traffic(prof, top, infos[-1]["iters"], args.steps, args.precision, N)},
+                     "traffic": None, "traffic_note": "not captured for the solve workload"},
         "kernels": kernels,
     }
     out["clocks"] = clk.summary()
@@ -502,27 +502,26 @@ def run_solve_reference(args):
 
 FLOW_SOLVER = dict(nsolv=3, tol=1e-6, norm=2)
 
-# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of the
-# persistent FP32 BiCGStab kernel per Krylov iteration on a 1M-unknown system,
-# from one ncu capture of its two launches in a 1M solve (746.2 MB over 23
-# iterations; profiles/bicgstab_persistent_solve_1M.md).  The roofline's
-# traffic is this figure times the iterations of an average launch.
-PERSIST_DRAM_BYTES_PER_ITER = 746.17e6 / 23
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one launch
+# of the reduced inner BiCGStab kernel on the 999,678-cell inlet: the mean of
+# two launches of this flow workload captured by ncu (velocity solves of a
+# few iterations each; ncu replays each launch from a cold L2, so the kernel's
+# ~75 MB working set is read once per launch and then stays in L2).
+REDUCED_DRAM_BYTES_PER_LAUNCH = (74_633_472 + 4_104_192 + 74_619_392 + 1_771_776) / 2
+REDUCED_CAPTURE_CELLS = 999_678
 
 
-PERSIST_CAPTURE_UNKNOWNS = 1_000_405
-
-
-def persist_traffic(prof, top, iters_per_step, steps, precision, unknowns):
-    """DRAM bytes of an average persistent launch, from the 1M capture; only
-    for workloads of that size (a smaller system stays in L2, a larger one
-    does not, so the figure does not scale)."""
-    if top != "bicgstab_persistent" or precision != "fp32_refine" or not prof[top]["launches"]:
-        return None
-    if not 0.8 <= unknowns / PERSIST_CAPTURE_UNKNOWNS <= 1.25:
-        return None
-    per_launch = iters_per_step * steps / prof[top]["launches"]
-    return round(PERSIST_DRAM_BYTES_PER_ITER * per_launch)
+def reduced_traffic(prof, top, unknowns):
+    """(DRAM bytes of a captured launch of the top kernel, how obtained), or
+    (None, why) when no capture of this kernel on this workload exists."""
+    if top != "bicgstab_reduced" or not prof[top]["launches"]:
+        return None, "not measured for this kernel"
+    if unknowns != REDUCED_CAPTURE_CELLS:
+        return None, "captured on the 999,678-cell inlet only"
+    return round(REDUCED_DRAM_BYTES_PER_LAUNCH), (
+        "ncu dram__bytes_read.sum + dram__bytes_write.sum, mean of two launches of this kernel on this workload "
+        "(velocity solves of a few iterations; cold L2 under ncu replay): the ~75 MB working set is read once per "
+        "launch and stays in L2, so an average launch's DRAM traffic is far below its algorithmic bytes")
 
 
 def flow_case(args, seed: int):
@@ -569,7 +568,7 @@ def flow_parity(case, seed, settings, precs):
     if int(z["cells"]) != case.grid.ncells or int(z["seed"]) != seed:
         return None
     idx, steps, n = z["sample"], z["eta"].shape[0], case.grid.ncells
-    out = {"vs": "FP64 oracle, natural order, solves to 1e-9 (committed fixture of the same case)",
+    out = {"vs": "FP64 oracle, natural order, solves to 1e-9 or 600 iterations (committed fixture of the same case)",
            "steps": int(steps), "sample_cells": int(idx.size)}
     for prec in precs:
         m = FlowModel(case, precision=prec, **settings)
@@ -718,6 +717,7 @@ def run_flow_ours(args):
                    "GBps": round(v["bytes"] / (v["ms"] / 1e3) / 1e9, 1) if v["ms"] > 0 else 0}
                for k, v in prof.items() if v["launches"]}
     all_bytes = sum(v["bytes"] for v in prof.values())
+    traffic, traffic_note = reduced_traffic(prof, top, g.ncells)
     out = {
         "metric": METRIC,
         "value": round(head["value"], 5),
@@ -742,8 +742,7 @@ def run_flow_ours(args):
         "gpu_launches": head["gpu_launches"],
         "roofline": {"bound": "hbm", "kernel": top, "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(ach / peak, 4), "peak_kind": peak_kind,
-                     "traffic": persist_traffic(prof, top, head["krylov_iters_per_step"], args.steps, args.precision,
-                                                g.ncells),
+                     "traffic": traffic, "traffic_note": traffic_note,
                      "step_GBps": round(all_bytes / (tot / 1e3) / 1e9, 1) if tot else 0},
         "kernels": kernels,
         "clocks": head["clocks"],
@@ -820,19 +819,23 @@ def run_flow_reference(args):
     t_step = float(np.mean(times))
     v = 1.0 / t_step
     # the reference's default thread count is one (NUM_THREADS, flow.F90:98):
-    # a bounded sample of outer iterations of the next step on one thread
-    O.set_threads(1)
-    n1 = 2 if not small else 0
+    # the same bounded sample (the first 2 outer iterations of a step) on all
+    # cores and on one thread, the whole-step time scaled by their ratio
     one = None
-    if n1:
-        t0 = time.perf_counter()
-        r1 = f.step(maxit=n1)
-        per = (time.perf_counter() - t0) / max(r1["niter"], 1)
-        one = {"value": round(1.0 / (per * np.mean(outer)), 6), "unit": "timesteps/s", "cores": 1,
-               "s_per_outer_iter": round(per, 3),
-               "sample": f"{r1['niter']} outer iterations of the step after the timed steps on one thread, "
-                         f"scaled by the {np.mean(outer):.1f} outer iterations per step measured above (estimate)"}
-    O.set_threads(threads)
+    if not small:
+        per = {}
+        for th in (threads, 1):
+            O.set_threads(th)
+            t0 = time.perf_counter()
+            r1 = f.step(maxit=2)
+            per[th] = (time.perf_counter() - t0) / max(r1["niter"], 1)
+        ratio = per[1] / per[threads]
+        one = {"value": round(v / ratio, 6), "unit": "timesteps/s", "cores": 1,
+               "s_per_outer_iter_1": round(per[1], 3), f"s_per_outer_iter_{threads}": round(per[threads], 3),
+               "sample": f"the first 2 outer iterations of the next two steps, one on {threads} threads and one on "
+                         f"one thread; the measured whole-step rate divided by their time ratio {ratio:.2f} "
+                         f"(estimate)"}
+        O.set_threads(threads)
     warm = "whole steps" if small else "steps of one outer iteration (untimed)"
     sample = (f"{args.warmup} warm-up {warm}, then {len(times)} whole timed steps (every outer iteration until "
               f"check_conv; {np.mean(outer):.1f} outer iterations per step), {sum(times):.1f} s")
@@ -850,6 +853,33 @@ def run_flow_reference(args):
            "cpu_1thread": one,
            "e2e": {"value": round(v, 6), "unit": "timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
+
+
+def ensemble_cpu_sample(specs, args, nsample: int = 2):
+    """Config 4's CPU baseline: the oracle (natural-order ILU(0)-BiCGStab to
+    1e-6, serial factor and sweeps, OpenMP elsewhere) steps the nsample
+    smallest members one whole step each; their time per cell-step, times the
+    cells of all members, estimates the sum of the member times of one
+    ensemble step."""
+    from cms2d_b200 import cases
+    from oracle import oracle as O
+    threads = os.cpu_count()
+    O.set_threads(threads)
+    sizes = [s["nx"] * s["ny"] for s in specs]
+    pick = sorted(range(len(specs)), key=lambda k: sizes[k])[:nsample]
+    t_cells, t_sec = 0, 0.0
+    for c in cases.ensemble_basins(len(specs), seed=23, nmin=args.ens_min, nmax=args.ens_max, members=pick):
+        f = O.FlowOracle(c)
+        f.set_solver(nsolv=3, precond=O.PC_ILU0, tol=1e-6, nswp_pp=200, nswp_uv=200, norm=2)
+        f.init()
+        t0 = time.perf_counter()
+        f.step()
+        t_sec += time.perf_counter() - t0
+        t_cells += c.grid.ncells
+    per_step = t_sec / t_cells * sum(sizes)
+    return {"value": round(len(specs) / per_step, 6), "unit": "member-timesteps/s", "cores": threads, "kind": "port",
+            "sample": f"one whole step of each of the {nsample} smallest members ({t_cells} cells, {t_sec:.1f} s), "
+                      f"scaled by cells to all {len(specs)} members (estimate of the sum of member times)"}
 
 
 def run_ensemble_ours(args):
@@ -952,6 +982,8 @@ def run_ensemble_ours(args):
         "device_gb": round(sum(m.device_bytes for m in e.members) / 1e9, 2),
         "clocks": clk.summary(),
     }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = ensemble_cpu_sample(specs, args)
     if args.ens_sequential and world == 1:
         # the same members stepped one after another with their own solver launches
         for m in e.members:  # each member's solver on the whole GPU again

@@ -5,6 +5,7 @@ include/cmsgpu.h); the Python modules here mirror the reference's interfaces
 on top of it and generate synthetic grids.
 """
 from . import grid  # noqa: F401
+from . import solver  # noqa: F401
 
 __all__ = ["grid", "solver"]
 __version__ = "0.1.0"

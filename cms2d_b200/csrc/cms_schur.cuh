@@ -363,6 +363,10 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
       if (!ph.ok) break;
       get_totals_w0<1>(A, s1, buf);
       buf ^= 1;
+      // a breakdown (r0.nu = 0) ends this inner solve with the iterate so far
+      // (the refinement's FP64 residual takes over); a non-finite sum is an error
+      if (!isfinite(s1[0])) { nonfinite = 1; break; }
+      if (s1[0] == 0.0) break;
       alf = rho / s1[0];
     }
     // B: t = Chat s, s = r - alf nu; t.s, t.t, r0.t, s.s, r0.s
@@ -399,12 +403,14 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
       omg = s5[0] / fmax(s5[1], SMALL);
       const double rr = fmax(s5[3] - 2.0 * omg * s5[0] + omg * omg * s5[1], 0.0);
       const double rho1 = s5[4] - omg * s5[2];
+      rel = sqrt(rr) / res0;
+      if (!isfinite(rel) || !isfinite(omg) || !isfinite(rho1)) { nonfinite = 1; break; }
+      pending = true;  // y += alf p + omg s is valid even at a breakdown below
+      if (rel < A.tol) { converged = 1; continue; }
+      // breakdown of the next step (omg = 0 or r0.r = 0): stop with this iterate
+      if (omg == 0.0 || rho1 == 0.0) break;
       bet = (rho1 / rho) * (alf / omg);
       rho = rho1;
-      rel = sqrt(rr) / res0;
-      pending = true;
-      if (!isfinite(rel) || !isfinite(bet)) { nonfinite = 1; break; }
-      if (rel < A.tol) converged = 1;
     }
   }
   // the last update (y only), x_B = S^-1 y, then x_0 = D0^-1 (b_0 + sum aoff x_B)

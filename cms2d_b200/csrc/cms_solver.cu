@@ -919,11 +919,12 @@ static SchurArgs make_schur_args(Solver* S, int tiles, int maxit, double tol) {
 }
 
 // Layout of the reduced kernel for this handle (cms_solver_opts.reduced_layout,
-// 0 = auto = 512 threads x 2 rows) and the tiles it takes: its resident blocks
+// 0 = auto = 1024 threads x 2 rows, the fastest on the 1M systems) and the
+// tiles it takes: its resident blocks
 // on the device, at most one per 256 rows.  0 tiles when it cannot launch.
 static int schur_layout_index(const Solver* S) {
   const int k = S->opts.reduced_layout;
-  return (k >= 1 && k <= kSchurLayouts) ? k - 1 : 1;
+  return (k >= 1 && k <= kSchurLayouts) ? k - 1 : 3;
 }
 static int schur_tiles(Solver* S, int layout) {
   const SchurLayout L = schur_layout(layout);
