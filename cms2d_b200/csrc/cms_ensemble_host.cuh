@@ -103,7 +103,7 @@ static int refine_batched(Ens* E, const std::vector<int>& act, const std::vector
   for (int j = 0; j < A_ && schur; ++j) {
     Solver* S = E->m[act[j]]->S;
     schur = S->opts.inner_relax == 2 && S->opts.ordering == CMS_ORDER_MULTICOLOR &&
-            schur_pattern(S) == CMS_OK;
+            schur_pattern(S, E->tiles[act[j]]) == CMS_OK;
   }
   for (int j = 0; j < A_; ++j) {
     Solver* S = E->m[act[j]]->S;

@@ -19,31 +19,31 @@
 // operator's rounding.
 //
 // Storage.  C S^-1 = I - Chat: Chat's off-diagonals in ELL slot-major order
-// over the reduced rows i = r - g1, each coupling one 8-byte element
-// cel = (device column, value bits), with the count per row in ccnt; built per
-// solve by k_schur_diag and k_schur_off from the FP32 matrix; sinv[r] = 1/d_r
-// for group-0 rows and 1/s_r (s_r = C_rr) for B rows.  The iteration's
-// vectors live interleaved per device row as float4 (r, nu, p, t) in two
-// buffers that alternate between iterations, so a neighbour's four values
-// come in one 16-byte gather.
+// over the reduced rows i = r - g1 (ccol: device column, coff: value, ccnt:
+// count per row), built per solve by k_schur_diag and k_schur_off from the
+// FP32 matrix; sinv[r] = 1/d_r for group-0 rows and 1/s_r (s_r = C_rr) for B
+// rows.  Vectors are indexed by device row (the B rows of the refinement's
+// FP32 work arrays).
 //
 // The persistent kernel.  One block per tile (the tiles of the persistent
 // ILU(0) kernel: tile t's B rows are toff[g][t]..toff[g][t+1] for g >= 1), a
-// BiCGStab iteration is two phases, each ending at the grid barrier that its
-// dot products need:
-//   A   from the current buffer, the previous iteration's update of the own
-//       rows (s = r - alpha nu, r' = s - w t, p' = r' + beta (p - w nu),
-//       y += alpha p + w s) and nu' = Chat p', where each gathered neighbour's
-//       p' is formed from its gathered (r, nu, p, t) by the same arithmetic;
-//       (r', nu', p') into the other buffer; r0.nu'.
-//   B   t = Chat s with s = r' - alpha' nu' formed per gathered (r', nu');
-//       t into the other buffer; t.s, t.t, r0.t, s.s, r0.s.
-// Every value a phase gathers was written before the last grid barrier and
-// every buffer a phase writes was last read before it, so no tile waits on
-// another between barriers.  The next residual norm comes from
-// ||r||^2 = s.s - 2 w t.s + w^2 t.t and the next r0.r from r0.s - w r0.t.
-// Waits and barriers are those of the persistent ILU(0) kernel (bounded,
-// cms_persist.cuh).
+// BiCGStab iteration is three phases:
+//   P0  the previous iteration's y/r update and the new search direction p
+//       (own rows, no neighbour values);
+//   A   nu = Chat p (after the neighbour tiles have finished P0) and r0.nu,
+//       reduced at a grid barrier;
+//   B   t = Chat s with s = r - alpha nu formed on the fly for each gathered
+//       neighbour, and t.s, t.t, r0.t, s.s, r0.s, reduced at a grid barrier;
+// the next residual norm comes from ||r||^2 = s.s - 2 w t.s + w^2 t.t and the
+// next r0.r from r0.s - w r0.t.  Waits and barriers are those of the
+// persistent ILU(0) kernel (bounded, cms_persist.cuh).
+//
+// Measured against this layout on one B200, same box, 1M-cell inlet flow
+// step (timesteps/s): 5.50 here; couplings packed as one 8-byte (column,
+// value) element and (r, nu) interleaved for one 8-byte gather, 5.24-5.33;
+// P0 and its neighbour wait dropped by forming each gathered neighbour's new
+// direction from a 16-byte (r, nu, p, t) gather in alternating buffers,
+// 4.72.  Separate 4-byte streams keep more loads in flight per thread.
 #pragma once
 #include "cms_persist.cuh"
 
@@ -56,7 +56,11 @@ struct SchurArgs {
   int KC;                  // slots of Chat (largest count)
   int ntiles, tile;
   const int* toff;         // [G][ntiles+1] tile row ranges per group
-  const int2* cel;         // [KC][nB] (column, value bits) of Chat's couplings
+  const int* dep_ptr;      // neighbour tiles under Chat's couplings
+  const int* dep_idx;
+  unsigned int* progress;  // [ntiles * kProgressStride] (zero at launch)
+  const int* ccol;         // [KC][nB]
+  const float* coff;       // [KC][nB]
   const signed char* ccnt; // [nB]
   const int* col;          // A's ELL (device order)
   const signed char* nlo;
@@ -65,8 +69,7 @@ struct SchurArgs {
   const float* sinv;       // [n]
   const float* b;
   float* x;
-  float4* q[2];            // [n] per device row (r, nu, p, t), two buffers
-  float *r0, *y;           // [n]
+  float *r, *r0, *p, *nu, *t, *y;
   double* part;            // [2][NSMAX][ntiles]
   GridBar* bar;
   DevState* st;
@@ -106,14 +109,13 @@ __global__ void __launch_bounds__(TPB) k_schur_diag(int n, int g1, int KL, const
 }
 
 // Chat's off-diagonals of reduced row i (r = g1 + i):
-// coff_rk = (aoff_rk [k in B] + sum_{j in group 0} aoff_rj aoff_jk / d_j) / s_k,
-// written as the value bits of cel (whose columns the host set once).
+// coff_rk = (aoff_rk [k in B] + sum_{j in group 0} aoff_rj aoff_jk / d_j) / s_k.
 __global__ void __launch_bounds__(TPB) k_schur_off(int n, int g1, int nB, int KL, int KC,
                                                    const int* __restrict__ col, const signed char* __restrict__ nlo,
                                                    const signed char* __restrict__ nup,
                                                    const float* __restrict__ aoff, const float* __restrict__ diag,
-                                                   const float* __restrict__ sinv, const signed char* __restrict__ ccnt,
-                                                   int2* __restrict__ cel) {
+                                                   const float* __restrict__ sinv, const int* __restrict__ ccol,
+                                                   const signed char* __restrict__ ccnt, float* __restrict__ coff) {
   for (int i = blockIdx.x * TPB + threadIdx.x; i < nB; i += gridDim.x * TPB) {
     const int r = g1 + i;
     const int kc = ccnt[i];
@@ -121,7 +123,7 @@ __global__ void __launch_bounds__(TPB) k_schur_off(int n, int g1, int nB, int KL
     double acc[KSC];
 #pragma unroll
     for (int q = 0; q < KSC; ++q) {
-      cc[q] = q < kc ? cel[(size_t)q * nB + i].x : -1;
+      cc[q] = q < kc ? ccol[(size_t)q * nB + i] : -1;
       acc[q] = 0.0;
     }
     auto add = [&](int k, double v) {
@@ -148,7 +150,7 @@ __global__ void __launch_bounds__(TPB) k_schur_off(int n, int g1, int nB, int KL
     }
 #pragma unroll
     for (int q = 0; q < KSC; ++q)
-      if (q < kc) cel[(size_t)q * nB + i].y = __float_as_int((float)(acc[q] * (double)sinv[cc[q]]));
+      if (q < KC) coff[(size_t)q * nB + i] = q < kc ? (float)(acc[q] * (double)sinv[cc[q]]) : 0.0f;
   }
 }
 
@@ -227,8 +229,8 @@ __device__ __forceinline__ void for_tile_rows(const int* s_lo, const int* s_pre,
   }
 }
 
-// acc[q] - sum_s c_s * w(gathered column) over the reduced row's couplings,
-// w given by a functor of the column.
+// acc[q] - sum_s coff[s] * w(col) over the reduced row's slots, w(k) given
+// by a functor of the gathered column.
 template <int NR, typename W>
 __device__ __forceinline__ void chat_sub(const SchurArgs& A, float (&acc)[NR], const int (&r)[NR], W&& w) {
   int kc[NR];
@@ -240,22 +242,12 @@ __device__ __forceinline__ void chat_sub(const SchurArgs& A, float (&acc)[NR], c
 #pragma unroll
       for (int q = 0; q < NR; ++q) {
         if (s < kc[q]) {
-          const int2 e = __ldg(&A.cel[(size_t)s * A.nB + (r[q] - A.g1)]);
-          acc[q] = acc[q] - __int_as_float(e.y) * w(e.x);
+          const size_t e = (size_t)s * A.nB + (r[q] - A.g1);
+          acc[q] = acc[q] - __ldg(&A.coff[e]) * w(__ldg(&A.ccol[e]));
         }
       }
     }
   }
-}
-
-// The new search direction of a row from its (r, nu, p, t) and the previous
-// iteration's scalars: s = r - a nu, r' = s - w t, p' = r' + b (p - w nu).
-// Owner and gathering neighbours use this one function, so they form the
-// same bits.
-__device__ __forceinline__ float next_p(float4 v, float a, float w, float be, float& rn, float& sv) {
-  sv = __fsub_rn(v.x, __fmul_rn(a, v.y));
-  rn = __fsub_rn(sv, __fmul_rn(w, v.w));
-  return __fadd_rn(rn, __fmul_rn(be, __fsub_rn(v.z, __fmul_rn(w, v.y))));
 }
 
 template <int BS, int NR>
@@ -275,7 +267,7 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
   }
   __syncthreads();
   const int n = A.n, g1 = A.g1;
-  // start: r = r0 = b_B - AB0 D0^-1 b_0 in buffer 0 with nu = p = t = 0, y = 0
+  // start: r = r0 = b_B - AB0 D0^-1 b_0, p = nu = t = y = 0
   double res0 = 0.0, rho = 0.0;
   {
     double s1[1] = {0.0};
@@ -303,13 +295,13 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
 #pragma unroll
       for (int q = 0; q < NR; ++q) {
         if (!ok[q]) continue;
-        A.q[0][r[q]] = make_float4(acc[q], 0.0f, 0.0f, 0.0f);
-        A.r0[r[q]] = acc[q];
-        A.y[r[q]] = 0.0f;
+        A.r[r[q]] = acc[q]; A.r0[r[q]] = acc[q];
+        A.p[r[q]] = 0.0f; A.nu[r[q]] = 0.0f; A.t[r[q]] = 0.0f; A.y[r[q]] = 0.0f;
         s1[0] += (double)acc[q] * (double)acc[q];
       }
     });
     put_partials_bs<1, BS>(A, s1, 0);
+    end_phase(A, ph);
     grid_barrier(A, ph);
     if (ph.ok) {
       get_totals_w0<1>(A, s1, 0);
@@ -317,43 +309,63 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
       rho = s1[0];
     }
   }
-  // alf, omg, bet of the previous iteration (0 before the first: p = r)
-  double alf = 0.0, omg = 0.0, bet = 0.0, rel = res0 > 0.0 ? 1.0 : 0.0;
-  int it = 0, converged = res0 > 0.0 ? 0 : 1, nonfinite = 0, buf = 1, cur = 0;
-  bool pending = false;  // y += alf p + omg s of the last iteration not yet applied
+  double alf = 1.0, omg = 1.0, bet = 0.0, rel = res0 > 0.0 ? 1.0 : 0.0;
+  int it = 0, converged = res0 > 0.0 ? 0 : 1, nonfinite = 0, buf = 1;
+  bool pending = false;  // an iteration's y/r update not yet applied
   while (ph.ok && !converged && it < A.maxit) {
     ++it;
-    const float4* qc = A.q[cur];
-    float4* qn = A.q[cur ^ 1];
-    // A: the previous update, p', nu' = Chat p', r0.nu'
+    // P0: the pending update, then p = r + bet (p - omg nu)
     {
       const float a = (float)alf, w = (float)omg, be = (float)bet;
-      double s1[1] = {0.0};
       for_tile_rows<NR>(s_lo, s_pre, 1, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR]) {
-        float4 v[NR];
-        float pn[NR], rn[NR], sv[NR], acc[NR], yv[NR], r0v[NR];
+        float rr[NR], pv[NR], nv[NR], tv[NR], yv[NR];
 #pragma unroll
         for (int q = 0; q < NR; ++q) {
-          v[q] = ldm(&qc[r[q]]);
-          yv[q] = ldm(&A.y[r[q]]);
-          r0v[q] = ldm(&A.r0[r[q]]);
-          pn[q] = next_p(v[q], a, w, be, rn[q], sv[q]);
-          acc[q] = pn[q];
+          rr[q] = ldm(&A.r[r[q]]);
+          pv[q] = ldm(&A.p[r[q]]);
+          nv[q] = ldm(&A.nu[r[q]]);
+          if (pending) {
+            tv[q] = ldm(&A.t[r[q]]);
+            yv[q] = ldm(&A.y[r[q]]);
+          }
         }
-        chat_sub(A, acc, r, [&](int k) {
-          float rk, sk;
-          return next_p(ldm(&qc[k]), a, w, be, rk, sk);
-        });
 #pragma unroll
         for (int q = 0; q < NR; ++q) {
           if (!ok[q]) continue;
-          if (pending) A.y[r[q]] = yv[q] + a * v[q].z + w * sv[q];
-          qn[r[q]] = make_float4(rn[q], acc[q], pn[q], 0.0f);
-          s1[0] += (double)r0v[q] * (double)acc[q];
+          float rn = rr[q];
+          if (pending) {
+            const float sv = rr[q] - a * nv[q];
+            A.y[r[q]] = yv[q] + a * pv[q] + w * sv;
+            rn = sv - w * tv[q];
+            A.r[r[q]] = rn;
+          }
+          A.p[r[q]] = rn + be * (pv[q] - w * nv[q]);
         }
       });
       pending = false;
+      end_phase(A, ph);
+    }
+    // A: nu = Chat p, r0.nu
+    {
+      double s1[1] = {0.0};
+      wait_neighbours(A, ph);
+      for_tile_rows<NR>(s_lo, s_pre, 1, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR]) {
+        float acc[NR], r0v[NR];
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+          acc[q] = ldm(&A.p[r[q]]);
+          r0v[q] = ldm(&A.r0[r[q]]);
+        }
+        chat_sub(A, acc, r, [&](int k) { return ldm(&A.p[k]); });
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+          if (!ok[q]) continue;
+          A.nu[r[q]] = acc[q];
+          s1[0] += (double)r0v[q] * (double)acc[q];
+        }
+      });
       put_partials_bs<1, BS>(A, s1, buf);
+      end_phase(A, ph);
       grid_barrier(A, ph);
       if (!ph.ok) break;
       get_totals_w0<1>(A, s1, buf);
@@ -364,7 +376,7 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
       if (s1[0] == 0.0) break;
       alf = rho / s1[0];
     }
-    // B: t = Chat s, s = r' - alf nu'; t.s, t.t, r0.t, s.s, r0.s
+    // B: t = Chat s, s = r - alf nu; t.s, t.t, r0.t, s.s, r0.s
     {
       double s5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
       const float a = (float)alf;
@@ -372,19 +384,15 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
         float acc[NR], sv[NR], r0v[NR];
 #pragma unroll
         for (int q = 0; q < NR; ++q) {
-          const float2 v = ldm(reinterpret_cast<const float2*>(&qn[r[q]]));
-          sv[q] = v.x - a * v.y;
+          sv[q] = ldm(&A.r[r[q]]) - a * ldm(&A.nu[r[q]]);
           r0v[q] = ldm(&A.r0[r[q]]);
           acc[q] = sv[q];
         }
-        chat_sub(A, acc, r, [&](int k) {
-          const float2 v = ldm(reinterpret_cast<const float2*>(&qn[k]));
-          return v.x - a * v.y;
-        });
+        chat_sub(A, acc, r, [&](int k) { return ldm(&A.r[k]) - a * ldm(&A.nu[k]); });
 #pragma unroll
         for (int q = 0; q < NR; ++q) {
           if (!ok[q]) continue;
-          reinterpret_cast<float*>(&qn[r[q]])[3] = acc[q];
+          A.t[r[q]] = acc[q];
           const double tq = acc[q], sq = sv[q], oq = r0v[q];
           s5[0] += tq * sq;
           s5[1] += tq * tq;
@@ -394,17 +402,17 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
         }
       });
       put_partials_bs<5, BS>(A, s5, buf);
+      end_phase(A, ph);
       grid_barrier(A, ph);
       if (!ph.ok) break;
       get_totals_w0<5>(A, s5, buf);
       buf ^= 1;
-      cur ^= 1;  // the buffer written this iteration holds (r', nu', p', t)
       omg = s5[0] / fmax(s5[1], SMALL);
       const double rr = fmax(s5[3] - 2.0 * omg * s5[0] + omg * omg * s5[1], 0.0);
       const double rho1 = s5[4] - omg * s5[2];
       rel = sqrt(rr) / res0;
       if (!isfinite(rel) || !isfinite(omg) || !isfinite(rho1)) { nonfinite = 1; break; }
-      pending = true;  // y += alf p' + omg s is valid even at a breakdown below
+      pending = true;  // y += alf p + omg s is valid even at a breakdown below
       if (rel < A.tol) { converged = 1; continue; }
       // breakdown of the next step (omg = 0 or r0.r = 0): stop with this iterate
       if (omg == 0.0 || rho1 == 0.0) break;
@@ -415,22 +423,19 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
   // the last update (y only), x_B = S^-1 y, then x_0 = D0^-1 (b_0 + sum aoff x_B)
   if (ph.ok && !nonfinite) {
     const float a = (float)alf, w = (float)omg;
-    const float4* qc = A.q[cur];
     for_tile_rows<NR>(s_lo, s_pre, 1, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR]) {
       float yv[NR], si[NR];
 #pragma unroll
       for (int q = 0; q < NR; ++q) {
         yv[q] = ldm(&A.y[r[q]]);
-        if (pending) {
-          const float4 v = ldm(&qc[r[q]]);
-          yv[q] = yv[q] + a * v.z + w * (v.x - a * v.y);
-        }
+        if (pending) yv[q] = yv[q] + a * ldm(&A.p[r[q]]) + w * (ldm(&A.r[r[q]]) - a * ldm(&A.nu[r[q]]));
         si[q] = __ldg(&A.sinv[r[q]]);
       }
 #pragma unroll
       for (int q = 0; q < NR; ++q)
         if (ok[q]) A.x[r[q]] = yv[q] * si[q];
     });
+    end_phase(A, ph);
     grid_barrier(A, ph);
     if (ph.ok) {
       for_tile_rows<NR>(s_lo, s_pre, 0, 0, [&](const int (&r)[NR], const bool (&ok)[NR]) {
@@ -470,7 +475,7 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
 
 // Block and row layouts of the reduced kernel: threads per block and rows per
 // thread per batch (cms_solver_opts.reduced_layout picks one; 0: the first).
-#define CMS_SCHUR_LAYOUTS(X) X(256, 2) X(512, 2) X(1024, 1) X(1024, 2)
+#define CMS_SCHUR_LAYOUTS(X) X(256, 2) X(512, 2) X(512, 4) X(1024, 2)
 constexpr int kSchurLayouts = 4;
 
 // Several independent systems (an ensemble) in one launch: bmap[b] = (member,

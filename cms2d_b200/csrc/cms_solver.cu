@@ -95,12 +95,12 @@ struct cms_solver {
   // reduced (Schur complement) inner solve of refinement (cms_schur.cuh):
   // Chat's pattern and values, 1/d and 1/s, neighbour tiles under Chat
   int sc_state = 0;  // 0 not built, 1 built, -1 not possible on this pattern
-  int sc_KC = 0;
+  int sc_KC = 0, sc_tiles = 0;
   long long sc_nnz = 0, sc_e0b = 0;  // stored entries of Chat; couplings between group 0 and B
-  int2* d_scel = nullptr;            // [KC][nB] (column, value bits)
-  float* d_ssinv = nullptr;
-  float4* d_sq = nullptr;            // [2][n] (r, nu, p, t) per device row, two buffers
+  int *d_sccol = nullptr, *d_sdep_ptr = nullptr, *d_sdep_idx = nullptr;
+  float *d_scoff = nullptr, *d_ssinv = nullptr;
   signed char* d_sccnt = nullptr;
+  size_t cap_sdep = 0;
   int cur_relax = 0;  // the FP32 factor in A32 is the two-phase one (k_ilu0_relax)
   int cur_fuse = 0;   // inner solves of refinement: update folded into the next iteration
   // MATRIX_SOLVER options 1, 2, 5-8: compass table (built on first use),
@@ -769,61 +769,107 @@ static int resid64(Solver* S, Mat<TA>& A, const double* b, const TX* x, double* 
 
 // Pattern of the reduced inner system (cms_schur.cuh): Chat's columns per B
 // row (direct couplings to B rows and the B neighbours of each group-0
-// neighbour, the row itself excluded), once per handle.  CMS_UNSUPPORTED when
-// the ordering has no independent first group or a reduced row has more than
-// KSC entries.
-static int schur_pattern(Solver* S) {
+// neighbour, the row itself excluded), once per handle; the neighbour-tile
+// lists under Chat for the persistent tiles, rebuilt when the tile count
+// changes.  CMS_UNSUPPORTED when the ordering has no independent first group
+// or a reduced row has more than KSC entries.
+static int schur_pattern(Solver* S, int tiles) {
   const HostPattern& P = S->hp;
   const int n = P.n;
-  if (S->sc_state != 0) return S->sc_state > 0 ? CMS_OK : CMS_UNSUPPORTED;
-  S->sc_state = -1;
-  if (P.G < 2 || P.G > GFLAT || P.gkl[0] != 0) return CMS_UNSUPPORTED;
-  const int g1 = P.gstart[1], nB = n - g1;
-  if (g1 <= 0 || nB <= 0) return CMS_UNSUPPORTED;
-  std::vector<int> tmp((size_t)nB * KSC);
-  std::vector<signed char> cnt(nB);
-  int KC = 0;
-  long long nnz = 0, e0b = 0;
-  for (int j = 0; j < g1; ++j) e0b += P.nup[j];
-  for (int i = 0; i < nB; ++i) {
-    const int r = g1 + i;
-    int loc[8 * KMAX];
-    int m = 0;
-    const int kl = P.nlo[r], ku = P.nup[r];
-    for (int s = 0; s < kl + ku; ++s) {
-      const int k = P.col[(size_t)(s < kl ? s : P.KL + (s - kl)) * n + r];
-      if (k >= g1) {
-        loc[m++] = k;
-        continue;
+  if (S->sc_state < 0) return CMS_UNSUPPORTED;
+  if (S->sc_state == 0) {
+    S->sc_state = -1;
+    if (P.G < 2 || P.G > GFLAT || P.gkl[0] != 0) return CMS_UNSUPPORTED;
+    const int g1 = P.gstart[1], nB = n - g1;
+    if (g1 <= 0 || nB <= 0) return CMS_UNSUPPORTED;
+    std::vector<int> tmp((size_t)nB * KSC);
+    std::vector<signed char> cnt(nB);
+    int KC = 0;
+    long long nnz = 0, e0b = 0;
+    for (int j = 0; j < g1; ++j) e0b += P.nup[j];
+    for (int i = 0; i < nB; ++i) {
+      const int r = g1 + i;
+      int loc[8 * KMAX];
+      int m = 0;
+      const int kl = P.nlo[r], ku = P.nup[r];
+      for (int s = 0; s < kl + ku; ++s) {
+        const int k = P.col[(size_t)(s < kl ? s : P.KL + (s - kl)) * n + r];
+        if (k >= g1) {
+          loc[m++] = k;
+          continue;
+        }
+        for (int t = 0; t < P.nup[k]; ++t) {
+          const int k2 = P.col[(size_t)(P.KL + t) * n + k];
+          if (k2 != r && m < 8 * KMAX) loc[m++] = k2;
+        }
       }
-      for (int t = 0; t < P.nup[k]; ++t) {
-        const int k2 = P.col[(size_t)(P.KL + t) * n + k];
-        if (k2 != r && m < 8 * KMAX) loc[m++] = k2;
-      }
+      std::sort(loc, loc + m);
+      const int mc = (int)(std::unique(loc, loc + m) - loc);
+      if (mc > KSC) return CMS_UNSUPPORTED;
+      std::copy(loc, loc + mc, tmp.begin() + (size_t)i * KSC);
+      cnt[i] = (signed char)mc;
+      KC = std::max(KC, mc);
+      nnz += mc;
     }
-    std::sort(loc, loc + m);
-    const int mc = (int)(std::unique(loc, loc + m) - loc);
-    if (mc > KSC) return CMS_UNSUPPORTED;
-    std::copy(loc, loc + mc, tmp.begin() + (size_t)i * KSC);
-    cnt[i] = (signed char)mc;
-    KC = std::max(KC, mc);
-    nnz += mc;
+    KC = std::max(KC, 1);
+    std::vector<int> ccol((size_t)KC * nB);
+    for (int i = 0; i < nB; ++i)
+      for (int q = 0; q < KC; ++q) ccol[(size_t)q * nB + i] = q < cnt[i] ? tmp[(size_t)i * KSC + q] : g1 + i;
+    CHK(S->alloc(&S->d_sccol, ccol.size()));
+    CHK(S->alloc(&S->d_scoff, ccol.size()));
+    CHK(S->alloc(&S->d_sccnt, (size_t)nB));
+    CHK(S->alloc(&S->d_ssinv, (size_t)n));
+    CHK(S->alloc(&S->d_sdep_ptr, (size_t)GRID_CAP + 1));
+    CMS_CUDA(cudaMemcpyAsync(S->d_sccol, ccol.data(), ccol.size() * sizeof(int), cudaMemcpyHostToDevice, S->stream));
+    CMS_CUDA(cudaMemcpyAsync(S->d_sccnt, cnt.data(), cnt.size(), cudaMemcpyHostToDevice, S->stream));
+    CMS_CUDA(cudaStreamSynchronize(S->stream));
+    S->sc_KC = KC;
+    S->sc_nnz = nnz;
+    S->sc_e0b = e0b;
+    S->sc_tiles = 0;
+    S->sc_state = 1;
   }
-  KC = std::max(KC, 1);
-  std::vector<int2> cel((size_t)KC * nB);
-  for (int i = 0; i < nB; ++i)
-    for (int q = 0; q < KC; ++q) cel[(size_t)q * nB + i] = make_int2(q < cnt[i] ? tmp[(size_t)i * KSC + q] : g1 + i, 0);
-  CHK(S->alloc(&S->d_scel, cel.size()));
-  CHK(S->alloc(&S->d_sccnt, (size_t)nB));
-  CHK(S->alloc(&S->d_ssinv, (size_t)n));
-  CHK(S->alloc(&S->d_sq, (size_t)2 * n));
-  CMS_CUDA(cudaMemcpyAsync(S->d_scel, cel.data(), cel.size() * sizeof(int2), cudaMemcpyHostToDevice, S->stream));
-  CMS_CUDA(cudaMemcpyAsync(S->d_sccnt, cnt.data(), cnt.size(), cudaMemcpyHostToDevice, S->stream));
+  if (S->sc_tiles == tiles) return CMS_OK;
+  // neighbour tiles under Chat (tile t = natural cells [t n / nt, (t+1) n / nt))
+  const int g1 = P.gstart[1], nB = n - g1;
+  std::vector<int> ccol((size_t)S->sc_KC * nB);
+  std::vector<signed char> cnt(nB);
+  CMS_CUDA(cudaMemcpyAsync(ccol.data(), S->d_sccol, ccol.size() * sizeof(int), cudaMemcpyDeviceToHost, S->stream));
+  CMS_CUDA(cudaMemcpyAsync(cnt.data(), S->d_sccnt, cnt.size(), cudaMemcpyDeviceToHost, S->stream));
   CMS_CUDA(cudaStreamSynchronize(S->stream));
-  S->sc_KC = KC;
-  S->sc_nnz = nnz;
-  S->sc_e0b = e0b;
-  S->sc_state = 1;
+  std::vector<int> tstart(tiles + 1);
+  for (int t = 0; t <= tiles; ++t) tstart[t] = (int)((long long)t * n / tiles);
+  std::vector<int> tile_nat(n);
+  for (int t = 0; t < tiles; ++t)
+    for (int c = tstart[t]; c < tstart[t + 1]; ++c) tile_nat[c] = t;
+  std::vector<std::vector<int>> dep(tiles);
+  auto add = [&](int a, int b) {
+    for (int q : dep[a]) if (q == b) return;
+    dep[a].push_back(b);
+  };
+  for (int i = 0; i < nB; ++i) {
+    const int ti = tile_nat[P.perm[g1 + i]];
+    for (int q = 0; q < cnt[i]; ++q) {
+      const int tj = tile_nat[P.perm[ccol[(size_t)q * nB + i]]];
+      if (tj != ti) { add(ti, tj); add(tj, ti); }
+    }
+  }
+  std::vector<int> dptr(tiles + 1, 0), didx;
+  for (int t = 0; t < tiles; ++t) {
+    std::sort(dep[t].begin(), dep[t].end());
+    didx.insert(didx.end(), dep[t].begin(), dep[t].end());
+    dptr[t + 1] = (int)didx.size();
+  }
+  if (didx.size() + 1 > S->cap_sdep) {
+    CHK(S->alloc(&S->d_sdep_idx, didx.size() + 1));
+    S->cap_sdep = didx.size() + 1;
+  }
+  CMS_CUDA(cudaMemcpyAsync(S->d_sdep_ptr, dptr.data(), dptr.size() * sizeof(int), cudaMemcpyHostToDevice, S->stream));
+  if (!didx.empty())
+    CMS_CUDA(cudaMemcpyAsync(S->d_sdep_idx, didx.data(), didx.size() * sizeof(int), cudaMemcpyHostToDevice,
+                             S->stream));
+  CMS_CUDA(cudaStreamSynchronize(S->stream));
+  S->sc_tiles = tiles;
   return CMS_OK;
 }
 
@@ -837,21 +883,20 @@ static int schur_numeric(Solver* S) {
                                                          S->A32.diag, S->d_ssinv)));
   KLAUNCH(S, P_SCHUR_BUILD, 8.0 * nnz + 10.0 * n + 4.0 * n + 8.0 * (double)S->sc_nnz + nB,
           (k_schur_off<<<gsz(nB), TPB, 0, S->stream>>>(n, g1, nB, P.KL, S->sc_KC, S->d_col, S->d_nlo, S->d_nup,
-                                                        S->A32.aoff, S->A32.diag, S->d_ssinv, S->d_sccnt,
-                                                        S->d_scel)));
+                                                        S->A32.aoff, S->A32.diag, S->d_ssinv, S->d_sccol,
+                                                        S->d_sccnt, S->d_scoff)));
   return CMS_OK;
 }
 
 // Algorithmic bytes of one reduced-system launch: the start (reduced
-// right-hand side), per iteration A (the row's (r, nu, p, t) read and
-// written, y read and written, r0, count, Chat) and B ((r, nu), r0, count,
-// Chat, t), and the end (y update, x_B, then x_0 from b, 1/d and the group-0
-// rows' couplings).
+// right-hand side), per iteration P0 (8 vector accesses per row), A (p, r0,
+// count, Chat, nu) and B (r, nu, r0, count, Chat, t), and the end (y update,
+// x_B, then x_0 from b, 1/d and the group-0 rows' couplings).
 static double schur_bytes(const Solver* S, int iters) {
   const HostPattern& P = S->hp;
   const double n = P.n, g1 = P.gstart[1], nB = n - g1, C = 8.0 * (double)S->sc_nnz, E = 8.0 * (double)S->sc_e0b;
   const double start = 4.0 * n + 4.0 * g1 + E + nB + 24.0 * nB;
-  const double it = (16.0 + 16.0 + 8.0 + 4.0 + 1.0) * nB + C + (8.0 + 4.0 + 1.0 + 4.0) * nB + C;
+  const double it = 32.0 * nB + (13.0 * nB + C) + (17.0 * nB + C);
   const double end = 24.0 * nB + 9.0 * g1 + E + 4.0 * nB + 4.0 * g1;
   return start + iters * it + end;
 }
@@ -863,11 +908,11 @@ static SchurArgs make_schur_args(Solver* S, int tiles, int maxit, double tol) {
   std::memset(&a, 0, sizeof(a));
   a.n = P.n; a.g1 = P.gstart[1]; a.nB = P.n - a.g1; a.KL = P.KL; a.G = P.G; a.KC = S->sc_KC;
   a.ntiles = tiles;
-  a.toff = S->d_toff;
-  a.cel = S->d_scel; a.ccnt = S->d_sccnt;
+  a.toff = S->d_toff; a.dep_ptr = S->d_sdep_ptr; a.dep_idx = S->d_sdep_idx; a.progress = S->d_progress;
+  a.ccol = S->d_sccol; a.coff = S->d_scoff; a.ccnt = S->d_sccnt;
   a.col = S->d_col; a.nlo = S->d_nlo; a.nup = S->d_nup; a.aoff = S->A32.aoff; a.sinv = S->d_ssinv;
   a.b = S->W32.b; a.x = S->W32.x;
-  a.q[0] = S->d_sq; a.q[1] = S->d_sq + P.n; a.r0 = S->W32.r0; a.y = S->W32.z;
+  a.r = S->W32.r; a.r0 = S->W32.r0; a.p = S->W32.p; a.nu = S->W32.u; a.t = S->W32.v; a.y = S->W32.z;
   a.part = S->d_ppart; a.bar = &S->d_st->bar; a.st = S->d_st;
   a.maxit = maxit; a.tol = tol; a.spin_limit = kSpinLimit;
   return a;
@@ -898,6 +943,7 @@ static int run_schur_bicgstab(Solver* S, int tiles, int maxit, double tol) {
   SchurArgs a = make_schur_args(S, tiles, maxit, tol);
   const SchurLayout L = schur_layout(schur_layout_index(S));
   CMS_CUDA(cudaMemsetAsync(&S->d_st->bar, 0, sizeof(GridBar), S->stream));
+  CMS_CUDA(cudaMemsetAsync(S->d_progress, 0, sizeof(unsigned int) * tiles * kProgressStride, S->stream));
   void* args[] = {&a};
   prof_begin(S);
   const cudaError_t e = cudaLaunchCooperativeKernel(L.single, dim3(tiles), dim3(L.bs), args, 0, S->stream);
@@ -934,7 +980,7 @@ static int run_refine(Solver* S, int nsolv, int maxit, double tol, cms_solve_inf
   bool schur = mc_persist && S->opts.inner_relax == 2;
   if (schur) {  // the tiles of the reduced kernel's layout
     const int nt = schur_tiles(S, schur_layout_index(S));
-    schur = nt > 0 && build_tiles(S, nt) == nt && schur_pattern(S) == CMS_OK;
+    schur = nt > 0 && build_tiles(S, nt) == nt && schur_pattern(S, S->ptiles) == CMS_OK;
   }
   const bool relax = !schur && mc_persist && S->opts.inner_relax && P.G > 2;
   struct RelaxScope {  // the flags describe A32's factor and its solves only while this solve runs
