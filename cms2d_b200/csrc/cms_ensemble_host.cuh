@@ -204,6 +204,10 @@ static int refine_batched(Ens* E, const std::vector<int>& act, const std::vector
         return CMS_DEVICE_ERROR;
       }
       R[j].inner_total += S->h_st->iter;
+      if (S->h_st->nonfinite) {  // no correction from an overflowed inner solve (as run_refine)
+        R[j].live = false;
+        continue;
+      }
       const int n = S->hp.n;
       KLAUNCH(S, P_VEC, (double)n * 20,
               (k_ir_correct<<<gsz(n), TPB, 0, S->stream>>>(n, S->W32.x, S->W64.x, S->d_st)));

@@ -1029,6 +1029,10 @@ static int run_refine(Solver* S, int nsolv, int maxit, double tol, cms_solve_inf
     CMS_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, S->stream));
     CMS_CUDA(cudaStreamSynchronize(S->stream));
     inner_total += (nsolv == 3) ? S->h_st->iter : S->h_st->inner;
+    // an FP32 inner solve that overflowed (a near-breakdown of its recurrence)
+    // gives no correction: keep the FP64 iterate and end the refinement (the
+    // FP64 residual above reports a non-finite system itself)
+    if (S->h_st->nonfinite) break;
     KLAUNCH(S, P_VEC, (double)n * 20,
             (k_ir_correct<<<gsz(n), TPB, 0, S->stream>>>(n, S->W32.x, S->W64.x, S->d_st)));
     ++steps;
