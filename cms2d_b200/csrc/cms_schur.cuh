@@ -76,8 +76,6 @@ struct SchurArgs {
   int maxit;
   double tol;
   unsigned int spin_limit;
-  int smem_rows;           // > 0: the tile's ccol and ccnt are cached in dynamic shared
-                           // memory for the launch (room for this many reduced rows)
 };
 
 // sinv: 1/d_r for group-0 rows, 1/s_r for B rows with
@@ -211,13 +209,12 @@ __device__ __forceinline__ void get_totals_w0(const SchurArgs& A, double (&tot)[
 }
 
 // Rows of this tile in groups ga..gb as one index space (ranges in shared
-// memory: s_lo first row of each group's range, s_pre prefix counts); f gets
-// the rows, their validity and their index in that space.
+// memory: s_lo first row of each group's range, s_pre prefix counts).
 template <int NR, typename F>
 __device__ __forceinline__ void for_tile_rows(const int* s_lo, const int* s_pre, int ga, int gb, F&& f) {
   const int k0 = s_pre[ga], k1 = s_pre[gb + 1];
   for (int base = k0 + (int)threadIdx.x; base < k1; base += NR * (int)blockDim.x) {
-    int r[NR], kk[NR];
+    int r[NR];
     bool ok[NR];
 #pragma unroll
     for (int q = 0; q < NR; ++q) {
@@ -227,23 +224,18 @@ __device__ __forceinline__ void for_tile_rows(const int* s_lo, const int* s_pre,
       int g = ga;
       while (g < gb && k >= s_pre[g + 1]) ++g;
       r[q] = s_lo[g] + (k - s_pre[g]);
-      kk[q] = k;
     }
-    f(r, ok, kk);
+    f(r, ok);
   }
 }
 
 // acc[q] - sum_s coff[s] * w(col) over the reduced row's slots, w(k) given
-// by a functor of the gathered column.  With the shared-memory cache the
-// columns and counts come from there (sc: [KC][smem_rows] columns, then the
-// counts), indexed by the row's place lk among the tile's reduced rows.
+// by a functor of the gathered column.
 template <int NR, typename W>
-__device__ __forceinline__ void chat_sub(const SchurArgs& A, float (&acc)[NR], const int (&r)[NR],
-                                         const int (&lk)[NR], const int* sc, W&& w) {
-  const signed char* scnt = reinterpret_cast<const signed char*>(sc + (size_t)A.KC * A.smem_rows);
+__device__ __forceinline__ void chat_sub(const SchurArgs& A, float (&acc)[NR], const int (&r)[NR], W&& w) {
   int kc[NR];
 #pragma unroll
-  for (int q = 0; q < NR; ++q) kc[q] = A.smem_rows ? scnt[lk[q]] : __ldg(&A.ccnt[r[q] - A.g1]);
+  for (int q = 0; q < NR; ++q) kc[q] = __ldg(&A.ccnt[r[q] - A.g1]);
 #pragma unroll
   for (int s = 0; s < KSC; ++s) {
     if (s < A.KC) {
@@ -251,8 +243,7 @@ __device__ __forceinline__ void chat_sub(const SchurArgs& A, float (&acc)[NR], c
       for (int q = 0; q < NR; ++q) {
         if (s < kc[q]) {
           const size_t e = (size_t)s * A.nB + (r[q] - A.g1);
-          const int c = A.smem_rows ? sc[s * A.smem_rows + lk[q]] : __ldg(&A.ccol[e]);
-          acc[q] = acc[q] - __ldg(&A.coff[e]) * w(c);
+          acc[q] = acc[q] - __ldg(&A.coff[e]) * w(__ldg(&A.ccol[e]));
         }
       }
     }
@@ -276,24 +267,11 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
   }
   __syncthreads();
   const int n = A.n, g1 = A.g1;
-  // the tile's reduced-row columns and counts into shared memory (constant
-  // for the launch; the host sized smem_rows for the largest tile)
-  extern __shared__ int sc[];
-  if (A.smem_rows) {
-    signed char* scnt = reinterpret_cast<signed char*>(sc + (size_t)A.KC * A.smem_rows);
-    for_tile_rows<1>(s_lo, s_pre, 1, G - 1, [&](const int (&r)[1], const bool (&ok)[1], const int (&kk)[1]) {
-      if (!ok[0]) return;
-      const int i = r[0] - g1, lk = kk[0] - s_pre[1];
-      scnt[lk] = __ldg(&A.ccnt[i]);
-      for (int s = 0; s < A.KC; ++s) sc[s * A.smem_rows + lk] = __ldg(&A.ccol[(size_t)s * A.nB + i]);
-    });
-    __syncthreads();
-  }
   // start: r = r0 = b_B - AB0 D0^-1 b_0, p = nu = t = y = 0
   double res0 = 0.0, rho = 0.0;
   {
     double s1[1] = {0.0};
-    for_tile_rows<NR>(s_lo, s_pre, 1, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR], const int (&kk)[NR]) {
+    for_tile_rows<NR>(s_lo, s_pre, 1, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR]) {
       float acc[NR];
       int kl[NR];
 #pragma unroll
@@ -339,7 +317,7 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
     // P0: the pending update, then p = r + bet (p - omg nu)
     {
       const float a = (float)alf, w = (float)omg, be = (float)bet;
-      for_tile_rows<NR>(s_lo, s_pre, 1, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR], const int (&kk)[NR]) {
+      for_tile_rows<NR>(s_lo, s_pre, 1, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR]) {
         float rr[NR], pv[NR], nv[NR], tv[NR], yv[NR];
 #pragma unroll
         for (int q = 0; q < NR; ++q) {
@@ -371,17 +349,14 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
     {
       double s1[1] = {0.0};
       wait_neighbours(A, ph);
-      for_tile_rows<NR>(s_lo, s_pre, 1, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR], const int (&kk)[NR]) {
+      for_tile_rows<NR>(s_lo, s_pre, 1, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR]) {
         float acc[NR], r0v[NR];
 #pragma unroll
         for (int q = 0; q < NR; ++q) {
           acc[q] = ldm(&A.p[r[q]]);
           r0v[q] = ldm(&A.r0[r[q]]);
         }
-        int lk[NR];
-#pragma unroll
-        for (int q = 0; q < NR; ++q) lk[q] = kk[q] - s_pre[1];
-        chat_sub(A, acc, r, lk, sc, [&](int k) { return ldm(&A.p[k]); });
+        chat_sub(A, acc, r, [&](int k) { return ldm(&A.p[k]); });
 #pragma unroll
         for (int q = 0; q < NR; ++q) {
           if (!ok[q]) continue;
@@ -405,7 +380,7 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
     {
       double s5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
       const float a = (float)alf;
-      for_tile_rows<NR>(s_lo, s_pre, 1, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR], const int (&kk)[NR]) {
+      for_tile_rows<NR>(s_lo, s_pre, 1, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR]) {
         float acc[NR], sv[NR], r0v[NR];
 #pragma unroll
         for (int q = 0; q < NR; ++q) {
@@ -413,10 +388,7 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
           r0v[q] = ldm(&A.r0[r[q]]);
           acc[q] = sv[q];
         }
-        int lk[NR];
-#pragma unroll
-        for (int q = 0; q < NR; ++q) lk[q] = kk[q] - s_pre[1];
-        chat_sub(A, acc, r, lk, sc, [&](int k) { return ldm(&A.r[k]) - a * ldm(&A.nu[k]); });
+        chat_sub(A, acc, r, [&](int k) { return ldm(&A.r[k]) - a * ldm(&A.nu[k]); });
 #pragma unroll
         for (int q = 0; q < NR; ++q) {
           if (!ok[q]) continue;
@@ -451,7 +423,7 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
   // the last update (y only), x_B = S^-1 y, then x_0 = D0^-1 (b_0 + sum aoff x_B)
   if (ph.ok && !nonfinite) {
     const float a = (float)alf, w = (float)omg;
-    for_tile_rows<NR>(s_lo, s_pre, 1, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR], const int (&kk)[NR]) {
+    for_tile_rows<NR>(s_lo, s_pre, 1, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR]) {
       float yv[NR], si[NR];
 #pragma unroll
       for (int q = 0; q < NR; ++q) {
@@ -466,7 +438,7 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
     end_phase(A, ph);
     grid_barrier(A, ph);
     if (ph.ok) {
-      for_tile_rows<NR>(s_lo, s_pre, 0, 0, [&](const int (&r)[NR], const bool (&ok)[NR], const int (&kk)[NR]) {
+      for_tile_rows<NR>(s_lo, s_pre, 0, 0, [&](const int (&r)[NR], const bool (&ok)[NR]) {
         float acc[NR], si[NR];
         int ku[NR];
 #pragma unroll

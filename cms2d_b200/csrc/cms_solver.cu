@@ -91,9 +91,6 @@ struct cms_solver {
   unsigned int* d_progress = nullptr;
   double* d_ppart = nullptr;
   int ptiles = 0;  // tiles (= blocks) of the persistent kernel; 0 not built, -1 not launchable
-  int tile_maxB = 0;  // most rows of groups >= 1 in one tile (the reduced kernel's shared-memory cache)
-  size_t sc_smem = 0;  // dynamic shared memory of the reduced kernel for sc_smem_tiles tiles (0: none)
-  int sc_smem_tiles = -1;
   size_t cap_toff = 0, cap_dep = 0;  // capacities of d_toff / d_dep_idx
   // reduced (Schur complement) inner solve of refinement (cms_schur.cuh):
   // Chat's pattern and values, 1/d and 1/s, neighbour tiles under Chat
@@ -480,12 +477,6 @@ static int build_tiles(Solver* S, int nt) {
       toff[(size_t)g * (nt + 1) + t] = r;
     }
   }
-  int maxB = 0;
-  for (int t = 0; t < nt; ++t) {
-    int rows = 0;
-    for (int g = 1; g < P.G; ++g) rows += toff[(size_t)g * (nt + 1) + t + 1] - toff[(size_t)g * (nt + 1) + t];
-    maxB = std::max(maxB, rows);
-  }
   // neighbour tiles (symmetric): tiles holding a row coupled to one of ours
   std::vector<std::vector<int>> dep(nt);
   auto add = [&](int a, int b) {
@@ -525,7 +516,6 @@ static int build_tiles(Solver* S, int nt) {
       cudaStreamSynchronize(s))
     return 0;
   S->ptiles = nt;
-  S->tile_maxB = maxB;
   return nt;
 }
 
@@ -948,37 +938,15 @@ static int schur_tiles(Solver* S, int layout) {
   return std::min(std::min(per * nsm, GRID_CAP), nblk(S->hp.n));
 }
 
-// Dynamic shared memory of the reduced kernel's column cache on `tiles` tiles:
-// room for the largest tile's reduced rows when it fits (200 KB) and every
-// block stays resident; 0 (global loads) otherwise.
-constexpr size_t kSchurSmemMax = 200 * 1024;
-static size_t schur_smem(Solver* S, const SchurLayout& L, int tiles) {
-  if (S->sc_smem_tiles == tiles) return S->sc_smem;
-  S->sc_smem_tiles = tiles;
-  S->sc_smem = 0;
-  const size_t need = ((size_t)S->tile_maxB * (S->sc_KC * 4 + 1) + 15) & ~(size_t)15;
-  int nsm = 0, per = 0;
-  if (S->tile_maxB > 0 && need <= kSchurSmemMax &&
-      cudaFuncSetAttribute(L.single, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need) == cudaSuccess &&
-      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, S->dev) == cudaSuccess &&
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, L.single, L.bs, need) == cudaSuccess &&
-      per * nsm >= tiles)
-    S->sc_smem = need;
-  cudaGetLastError();
-  return S->sc_smem;
-}
-
 // The reduced FP32 inner solve (W32.b -> W32.x) as one cooperative launch.
 static int run_schur_bicgstab(Solver* S, int tiles, int maxit, double tol) {
   SchurArgs a = make_schur_args(S, tiles, maxit, tol);
   const SchurLayout L = schur_layout(schur_layout_index(S));
-  const size_t smem = schur_smem(S, L, tiles);
-  a.smem_rows = smem ? S->tile_maxB : 0;
   CMS_CUDA(cudaMemsetAsync(&S->d_st->bar, 0, sizeof(GridBar), S->stream));
   CMS_CUDA(cudaMemsetAsync(S->d_progress, 0, sizeof(unsigned int) * tiles * kProgressStride, S->stream));
   void* args[] = {&a};
   prof_begin(S);
-  const cudaError_t e = cudaLaunchCooperativeKernel(L.single, dim3(tiles), dim3(L.bs), args, smem, S->stream);
+  const cudaError_t e = cudaLaunchCooperativeKernel(L.single, dim3(tiles), dim3(L.bs), args, 0, S->stream);
   if (e != cudaSuccess) {
     std::snprintf(g_last_error, sizeof(g_last_error), "cooperative launch (reduced BiCGStab): %s",
                   cudaGetErrorString(e));
