@@ -593,6 +593,79 @@ def flow_parity(case, seed, settings, precs):
     return out
 
 
+def other_configs(args, dev, flush):
+    """Short measurements of configs 1 and 3 in the default run: the 200 x 100
+    Cartesian tidal basin (dt = 600 s) stepped by the GPU in both precisions
+    and by the oracle (whole steps, one thread and all cores), and the
+    solver-sweep systems at 0.25M and 1M unknowns solved to 1e-6 in both
+    precisions (device-resident inputs, L2 flushed before each solve)."""
+    import torch
+    from cms2d_b200 import cases
+    from cms2d_b200 import solver as S
+    from cms2d_b200.flow import FlowModel
+    from oracle import oracle as O
+    out = {}
+    basin = cases.tidal_basin(200, 100, 20.0, seed=11)
+    c1 = {"workload": f"config 1: Cartesian tidal basin {basin.grid.ncells} cells (20 m), dt=600 s, "
+                      f"ILU0-BiCGStab solves to 1e-6 (L2)"}
+    for prec in ("fp32_refine", "fp64"):
+        m = FlowModel(basin, precision=prec, **dict(FLOW_SOLVER, nswp_pp=args.nswp, nswp_uv=args.nswp))
+        m.init()
+        for _ in range(3):
+            m.step()
+        st = torch.cuda.ExternalStream(_lib_stream(m), device=dev)
+        ms, nstep = 0.0, 12
+        for _ in range(nstep):
+            flush.fill_(1.0)
+            torch.cuda.synchronize(dev)
+            e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(st); m.step(); e1.record(st); e1.synchronize()
+            ms += e0.elapsed_time(e1)
+        c1[prec] = {"timesteps_per_s": round(nstep / (ms / 1e3), 3), "steps": nstep}
+        m.close()
+    if not args.no_cpu_baseline:
+        for th in (1, os.cpu_count()):
+            O.set_threads(th)
+            f = O.FlowOracle(basin)
+            f.set_solver(nsolv=3, precond=O.PC_ILU0, tol=1e-6, nswp_pp=args.nswp, nswp_uv=args.nswp, norm=2)
+            f.init()
+            f.step()
+            t0 = time.perf_counter()
+            for _ in range(3):
+                f.step()
+            c1[f"cpu_{th}_threads"] = {"timesteps_per_s": round(3 / (time.perf_counter() - t0), 3), "steps": 3,
+                                        "kind": "port (oracle)"}
+    out["config1"] = c1
+    c3 = {"workload": "config 3: solver-sweep pressure-correction systems, ILU0-BiCGStab to ||r||2/||r0||2 <= 1e-6"}
+    for cells in (250_000, 1_000_000):
+        g, acoef, ss, sp, phi = build_solve_case(cells, seed=17)
+        ta, tsp, tss0, tph0 = (torch.from_numpy(x).to(dev) for x in (acoef, sp, ss, phi))
+        row = {"unknowns": g.ncells}
+        for prec in ("fp32_refine", "fp64"):
+            s = S.Solver(g, precision=prec, tol=1e-6, norm=2, verify=False, nsolv=3)
+            st = torch.cuda.ExternalStream(s.stream_handle, device=dev)
+            res = torch.zeros_like(tss0)
+            ms, info = 0.0, None
+            for q in range(5):
+                tss = tss0.clone(); tph = tph0.clone(); flush.fill_(1.0); torch.cuda.synchronize(dev)
+                e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                info = s.solve(ta, tss, tsp, res, tph, relax=1.0, nswp=5000, nsolv=3)
+                e1.record(st); e1.synchronize()
+                if q >= 2:
+                    ms += e0.elapsed_time(e1)
+            row[prec] = {"ms_per_solve": round(ms / 3, 3), "iters": info["iters"], "status": info["status"]}
+            s.close()
+        c3[str(g.ncells)] = row
+    out["config3"] = c3
+    return out
+
+
+def _lib_stream(m):
+    from cms2d_b200 import _lib
+    return _lib.lib().cms_solver_stream(m.solver_handle)
+
+
 def _profile_read(L, h):
     import ctypes as C
     from cms2d_b200.solver import Solver
@@ -756,6 +829,8 @@ def run_flow_ours(args):
                             "speedup_of_headline": round(head["value"] / c["value"], 4)}
     if rank == 0 and not args.no_parity:
         out["parity"] = flow_parity(case, 11 + rank, settings, precs)
+    if rank == 0 and world == 1 and not args.no_other_configs and args.case == "inlet":
+        out["other_configs"] = other_configs(args, dev, flush)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = flow_cpu_sample(case, head["outer_iters"], args.cpu_outer)
     if world > 1:
@@ -1025,6 +1100,8 @@ def main():
     ap.add_argument("--inner-max", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-parity", action="store_true", help="flow: skip the error check against the oracle fixture")
+    ap.add_argument("--no-other-configs", action="store_true",
+                    help="flow: skip the short config 1 and config 3 measurements")
     ap.add_argument("--iter-part", default="all", choices=["all", "gpu", "cpu"],
                     help="iterations workload: the GPU columns, the oracle columns, or both")
     ap.add_argument("--ref-budget", type=float, default=400.0,

@@ -43,7 +43,9 @@
 // value) element and (r, nu) interleaved for one 8-byte gather, 5.24-5.33;
 // P0 and its neighbour wait dropped by forming each gathered neighbour's new
 // direction from a 16-byte (r, nu, p, t) gather in alternating buffers,
-// 4.72.  Separate 4-byte streams keep more loads in flight per thread.
+// 4.72; the tile's columns and counts cached in shared memory for the
+// launch, 5.10 (the fill costs every launch and the velocity solves' launches
+// are short).  Separate 4-byte streams keep more loads in flight per thread.
 #pragma once
 #include "cms_persist.cuh"
 
