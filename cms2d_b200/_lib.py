@@ -82,6 +82,8 @@ def lib():
     L.cms_solver_launches.restype = C.c_longlong
     L.cms_solver_profile.argtypes = [vp, i]
     L.cms_solver_wait_selftest.argtypes = [vp, C.c_uint]
+    L.cms_solver_refine_fallbacks.argtypes = [vp]
+    L.cms_solver_refine_fallbacks.restype = C.c_longlong
     L.cms_solver_persist_wait_selftest.argtypes = [vp, C.c_uint, C.c_int]
     L.cms_solver_profile_read.argtypes = [vp, i, vp, vp, vp]
     L.cms_solver_set_tiles.argtypes = [vp, i]

@@ -72,21 +72,16 @@ static int ensemble_layout(Ens* E, int total) {
   return CMS_OK;
 }
 
-// Per-member refinement state (run_refine's locals).
-struct RefineMember {
-  int steps = 0, inner_total = 0, maxit = 0, imax = 0, rmax = 0;
-  double nrm0 = -1.0, rel = 1.0, tol = 0.0, itol = 0.0;
-  bool live = true;
-  cms_solve_info* info = nullptr;
-};
-
 // run_refine for several members at once: FP64 residuals per member, then
 // one batched launch for the FP32 inner BiCGStab solves of every member
-// that continues.  act: member indices; nswp: iteration caps.
+// that continues.  act: member indices; nswp: iteration caps.  A member whose
+// last inner correction made its FP64 residual larger (or overflowed) has it
+// undone and finishes on its own with the exact factor (refine_exact).
 static int refine_batched(Ens* E, const std::vector<int>& act, const std::vector<int>& nswp,
                           std::vector<cms_solve_info*>& infos) {
   const int A_ = (int)act.size();
-  std::vector<RefineMember> R(A_);
+  std::vector<RefineState> R(A_);
+  std::vector<char> live(A_, 1);
   struct Reset {  // cur_relax describes A32's factor only during this solve
     Ens* e;
     const std::vector<int>& a;
@@ -105,11 +100,12 @@ static int refine_batched(Ens* E, const std::vector<int>& act, const std::vector
     schur = S->opts.inner_relax == 2 && S->opts.ordering == CMS_ORDER_MULTICOLOR &&
             schur_pattern(S, E->tiles[act[j]]) == CMS_OK;
   }
+  bool relax_any = false;
   for (int j = 0; j < A_; ++j) {
     Solver* S = E->m[act[j]]->S;
     const HostPattern& P = S->hp;
     const int n = P.n;
-    RefineMember& rm = R[j];
+    RefineState& rm = R[j];
     rm.info = infos[j];
     rm.maxit = S->opts.max_iters > 0 ? S->opts.max_iters : nswp[j];
     rm.tol = S->opts.tol > 0 ? S->opts.tol : 1e-3;
@@ -126,31 +122,24 @@ static int refine_batched(Ens* E, const std::vector<int>& act, const std::vector
                                                                    S->d_nup, S->A32.aoff, S->A32.diag, S->A32.luoff,
                                                                    S->A32.invd)));
       S->cur_relax = 1;
+      relax_any = true;
     } else {
       CHK(factor<float>(S, S->A32));
     }
   }
+  const bool inexact = schur || relax_any;
   for (;;) {
-    for (int j = 0; j < A_; ++j) {
-      if (!R[j].live) continue;
-      Solver* S = E->m[act[j]]->S;
-      CHK(resid64<double, double>(S, S->A64, S->W64.b, S->W64.x, S->W64.r, nullptr, S_NRM2));
-      CMS_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, S->stream));
-    }
     std::vector<int> cont;
     for (int j = 0; j < A_; ++j) {
-      if (!R[j].live) continue;
+      if (!live[j]) continue;
       Solver* S = E->m[act[j]]->S;
-      RefineMember& rm = R[j];
-      CMS_CUDA(cudaStreamSynchronize(S->stream));
-      const double nrm = std::sqrt(S->h_st->s[S_NRM2]);
-      if (rm.nrm0 < 0) rm.nrm0 = nrm;
-      rm.rel = rm.nrm0 > 0 ? nrm / rm.nrm0 : 0.0;
-      if (!std::isfinite(rm.rel)) {
-        rm.info->status = CMS_NONFINITE;
-        rm.live = false;
-      } else if (rm.rel <= rm.tol || rm.steps >= rm.rmax || rm.inner_total >= rm.maxit) {
-        rm.live = false;
+      bool go = true, worse = false;
+      CHK(refine_check(S, R[j], go, worse));
+      if (worse) {
+        if (go && inexact) CHK(refine_exact(S, 3, R[j]));
+        live[j] = 0;
+      } else if (!go) {
+        live[j] = 0;
       } else {
         cont.push_back(j);
       }
@@ -205,30 +194,22 @@ static int refine_batched(Ens* E, const std::vector<int>& act, const std::vector
       }
       R[j].inner_total += S->h_st->iter;
       if (S->h_st->nonfinite) {  // no correction from an overflowed inner solve (as run_refine)
-        R[j].live = false;
+        if (inexact) CHK(refine_exact(S, 3, R[j]));
+        live[j] = 0;
         continue;
       }
-      const int n = S->hp.n;
-      KLAUNCH(S, P_VEC, (double)n * 20,
-              (k_ir_correct<<<gsz(n), TPB, 0, S->stream>>>(n, S->W32.x, S->W64.x, S->d_st)));
-      ++R[j].steps;
+      CHK(refine_correct(S, R[j]));
     }
   }
   for (int j = 0; j < A_; ++j) {
-    RefineMember& rm = R[j];
     Solver* S = E->m[act[j]]->S;
     CMS_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, S->stream));
   }
   for (int j = 0; j < A_; ++j) {
-    RefineMember& rm = R[j];
     Solver* S = E->m[act[j]]->S;
     CMS_CUDA(cudaStreamSynchronize(S->stream));
-    rm.info->iters = rm.inner_total;
-    rm.info->inner = rm.inner_total;
-    rm.info->refine_steps = rm.steps;
-    rm.info->relres = rm.rel;
-    rm.info->rmom = S->h_st->s[S_RMOM];
-    if (rm.info->status == CMS_OK && rm.rel > rm.tol) rm.info->status = CMS_NOT_CONVERGED;
+    refine_finish(R[j]);
+    R[j].info->rmom = S->h_st->s[S_RMOM];
   }
   return CMS_OK;
 }

@@ -526,6 +526,13 @@ __global__ void __launch_bounds__(TPB) k_ir_correct(int n, const float* __restri
   for (int i = blockIdx.x * TPB + threadIdx.x; i < n; i += gridDim.x * TPB) x[i] += scale * (double)d[i];
 }
 
+// Undoes the last correction (the same scale, opposite sign).
+__global__ void __launch_bounds__(TPB) k_ir_undo(int n, const float* __restrict__ d, double* __restrict__ x,
+                                                 const DevState* st) {
+  const double scale = st->s[S_IRSCALE];
+  for (int i = blockIdx.x * TPB + threadIdx.x; i < n; i += gridDim.x * TPB) x[i] -= scale * (double)d[i];
+}
+
 // r32 = r64 / ||r64||_2 (the FP32 correction solve sees a unit-norm right-hand side)
 __global__ void __launch_bounds__(TPB) k_ir_scale(int n, const double* __restrict__ r, float* __restrict__ r32,
                                                   DevState* st) {

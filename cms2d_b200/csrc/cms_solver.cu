@@ -101,6 +101,7 @@ struct cms_solver {
   float *d_scoff = nullptr, *d_ssinv = nullptr;
   signed char* d_sccnt = nullptr;
   size_t cap_sdep = 0;
+  long long reduced_fallbacks = 0;  // refinements finished on the exact factor after a bad inner correction
   int cur_relax = 0;  // the FP32 factor in A32 is the two-phase one (k_ilu0_relax)
   int cur_fuse = 0;   // inner solves of refinement: update folded into the next iteration
   // MATRIX_SOLVER options 1, 2, 5-8: compass table (built on first use),
@@ -966,6 +967,92 @@ static int run_schur_bicgstab(Solver* S, int tiles, int maxit, double tol) {
   return CMS_OK;
 }
 
+// State of one system's refinement (run_refine's loop, shared with the
+// ensembles' batched refinement).
+struct RefineState {
+  int steps = 0, inner_total = 0, maxit = 0, imax = 0, rmax = 0;
+  double nrm0 = -1.0, prev = -1.0, rel = 1.0, tol = 0.0, itol = 0.0;
+  cms_solve_info* info = nullptr;
+};
+
+// The FP64 residual of x64; go = false when the refinement ends (converged,
+// capped or non-finite).  A correction that made the residual more than
+// kRefineWorse times larger is undone (x64 -= the last correction, residual
+// recomputed): worse = true.  BiCGStab's corrections are not monotone, so a
+// small rise is kept; a failed inner solve raises it by orders of magnitude.
+constexpr double kRefineWorse = 4.0;
+static int refine_check(Solver* S, RefineState& R, bool& go, bool& worse) {
+  const int n = S->hp.n;
+  worse = false;
+  CHK(resid64<double, double>(S, S->A64, S->W64.b, S->W64.x, S->W64.r, nullptr, S_NRM2));
+  CMS_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, S->stream));
+  CMS_CUDA(cudaStreamSynchronize(S->stream));
+  double nrm = std::sqrt(S->h_st->s[S_NRM2]);
+  if (R.steps > 0 && R.prev >= 0.0 && !(nrm <= kRefineWorse * R.prev)) {
+    KLAUNCH(S, P_VEC, (double)n * 20, (k_ir_undo<<<gsz(n), TPB, 0, S->stream>>>(n, S->W32.x, S->W64.x, S->d_st)));
+    CHK(resid64<double, double>(S, S->A64, S->W64.b, S->W64.x, S->W64.r, nullptr, S_NRM2));
+    CMS_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, S->stream));
+    CMS_CUDA(cudaStreamSynchronize(S->stream));
+    nrm = std::sqrt(S->h_st->s[S_NRM2]);
+    worse = true;
+  }
+  if (R.nrm0 < 0) R.nrm0 = nrm;
+  R.prev = nrm;
+  R.rel = R.nrm0 > 0 ? nrm / R.nrm0 : 0.0;
+  go = true;
+  if (!std::isfinite(R.rel)) {
+    R.info->status = CMS_NONFINITE;
+    go = false;
+  } else if (R.rel <= R.tol || R.steps >= R.rmax || R.inner_total >= R.maxit) {
+    go = false;
+  }
+  return CMS_OK;
+}
+
+// Applies the inner solve's correction (W32.x, scaled by the residual norm).
+static int refine_correct(Solver* S, RefineState& R) {
+  const int n = S->hp.n;
+  KLAUNCH(S, P_VEC, (double)n * 20, (k_ir_correct<<<gsz(n), TPB, 0, S->stream>>>(n, S->W32.x, S->W64.x, S->d_st)));
+  ++R.steps;
+  return CMS_OK;
+}
+
+// The rest of a refinement with the exact multicolour ILU(0) inner BiCGStab
+// (or GMRES), from the current x64 and residual: the fallback of a reduced
+// inner solve whose correction made the residual larger.
+static int refine_exact(Solver* S, int nsolv, RefineState& R) {
+  const int n = S->hp.n;
+  S->cur_relax = 0;
+  CHK(factor<float>(S, S->A32));
+  ++S->reduced_fallbacks;
+  bool go = true, worse = false;
+  for (;;) {
+    KLAUNCH(S, P_VEC, (double)n * 12, (k_ir_scale<<<gsz(n), TPB, 0, S->stream>>>(n, S->W64.r, S->W32.b, S->d_st)));
+    if (nsolv == 3) {
+      CHK(run_bicgstab<float>(S, S->A32, S->W32, R.imax, 2, R.itol, 1, false));
+    } else {
+      CMS_CUDA(cudaMemsetAsync(S->W32.x, 0, sizeof(float) * n, S->stream));
+      CHK(run_gmres<float>(S, S->A32, S->W32, R.imax, R.itol, false));
+    }
+    CMS_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, S->stream));
+    CMS_CUDA(cudaStreamSynchronize(S->stream));
+    R.inner_total += (nsolv == 3) ? S->h_st->iter : S->h_st->inner;
+    if (S->h_st->nonfinite) break;
+    CHK(refine_correct(S, R));
+    CHK(refine_check(S, R, go, worse));
+    if (!go || worse) break;
+  }
+  return CMS_OK;
+}
+
+static void refine_finish(RefineState& R) {
+  R.info->iters = R.inner_total;
+  R.info->inner = R.inner_total;
+  R.info->refine_steps = R.steps;
+  R.info->relres = R.rel;
+  if (R.info->status == CMS_OK && R.rel > R.tol) R.info->status = CMS_NOT_CONVERGED;
+}
+
 // Iterative refinement: FP64 residual/correction, FP32 matrix + factor + Krylov.
 static int run_refine(Solver* S, int nsolv, int maxit, double tol, cms_solve_info* info) {
   const HostPattern& P = S->hp;
@@ -999,49 +1086,44 @@ static int run_refine(Solver* S, int nsolv, int maxit, double tol, cms_solve_inf
   } else {
     CHK(factor<float>(S, S->A32));
   }
-  int steps = 0, inner_total = 0;
-  double nrm0 = -1.0, rel = 1.0;
-  const double itol = S->opts.inner_tol > 0 ? S->opts.inner_tol : 1e-3;
-  const int imax = S->opts.inner_max > 0 ? S->opts.inner_max : 50;
-  const int rmax = S->opts.max_refine > 0 ? S->opts.max_refine : 30;
+  RefineState R;
+  R.info = info;
+  R.tol = tol;
+  R.maxit = maxit;
+  R.itol = S->opts.inner_tol > 0 ? S->opts.inner_tol : 1e-3;
+  R.imax = S->opts.inner_max > 0 ? S->opts.inner_max : 50;
+  R.rmax = S->opts.max_refine > 0 ? S->opts.max_refine : 30;
   for (;;) {
-    CHK(resid64<double, double>(S, S->A64, S->W64.b, S->W64.x, S->W64.r, nullptr, S_NRM2));
-    CMS_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, S->stream));
-    CMS_CUDA(cudaStreamSynchronize(S->stream));
-    const double nrm = std::sqrt(S->h_st->s[S_NRM2]);
-    if (nrm0 < 0) nrm0 = nrm;
-    rel = nrm0 > 0 ? nrm / nrm0 : 0.0;
-    if (!std::isfinite(rel)) {
-      info->status = CMS_NONFINITE;
+    bool go = true, worse = false;
+    CHK(refine_check(S, R, go, worse));
+    if (worse) {  // the last inner correction was no good
+      if (go && (schur || relax)) CHK(refine_exact(S, nsolv, R));
       break;
     }
-    if (rel <= tol || steps >= rmax || inner_total >= maxit) break;
+    if (!go) break;
     // inner FP32 solve A32 d = r/||r|| from d = 0 (factor already built)
     KLAUNCH(S, P_VEC, (double)n * 12, (k_ir_scale<<<gsz(n), TPB, 0, S->stream>>>(n, S->W64.r, S->W32.b, S->d_st)));
     if (schur) {
-      CHK(run_schur_bicgstab(S, S->ptiles, imax, itol));  // tiles built above for its layout
+      CHK(run_schur_bicgstab(S, S->ptiles, R.imax, R.itol));  // tiles built above for its layout
     } else if (nsolv == 3) {
-      CHK(run_bicgstab<float>(S, S->A32, S->W32, imax, 2, itol, 1, false));
+      CHK(run_bicgstab<float>(S, S->A32, S->W32, R.imax, 2, R.itol, 1, false));
     } else {
       CMS_CUDA(cudaMemsetAsync(S->W32.x, 0, sizeof(float) * n, S->stream));
-      CHK(run_gmres<float>(S, S->A32, S->W32, imax, itol, false));
+      CHK(run_gmres<float>(S, S->A32, S->W32, R.imax, R.itol, false));
     }
     CMS_CUDA(cudaMemcpyAsync(S->h_st, S->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, S->stream));
     CMS_CUDA(cudaStreamSynchronize(S->stream));
-    inner_total += (nsolv == 3) ? S->h_st->iter : S->h_st->inner;
+    R.inner_total += (nsolv == 3) ? S->h_st->iter : S->h_st->inner;
     // an FP32 inner solve that overflowed (a near-breakdown of its recurrence)
-    // gives no correction: keep the FP64 iterate and end the refinement (the
-    // FP64 residual above reports a non-finite system itself)
-    if (S->h_st->nonfinite) break;
-    KLAUNCH(S, P_VEC, (double)n * 20,
-            (k_ir_correct<<<gsz(n), TPB, 0, S->stream>>>(n, S->W32.x, S->W64.x, S->d_st)));
-    ++steps;
+    // gives no correction: with the reduced or two-phase form the rest runs
+    // on the exact factor, else the refinement ends with the FP64 iterate
+    if (S->h_st->nonfinite) {
+      if (schur || relax) CHK(refine_exact(S, nsolv, R));
+      break;
+    }
+    CHK(refine_correct(S, R));
   }
-  info->iters = inner_total;
-  info->inner = inner_total;
-  info->refine_steps = steps;
-  info->relres = rel;
-  if (info->status == CMS_OK && rel > tol) info->status = CMS_NOT_CONVERGED;
+  refine_finish(R);
   return CMS_OK;
 }
 
@@ -1316,6 +1398,8 @@ void cms_solver_destroy(cms_solver* s) {
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
 }
+
+long long cms_solver_refine_fallbacks(const cms_solver* s) { return s ? s->reduced_fallbacks : 0; }
 
 // ---- reference-shaped global API ----
 static cms_solver* g_solver = nullptr;

@@ -161,6 +161,10 @@ size_t cms_solver_device_bytes(const cms_solver* s);
 int cms_solver_get_perm(const cms_solver* s, int* perm);
 /* Kernel launches issued by the handle since creation (counted on the host). */
 long long cms_solver_launches(const cms_solver* s);
+/* Refinements that finished on the exact multicolour ILU(0) inner solve
+ * because a reduced or two-phase inner correction made the FP64 residual
+ * more than 4 times larger or overflowed (the correction is undone first). */
+long long cms_solver_refine_fallbacks(const cms_solver* s);
 /* Kernel-class timing with CUDA events on the handle's stream.  Classes:
  * 0 prologue, 1 ILU(0) factor, 2 forward sweep, 3 backward sweep, 4 SpMV,
  * 5 vector/reduction kernels, 6 FP64 residual, 7 scalar kernels, 8 flow-step

@@ -161,3 +161,20 @@ def test_device_tide_matches_host_levels(kind):
         out.append(m.get("eta")[: c.grid.ncells].copy())
         m.close()
     assert np.abs(out[0] - out[1]).max() <= 1e-10
+
+
+@pytest.mark.parametrize("precision", ["fp32_refine", "fp64"])
+def test_flow_step_is_deterministic(precision):
+    """Two models of one case step to the same bits: the persistent kernels'
+    dot products are summed in a fixed order and nothing depends on timing."""
+    c = cases.tidal_inlet(12000, seed=6)
+    out = []
+    for _ in range(2):
+        m = FlowModel(c, precision=precision, nsolv=3, tol=1e-6, norm=2, nswp_pp=200, nswp_uv=200)
+        m.init()
+        hist = [m.step()["krylov_iters"] for _ in range(4)]
+        out.append((hist, m.get("eta").copy(), m.get("u").copy()))
+        m.close()
+    assert out[0][0] == out[1][0]
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+    np.testing.assert_array_equal(out[0][2], out[1][2])
