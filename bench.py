@@ -1138,7 +1138,7 @@ def main():
                     help="reference arm: seconds of whole timed CPU steps (at least one step)")
     ap.add_argument("--ncu", action="store_true", help="warm-up and timed steps only (profiler runs)")
     ap.add_argument("--reduced-layout", type=int, default=0,
-                    help="threads x rows layout of the reduced inner solve (0 auto, 1-4)")
+                    help="threads x rows layout and form of the reduced inner solve (0 auto, 1-7; cms_solver_opts.reduced_layout)")
     ap.add_argument("--multi-kernel", action="store_true",
                     help="BiCGStab as one launch per phase instead of one persistent launch per solve")
     args = ap.parse_args()

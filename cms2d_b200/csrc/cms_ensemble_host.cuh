@@ -100,6 +100,13 @@ static int refine_batched(Ens* E, const std::vector<int>& act, const std::vector
     schur = S->opts.inner_relax == 2 && S->opts.ordering == CMS_ORDER_MULTICOLOR &&
             schur_pattern(S, E->tiles[act[j]]) == CMS_OK;
   }
+  // the single-reduction form when every member's layout option asks for it
+  // and every member's pattern is symmetric (the launch is one kernel)
+  bool sr = schur;
+  for (int j = 0; j < A_ && sr; ++j) {
+    Solver* S = E->m[act[j]]->S;
+    sr = schur_layout(schur_layout_index(S)).sr && S->sc_sym;
+  }
   bool relax_any = false;
   for (int j = 0; j < A_; ++j) {
     Solver* S = E->m[act[j]]->S;
@@ -171,8 +178,8 @@ static int refine_batched(Ens* E, const std::vector<int>& act, const std::vector
     if (schur) {
       void* kargs[] = {&E->d_sargs, &E->d_bmap};
       // the layout the ensemble's tile split was sized for (256 threads per block)
-      CMS_CUDA(cudaLaunchCooperativeKernel((const void*)k_schur_batched<TPB, 2>, dim3(blocks), dim3(TPB), kargs, 0,
-                                           E->stream));
+      const void* kern = sr ? (const void*)k_schur_batched<TPB, 2, 1> : (const void*)k_schur_batched<TPB, 2, 0>;
+      CMS_CUDA(cudaLaunchCooperativeKernel(kern, dim3(blocks), dim3(TPB), kargs, 0, E->stream));
     } else {
       void* kargs[] = {&E->d_args, &E->d_bmap};
       CMS_CUDA(cudaLaunchCooperativeKernel((const void*)k_bicg_batched<float>, dim3(blocks), dim3(TPB), kargs, 0,

@@ -47,7 +47,7 @@
 namespace cms {
 
 constexpr int kProgressStride = 32;  // unsigned ints between two tiles' progress counters (128 bytes)
-constexpr int NSMAX = 6;  // sums per reduction (partial-sum buffer stride)
+constexpr int NSMAX = 9;  // sums per reduction (partial-sum buffer stride)
 
 __device__ __forceinline__ void red_release_add(unsigned int* p, unsigned int v) {
   asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");

@@ -72,6 +72,10 @@ struct SchurArgs {
   const float* b;
   float* x;
   float *r, *r0, *p, *nu, *t, *y;
+  // single-reduction form only: the transpose slot map (ctr[e] = offset of
+  // Chat's entry (k, i) for the entry e = (i, k)), u = op r, q = op nu, s, f0
+  const int* ctr;          // [KC][nB]
+  float *u, *q, *s, *f0;
   double* part;            // [2][NSMAX][ntiles]
   GridBar* bar;
   DevState* st;
@@ -156,10 +160,14 @@ __global__ void __launch_bounds__(TPB) k_schur_off(int n, int g1, int nB, int KL
   }
 }
 
-// Block sums of NS values for blocks of BS threads (valid in thread 0).
+// This block's partial sums of NS values into buffer buf: warp sums in
+// shared memory, then warp q adds value q over the block's warps (fixed
+// order) and its lane 0 stores it.  The stores are ordered before the
+// phase's progress release by end_phase's __syncthreads.
 template <int NS, int BS>
-__device__ __forceinline__ void block_sum_bs(double (&v)[NS]) {
-  __shared__ double sm[NS][BS / 32];
+__device__ __forceinline__ void put_partials_bs(const SchurArgs& A, double (&v)[NS], int buf) {
+  constexpr int NW = BS / 32;
+  __shared__ double sm[NS][NW];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
   for (int q = 0; q < NS; ++q) v[q] = warp_sum(v[q]);
@@ -168,42 +176,36 @@ __device__ __forceinline__ void block_sum_bs(double (&v)[NS]) {
     for (int q = 0; q < NS; ++q) sm[q][wid] = v[q];
   }
   __syncthreads();
-  if (wid == 0) {
-#pragma unroll
-    for (int q = 0; q < NS; ++q) v[q] = warp_sum(lane < BS / 32 ? sm[q][lane] : 0.0);
+  for (int q = wid; q < NS; q += NW) {
+    const double x = warp_sum(lane < NW ? sm[q][lane] : 0.0);
+    if (lane == 0) A.part[((size_t)buf * NSMAX + q) * A.ntiles + A.tile] = x;
   }
 }
 
-// This block's partial sums of NS values into buffer buf.
+// After a grid barrier: the grid totals, value q summed by warp q (lane l
+// adds tiles l, l + 32, ... in that order, then a butterfly), so every block
+// forms the same bits; then shared with the block.  Four tiles' loads are
+// issued before their adds.
 template <int NS, int BS>
-__device__ __forceinline__ void put_partials_bs(const SchurArgs& A, double (&v)[NS], int buf) {
-  block_sum_bs<NS, BS>(v);
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int q = 0; q < NS; ++q) A.part[((size_t)buf * NSMAX + q) * A.ntiles + A.tile] = v[q];
-  }
-}
-
-// After a grid barrier: the grid totals, summed by the first warp in a fixed
-// order (lane l adds tiles l, l + 32, ..., then a butterfly), so every block
-// forms the same bits; then shared with the block.
-template <int NS>
 __device__ __forceinline__ void get_totals_w0(const SchurArgs& A, double (&tot)[NS], int buf) {
+  constexpr int NW = BS / 32;
   __shared__ double bc[NS];
-  if (threadIdx.x < 32) {
-    double acc[NS];
-#pragma unroll
-    for (int q = 0; q < NS; ++q) acc[q] = 0.0;
-    for (int b = threadIdx.x; b < A.ntiles; b += 32) {
-#pragma unroll
-      for (int q = 0; q < NS; ++q) acc[q] += __ldcg(&A.part[((size_t)buf * NSMAX + q) * A.ntiles + b]);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nt = A.ntiles;
+  for (int q = wid; q < NS; q += NW) {
+    const double* src = A.part + ((size_t)buf * NSMAX + q) * nt;
+    double acc = 0.0;
+    int b = lane;
+    for (; b + 96 < nt; b += 128) {
+      const double v0 = __ldcg(src + b), v1 = __ldcg(src + b + 32), v2 = __ldcg(src + b + 64),
+                   v3 = __ldcg(src + b + 96);
+      acc += v0;
+      acc += v1;
+      acc += v2;
+      acc += v3;
     }
-#pragma unroll
-    for (int q = 0; q < NS; ++q) acc[q] = warp_sum(acc[q]);
-    if (threadIdx.x == 0) {
-#pragma unroll
-      for (int q = 0; q < NS; ++q) bc[q] = acc[q];
-    }
+    for (; b < nt; b += 32) acc += __ldcg(src + b);
+    acc = warp_sum(acc);
+    if (lane == 0) bc[q] = acc;
   }
   __syncthreads();
 #pragma unroll
@@ -306,7 +308,7 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
     end_phase(A, ph);
     grid_barrier(A, ph);
     if (ph.ok) {
-      get_totals_w0<1>(A, s1, 0);
+      get_totals_w0<1, BS>(A, s1, 0);
       res0 = sqrt(s1[0]);
       rho = s1[0];
     }
@@ -370,7 +372,7 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
       end_phase(A, ph);
       grid_barrier(A, ph);
       if (!ph.ok) break;
-      get_totals_w0<1>(A, s1, buf);
+      get_totals_w0<1, BS>(A, s1, buf);
       buf ^= 1;
       // a breakdown (r0.nu = 0) ends this inner solve with the iterate so far
       // (the refinement's FP64 residual takes over); a non-finite sum is an error
@@ -407,7 +409,7 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
       end_phase(A, ph);
       grid_barrier(A, ph);
       if (!ph.ok) break;
-      get_totals_w0<5>(A, s5, buf);
+      get_totals_w0<5, BS>(A, s5, buf);
       buf ^= 1;
       omg = s5[0] / fmax(s5[1], SMALL);
       const double rr = fmax(s5[3] - 2.0 * omg * s5[0] + omg * omg * s5[1], 0.0);
@@ -475,14 +477,289 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
   }
 }
 
-// Block and row layouts of the reduced kernel: threads per block and rows per
-// thread per batch (cms_solver_opts.reduced_layout picks one; 0: the first).
-#define CMS_SCHUR_LAYOUTS(X) X(256, 2) X(512, 2) X(512, 4) X(1024, 2)
-constexpr int kSchurLayouts = 4;
+// Single-reduction form of the same iteration (the reorganisation of L. T.
+// Yang and R. P. Brent, "The improved BiCGStab method for large and sparse
+// unsymmetric linear systems on parallel distributed memory architectures",
+// 2002): one grid barrier per iteration instead of two.  With op = I - Chat,
+// u = op r and q = op nu (nu = op p), the search direction's image and t
+// follow without a product of their own,
+//   nu' = u' + bet (nu - omg q),   t = op s = u - alf q,
+// and r0.nu', which alf needs before q is known, from
+//   r0.nu' = r0.u' + bet (r0.nu - omg r0.q),   r0.u' = f0.r',   f0 = op^T r0
+// (f0 once per launch; Chat's pattern is structurally symmetric, so op^T's
+// row i gathers over row i's own columns with the coefficients at the
+// transpose slots ctr).  An iteration is two phases:
+//   X  r = s - omg t (own rows and each gathered neighbour), u = op r, the
+//      pending y update, p = r + bet (p - omg nu), nu = u + bet (nu - omg q);
+//   Y  (after the neighbour tiles have finished X) q = op nu, s = r - alf nu,
+//      t = u - alf q, and t.s, t.t, s.s, r0.s, r0.t, f0.s, f0.t, r0.q, r0.nu,
+//      reduced at a grid barrier.
+// r0.nu is summed from the vector (not carried by the recurrence), so the
+// recurrence extrapolates one iteration at a time.  Y overwrites s and t of
+// its own rows: every neighbour that gathers them in X has finished X (the
+// neighbour wait), and the next X starts after the grid barrier.
+template <int BS, int NR>
+__device__ __forceinline__ void schur_body_sr(const SchurArgs& A) {
+  const int G = A.G;
+  PhaseState ph{0u, 0u, true, true};
+  __shared__ int s_lo[GFLAT], s_pre[GFLAT + 1];
+  if (threadIdx.x == 0) {
+    int acc = 0;
+    for (int g = 0; g < G; ++g) {
+      const int* o = A.toff + (size_t)g * (A.ntiles + 1) + A.tile;
+      s_lo[g] = __ldg(o);
+      s_pre[g] = acc;
+      acc += __ldg(o + 1) - __ldg(o);
+    }
+    s_pre[G] = acc;
+  }
+  __syncthreads();
+  const int n = A.n, g1 = A.g1;
+  // start, first phase: r0 = s = b_B - AB0 D0^-1 b_0, y = 0
+  for_tile_rows<NR>(s_lo, s_pre, 1, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR]) {
+    float acc[NR];
+    int kl[NR];
+#pragma unroll
+    for (int q = 0; q < NR; ++q) {
+      acc[q] = __ldg(&A.b[r[q]]);
+      kl[q] = __ldg(&A.nlo[r[q]]);
+    }
+#pragma unroll
+    for (int s = 0; s < KMAX; ++s) {
+      if (s < A.KL) {
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+          if (s < kl[q]) {
+            const size_t e = (size_t)s * n + r[q];
+            const int j = __ldg(&A.col[e]);
+            if (j < g1) acc[q] = acc[q] + __ldg(&A.aoff[e]) * (__ldg(&A.b[j]) * __ldg(&A.sinv[j]));
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < NR; ++q) {
+      if (!ok[q]) continue;
+      A.r0[r[q]] = acc[q]; A.s[r[q]] = acc[q]; A.y[r[q]] = 0.0f;
+    }
+  });
+  end_phase(A, ph);
+  // start, second phase: f0 = op^T r0, u = nu = op r0, p = r0; r0.r0, f0.r0
+  double res0 = 0.0, rho = 0.0, alf = 0.0;
+  int converged = 0, nonfinite = 0;
+  bool stop = false;
+  {
+    double s2[2] = {0.0, 0.0};
+    wait_neighbours(A, ph);
+    for_tile_rows<NR>(s_lo, s_pre, 1, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR]) {
+      float ua[NR], fa[NR], r0v[NR];
+      int kc[NR];
+#pragma unroll
+      for (int q = 0; q < NR; ++q) {
+        r0v[q] = ldm(&A.r0[r[q]]);
+        ua[q] = r0v[q];
+        fa[q] = r0v[q];
+        kc[q] = __ldg(&A.ccnt[r[q] - g1]);
+      }
+#pragma unroll
+      for (int s = 0; s < KSC; ++s) {
+        if (s < A.KC) {
+#pragma unroll
+          for (int q = 0; q < NR; ++q) {
+            if (s < kc[q]) {
+              const size_t e = (size_t)s * A.nB + (r[q] - g1);
+              const float rk = ldm(&A.r0[__ldg(&A.ccol[e])]);
+              ua[q] = ua[q] - __ldg(&A.coff[e]) * rk;
+              fa[q] = fa[q] - __ldg(&A.coff[__ldg(&A.ctr[e])]) * rk;
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < NR; ++q) {
+        if (!ok[q]) continue;
+        A.f0[r[q]] = fa[q]; A.u[r[q]] = ua[q]; A.nu[r[q]] = ua[q]; A.p[r[q]] = r0v[q];
+        s2[0] += (double)r0v[q] * (double)r0v[q];
+        s2[1] += (double)fa[q] * (double)r0v[q];
+      }
+    });
+    put_partials_bs<2, BS>(A, s2, 0);
+    end_phase(A, ph);
+    grid_barrier(A, ph);
+    if (ph.ok) {
+      get_totals_w0<2, BS>(A, s2, 0);
+      res0 = sqrt(s2[0]);
+      rho = s2[0];
+      if (res0 == 0.0) converged = 1;
+      else if (!isfinite(s2[1]) || !isfinite(res0)) nonfinite = 1;
+      else if (s2[1] == 0.0) stop = true;  // breakdown before the first step
+      else alf = rho / s2[1];
+    }
+  }
+  double omg = 0.0, bet = 0.0, alf_n = alf, rel = res0 > 0.0 ? 1.0 : 0.0;
+  int it = 0, buf = 1;
+  bool pending = false;  // an iteration's y update not yet applied
+  while (ph.ok && !converged && !nonfinite && !stop && it < A.maxit) {
+    ++it;
+    // X: r = s - omg t, u = op r, the pending y update, p and nu
+    if (it > 1) {
+      const float a = (float)alf, w = (float)omg, be = (float)bet;
+      for_tile_rows<NR>(s_lo, s_pre, 1, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR]) {
+        float sv[NR], yv[NR], pv[NR], nv[NR], qv[NR], rv[NR], acc[NR];
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+          sv[q] = ldm(&A.s[r[q]]);
+          rv[q] = sv[q] - w * ldm(&A.t[r[q]]);
+          yv[q] = ldm(&A.y[r[q]]);
+          pv[q] = ldm(&A.p[r[q]]);
+          nv[q] = ldm(&A.nu[r[q]]);
+          qv[q] = ldm(&A.q[r[q]]);
+          acc[q] = rv[q];
+        }
+        chat_sub(A, acc, r, [&](int k) { return ldm(&A.s[k]) - w * ldm(&A.t[k]); });
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+          if (!ok[q]) continue;
+          A.y[r[q]] = yv[q] + a * pv[q] + w * sv[q];
+          A.u[r[q]] = acc[q];
+          A.p[r[q]] = rv[q] + be * (pv[q] - w * nv[q]);
+          A.nu[r[q]] = acc[q] + be * (nv[q] - w * qv[q]);
+        }
+      });
+      pending = false;
+      alf = alf_n;
+      end_phase(A, ph);
+    }
+    // Y: q = op nu, s = r - alf nu, t = u - alf q, nine sums
+    {
+      double s9[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+      const float a = (float)alf, w = (float)omg;
+      const bool first = it == 1;
+      wait_neighbours(A, ph);
+      for_tile_rows<NR>(s_lo, s_pre, 1, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR]) {
+        float rv[NR], nv[NR], uv[NR], r0v[NR], f0v[NR], acc[NR];
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+          r0v[q] = ldm(&A.r0[r[q]]);
+          rv[q] = first ? r0v[q] : ldm(&A.s[r[q]]) - w * ldm(&A.t[r[q]]);
+          nv[q] = ldm(&A.nu[r[q]]);
+          uv[q] = ldm(&A.u[r[q]]);
+          f0v[q] = ldm(&A.f0[r[q]]);
+          acc[q] = nv[q];
+        }
+        chat_sub(A, acc, r, [&](int k) { return ldm(&A.nu[k]); });
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+          if (!ok[q]) continue;
+          const float sn = rv[q] - a * nv[q], tn = uv[q] - a * acc[q];
+          A.q[r[q]] = acc[q];
+          A.s[r[q]] = sn;
+          A.t[r[q]] = tn;
+          const double sd = sn, td = tn, od = r0v[q], fd = f0v[q];
+          s9[0] += td * sd;
+          s9[1] += td * td;
+          s9[2] += sd * sd;
+          s9[3] += od * sd;
+          s9[4] += od * td;
+          s9[5] += fd * sd;
+          s9[6] += fd * td;
+          s9[7] += od * (double)acc[q];
+          s9[8] += od * (double)nv[q];
+        }
+      });
+      put_partials_bs<9, BS>(A, s9, buf);
+      end_phase(A, ph);
+      grid_barrier(A, ph);
+      if (!ph.ok) break;
+      get_totals_w0<9, BS>(A, s9, buf);
+      buf ^= 1;
+      omg = s9[0] / fmax(s9[1], SMALL);
+      const double rr = fmax(s9[2] - 2.0 * omg * s9[0] + omg * omg * s9[1], 0.0);
+      const double rho1 = s9[3] - omg * s9[4];
+      rel = sqrt(rr) / res0;
+      if (!isfinite(rel) || !isfinite(omg) || !isfinite(rho1)) { nonfinite = 1; break; }
+      pending = true;  // y += alf p + omg s is valid even at a breakdown below
+      if (rel < A.tol) { converged = 1; continue; }
+      // breakdown of the next step (omg = 0, r0.r = 0 or r0.nu = 0): stop with this iterate
+      if (omg == 0.0 || rho1 == 0.0) break;
+      bet = (rho1 / rho) * (alf / omg);
+      rho = rho1;
+      const double tau = (s9[5] - omg * s9[6]) + bet * (s9[8] - omg * s9[7]);
+      if (!isfinite(tau) || !isfinite(bet)) { nonfinite = 1; break; }
+      if (tau == 0.0) break;
+      alf_n = rho / tau;
+    }
+  }
+  // the last update (y only), x_B = S^-1 y, then x_0 = D0^-1 (b_0 + sum aoff x_B)
+  if (ph.ok && !nonfinite) {
+    const float a = (float)alf, w = (float)omg;
+    for_tile_rows<NR>(s_lo, s_pre, 1, G - 1, [&](const int (&r)[NR], const bool (&ok)[NR]) {
+      float yv[NR], si[NR];
+#pragma unroll
+      for (int q = 0; q < NR; ++q) {
+        yv[q] = ldm(&A.y[r[q]]);
+        if (pending) yv[q] = yv[q] + a * ldm(&A.p[r[q]]) + w * ldm(&A.s[r[q]]);
+        si[q] = __ldg(&A.sinv[r[q]]);
+      }
+#pragma unroll
+      for (int q = 0; q < NR; ++q)
+        if (ok[q]) A.x[r[q]] = yv[q] * si[q];
+    });
+    end_phase(A, ph);
+    grid_barrier(A, ph);
+    if (ph.ok) {
+      for_tile_rows<NR>(s_lo, s_pre, 0, 0, [&](const int (&r)[NR], const bool (&ok)[NR]) {
+        float acc[NR], si[NR];
+        int ku[NR];
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+          acc[q] = __ldg(&A.b[r[q]]);
+          si[q] = __ldg(&A.sinv[r[q]]);
+          ku[q] = __ldg(&A.nup[r[q]]);
+        }
+#pragma unroll
+        for (int t2 = 0; t2 < KMAX; ++t2) {
+#pragma unroll
+          for (int q = 0; q < NR; ++q) {
+            if (t2 < ku[q]) {
+              const size_t e = (size_t)(A.KL + t2) * n + r[q];
+              acc[q] = acc[q] + __ldg(&A.aoff[e]) * ldm(&A.x[__ldg(&A.col[e])]);
+            }
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < NR; ++q)
+          if (ok[q]) A.x[r[q]] = acc[q] * si[q];
+      });
+    }
+  }
+  if (A.tile == 0 && threadIdx.x == 0) {
+    A.st->iter = it;
+    A.st->s[S_RELRES] = rel;
+    A.st->s[S_RES0] = res0;
+    A.st->converged = converged;
+    A.st->nonfinite = nonfinite;
+    A.st->done = 1;
+  }
+}
+
+// Block and row layouts of the reduced kernel: threads per block, rows per
+// thread per batch, and the iteration form (0: three phases and two grid
+// barriers per iteration, schur_body; 1: single reduction, schur_body_sr).
+// cms_solver_opts.reduced_layout picks one by its position (1-based).
+#define CMS_SCHUR_LAYOUTS(X) X(256, 2, 0) X(512, 2, 0) X(512, 4, 0) X(1024, 2, 0) X(1024, 2, 1) X(512, 2, 1) \
+  X(256, 2, 1)
+constexpr int kSchurLayouts = 7;
+
+template <int BS, int NR, int SR>
+__device__ __forceinline__ void schur_run(const SchurArgs& A) {
+  if constexpr (SR != 0) schur_body_sr<BS, NR>(A);
+  else schur_body<BS, NR>(A);
+}
 
 // Several independent systems (an ensemble) in one launch: bmap[b] = (member,
 // tile) of block b; members share nothing but the launch.
-template <int BS, int NR>
+template <int BS, int NR, int SR>
 __global__ void __launch_bounds__(BS, 1024 / BS) k_schur_batched(const SchurArgs* __restrict__ members,
                                                                   const int2* __restrict__ bmap) {
   __shared__ SchurArgs sA;
@@ -492,11 +769,11 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_schur_batched(const SchurArgs
     sA.tile = mt.y;
   }
   __syncthreads();
-  schur_body<BS, NR>(sA);
+  schur_run<BS, NR, SR>(sA);
 }
 
 // One system: block b works on tile b.
-template <int BS, int NR>
+template <int BS, int NR, int SR>
 __global__ void __launch_bounds__(BS, 1024 / BS) k_schur_bicg(SchurArgs A) {
   __shared__ SchurArgs sA;
   if (threadIdx.x == 0) {
@@ -505,22 +782,24 @@ __global__ void __launch_bounds__(BS, 1024 / BS) k_schur_bicg(SchurArgs A) {
     sA.tile = blockIdx.x;
   }
   __syncthreads();
-  schur_body<BS, NR>(sA);
+  schur_run<BS, NR, SR>(sA);
 }
 
-// Kernel, block size of layout k.
+// Kernels, block size and form of layout k.
 struct SchurLayout {
   const void* single;
   const void* batched;
   int bs;
+  int sr;
 };
 inline SchurLayout schur_layout(int k) {
   int q = 0;
-#define CMS_SCHUR_PICK(B, R) \
-  if (q++ == k) return SchurLayout{(const void*)k_schur_bicg<B, R>, (const void*)k_schur_batched<B, R>, B};
+#define CMS_SCHUR_PICK(B, R, F)                                                                            \
+  if (q++ == k)                                                                                            \
+    return SchurLayout{(const void*)k_schur_bicg<B, R, F>, (const void*)k_schur_batched<B, R, F>, B, F};
   CMS_SCHUR_LAYOUTS(CMS_SCHUR_PICK)
 #undef CMS_SCHUR_PICK
-  return SchurLayout{(const void*)k_schur_bicg<256, 2>, (const void*)k_schur_batched<256, 2>, 256};
+  return SchurLayout{(const void*)k_schur_bicg<256, 2, 0>, (const void*)k_schur_batched<256, 2, 0>, 256, 0};
 }
 
 }  // namespace cms

@@ -96,8 +96,9 @@ struct cms_solver {
   // Chat's pattern and values, 1/d and 1/s, neighbour tiles under Chat
   int sc_state = 0;  // 0 not built, 1 built, -1 not possible on this pattern
   int sc_KC = 0, sc_tiles = 0;
+  int sc_sym = 0;    // Chat's pattern is structurally symmetric (d_sctr built)
   long long sc_nnz = 0, sc_e0b = 0;  // stored entries of Chat; couplings between group 0 and B
-  int *d_sccol = nullptr, *d_sdep_ptr = nullptr, *d_sdep_idx = nullptr;
+  int *d_sccol = nullptr, *d_sdep_ptr = nullptr, *d_sdep_idx = nullptr, *d_sctr = nullptr;
   float *d_scoff = nullptr, *d_ssinv = nullptr;
   signed char* d_sccnt = nullptr;
   size_t cap_sdep = 0;
@@ -425,19 +426,21 @@ static int bicg_iter(Solver* S, Mat<T>& A, Work<T>& W) {
 // Blocks of the persistent kernels that can be resident at once on the
 // device (cooperative launch limit); 0 when it cannot be launched.
 static int persist_capacity(int dev) {
-  int coop = 0, nsm = 0, per32 = 0, per64 = 0, perb = 0, pers = 0, persb = 0;
+  int coop = 0, nsm = 0, per32 = 0, per64 = 0, perb = 0, pers = 0, persb = 0, persr = 0;
   if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop ||
       cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per32, k_bicg_persistent<float>, TPB, 0) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per64, k_bicg_persistent<double>, TPB, 0) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perb, k_bicg_batched<float>, TPB, 0) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pers, k_schur_bicg<TPB, 2>, TPB, 0) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&persb, k_schur_batched<TPB, 2>, TPB, 0) != cudaSuccess ||
-      std::min(std::min(std::min(std::min(per32, per64), perb), pers), persb) <= 0) {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pers, k_schur_bicg<TPB, 2, 0>, TPB, 0) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&persb, k_schur_batched<TPB, 2, 0>, TPB, 0) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&persr, k_schur_batched<TPB, 2, 1>, TPB, 0) != cudaSuccess ||
+      std::min(std::min(std::min(std::min(std::min(per32, per64), perb), pers), persb), persr) <= 0) {
     cudaGetLastError();
     return 0;
   }
-  return std::min(std::min(std::min(std::min(std::min(per32, per64), perb), pers), persb) * nsm, GRID_CAP);
+  return std::min(std::min(std::min(std::min(std::min(std::min(per32, per64), perb), pers), persb), persr) * nsm,
+                  GRID_CAP);
 }
 
 static int build_tiles(Solver* S, int nt);
@@ -816,6 +819,27 @@ static int schur_pattern(Solver* S, int tiles) {
     std::vector<int> ccol((size_t)KC * nB);
     for (int i = 0; i < nB; ++i)
       for (int q = 0; q < KC; ++q) ccol[(size_t)q * nB + i] = q < cnt[i] ? tmp[(size_t)i * KSC + q] : g1 + i;
+    // transpose slots for the single-reduction form: entry (i, k) at slot q
+    // -> offset of entry (k, i); absent when the pattern is not symmetric
+    std::vector<int> ctr((size_t)KC * nB);
+    bool sym = true;
+    for (int i = 0; i < nB && sym; ++i) {
+      for (int q = 0; q < KC; ++q) {
+        const size_t e = (size_t)q * nB + i;
+        ctr[e] = (int)e;
+        if (q >= cnt[i]) continue;
+        const int kk = tmp[(size_t)i * KSC + q] - g1;
+        const int* row = &tmp[(size_t)kk * KSC];
+        const int* hit = std::lower_bound(row, row + cnt[kk], g1 + i);
+        if (hit == row + cnt[kk] || *hit != g1 + i) { sym = false; break; }
+        ctr[e] = (int)((size_t)(hit - row) * nB + kk);
+      }
+    }
+    if (sym && (size_t)KC * nB <= (size_t)INT32_MAX) {
+      CHK(S->alloc(&S->d_sctr, ctr.size()));
+      CMS_CUDA(cudaMemcpyAsync(S->d_sctr, ctr.data(), ctr.size() * sizeof(int), cudaMemcpyHostToDevice, S->stream));
+      S->sc_sym = 1;
+    }
     CHK(S->alloc(&S->d_sccol, ccol.size()));
     CHK(S->alloc(&S->d_scoff, ccol.size()));
     CHK(S->alloc(&S->d_sccnt, (size_t)nB));
@@ -892,10 +916,20 @@ static int schur_numeric(Solver* S) {
 // Algorithmic bytes of one reduced-system launch: the start (reduced
 // right-hand side), per iteration P0 (8 vector accesses per row), A (p, r0,
 // count, Chat, nu) and B (r, nu, r0, count, Chat, t), and the end (y update,
-// x_B, then x_0 from b, 1/d and the group-0 rows' couplings).
-static double schur_bytes(const Solver* S, int iters) {
+// x_B, then x_0 from b, 1/d and the group-0 rows' couplings).  Single-
+// reduction form (sr): the start adds the transposed product (r0, count,
+// Chat, transpose slots; f0, u, nu, p written), an iteration is X (s, t, y,
+// p, nu, q, count, Chat; y, u, p, nu written) and Y (s, t, nu, u, r0, f0,
+// count, Chat; q, s, t written), the end reads y, p, s.
+static double schur_bytes(const Solver* S, int iters, int sr) {
   const HostPattern& P = S->hp;
   const double n = P.n, g1 = P.gstart[1], nB = n - g1, C = 8.0 * (double)S->sc_nnz, E = 8.0 * (double)S->sc_e0b;
+  if (sr) {
+    const double start = 4.0 * n + 4.0 * g1 + E + nB + 12.0 * nB + (5.0 * nB + C + 4.0 * (double)S->sc_nnz + 16.0 * nB);
+    const double it = (41.0 * nB + C) + (37.0 * nB + C);
+    const double end = 20.0 * nB + 9.0 * g1 + E + 4.0 * nB + 4.0 * g1;
+    return start + iters * it + end;
+  }
   const double start = 4.0 * n + 4.0 * g1 + E + nB + 24.0 * nB;
   const double it = 32.0 * nB + (13.0 * nB + C) + (17.0 * nB + C);
   const double end = 24.0 * nB + 9.0 * g1 + E + 4.0 * nB + 4.0 * g1;
@@ -914,18 +948,31 @@ static SchurArgs make_schur_args(Solver* S, int tiles, int maxit, double tol) {
   a.col = S->d_col; a.nlo = S->d_nlo; a.nup = S->d_nup; a.aoff = S->A32.aoff; a.sinv = S->d_ssinv;
   a.b = S->W32.b; a.x = S->W32.x;
   a.r = S->W32.r; a.r0 = S->W32.r0; a.p = S->W32.p; a.nu = S->W32.u; a.t = S->W32.v; a.y = S->W32.z;
+  a.ctr = S->d_sctr; a.u = S->W32.vv[1]; a.q = S->W32.vv[2]; a.s = S->W32.vv[3]; a.f0 = S->W32.vv[4];
   a.part = S->d_ppart; a.bar = &S->d_st->bar; a.st = S->d_st;
   a.maxit = maxit; a.tol = tol; a.spin_limit = kSpinLimit;
   return a;
 }
 
 // Layout of the reduced kernel for this handle (cms_solver_opts.reduced_layout,
-// 0 = auto = 1024 threads x 2 rows, the fastest on the 1M systems) and the
-// tiles it takes: its resident blocks
-// on the device, at most one per 256 rows.  0 tiles when it cannot launch.
+// 0 = auto = 1024 threads x 2 rows in the single-reduction form, the fastest
+// on the 1M systems) and the tiles it takes: its resident blocks on the
+// device, at most one per 256 rows.  0 tiles when it cannot launch.
 static int schur_layout_index(const Solver* S) {
   const int k = S->opts.reduced_layout;
-  return (k >= 1 && k <= kSchurLayouts) ? k - 1 : 3;
+  return (k >= 1 && k <= kSchurLayouts) ? k - 1 : 4;
+}
+// The layout that runs: a single-reduction layout needs a symmetric pattern
+// of Chat; otherwise the three-phase layout of the same block and row shape.
+static int schur_layout_run(const Solver* S) {
+  const int k = schur_layout_index(S);
+  const SchurLayout L = schur_layout(k);
+  if (!L.sr || S->sc_sym) return k;
+  for (int j = 0; j < kSchurLayouts; ++j) {
+    const SchurLayout M = schur_layout(j);
+    if (!M.sr && M.bs == L.bs) return j;
+  }
+  return 0;
 }
 static int schur_tiles(Solver* S, int layout) {
   const SchurLayout L = schur_layout(layout);
@@ -942,7 +989,7 @@ static int schur_tiles(Solver* S, int layout) {
 // The reduced FP32 inner solve (W32.b -> W32.x) as one cooperative launch.
 static int run_schur_bicgstab(Solver* S, int tiles, int maxit, double tol) {
   SchurArgs a = make_schur_args(S, tiles, maxit, tol);
-  const SchurLayout L = schur_layout(schur_layout_index(S));
+  const SchurLayout L = schur_layout(schur_layout_run(S));
   CMS_CUDA(cudaMemsetAsync(&S->d_st->bar, 0, sizeof(GridBar), S->stream));
   CMS_CUDA(cudaMemsetAsync(S->d_progress, 0, sizeof(unsigned int) * tiles * kProgressStride, S->stream));
   void* args[] = {&a};
@@ -963,7 +1010,7 @@ static int run_schur_bicgstab(Solver* S, int tiles, int maxit, double tol) {
     std::snprintf(g_last_error, sizeof(g_last_error), "reduced BiCGStab: a grid barrier wait timed out");
     return CMS_DEVICE_ERROR;
   }
-  if (recorded) S->prof_recs.back().bytes = schur_bytes(S, S->h_st->iter);
+  if (recorded) S->prof_recs.back().bytes = schur_bytes(S, S->h_st->iter, L.sr);
   return CMS_OK;
 }
 

@@ -79,9 +79,15 @@ typedef struct cms_solver_opts {
                         card, default 1.8: flow.F90:131)                                */
   int nswp0_vel;     /* nswp0(2), the velocity iteration count the hybrid solver
                         (nsolv 5) triples for n = 4, 5 (solvers.f90:265); default 5  */
-  int reduced_layout; /* block and row layout of the reduced inner solve: 0 auto,
-                        1 256 threads x 2 rows, 2 512 x 2, 3 512 x 4, 4 1024 x 2;
-                        the tiles follow the layout's resident block count      */
+  int reduced_layout; /* block and row layout of the reduced inner solve: 0 auto
+                        (= 5), 1 256 threads x 2 rows, 2 512 x 2, 3 512 x 4, 4 1024 x 2
+                        (three phases, two grid barriers per iteration); 5 1024 x 2,
+                        6 512 x 2, 7 256 x 2 in the single-reduction form (one
+                        barrier per iteration; needs a structurally symmetric
+                        reduced pattern, else the three-phase layout of the same
+                        block size runs).  The tiles follow the layout's resident
+                        block count; ensembles take the form of their members'
+                        option at 256 threads x 2 rows                           */
 } cms_solver_opts;
 
 typedef struct cms_solve_info {

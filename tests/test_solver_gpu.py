@@ -281,3 +281,27 @@ def test_inner_solve_forms(kind):
                                      if g.cell2cell[i, k] > n) for i in range(n)])
         x = spla.spsolve(A.tocsc(), rhs)
         assert np.abs(res[2][1] - x).max() <= 1e-6 * np.abs(x).max()
+
+
+@pytest.mark.parametrize("kind", ["cart", "tel", "big"])
+def test_reduced_layouts(kind):
+    """Every block/row layout of the reduced inner solve, in the three-phase
+    and the single-reduction form, converges to the same solution; the
+    single-reduction form's iteration counts stay close to the three-phase
+    form's (the same iterates up to rounding)."""
+    g = {"big": lambda: G.solver_test_grid(250_000), "tel": lambda: _grids()["tel"],
+         "cart": lambda: G.cartesian_grid(300, 200)}[kind]()
+    acoef, ss, sp, phi = G.random_system(g, seed=11)
+    res = {}
+    for layout in range(1, 8):
+        s = S.Solver(g, precision="fp32_refine", tol=1e-8, norm=2, inner_relax=2, reduced_layout=layout)
+        a, b, c, p = _copy(acoef, ss, sp, phi)
+        r = np.zeros_like(b)
+        info = s.solve(a, b, c, r, p, nswp=2000, nsolv=3)
+        assert info["status"] == 0 and info["true_relres"] <= 1e-8, (layout, info)
+        res[layout] = (info, p[: g.ncells].copy())
+    print(kind, {k: (v[0]["iters"], v[0]["refine_steps"]) for k, v in res.items()})
+    p0 = res[4][1]
+    for layout, (info, p) in res.items():
+        assert np.abs(p - p0).max() <= 1e-6 * np.abs(p0).max(), layout
+    assert res[5][0]["iters"] <= 1.5 * res[4][0]["iters"] + 10, (res[5][0], res[4][0])
