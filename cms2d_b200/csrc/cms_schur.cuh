@@ -73,9 +73,11 @@ struct SchurArgs {
   float* x;
   float *r, *r0, *p, *nu, *t, *y;
   // single-reduction form only: the transpose slot map (ctr[e] = offset of
-  // Chat's entry (k, i) for the entry e = (i, k)), u = op r, q = op nu, s, f0
+  // Chat's entry (k, i) for the entry e = (i, k)), u = op r, q = op nu, f0,
+  // and s, t interleaved per row (one 8-byte gather in X)
   const int* ctr;          // [KC][nB]
-  float *u, *q, *s, *f0;
+  float *u, *q, *f0;
+  float2* s_t;
   double* part;            // [2][NSMAX][ntiles]
   GridBar* bar;
   DevState* st;
@@ -540,7 +542,7 @@ __device__ __forceinline__ void schur_body_sr(const SchurArgs& A) {
 #pragma unroll
     for (int q = 0; q < NR; ++q) {
       if (!ok[q]) continue;
-      A.r0[r[q]] = acc[q]; A.s[r[q]] = acc[q]; A.y[r[q]] = 0.0f;
+      A.r0[r[q]] = acc[q]; A.s_t[r[q]] = make_float2(acc[q], 0.0f); A.y[r[q]] = 0.0f;
     }
   });
   end_phase(A, ph);
@@ -608,15 +610,19 @@ __device__ __forceinline__ void schur_body_sr(const SchurArgs& A) {
         float sv[NR], yv[NR], pv[NR], nv[NR], qv[NR], rv[NR], acc[NR];
 #pragma unroll
         for (int q = 0; q < NR; ++q) {
-          sv[q] = ldm(&A.s[r[q]]);
-          rv[q] = sv[q] - w * ldm(&A.t[r[q]]);
+          const float2 st2 = ldm(&A.s_t[r[q]]);
+          sv[q] = st2.x;
+          rv[q] = st2.x - w * st2.y;
           yv[q] = ldm(&A.y[r[q]]);
           pv[q] = ldm(&A.p[r[q]]);
           nv[q] = ldm(&A.nu[r[q]]);
           qv[q] = ldm(&A.q[r[q]]);
           acc[q] = rv[q];
         }
-        chat_sub(A, acc, r, [&](int k) { return ldm(&A.s[k]) - w * ldm(&A.t[k]); });
+        chat_sub(A, acc, r, [&](int k) {
+          const float2 st2 = ldm(&A.s_t[k]);
+          return st2.x - w * st2.y;
+        });
 #pragma unroll
         for (int q = 0; q < NR; ++q) {
           if (!ok[q]) continue;
@@ -641,7 +647,8 @@ __device__ __forceinline__ void schur_body_sr(const SchurArgs& A) {
 #pragma unroll
         for (int q = 0; q < NR; ++q) {
           r0v[q] = ldm(&A.r0[r[q]]);
-          rv[q] = first ? r0v[q] : ldm(&A.s[r[q]]) - w * ldm(&A.t[r[q]]);
+          const float2 st2 = ldm(&A.s_t[r[q]]);
+          rv[q] = first ? r0v[q] : st2.x - w * st2.y;
           nv[q] = ldm(&A.nu[r[q]]);
           uv[q] = ldm(&A.u[r[q]]);
           f0v[q] = ldm(&A.f0[r[q]]);
@@ -653,8 +660,7 @@ __device__ __forceinline__ void schur_body_sr(const SchurArgs& A) {
           if (!ok[q]) continue;
           const float sn = rv[q] - a * nv[q], tn = uv[q] - a * acc[q];
           A.q[r[q]] = acc[q];
-          A.s[r[q]] = sn;
-          A.t[r[q]] = tn;
+          A.s_t[r[q]] = make_float2(sn, tn);
           const double sd = sn, td = tn, od = r0v[q], fd = f0v[q];
           s9[0] += td * sd;
           s9[1] += td * td;
@@ -668,8 +674,7 @@ __device__ __forceinline__ void schur_body_sr(const SchurArgs& A) {
         }
       });
       put_partials_bs<9, BS>(A, s9, buf);
-      end_phase(A, ph);
-      grid_barrier(A, ph);
+      grid_barrier(A, ph);  // (no progress release: every tile skips the same one)
       if (!ph.ok) break;
       get_totals_w0<9, BS>(A, s9, buf);
       buf ^= 1;
@@ -698,7 +703,7 @@ __device__ __forceinline__ void schur_body_sr(const SchurArgs& A) {
 #pragma unroll
       for (int q = 0; q < NR; ++q) {
         yv[q] = ldm(&A.y[r[q]]);
-        if (pending) yv[q] = yv[q] + a * ldm(&A.p[r[q]]) + w * ldm(&A.s[r[q]]);
+        if (pending) yv[q] = yv[q] + a * ldm(&A.p[r[q]]) + w * ldm(&A.s_t[r[q]]).x;
         si[q] = __ldg(&A.sinv[r[q]]);
       }
 #pragma unroll

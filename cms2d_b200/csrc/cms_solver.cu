@@ -99,7 +99,7 @@ struct cms_solver {
   int sc_sym = 0;    // Chat's pattern is structurally symmetric (d_sctr built)
   long long sc_nnz = 0, sc_e0b = 0;  // stored entries of Chat; couplings between group 0 and B
   int *d_sccol = nullptr, *d_sdep_ptr = nullptr, *d_sdep_idx = nullptr, *d_sctr = nullptr;
-  float *d_scoff = nullptr, *d_ssinv = nullptr;
+  float *d_scoff = nullptr, *d_ssinv = nullptr, *d_sst = nullptr;
   signed char* d_sccnt = nullptr;
   size_t cap_sdep = 0;
   long long reduced_fallbacks = 0;  // refinements finished on the exact factor after a bad inner correction
@@ -837,6 +837,7 @@ static int schur_pattern(Solver* S, int tiles) {
     }
     if (sym && (size_t)KC * nB <= (size_t)INT32_MAX) {
       CHK(S->alloc(&S->d_sctr, ctr.size()));
+      CHK(S->alloc(&S->d_sst, (size_t)2 * n));
       CMS_CUDA(cudaMemcpyAsync(S->d_sctr, ctr.data(), ctr.size() * sizeof(int), cudaMemcpyHostToDevice, S->stream));
       S->sc_sym = 1;
     }
@@ -948,7 +949,8 @@ static SchurArgs make_schur_args(Solver* S, int tiles, int maxit, double tol) {
   a.col = S->d_col; a.nlo = S->d_nlo; a.nup = S->d_nup; a.aoff = S->A32.aoff; a.sinv = S->d_ssinv;
   a.b = S->W32.b; a.x = S->W32.x;
   a.r = S->W32.r; a.r0 = S->W32.r0; a.p = S->W32.p; a.nu = S->W32.u; a.t = S->W32.v; a.y = S->W32.z;
-  a.ctr = S->d_sctr; a.u = S->W32.vv[1]; a.q = S->W32.vv[2]; a.s = S->W32.vv[3]; a.f0 = S->W32.vv[4];
+  a.ctr = S->d_sctr; a.u = S->W32.vv[1]; a.q = S->W32.vv[2]; a.f0 = S->W32.vv[3];
+  a.s_t = reinterpret_cast<float2*>(S->d_sst);
   a.part = S->d_ppart; a.bar = &S->d_st->bar; a.st = S->d_st;
   a.maxit = maxit; a.tol = tol; a.spin_limit = kSpinLimit;
   return a;
