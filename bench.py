@@ -835,6 +835,8 @@ def run_flow_ours(args):
                    "cells": g.ncells, "precision": args.precision, "ordering": "multicolor",
                    "solver": "BiCGStab + ILU(0)", "parallelism": f"replicas x{world}",
                    "solver_kernels": "per-phase launches" if args.multi_kernel else "persistent cooperative",
+                   "inner_solves": (f"tol {args.inner_tol:g}" if args.inner_tol > 0 else "adaptive tol")
+                                   + (f", cap {args.inner_max}" if args.inner_max > 0 else ", cap = remaining budget"),
                    "l2": "flushed between steps (256 MB write)"},
         "outer_iters_per_step": head["outer_iters"],
         "krylov_iters_per_step": head["krylov_iters_per_step"],
@@ -1125,9 +1127,11 @@ def main():
     ap.add_argument("--case", default="inlet", choices=["inlet", "basin", "flat"],
                     help="flow workload: 1M telescoping inlet (default), the 200x100 basin or an intertidal flat")
     ap.add_argument("--precision", default="fp32_refine", choices=["fp32_refine", "fp64"])
-    ap.add_argument("--inner-tol", type=float, default=1e-3,
-                    help="refinement: relative residual reduction asked of each FP32 inner solve")
-    ap.add_argument("--inner-max", type=int, default=50)
+    ap.add_argument("--inner-tol", type=float, default=0.0,
+                    help="refinement: relative residual reduction asked of each FP32 inner solve "
+                         "(0: adaptive, cms_solver_opts.inner_tol)")
+    ap.add_argument("--inner-max", type=int, default=0,
+                    help="refinement: iteration cap of each FP32 inner solve (0: the solve's remaining budget)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-parity", action="store_true", help="flow: skip the error check against the oracle fixture")
     ap.add_argument("--no-other-configs", action="store_true",

@@ -116,8 +116,6 @@ static int refine_batched(Ens* E, const std::vector<int>& act, const std::vector
     rm.info = infos[j];
     rm.maxit = S->opts.max_iters > 0 ? S->opts.max_iters : nswp[j];
     rm.tol = S->opts.tol > 0 ? S->opts.tol : 1e-3;
-    rm.itol = S->opts.inner_tol > 0 ? S->opts.inner_tol : 1e-3;
-    rm.imax = S->opts.inner_max > 0 ? S->opts.inner_max : 50;
     rm.rmax = S->opts.max_refine > 0 ? S->opts.max_refine : 30;
     const bool relax = S->opts.inner_relax && S->opts.ordering == CMS_ORDER_MULTICOLOR && P.G > 2;
     S->cur_fuse = 1;
@@ -162,6 +160,7 @@ static int refine_batched(Ens* E, const std::vector<int>& act, const std::vector
               (k_ir_scale<<<gsz(n), TPB, 0, S->stream>>>(n, S->W64.r, S->W32.b, S->d_st)));
       CMS_CUDA(cudaMemsetAsync(&S->d_st->bar, 0, sizeof(GridBar), S->stream));
       CMS_CUDA(cudaMemsetAsync(S->d_progress, 0, sizeof(unsigned int) * E->tiles[i] * kProgressStride, S->stream));
+      refine_inner_limits(S->opts, R[j]);
       if (schur) E->h_sargs[c] = make_schur_args(S, E->tiles[i], R[j].imax, R[j].itol);
       else E->h_args[c] = make_args<float>(S, S->A32, S->W32, E->tiles[i], R[j].imax, 2, R[j].itol, 1);
       for (int t = 0; t < E->tiles[i]; ++t) E->h_bmap[blocks++] = make_int2(c, t);

@@ -1367,8 +1367,8 @@ void cms_flow_default_opts(cms_flow_opts* o) {
   o->nswp_uv = 5;
   o->maxit = 0;
   o->skewcor = 1;
-  o->inner_tol = 1.0e-3;
-  o->inner_max = 50;
+  o->inner_tol = 0.0;
+  o->inner_max = 0;
   o->hdry = 0.05;
   o->ponding = 0;
   o->narrowchannels = 0;

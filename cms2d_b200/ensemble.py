@@ -41,7 +41,7 @@ class EnsembleModel:
     """Independent flow models (one per case) stepped together."""
 
     def __init__(self, cases, precision: str = "fp32_refine", nsolv: int = 3, tol: float = 1e-6, norm: int = 2,
-                 nswp_pp: int = 200, nswp_uv: int = 200, inner_tol: float = 1e-3, inner_max: int = 50, **kw):
+                 nswp_pp: int = 200, nswp_uv: int = 200, inner_tol: float = 0.0, inner_max: int = 0, **kw):
         L = _lib.lib()
         _bind(L)
         self.cases = list(cases)

@@ -74,7 +74,7 @@ class FlowModel:
 
     def __init__(self, case, nsolv: int = 4, ordering: str = "multicolor", precision: str = "fp64",
                  tol: float = 1e-3, norm: int = 1, nswp_pp: int | None = None, nswp_uv: int | None = None,
-                 maxit: int = 0, skewcor: bool = True, inner_tol: float = 1e-3, inner_max: int = 50,
+                 maxit: int = 0, skewcor: bool = True, inner_tol: float = 0.0, inner_max: int = 0,
                  multi_kernel: bool = False, hdry: float = 0.05, ponding: bool = False,
                  narrowchannels: bool = False, relaxsor: float = 1.8, ndsch: int = 4, reduced_layout: int = 0):
         L = _lib.lib()

@@ -75,7 +75,7 @@ class Solver:
     """
 
     def __init__(self, grid, iwet=None, ordering: str = "multicolor", precision: str = "fp64", tol: float = 1e-3,
-                 norm: int = 1, max_iters: int = 0, inner_tol: float = 1e-3, inner_max: int = 50,
+                 norm: int = 1, max_iters: int = 0, inner_tol: float = 0.0, inner_max: int = 0,
                  max_refine: int = 30, verify: bool = True, nsolv: int = NSOLV_DEFAULT,
                  multi_kernel: bool = False, inner_relax: int = 2, relaxsor: float = 1.8, nswp0_vel: int = 5,
                  reduced_layout: int = 0):

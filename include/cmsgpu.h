@@ -57,8 +57,13 @@ typedef struct cms_solver_opts {
   double tol;        /* relative tolerance; the reference hard-codes 1e-3
                         (pbicgstab.f90:95, pgmres.f90:19)                              */
   int max_iters;     /* > 0 overrides the nswp argument                                */
-  double inner_tol;  /* refinement: relative L2 reduction asked of each FP32 solve     */
-  int inner_max;     /* refinement: iteration cap of each FP32 solve                   */
+  double inner_tol;  /* refinement: relative L2 reduction asked of each FP32 solve;
+                        0 (default): 0.5 tol / (the outer relative residual before
+                        the solve), kept within [1e-5, 1e-3]                         */
+  int inner_max;     /* refinement: iteration cap of each FP32 solve; 0 (default):
+                        the solve's remaining iteration budget (nswp or max_iters
+                        minus the inner iterations so far); a cap > 0 is also
+                        bounded by that budget                                       */
   int max_refine;    /* refinement: cap on FP64 residual/correction steps              */
   int verify;        /* 1: compute the FP64 true residual after the solve (one extra
                         pass); 0: skip it (true_relres = -1)                           */
@@ -236,8 +241,8 @@ typedef struct cms_flow_opts {
   int nswp_uv;
   int maxit;         /* outer iterations; 0: 20 + ncells/10000 (flow.F90:784,792)  */
   int skewcor;       /* skewness corrections on telescoping grids (flow.F90:108)   */
-  double inner_tol;  /* refinement: FP32 solve tolerance                           */
-  int inner_max;
+  double inner_tol;  /* refinement: as cms_solver_opts.inner_tol (0: adaptive)     */
+  int inner_max;     /* refinement: as cms_solver_opts.inner_max (0: the budget)   */
   int multi_kernel;  /* solver kernels, as cms_solver_opts.multi_kernel            */
   double hdry;       /* drying depth (flow.F90:51, hmin = hdry); 0: 0.05 m          */
   int ponding;       /* keep isolated water bodies (flow.F90:54; default 0)         */

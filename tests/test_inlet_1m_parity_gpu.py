@@ -11,8 +11,8 @@ statistics over all cells.
 
 The GPU runs the bench's settings: BiCGStab + ILU(0) solves to a 1e-6
 relative L2 residual (cap 200), multicolour order, the outer loop ended by
-check_conv; once as the FP32 + FP64 refinement headline (inner tolerance
-1e-3, reduced inner form) and once as the plain FP64 drop-in.  Errors are
+check_conv; once as the FP32 + FP64 refinement headline (adaptive inner
+tolerance, reduced inner form) and once as the plain FP64 drop-in.  Errors are
 the largest difference over the sample cells and steps relative to the
 largest oracle value, |eta| for the water level and |(u, v)| for the
 velocity.  Bounds: 1e-6 for the FP64 drop-in, 1e-5 after refinement.
@@ -27,7 +27,7 @@ from cms2d_b200.flow import FlowModel
 
 FIXTURE = os.path.join(os.path.dirname(__file__), "golden", "inlet_1m_oracle.npz")
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not os.path.exists(FIXTURE), reason="oracle fixture not generated")]
-SETTINGS = dict(nsolv=3, tol=1e-6, norm=2, nswp_pp=200, nswp_uv=200, inner_tol=1e-3, inner_max=50)
+SETTINGS = dict(nsolv=3, tol=1e-6, norm=2, nswp_pp=200, nswp_uv=200)
 BOUND = {"fp64": 1e-6, "fp32_refine": 1e-5}
 
 
