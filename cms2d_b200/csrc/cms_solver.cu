@@ -951,6 +951,7 @@ static SchurArgs make_schur_args(Solver* S, int tiles, int maxit, double tol) {
   a.r = S->W32.r; a.r0 = S->W32.r0; a.p = S->W32.p; a.nu = S->W32.u; a.t = S->W32.v; a.y = S->W32.z;
   a.ctr = S->d_sctr; a.u = S->W32.vv[1]; a.q = S->W32.vv[2]; a.f0 = S->W32.vv[3];
   a.s_t = reinterpret_cast<float2*>(S->d_sst);
+  a.yb = S->W32.vv[4];
   a.part = S->d_ppart; a.bar = &S->d_st->bar; a.st = S->d_st;
   a.maxit = maxit; a.tol = tol; a.spin_limit = kSpinLimit;
   return a;
