@@ -9,13 +9,23 @@ reference's small guards stall it), the outer loop ended by check_conv;
 water level and velocities at 8192 seeded cells after every step, and
 statistics over all cells.
 
-The GPU runs the bench's settings: BiCGStab + ILU(0) solves to a 1e-6
-relative L2 residual (cap 200), multicolour order, the outer loop ended by
-check_conv; once as the FP32 + FP64 refinement headline (adaptive inner
-tolerance, reduced inner form) and once as the plain FP64 drop-in.  Errors are
-the largest difference over the sample cells and steps relative to the
-largest oracle value, |eta| for the water level and |(u, v)| for the
-velocity.  Bounds: 1e-6 for the FP64 drop-in, 1e-5 after refinement.
+Two settings, each for the FP32 + FP64 refinement headline (reduced inner
+form, adaptive inner tolerance) and for the plain FP64 drop-in:
+
+* the oracle's own (BiCGStab + ILU(0) solves to a 1e-9 relative L2 residual
+  or 600 iterations, multicolour order): both precisions take the oracle's
+  outer iteration counts step by step, and the bounds are 1e-7 for the water
+  level and 2e-5 for the velocity (measured on a B200: at most 6e-9 and 1e-5,
+  the velocity's largest in the first step from the cold start);
+* the bench's (1e-6 or 200 iterations): the pressure-correction solves end at
+  the 200-iteration cap (median relative residual ~3e-4 for both precisions,
+  as for the FP64 drop-in at these settings), so the outer loop can
+  stop an iteration earlier than the oracle's; bounds 1e-6 and 2e-4
+  (measured: 6e-8 and 8e-5).
+
+Errors are the largest difference over the sample cells and steps relative
+to the largest oracle value, |eta| for the water level and |(u, v)| for the
+velocity; the whole-grid statistics are compared too.
 """
 import os
 
@@ -27,8 +37,9 @@ from cms2d_b200.flow import FlowModel
 
 FIXTURE = os.path.join(os.path.dirname(__file__), "golden", "inlet_1m_oracle.npz")
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not os.path.exists(FIXTURE), reason="oracle fixture not generated")]
-SETTINGS = dict(nsolv=3, tol=1e-6, norm=2, nswp_pp=200, nswp_uv=200)
-BOUND = {"fp64": 1e-6, "fp32_refine": 1e-5}
+SETTINGS = {"oracle": dict(nsolv=3, tol=1e-9, norm=2, nswp_pp=600, nswp_uv=600),
+            "bench": dict(nsolv=3, tol=1e-6, norm=2, nswp_pp=200, nswp_uv=200)}
+BOUND = {"oracle": (1e-7, 2e-5), "bench": (1e-6, 2e-4)}  # (water level, velocity)
 
 
 @pytest.fixture(scope="module")
@@ -39,17 +50,21 @@ def inlet():
     return case, z
 
 
+@pytest.mark.parametrize("setting", ["oracle", "bench"])
 @pytest.mark.parametrize("precision", ["fp32_refine", "fp64"])
-def test_inlet_1m_matches_fp64_oracle(inlet, precision):
+def test_inlet_1m_matches_fp64_oracle(inlet, precision, setting):
     case, z = inlet
     n = case.grid.ncells
     idx = z["sample"]
-    m = FlowModel(case, precision=precision, **SETTINGS)
+    b_eta, b_vel = BOUND[setting]
+    m = FlowModel(case, precision=precision, **SETTINGS[setting])
     m.init()
     e_eta = e_vel = 0.0
+    niter = []
     for s in range(z["eta"].shape[0]):
         info = m.step()
         assert info["status"] == 0 and info["iconv"] == 2, info
+        niter.append(int(info["niter"]))
         eta, u, v = (m.get(k)[:n] for k in ("eta", "u", "v"))
         eo, uo, vo = z["eta"][s], z["u"][s], z["v"][s]
         e_eta = max(e_eta, float(np.abs(eta[idx] - eo).max() / np.abs(eo).max()))
@@ -58,8 +73,12 @@ def test_inlet_1m_matches_fp64_oracle(inlet, precision):
         h = m.get("h")[:n]
         st = np.array([eta.mean(), eta.min(), eta.max(), np.sqrt(np.mean(eta * eta)), np.abs(u).max(),
                        np.abs(v).max(), h.sum()])
-        np.testing.assert_allclose(st, z["stats"][s], rtol=10 * BOUND[precision], atol=1e-12)
+        np.testing.assert_allclose(st, z["stats"][s], rtol=b_vel, atol=1e-12)
     m.close()
-    print(precision, {"eta_max_rel": e_eta, "vel_max_rel": e_vel})
-    assert e_eta <= BOUND[precision]
-    assert e_vel <= BOUND[precision]
+    print(precision, setting, {"eta_max_rel": e_eta, "vel_max_rel": e_vel, "outer": niter})
+    if setting == "oracle":
+        assert niter == [int(q) for q in z["niter"]]
+    else:
+        assert all(abs(a - int(b)) <= 1 for a, b in zip(niter, z["niter"]))
+    assert e_eta <= b_eta
+    assert e_vel <= b_vel
