@@ -120,26 +120,32 @@ __global__ void __launch_bounds__(TPB) k_schur_diag(int n, int g1, int KL, const
 
 // Chat's off-diagonals of reduced row i (r = g1 + i):
 // coff_rk = (aoff_rk [k in B] + sum_{j in group 0} aoff_rj aoff_jk / d_j) / s_k.
-__global__ void __launch_bounds__(TPB) k_schur_off(int n, int g1, int nB, int KL, int KC,
+// A thread's columns and FP64 accumulators live in shared memory, so four
+// blocks fit on an SM (with them in registers the kernel took 110 registers
+// and two blocks; its chains of dependent gathers need the extra warps).
+__global__ void __launch_bounds__(TPB, 4) k_schur_off(int n, int g1, int nB, int KL, int KC,
                                                    const int* __restrict__ col, const signed char* __restrict__ nlo,
                                                    const signed char* __restrict__ nup,
                                                    const float* __restrict__ aoff, const float* __restrict__ diag,
                                                    const float* __restrict__ sinv, const int* __restrict__ ccol,
                                                    const signed char* __restrict__ ccnt, float* __restrict__ coff) {
+  __shared__ double s_acc[KSC][TPB];  // this thread's columns and accumulators: column threadIdx.x
+  __shared__ int s_cc[KSC][TPB];
+  double* acc = &s_acc[0][threadIdx.x];
+  int* cc = &s_cc[0][threadIdx.x];
   for (int i = blockIdx.x * TPB + threadIdx.x; i < nB; i += gridDim.x * TPB) {
     const int r = g1 + i;
     const int kc = ccnt[i];
-    int cc[KSC];
-    double acc[KSC];
-#pragma unroll
-    for (int q = 0; q < KSC; ++q) {
-      cc[q] = q < kc ? ccol[(size_t)q * nB + i] : -1;
-      acc[q] = 0.0;
+    for (int q = 0; q < kc; ++q) {
+      cc[q * TPB] = ccol[(size_t)q * nB + i];
+      acc[q * TPB] = 0.0;
     }
-    auto add = [&](int k, double v) {
-#pragma unroll
-      for (int q = 0; q < KSC; ++q)
-        if (cc[q] == k) acc[q] += v;
+    auto add = [&](int k, double v) {  // a row's columns are distinct
+      for (int q = 0; q < kc; ++q)
+        if (cc[q * TPB] == k) {
+          acc[q * TPB] += v;
+          break;
+        }
     };
     const int kl = nlo[r], ku = nup[r];
     for (int s = 0; s < kl + ku; ++s) {
@@ -158,9 +164,8 @@ __global__ void __launch_bounds__(TPB) k_schur_off(int n, int g1, int nB, int KL
         if (k2 != r) add(k2, w * (double)aoff[e2]);
       }
     }
-#pragma unroll
-    for (int q = 0; q < KSC; ++q)
-      if (q < KC) coff[(size_t)q * nB + i] = q < kc ? (float)(acc[q] * (double)sinv[cc[q]]) : 0.0f;
+    for (int q = 0; q < KC; ++q)
+      coff[(size_t)q * nB + i] = q < kc ? (float)(acc[q * TPB] * (double)sinv[cc[q * TPB]]) : 0.0f;
   }
 }
 
