@@ -193,8 +193,9 @@ __device__ __forceinline__ void put_partials_bs(const SchurArgs& A, double (&v)[
 
 // After a grid barrier: the grid totals, value q summed by warp q (lane l
 // adds tiles l, l + 32, ... in that order, then a butterfly), so every block
-// forms the same bits; then shared with the block.  Four tiles' loads are
-// issued before their adds.
+// forms the same bits; then shared with the block.  A lane's loads for up
+// to 256 tiles are issued before their adds (one round trip; the missing ones
+// add 0, which changes no bits).
 template <int NS, int BS>
 __device__ __forceinline__ void get_totals_w0(const SchurArgs& A, double (&tot)[NS], int buf) {
   constexpr int NW = BS / 32;
@@ -203,16 +204,13 @@ __device__ __forceinline__ void get_totals_w0(const SchurArgs& A, double (&tot)[
   for (int q = wid; q < NS; q += NW) {
     const double* src = A.part + ((size_t)buf * NSMAX + q) * nt;
     double acc = 0.0;
-    int b = lane;
-    for (; b + 96 < nt; b += 128) {
-      const double v0 = __ldcg(src + b), v1 = __ldcg(src + b + 32), v2 = __ldcg(src + b + 64),
-                   v3 = __ldcg(src + b + 96);
-      acc += v0;
-      acc += v1;
-      acc += v2;
-      acc += v3;
+    for (int b = lane; b < nt; b += 256) {
+      double v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) v[u] = b + 32 * u < nt ? __ldcg(src + b + 32 * u) : 0.0;
+#pragma unroll
+      for (int u = 0; u < 8; ++u) acc += v[u];
     }
-    for (; b < nt; b += 32) acc += __ldcg(src + b);
     acc = warp_sum(acc);
     if (lane == 0) bc[q] = acc;
   }
