@@ -1465,11 +1465,11 @@ void orcf_set_wetdry(void* h, int ponding, int narrowchannels) {
   f->P.narrowchannels = narrowchannels != 0;
 }
 int orcf_njoint(void* h) { return (int)static_cast<Flow*>(h)->idjoint.size(); }
+// ADVECTION_SCHEME card (flow.F90:533-545): 0 none .. 4 exponential
+void orcf_set_scheme(void* h, int ndsch) { static_cast<Flow*>(h)->P.ndsch = ndsch; }
 // DRYING_DEPTH card: hmin = hdry, hdry1 = 5 hdry, hdry2 = 2 hdry (flow.F90:686-693).
 // The one- and two-cell depths only matter with narrow channels off, when
 // flow.F90:686-689 overwrites the DRYING_DEPTH_ONE_CELL/TWO_CELL cards.
-// ADVECTION_SCHEME card (flow.F90:533-545): 0 none .. 4 exponential
-void orcf_set_scheme(void* h, int ndsch) { static_cast<Flow*>(h)->P.ndsch = ndsch; }
 void orcf_set_hdry(void* h, double hdry) {
   auto* f = static_cast<Flow*>(h);
   f->P.hmin = hdry; f->P.hdry = hdry; f->P.hdry1 = 5.0 * hdry; f->P.hdry2 = 2.0 * hdry;
