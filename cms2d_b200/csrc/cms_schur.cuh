@@ -53,6 +53,7 @@ namespace cms {
 
 constexpr int KSC = 16;  // largest off-diagonal count of a reduced row the kernels take
 constexpr double kDiverge = 100.0;  // single-reduction form: stop when the residual is this many times the best
+constexpr int kStall = 100;         // single-reduction form: stop after this many iterations without a new best
 
 struct SchurArgs {
   int n, g1, nB, KL, G;
@@ -508,7 +509,10 @@ __device__ __forceinline__ void schur_body(const SchurArgs& A) {
 // drift to 1e-2; the refinement then restarts from the best iterate's
 // residual (measured: median/90th/largest final residuals of those solves
 // 3.3e-4/1.4e-2/6.9e-2 against 4.4e-4/2.1e-2/0.19 returning the last iterate,
-// same step time; stopping at 10 times the best was 3 % slower).  Y overwrites s and t of
+// same step time; stopping at 10 times the best was 3 % slower).  kStall
+// iterations without a smaller residual end it too: an FP32 solve asked for
+// more than its arithmetic can reach would otherwise spend the whole budget
+// of an outer solve (a 1e-9 solve's 600 iterations) on one restart.  Y overwrites s and t of
 // its own rows: every neighbour that gathers them in X has finished X (the
 // neighbour wait), and the next X starts after the grid barrier.
 template <int BS, int NR>
@@ -613,6 +617,7 @@ __device__ __forceinline__ void schur_body_sr(const SchurArgs& A) {
   // squared residual norms: the tests below need no square root or division
   const double tol2 = (A.tol * res0) * (A.tol * res0);
   double rr_last = res0 * res0, best2 = rr_last;
+  int it_best = 0;
   int it = 0, buf = 1;
   bool pending = false;  // an iteration's y update not yet applied
   bool save = false;     // the pending iterate has the smallest residual so far (yb holds the best otherwise)
@@ -704,13 +709,18 @@ __device__ __forceinline__ void schur_body_sr(const SchurArgs& A) {
       if (!isfinite(rr) || !isfinite(omg) || !isfinite(rho1)) { rel = rr; nonfinite = 1; break; }
       pending = true;  // y += alf p + omg s is valid even at a breakdown below
       save = rr < best2;
-      if (save) best2 = rr;
+      if (save) {
+        best2 = rr;
+        it_best = it;
+      }
       if (rr < tol2) { converged = 1; continue; }
       // breakdown of the next step (omg = 0, r0.r = 0 or r0.nu = 0): stop with this iterate
       if (omg == 0.0 || rho1 == 0.0) break;
       // divergence: the residual kDiverge times the best one; the best iterate
       // is the result (the refinement restarts from its residual)
       if (rr > (kDiverge * kDiverge) * best2) break;
+      // stagnation: kStall iterations without a smaller residual
+      if (it - it_best >= kStall) break;
       bet = (rho1 / rho) * (alf / omg);
       rho = rho1;
       const double tau = (s9[5] - omg * s9[6]) + bet * (s9[8] - omg * s9[7]);

@@ -59,7 +59,7 @@ typedef struct cms_solver_opts {
   int max_iters;     /* > 0 overrides the nswp argument                                */
   double inner_tol;  /* refinement: relative L2 reduction asked of each FP32 solve;
                         0 (default): 0.5 tol / (the outer relative residual before
-                        the solve), kept within [1e-5, 1e-3]                         */
+                        the solve), kept within [1e-6, 1e-3]                         */
   int inner_max;     /* refinement: iteration cap of each FP32 solve; 0 (default):
                         the solve's remaining iteration budget (nswp or max_iters
                         minus the inner iterations so far); a cap > 0 is also
