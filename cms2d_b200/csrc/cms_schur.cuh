@@ -25,9 +25,12 @@
 // rows.  Vectors are indexed by device row (the B rows of the refinement's
 // FP32 work arrays).
 //
-// The persistent kernel.  One block per tile (the tiles of the persistent
-// ILU(0) kernel: tile t's B rows are toff[g][t]..toff[g][t+1] for g >= 1), a
-// BiCGStab iteration is three phases:
+// The persistent kernels.  One block per tile (the tiles of the persistent
+// ILU(0) kernel: tile t's B rows are toff[g][t]..toff[g][t+1] for g >= 1).
+// Two iteration forms: the single-reduction form (schur_body_sr, the
+// default layouts; one grid barrier per iteration, described at its
+// definition) and the three-phase form (schur_body), a BiCGStab iteration
+// in three phases:
 //   P0  the previous iteration's y/r update and the new search direction p
 //       (own rows, no neighbour values);
 //   A   nu = Chat p (after the neighbour tiles have finished P0) and r0.nu,
@@ -38,14 +41,14 @@
 // next r0.r from r0.s - w r0.t.  Waits and barriers are those of the
 // persistent ILU(0) kernel (bounded, cms_persist.cuh).
 //
-// Measured against this layout on one B200, same box, 1M-cell inlet flow
-// step (timesteps/s): 5.50 here; couplings packed as one 8-byte (column,
-// value) element and (r, nu) interleaved for one 8-byte gather, 5.24-5.33;
-// P0 and its neighbour wait dropped by forming each gathered neighbour's new
-// direction from a 16-byte (r, nu, p, t) gather in alternating buffers,
-// 4.72; the tile's columns and counts cached in shared memory for the
-// launch, 5.10 (the fill costs every launch and the velocity solves' launches
-// are short).  Separate 4-byte streams keep more loads in flight per thread.
+// Measured on the three-phase form, one B200, same box, 1M-cell inlet flow
+// step (timesteps/s): 5.50 as written; couplings packed as one 8-byte
+// (column, value) element and (r, nu) interleaved for one 8-byte gather,
+// 5.24-5.33; P0 and its neighbour wait dropped by forming each gathered
+// neighbour's new direction from a 16-byte (r, nu, p, t) gather in
+// alternating buffers, 4.72; the tile's columns and counts cached in shared
+// memory for the launch, 5.10.  Separate 4-byte streams keep more loads in
+// flight per thread.
 #pragma once
 #include "cms_persist.cuh"
 
