@@ -920,14 +920,15 @@ static int schur_numeric(Solver* S) {
 // x_B, then x_0 from b, 1/d and the group-0 rows' couplings).  Single-
 // reduction form (sr): the start adds the transposed product (r0, count,
 // Chat, transpose slots; f0, u, nu, p written), an iteration is X (s, t, y,
-// p, nu, q, count, Chat; y, u, p, nu written) and Y (s, t, nu, u, r0, f0,
-// count, Chat; q, s, t written), the end reads y, p, s.
+// p, nu, q, Chat; y, u, p, nu written) and Y (s, t, nu, u, r0, f0, Chat; q,
+// s, t written), the end reads y, p, s.  Chat counts its stored couplings
+// only (the kernel also reads the padding slots, which are not needed).
 static double schur_bytes(const Solver* S, int iters, int sr) {
   const HostPattern& P = S->hp;
   const double n = P.n, g1 = P.gstart[1], nB = n - g1, C = 8.0 * (double)S->sc_nnz, E = 8.0 * (double)S->sc_e0b;
   if (sr) {
     const double start = 4.0 * n + 4.0 * g1 + E + nB + 12.0 * nB + (5.0 * nB + C + 4.0 * (double)S->sc_nnz + 16.0 * nB);
-    const double it = (41.0 * nB + C) + (37.0 * nB + C);
+    const double it = (40.0 * nB + C) + (36.0 * nB + C);
     const double end = 20.0 * nB + 9.0 * g1 + E + 4.0 * nB + 4.0 * g1;
     return start + iters * it + end;
   }
