@@ -72,6 +72,12 @@ class Solver:
     inner_relax: FP32 inner BiCGStab of refinement on a multicolour ordering:
                2 the reduced (Schur complement) system, 1 the two-phase
                factor, 0 the exact multicolour ILU(0) (True/False mean 1/0).
+    inner_tol/inner_max: refinement's inner solves; 0 (default): each may use
+               the solve's remaining iteration budget and is asked for
+               0.5 tol / (outer residual so far) within [1e-6, 1e-3].
+    reduced_layout: block/row layout and iteration form of the reduced inner
+               solve (0 auto: 1024 threads x 2 rows, single reduction;
+               cms_solver_opts.reduced_layout).
     """
 
     def __init__(self, grid, iwet=None, ordering: str = "multicolor", precision: str = "fp64", tol: float = 1e-3,
