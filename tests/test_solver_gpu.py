@@ -2,7 +2,7 @@
 
 Tolerances: FP64 solution within 1e-10 relative of the oracle and the same
 iteration count; FP32 within 1e-4; FP32+FP64-refinement within 1e-5 of the
-FP64 oracle solution (the north-star bound for the refined solver).
+FP64 oracle solution (the accuracy required of the refined solver).
 """
 import numpy as np
 import pytest
