@@ -6,6 +6,13 @@ the solve).  Its backward pass solves A^T lam = dL/dx on the GPU
 (``cms_solver_adjoint_dev_d``: ILU(0)-BiCGStab on the transposed system) and
 returns dL/dacoef, dL/dss and dL/dsp in the solve() layout.  FP64 CUDA
 tensors, natural order, acoef [ncellsD, nmaxfaces].
+
+``friction_sink_fn(coefman, h, uv, area, spuv0)`` is the momentum equations'
+bottom-friction sink sp = spuv0 - Cd(n) |u| A with the Manning closure
+(``cms_fric_sink_dev_d``); its backward pass (``cms_fric_sink_adjoint_dev_d``)
+turns dL/dsp into dL/dn.  Chained with ``solve_fn`` it gives the gradient of
+a loss on a momentum solve's solution with respect to per-cell Manning's n,
+with the depth, the speed |u| and the cell areas held fixed.
 """
 from __future__ import annotations
 
@@ -21,6 +28,8 @@ def _bind(L):
         return
     vp, d, i = C.c_void_p, C.c_double, C.c_int
     L.cms_solver_adjoint_dev_d.argtypes = [vp] * 6 + [d, vp, d, i] + [vp] * 4 + [C.POINTER(_lib.SolveInfo)]
+    L.cms_fric_sink_dev_d.argtypes = [i, d] + [vp] * 7
+    L.cms_fric_sink_adjoint_dev_d.argtypes = [i, d] + [vp] * 7
     L._adj_bound = True
 
 
@@ -67,3 +76,48 @@ def solve_fn(solver, acoef, ss, sp, phi, relax: float = 1.0, nswp: int = 2000, t
     tolerance, norm 2, FP64 for gradients); tol and nswp bound the adjoint
     solve."""
     return _SolveFn.apply(acoef, ss, sp, phi, solver, relax, nswp, tol)
+
+
+class _FricSinkFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, coefman, h, uv, area, spuv0, grav):
+        n = coefman.numel()
+        sp = spuv0.detach().clone()
+        L = _lib.lib()
+        _bind(L)
+        stream = C.c_void_p(torch.cuda.current_stream(coefman.device).cuda_stream)
+        rc = L.cms_fric_sink_dev_d(n, float(grav), _ptr(coefman.detach()), _ptr(h), _ptr(uv), _ptr(area),
+                                   _ptr(spuv0.detach()), _ptr(sp), stream)
+        _lib.check(rc, "cms_fric_sink_dev_d")
+        ctx.save_for_backward(coefman.detach(), h, uv, area)
+        ctx.grav = float(grav)
+        return sp
+
+    @staticmethod
+    def backward(ctx, gsp):
+        coefman, h, uv, area = ctx.saved_tensors
+        n = coefman.numel()
+        g = gsp.detach().to(torch.float64).contiguous()
+        gn = torch.empty_like(coefman)
+        L = _lib.lib()
+        _bind(L)
+        stream = C.c_void_p(torch.cuda.current_stream(coefman.device).cuda_stream)
+        rc = L.cms_fric_sink_adjoint_dev_d(n, ctx.grav, _ptr(coefman), _ptr(h), _ptr(uv), _ptr(area), _ptr(g),
+                                           _ptr(gn), stream)
+        _lib.check(rc, "cms_fric_sink_adjoint_dev_d")
+        gsp0 = g if ctx.needs_input_grad[4] else None
+        return gn, None, None, None, gsp0, None
+
+
+def friction_sink_fn(coefman, h, uv, area, spuv0, grav: float = 9.81):
+    """sp = spuv0 - Cd(n) |u| A over the first coefman.numel() cells (the
+    rest of spuv0, e.g. dummy cells, is copied), with gradients for coefman
+    (Manning's n) and spuv0.  FP64 CUDA tensors; h, uv and area are held
+    fixed."""
+    for t in (coefman, h, uv, area, spuv0):
+        if t.dtype != torch.float64 or not t.is_cuda or not t.is_contiguous():
+            raise ValueError("friction_sink_fn takes contiguous float64 CUDA tensors")
+    if not (h.numel() >= coefman.numel() and uv.numel() >= coefman.numel() and area.numel() >= coefman.numel()
+            and spuv0.numel() >= coefman.numel()):
+        raise ValueError("h, uv, area and spuv0 need at least coefman.numel() entries")
+    return _FricSinkFn.apply(coefman, h, uv, area, spuv0, grav)

@@ -143,7 +143,72 @@ static int solve_adjoint(Solver* S, const double* acoef, const double* ss, const
   return info->status;
 }
 
+// Bottom-friction sink of the momentum assembly and its adjoint.  Manning
+// closure (fric_eval, friction.F90:647-662; fric_lib.f90:965-966) as the
+// flow step evaluates it (kf_fric_vis):
+//   Cd = g n^2 / hh^p,   hh = max(min(10, h), 0.1 n),   p = 0.3333,
+// and the sink of coeffsourcesink_uv (flow_imp.F90:409-574, kf_coef_uv):
+//   sp = spuv0 - Cd |u| A.
+// With h, |u| and A held fixed, dsp/dn = -|u| A dCd/dn, where dCd/dn =
+// 2 g n / hh^p on the depth branch and (2 - p) Cd / n where 0.1 n is the
+// larger (a kink where the two meet; the depth branch is taken there).
+constexpr double kManningP = 0.3333;
+
+__device__ __forceinline__ double manning_cd(double g, double n, double h, double* dcd) {
+  const double hd = fmin(10.0, h);
+  const double hh = fmax(hd, 0.1 * n);
+  const double cd = g * n * n / pow(hh, kManningP);
+  if (dcd) *dcd = (0.1 * n > hd) ? (2.0 - kManningP) * cd / n : 2.0 * g * n / pow(hh, kManningP);
+  return cd;
+}
+
+__global__ void __launch_bounds__(TPB) k_fric_sink(int n, double g, const double* __restrict__ coefman,
+                                                   const double* __restrict__ h, const double* __restrict__ uv,
+                                                   const double* __restrict__ area,
+                                                   const double* __restrict__ spuv0, double* __restrict__ sp) {
+  for (int i = blockIdx.x * TPB + threadIdx.x; i < n; i += gridDim.x * TPB)
+    sp[i] = spuv0[i] - manning_cd(g, coefman[i], h[i], nullptr) * uv[i] * area[i];
+}
+
+__global__ void __launch_bounds__(TPB) k_fric_sink_adjoint(int n, double g, const double* __restrict__ coefman,
+                                                           const double* __restrict__ h,
+                                                           const double* __restrict__ uv,
+                                                           const double* __restrict__ area,
+                                                           const double* __restrict__ gsp,
+                                                           double* __restrict__ gn) {
+  for (int i = blockIdx.x * TPB + threadIdx.x; i < n; i += gridDim.x * TPB) {
+    double dcd;
+    manning_cd(g, coefman[i], h[i], &dcd);
+    gn[i] = -gsp[i] * uv[i] * area[i] * dcd;
+  }
+}
+
+static int fric_launch_check(const char* what) {
+  const cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) return CMS_OK;
+  std::snprintf(g_last_error, sizeof(g_last_error), "%s: %s", what, cudaGetErrorString(e));
+  return CMS_DEVICE_ERROR;
+}
+
 }  // namespace cms
+
+extern "C" int cms_fric_sink_dev_d(int n, double grav, const double* coefman, const double* h, const double* uv,
+                                   const double* area, const double* spuv0, double* sp, void* stream) {
+  if (n <= 0 || !coefman || !h || !uv || !area || !spuv0 || !sp) return CMS_BAD_ARGUMENT;
+  const int blocks = std::max(1, std::min((n + cms::TPB - 1) / cms::TPB, 148 * 8));
+  cms::k_fric_sink<<<blocks, cms::TPB, 0, (cudaStream_t)stream>>>(n, grav, coefman, h, uv, area, spuv0, sp);
+  return cms::fric_launch_check("cms_fric_sink_dev_d");
+}
+
+extern "C" int cms_fric_sink_adjoint_dev_d(int n, double grav, const double* coefman, const double* h,
+                                           const double* uv, const double* area, const double* grad_sp,
+                                           double* grad_coefman, void* stream) {
+  if (n <= 0 || !coefman || !h || !uv || !area || !grad_sp || !grad_coefman) return CMS_BAD_ARGUMENT;
+  const int blocks = std::max(1, std::min((n + cms::TPB - 1) / cms::TPB, 148 * 8));
+  cms::k_fric_sink_adjoint<<<blocks, cms::TPB, 0, (cudaStream_t)stream>>>(n, grav, coefman, h, uv, area, grad_sp,
+                                                                          grad_coefman);
+  return cms::fric_launch_check("cms_fric_sink_adjoint_dev_d");
+}
 
 extern "C" int cms_solver_adjoint_dev_d(cms_solver* s, const double* acoef, const double* ss, const double* sp,
                                         const double* phi0, const double* x, double relax, const double* g,

@@ -200,6 +200,19 @@ int cms_solver_adjoint_dev_d(cms_solver* s, const double* acoef, const double* s
                              const double* phi0, const double* x, double relax, const double* g, double tol,
                              int maxit, double* lam, double* grad_acoef, double* grad_ss, double* grad_sp,
                              cms_solve_info* info);
+/* Bottom-friction sink of the momentum equations and its adjoint (the
+ * adjoint has no counterpart in the reference), FP64 device pointers over n
+ * cells, on stream (a cudaStream_t, NULL: the legacy default stream; the
+ * calls do not wait).  Forward: sp = spuv0 - Cd(n) |u| A with the Manning
+ * closure Cd = g n^2 / max(min(10, h), 0.1 n)^0.3333 (fric_eval,
+ * friction.F90:647-662, fric_lib.f90:965-966; the sink of coeffsourcesink_uv,
+ * flow_imp.F90:409-574), coefman = n, uv = |u|, area = A.  Adjoint: given
+ * grad_sp = dL/dsp (from cms_solver_adjoint_dev_d), writes
+ * grad_coefman = dL/dn = -grad_sp |u| A dCd/dn with h, |u| and A held fixed. */
+int cms_fric_sink_dev_d(int n, double grav, const double* coefman, const double* h, const double* uv,
+                        const double* area, const double* spuv0, double* sp, void* stream);
+int cms_fric_sink_adjoint_dev_d(int n, double grav, const double* coefman, const double* h, const double* uv,
+                                const double* area, const double* grad_sp, double* grad_coefman, void* stream);
 /* Blocks (tiles) of the handle's persistent BiCGStab launch: 0 restores the
  * default (the device's resident capacity, at most one block per 256 rows);
  * returns the count in use, or a negative CMS_* code. */
