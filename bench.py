@@ -505,11 +505,11 @@ FLOW_SOLVER = dict(nsolv=3, tol=1e-6, norm=2)
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one launch
 # of the reduced inner BiCGStab kernel on the 999,678-cell inlet flow step:
 # the mean over 30 consecutive launches of this workload captured by ncu
-# (from the second step on: velocity solves at ~130 MB each and
-# pressure-correction solves at 560-710 MB; replayed from a cold L2).  The
-# kernel's working set (~70 MB) stays mostly in the 126 MB L2, so a launch's
-# DRAM traffic is a few reads of it, far below its algorithmic bytes.
-REDUCED_DRAM_BYTES_PER_LAUNCH = 276_822_221
+# (velocity solves at 130-137 MB each, pressure-correction solves at
+# 765-969 MB; replayed from a cold L2).  The kernel's working set (~70 MB)
+# stays mostly in the 126 MB L2, so a launch's DRAM traffic is a few reads of
+# it, far below its algorithmic bytes.
+REDUCED_DRAM_BYTES_PER_LAUNCH = 369_075_183
 REDUCED_CAPTURE_CELLS = 999_678
 
 
