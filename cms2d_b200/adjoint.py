@@ -13,6 +13,12 @@ bottom-friction sink sp = spuv0 - Cd(n) |u| A with the Manning closure
 turns dL/dsp into dL/dn.  Chained with ``solve_fn`` it gives the gradient of
 a loss on a momentum solve's solution with respect to per-cell Manning's n,
 with the depth, the speed |u| and the cell areas held fixed.
+
+``momentum_coef_fn(ncface, ncells, visk, hk, ds, flux, ndsch)`` is the
+momentum equations' face coefficients acoef = scheme(visk hk ds, flux)
+(``cms_momentum_coef_dev_d``, the ADVECTION_SCHEME functions); its backward
+pass (``cms_momentum_coef_adjoint_dev_d``) gives dL/dvisk, dL/dhk and
+dL/dflux from dL/dacoef.
 """
 from __future__ import annotations
 
@@ -30,6 +36,8 @@ def _bind(L):
     L.cms_solver_adjoint_dev_d.argtypes = [vp] * 6 + [d, vp, d, i] + [vp] * 4 + [C.POINTER(_lib.SolveInfo)]
     L.cms_fric_sink_dev_d.argtypes = [i, d] + [vp] * 7
     L.cms_fric_sink_adjoint_dev_d.argtypes = [i, d] + [vp] * 7
+    L.cms_momentum_coef_dev_d.argtypes = [i, i, i] + [vp] * 7
+    L.cms_momentum_coef_adjoint_dev_d.argtypes = [i, i, i] + [vp] * 10
     L._adj_bound = True
 
 
@@ -121,3 +129,47 @@ def friction_sink_fn(coefman, h, uv, area, spuv0, grav: float = 9.81):
             and spuv0.numel() >= coefman.numel()):
         raise ValueError("h, uv, area and spuv0 need at least coefman.numel() entries")
     return _FricSinkFn.apply(coefman, h, uv, area, spuv0, grav)
+
+
+class _MomCoefFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, visk, hk, flux, ds, ncface, ncells, ndsch):
+        nD, nmf = visk.shape
+        acoef = torch.zeros_like(visk)
+        L = _lib.lib()
+        _bind(L)
+        stream = C.c_void_p(torch.cuda.current_stream(visk.device).cuda_stream)
+        rc = L.cms_momentum_coef_dev_d(int(ncells), int(nmf), int(ndsch), _ptr(ncface), _ptr(visk.detach()),
+                                       _ptr(hk.detach()), _ptr(ds), _ptr(flux.detach()), _ptr(acoef), stream)
+        _lib.check(rc, "cms_momentum_coef_dev_d")
+        ctx.save_for_backward(visk.detach(), hk.detach(), flux.detach(), ds, ncface)
+        ctx.ncells, ctx.ndsch = int(ncells), int(ndsch)
+        return acoef
+
+    @staticmethod
+    def backward(ctx, ga):
+        visk, hk, flux, ds, ncface = ctx.saved_tensors
+        g = ga.detach().to(torch.float64).contiguous()
+        gv = torch.zeros_like(visk) if ctx.needs_input_grad[0] else None
+        gh = torch.zeros_like(hk) if ctx.needs_input_grad[1] else None
+        gf = torch.zeros_like(flux) if ctx.needs_input_grad[2] else None
+        L = _lib.lib()
+        _bind(L)
+        stream = C.c_void_p(torch.cuda.current_stream(visk.device).cuda_stream)
+        rc = L.cms_momentum_coef_adjoint_dev_d(ctx.ncells, int(visk.shape[1]), ctx.ndsch, _ptr(ncface), _ptr(visk),
+                                               _ptr(hk), _ptr(ds), _ptr(flux), _ptr(g), _ptr(gv), _ptr(gh),
+                                               _ptr(gf), stream)
+        _lib.check(rc, "cms_momentum_coef_adjoint_dev_d")
+        return gv, gh, gf, None, None, None, None
+
+
+def momentum_coef_fn(ncface, ncells: int, visk, hk, ds, flux, ndsch: int = 4):
+    """acoef [ncellsD, nmaxfaces] = scheme(visk hk ds, flux) on the faces of
+    the active cells (zero elsewhere), with gradients for visk, hk and flux.
+    FP64 CUDA tensors of acoef's shape for the face fields, int32 ncface."""
+    for t in (visk, hk, ds, flux):
+        if t.dtype != torch.float64 or not t.is_cuda or not t.is_contiguous() or t.shape != visk.shape:
+            raise ValueError("momentum_coef_fn takes contiguous float64 CUDA face arrays of one shape")
+    if ncface.dtype != torch.int32 or not ncface.is_cuda or ncface.numel() < ncells:
+        raise ValueError("ncface: int32 CUDA tensor with an entry per active cell")
+    return _MomCoefFn.apply(visk, hk, flux, ds, ncface, ncells, ndsch)

@@ -183,6 +183,97 @@ __global__ void __launch_bounds__(TPB) k_fric_sink_adjoint(int n, double g, cons
   }
 }
 
+// Momentum face coefficients of coeffsourcesink_uv (flow_imp.F90:409-574)
+// and their adjoint: acoef(k,i) = scheme(D, F) with D = visk hk ds for the
+// faces k < ncface(i) of the active cells, in the solve() layout
+// ([ncellsD][nmaxfaces], natural order); the scheme is the flow step's own
+// schemecoef (comp_lib.f90:40-109).  scheme_grad gives dA/dD and dA/dF of
+// the branch the forward value takes (each function is piecewise smooth in
+// (D, F); at a branch boundary the branch the comparisons below select).
+__device__ __forceinline__ void scheme_grad(int ndsch, double dk, double fk, double& gD, double& gF) {
+  const double absf = fabs(fk), sf = fk > 0.0 ? 1.0 : (fk < 0.0 ? -1.0 : 0.0);
+  const double up = fk < 0.0 ? -1.0 : 0.0;  // d max(0, -F) / dF
+  gD = 0.0;
+  gF = 0.0;
+  switch (ndsch) {
+    case 0:
+      return;
+    case 2: {  // hybrid: D max(0, 1 - P/2), P = |F| / max(D, 1e-6)
+      const double dp = fmax(dk, 1.0e-6), ddp = dk >= 1.0e-6 ? 1.0 : 0.0;
+      const double pk = absf / dp, pD = -absf / (dp * dp) * ddp, pF = sf / dp;
+      const double gg = 1.0 - 0.5 * pk;
+      if (gg > 0.0) {
+        gD = gg - 0.5 * dk * pD;
+        gF = -0.5 * dk * pF;
+      }
+      gF += up;
+      return;
+    }
+    case 3: {  // power law: D (1 - P^5), P = |F| / max(max(D, |F|), 1e-6)
+      const double mm = fmax(dk, absf);
+      const double m = fmax(mm, 1.0e-6);
+      double mD = 0.0, mF = 0.0;
+      if (mm >= 1.0e-6) {
+        if (dk >= absf) mD = 1.0;
+        else mF = sf;
+      }
+      const double pk = absf / m, pD = -absf / (m * m) * mD, pF = sf / m - absf / (m * m) * mF;
+      const double p4 = pk * pk * pk * pk;
+      gD = (1.0 - p4 * pk) - 5.0 * dk * p4 * pD;
+      gF = -5.0 * dk * p4 * pF + up;
+      return;
+    }
+    case 4: {  // exponential: D P / max(e^P - 1, 1e-6), P = |F| / max(max(D, 1e-6), |F|)
+      const double dp = fmax(dk, 1.0e-6);
+      const double m = fmax(dp, absf);
+      const double mD = (dk >= 1.0e-6 && dp >= absf) ? 1.0 : 0.0, mF = absf > dp ? sf : 0.0;
+      const double pk = absf / m, pD = -absf / (m * m) * mD, pF = sf / m - absf / (m * m) * mF;
+      const double ex = exp(pk), e = fmax(ex - 1.0, 1.0e-6), eP = (ex - 1.0 > 1.0e-6) ? ex : 0.0;
+      gD = pk / e + dk * pD / e - dk * pk * eP * pD / (e * e);
+      gF = dk * pF / e - dk * pk * eP * pF / (e * e) + up;
+      return;
+    }
+    default:  // upwind: D + max(0, -F)
+      gD = 1.0;
+      gF = up;
+      return;
+  }
+}
+
+__global__ void __launch_bounds__(TPB) k_mom_coef(int n, int nmf, int ndsch, const int* __restrict__ ncface,
+                                                  const double* __restrict__ visk, const double* __restrict__ hk,
+                                                  const double* __restrict__ ds, const double* __restrict__ flux,
+                                                  double* __restrict__ acoef) {
+  for (int i = blockIdx.x * TPB + threadIdx.x; i < n; i += gridDim.x * TPB) {
+    const int nf = ncface[i];
+    for (int k = 0; k < nf; ++k) {
+      const size_t f = (size_t)i * nmf + k;
+      acoef[f] = schemecoef(ndsch, visk[f] * hk[f] * ds[f], flux[f]);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(TPB) k_mom_coef_adjoint(int n, int nmf, int ndsch, const int* __restrict__ ncface,
+                                                          const double* __restrict__ visk,
+                                                          const double* __restrict__ hk,
+                                                          const double* __restrict__ ds,
+                                                          const double* __restrict__ flux,
+                                                          const double* __restrict__ ga, double* __restrict__ gvisk,
+                                                          double* __restrict__ ghk, double* __restrict__ gflux) {
+  for (int i = blockIdx.x * TPB + threadIdx.x; i < n; i += gridDim.x * TPB) {
+    const int nf = ncface[i];
+    for (int k = 0; k < nmf; ++k) {
+      const size_t f = (size_t)i * nmf + k;
+      double gD = 0.0, gF = 0.0;
+      if (k < nf) scheme_grad(ndsch, visk[f] * hk[f] * ds[f], flux[f], gD, gF);
+      const double g = ga[f];
+      if (gvisk) gvisk[f] = g * gD * hk[f] * ds[f];
+      if (ghk) ghk[f] = g * gD * visk[f] * ds[f];
+      if (gflux) gflux[f] = g * gF;
+    }
+  }
+}
+
 static int fric_launch_check(const char* what) {
   const cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) return CMS_OK;
@@ -208,6 +299,32 @@ extern "C" int cms_fric_sink_adjoint_dev_d(int n, double grav, const double* coe
   cms::k_fric_sink_adjoint<<<blocks, cms::TPB, 0, (cudaStream_t)stream>>>(n, grav, coefman, h, uv, area, grad_sp,
                                                                           grad_coefman);
   return cms::fric_launch_check("cms_fric_sink_adjoint_dev_d");
+}
+
+extern "C" int cms_momentum_coef_dev_d(int ncells, int nmaxfaces, int ndsch, const int* ncface, const double* visk,
+                                       const double* hk, const double* ds, const double* flux, double* acoef,
+                                       void* stream) {
+  if (ncells <= 0 || nmaxfaces <= 0 || nmaxfaces > 8 || ndsch < 0 || ndsch > 4 || !ncface || !visk || !hk || !ds ||
+      !flux || !acoef)
+    return CMS_BAD_ARGUMENT;
+  const int blocks = std::max(1, std::min((ncells + cms::TPB - 1) / cms::TPB, 148 * 8));
+  cms::k_mom_coef<<<blocks, cms::TPB, 0, (cudaStream_t)stream>>>(ncells, nmaxfaces, ndsch, ncface, visk, hk, ds,
+                                                                 flux, acoef);
+  return cms::fric_launch_check("cms_momentum_coef_dev_d");
+}
+
+extern "C" int cms_momentum_coef_adjoint_dev_d(int ncells, int nmaxfaces, int ndsch, const int* ncface,
+                                               const double* visk, const double* hk, const double* ds,
+                                               const double* flux, const double* grad_acoef, double* grad_visk,
+                                               double* grad_hk, double* grad_flux, void* stream) {
+  if (ncells <= 0 || nmaxfaces <= 0 || nmaxfaces > 8 || ndsch < 0 || ndsch > 4 || !ncface || !visk || !hk || !ds ||
+      !flux || !grad_acoef)
+    return CMS_BAD_ARGUMENT;
+  const int blocks = std::max(1, std::min((ncells + cms::TPB - 1) / cms::TPB, 148 * 8));
+  cms::k_mom_coef_adjoint<<<blocks, cms::TPB, 0, (cudaStream_t)stream>>>(ncells, nmaxfaces, ndsch, ncface, visk, hk,
+                                                                         ds, flux, grad_acoef, grad_visk, grad_hk,
+                                                                         grad_flux);
+  return cms::fric_launch_check("cms_momentum_coef_adjoint_dev_d");
 }
 
 extern "C" int cms_solver_adjoint_dev_d(cms_solver* s, const double* acoef, const double* ss, const double* sp,

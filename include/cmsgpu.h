@@ -213,6 +213,22 @@ int cms_fric_sink_dev_d(int n, double grav, const double* coefman, const double*
                         const double* area, const double* spuv0, double* sp, void* stream);
 int cms_fric_sink_adjoint_dev_d(int n, double grav, const double* coefman, const double* h, const double* uv,
                                 const double* area, const double* grad_sp, double* grad_coefman, void* stream);
+/* Momentum face coefficients and their adjoint (the adjoint has no
+ * counterpart in the reference), FP64 device pointers in the solve() face
+ * layout ([ncellsD][nmaxfaces], natural order; faces k < ncface(i) of the
+ * ncells active cells), on stream (NULL: the legacy default stream; no
+ * wait).  Forward: acoef = scheme(visk hk ds, flux) with the
+ * ADVECTION_SCHEME coefficient function ndsch (0 none, 1 upwind, 2 hybrid,
+ * 3 power law, 4 exponential; comp_lib.f90:40-109, as coeffsourcesink_uv
+ * calls it, flow_imp.F90:120-126); other entries untouched.  Adjoint: given
+ * grad_acoef = dL/dacoef (from cms_solver_adjoint_dev_d), writes dL/dvisk,
+ * dL/dhk and dL/dflux for every face slot of the active cells (0 beyond
+ * ncface); any of the three outputs may be NULL. */
+int cms_momentum_coef_dev_d(int ncells, int nmaxfaces, int ndsch, const int* ncface, const double* visk,
+                            const double* hk, const double* ds, const double* flux, double* acoef, void* stream);
+int cms_momentum_coef_adjoint_dev_d(int ncells, int nmaxfaces, int ndsch, const int* ncface, const double* visk,
+                                    const double* hk, const double* ds, const double* flux, const double* grad_acoef,
+                                    double* grad_visk, double* grad_hk, double* grad_flux, void* stream);
 /* Blocks (tiles) of the handle's persistent BiCGStab launch: 0 restores the
  * default (the device's resident capacity, at most one block per 256 rows);
  * returns the count in use, or a negative CMS_* code. */
