@@ -19,6 +19,13 @@ momentum equations' face coefficients acoef = scheme(visk hk ds, flux)
 (``cms_momentum_coef_dev_d``, the ADVECTION_SCHEME functions); its backward
 pass (``cms_momentum_coef_adjoint_dev_d``) gives dL/dvisk, dL/dhk and
 dL/dflux from dL/dacoef.
+
+``pp_coef_fn(...)`` is the pressure-correction coefficients built from the
+momentum system (``cms_pp_coef_dev_d``, coefsourcesink_pp without the
+skewness correction); its backward pass (``cms_pp_coef_adjoint_dev_d``)
+gives dL/dacoef_u, dL/dsp_u and dL/dhk.  Chained with friction_sink_fn and
+solve_fn, Manning's n reaches the pressure-correction solve through the
+momentum diagonal.
 """
 from __future__ import annotations
 
@@ -38,6 +45,8 @@ def _bind(L):
     L.cms_fric_sink_adjoint_dev_d.argtypes = [i, d] + [vp] * 7
     L.cms_momentum_coef_dev_d.argtypes = [i, i, i] + [vp] * 7
     L.cms_momentum_coef_adjoint_dev_d.argtypes = [i, i, i] + [vp] * 10
+    L.cms_pp_coef_dev_d.argtypes = [i, i, vp, vp, vp, d] + [vp] * 9
+    L.cms_pp_coef_adjoint_dev_d.argtypes = [i, i, vp, vp, vp, d] + [vp] * 12
     L._adj_bound = True
 
 
@@ -173,3 +182,57 @@ def momentum_coef_fn(ncface, ncells: int, visk, hk, ds, flux, ndsch: int = 4):
     if ncface.dtype != torch.int32 or not ncface.is_cuda or ncface.numel() < ncells:
         raise ValueError("ncface: int32 CUDA tensor with an entry per active cell")
     return _MomCoefFn.apply(visk, hk, flux, ds, ncface, ncells, ndsch)
+
+
+class _PPCoefFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, acoef_u, sp_u, hk, geo):
+        c2c, ncface, iwet, relax, area, ds, dn, fintp, ncells = geo
+        nD, nmf = acoef_u.shape
+        out = torch.zeros_like(acoef_u)
+        L = _lib.lib()
+        _bind(L)
+        stream = C.c_void_p(torch.cuda.current_stream(acoef_u.device).cuda_stream)
+        rc = L.cms_pp_coef_dev_d(int(ncells), int(nmf), _ptr(c2c), _ptr(ncface), _ptr(iwet), float(relax),
+                                 _ptr(acoef_u.detach()), _ptr(sp_u.detach()), _ptr(area), _ptr(hk.detach()),
+                                 _ptr(ds), _ptr(dn), _ptr(fintp), _ptr(out), stream)
+        _lib.check(rc, "cms_pp_coef_dev_d")
+        ctx.save_for_backward(acoef_u.detach(), sp_u.detach(), hk.detach())
+        ctx.geo = geo
+        return out
+
+    @staticmethod
+    def backward(ctx, ga):
+        acoef_u, sp_u, hk = ctx.saved_tensors
+        c2c, ncface, iwet, relax, area, ds, dn, fintp, ncells = ctx.geo
+        g = ga.detach().to(torch.float64).contiguous()
+        gac = torch.zeros_like(acoef_u) if ctx.needs_input_grad[0] else None
+        gsp = torch.zeros_like(sp_u) if ctx.needs_input_grad[1] else None
+        ghk = torch.zeros_like(hk) if ctx.needs_input_grad[2] else None
+        L = _lib.lib()
+        _bind(L)
+        stream = C.c_void_p(torch.cuda.current_stream(acoef_u.device).cuda_stream)
+        rc = L.cms_pp_coef_adjoint_dev_d(int(ncells), int(acoef_u.shape[1]), _ptr(c2c), _ptr(ncface), _ptr(iwet),
+                                         float(relax), _ptr(acoef_u), _ptr(sp_u), _ptr(area), _ptr(hk), _ptr(ds),
+                                         _ptr(dn), _ptr(fintp), _ptr(g), _ptr(gac), _ptr(gsp), _ptr(ghk), stream)
+        _lib.check(rc, "cms_pp_coef_adjoint_dev_d")
+        return gac, gsp, ghk, None
+
+
+def pp_coef_fn(cell2cell, ncface, iwet, ncells: int, relax: float, acoef_u, sp_u, area, hk, ds, dn, fintp):
+    """Pressure-correction coefficients [ncellsD, nmaxfaces] from the momentum
+    system (acoef_u, sp_u), with gradients for acoef_u, sp_u and hk.  int32
+    CUDA tensors cell2cell (1-based, [ncellsD, nmaxfaces]), ncface, iwet
+    (ncellsD entries); float64 CUDA tensors otherwise (face fields of
+    acoef_u's shape, area per cell)."""
+    for t in (cell2cell, ncface, iwet):
+        if t.dtype != torch.int32 or not t.is_cuda or not t.is_contiguous():
+            raise ValueError("cell2cell, ncface, iwet: contiguous int32 CUDA tensors")
+    for t in (acoef_u, hk, ds, dn, fintp):
+        if t.dtype != torch.float64 or not t.is_cuda or not t.is_contiguous() or t.shape != acoef_u.shape:
+            raise ValueError("face fields: contiguous float64 CUDA tensors of acoef_u's shape")
+    for t in (sp_u, area):
+        if t.dtype != torch.float64 or not t.is_cuda or not t.is_contiguous():
+            raise ValueError("sp_u, area: contiguous float64 CUDA tensors")
+    geo = (cell2cell, ncface, iwet, relax, area, ds, dn, fintp, ncells)
+    return _PPCoefFn.apply(acoef_u, sp_u, hk, geo)

@@ -274,6 +274,131 @@ __global__ void __launch_bounds__(TPB) k_mom_coef_adjoint(int n, int nmf, int nd
   }
 }
 
+// Pressure-correction coefficients of coefsourcesink_pp (flow_imp.F90:577-794,
+// the flow step's kf_pp_cell / kf_pp_face without skewness correction) from the
+// momentum coefficients, and their adjoint.  Per active cell
+//   Dn = sum_k acoef_u(k,i) - sp_u(i),  apu = iwet relax / max(Dn, 1e-6),
+//   ap = apu A,  sumu = (sum_k acoef_u) apu,
+// per face k < ncface(i) to a wet cell c (else 0):
+//   a_pp = hk^2 ds ap_f / (1 - sumu_f) / dn,
+// with ap_f, sumu_f the cell values for a dummy neighbour and
+// fintp ap(c) + (1 - fintp) ap(i) (the same for sumu) for an active one.
+// Face fields in the solve() layout ([ncellsD][nmaxfaces], 1-based cell2cell);
+// fintp(kb, c) = 1 - fintp(k, i) on the two sides of a face keeps a_pp
+// symmetric, as the flow step's mirrored faces.
+struct PPCell {
+  double ap, sumu, asum, dn;
+};
+__device__ __forceinline__ PPCell pp_cell(int i, int nmf, const int* ncface, const int* iwet, double relax,
+                                          const double* acoef_u, const double* sp_u, const double* area) {
+  PPCell c;
+  c.asum = 0.0;
+  for (int k = 0; k < ncface[i]; ++k) c.asum += acoef_u[(size_t)i * nmf + k];
+  c.dn = c.asum - sp_u[i];
+  const double apu = iwet[i] * relax / fmax(c.dn, 1.0e-6);
+  c.ap = apu * area[i];
+  c.sumu = c.asum * apu;
+  return c;
+}
+
+__global__ void __launch_bounds__(TPB) k_pp_coef(int n, int nmf, const int* __restrict__ c2c,
+                                                 const int* __restrict__ ncface, const int* __restrict__ iwet,
+                                                 double relax, const double* __restrict__ acoef_u,
+                                                 const double* __restrict__ sp_u, const double* __restrict__ area,
+                                                 const double* __restrict__ hk, const double* __restrict__ ds,
+                                                 const double* __restrict__ dn, const double* __restrict__ fintp,
+                                                 double* __restrict__ acoef_pp) {
+  for (int i = blockIdx.x * TPB + threadIdx.x; i < n; i += gridDim.x * TPB) {
+    const PPCell ci = pp_cell(i, nmf, ncface, iwet, relax, acoef_u, sp_u, area);
+    for (int k = 0; k < ncface[i]; ++k) {
+      const size_t f = (size_t)i * nmf + k;
+      const int c = c2c[f] - 1;
+      double a = 0.0;
+      if (iwet[i] * iwet[c] != 0) {
+        const double K = hk[f] * hk[f] * ds[f] / dn[f];
+        if (c >= n) {
+          a = K * ci.ap / (1.0 - ci.sumu);
+        } else {
+          const PPCell cc = pp_cell(c, nmf, ncface, iwet, relax, acoef_u, sp_u, area);
+          const double fk = fintp[f];
+          a = K * (fk * cc.ap + (1.0 - fk) * ci.ap) / (1.0 - (fk * cc.sumu + (1.0 - fk) * ci.sumu));
+        }
+      }
+      acoef_pp[f] = a;
+    }
+  }
+}
+
+// The adjoint as a gather: cell j collects dL/dap(j) and dL/dsumu(j) from its
+// own faces (weight 1 - fintp, or 1 for a dummy neighbour) and from the faces
+// of its neighbours that point back to it (weight their fintp), then turns
+// them into dL/dacoef_u(., j) (one value for the row's faces) and dL/dsp_u(j);
+// dL/dhk from the face's own coefficient.
+__global__ void __launch_bounds__(TPB) k_pp_coef_adjoint(int n, int nmf, const int* __restrict__ c2c,
+                                                         const int* __restrict__ ncface,
+                                                         const int* __restrict__ iwet, double relax,
+                                                         const double* __restrict__ acoef_u,
+                                                         const double* __restrict__ sp_u,
+                                                         const double* __restrict__ area,
+                                                         const double* __restrict__ hk,
+                                                         const double* __restrict__ ds,
+                                                         const double* __restrict__ dn,
+                                                         const double* __restrict__ fintp,
+                                                         const double* __restrict__ ga, double* __restrict__ gacoef_u,
+                                                         double* __restrict__ gsp_u, double* __restrict__ ghk) {
+  for (int j = blockIdx.x * TPB + threadIdx.x; j < n; j += gridDim.x * TPB) {
+    const PPCell cj = pp_cell(j, nmf, ncface, iwet, relax, acoef_u, sp_u, area);
+    double gap = 0.0, gsu = 0.0;
+    const int nfj = ncface[j];
+    for (int k = 0; k < nmf; ++k) {
+      const size_t f = (size_t)j * nmf + k;
+      double gh = 0.0;
+      const int c = k < nfj ? c2c[f] - 1 : -1;
+      if (c >= 0 && iwet[j] * iwet[c] != 0) {
+        const double K = hk[f] * hk[f] * ds[f] / dn[f], dK = 2.0 * hk[f] * ds[f] / dn[f];
+        if (c >= n) {
+          const double den = 1.0 - cj.sumu;
+          gap += ga[f] * K / den;
+          gsu += ga[f] * K * cj.ap / (den * den);
+          gh = ga[f] * dK * cj.ap / den;
+        } else {
+          const PPCell cc = pp_cell(c, nmf, ncface, iwet, relax, acoef_u, sp_u, area);
+          const double fk = fintp[f];
+          const double apv = fk * cc.ap + (1.0 - fk) * cj.ap, den = 1.0 - (fk * cc.sumu + (1.0 - fk) * cj.sumu);
+          gap += ga[f] * K / den * (1.0 - fk);
+          gsu += ga[f] * K * apv / (den * den) * (1.0 - fk);
+          gh = ga[f] * dK * apv / den;
+          // the neighbour's faces that point back to j
+          for (int kb = 0; kb < ncface[c]; ++kb) {
+            const size_t fb = (size_t)c * nmf + kb;
+            if (c2c[fb] - 1 != j) continue;
+            const double Kb = hk[fb] * hk[fb] * ds[fb] / dn[fb], fkb = fintp[fb];
+            const double apb = fkb * cj.ap + (1.0 - fkb) * cc.ap;
+            const double denb = 1.0 - (fkb * cj.sumu + (1.0 - fkb) * cc.sumu);
+            gap += ga[fb] * Kb / denb * fkb;
+            gsu += ga[fb] * Kb * apb / (denb * denb) * fkb;
+          }
+        }
+      }
+      if (ghk) ghk[f] = gh;
+    }
+    // ap = w r A / max(Dn, 1e-6), sumu = asum w r / max(Dn, 1e-6), Dn = asum - sp
+    const double w = iwet[j] * relax;
+    double gasum, gsp;
+    if (cj.dn > 1.0e-6) {
+      const double d2 = cj.dn * cj.dn;
+      gasum = gap * (-w * area[j] / d2) + gsu * (w * (-sp_u[j]) / d2);
+      gsp = gap * (w * area[j] / d2) + gsu * (w * cj.asum / d2);
+    } else {
+      gasum = gsu * w / 1.0e-6;
+      gsp = 0.0;
+    }
+    if (gacoef_u)
+      for (int k = 0; k < nmf; ++k) gacoef_u[(size_t)j * nmf + k] = k < nfj ? gasum : 0.0;
+    if (gsp_u) gsp_u[j] = gsp;
+  }
+}
+
 static int fric_launch_check(const char* what) {
   const cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) return CMS_OK;
@@ -325,6 +450,35 @@ extern "C" int cms_momentum_coef_adjoint_dev_d(int ncells, int nmaxfaces, int nd
                                                                          ds, flux, grad_acoef, grad_visk, grad_hk,
                                                                          grad_flux);
   return cms::fric_launch_check("cms_momentum_coef_adjoint_dev_d");
+}
+
+extern "C" int cms_pp_coef_dev_d(int ncells, int nmaxfaces, const int* cell2cell, const int* ncface, const int* iwet,
+                                 double relax, const double* acoef_u, const double* sp_u, const double* area,
+                                 const double* hk, const double* ds, const double* dn, const double* fintp,
+                                 double* acoef_pp, void* stream) {
+  if (ncells <= 0 || nmaxfaces <= 0 || nmaxfaces > 8 || relax <= 0.0 || !cell2cell || !ncface || !iwet ||
+      !acoef_u || !sp_u || !area || !hk || !ds || !dn || !fintp || !acoef_pp)
+    return CMS_BAD_ARGUMENT;
+  const int blocks = std::max(1, std::min((ncells + cms::TPB - 1) / cms::TPB, 148 * 8));
+  cms::k_pp_coef<<<blocks, cms::TPB, 0, (cudaStream_t)stream>>>(ncells, nmaxfaces, cell2cell, ncface, iwet, relax,
+                                                                acoef_u, sp_u, area, hk, ds, dn, fintp, acoef_pp);
+  return cms::fric_launch_check("cms_pp_coef_dev_d");
+}
+
+extern "C" int cms_pp_coef_adjoint_dev_d(int ncells, int nmaxfaces, const int* cell2cell, const int* ncface,
+                                         const int* iwet, double relax, const double* acoef_u, const double* sp_u,
+                                         const double* area, const double* hk, const double* ds, const double* dn,
+                                         const double* fintp, const double* grad_acoef_pp, double* grad_acoef_u,
+                                         double* grad_sp_u, double* grad_hk, void* stream) {
+  if (ncells <= 0 || nmaxfaces <= 0 || nmaxfaces > 8 || relax <= 0.0 || !cell2cell || !ncface || !iwet ||
+      !acoef_u || !sp_u || !area || !hk || !ds || !dn || !fintp || !grad_acoef_pp)
+    return CMS_BAD_ARGUMENT;
+  const int blocks = std::max(1, std::min((ncells + cms::TPB - 1) / cms::TPB, 148 * 8));
+  cms::k_pp_coef_adjoint<<<blocks, cms::TPB, 0, (cudaStream_t)stream>>>(ncells, nmaxfaces, cell2cell, ncface, iwet,
+                                                                        relax, acoef_u, sp_u, area, hk, ds, dn,
+                                                                        fintp, grad_acoef_pp, grad_acoef_u, grad_sp_u,
+                                                                        grad_hk);
+  return cms::fric_launch_check("cms_pp_coef_adjoint_dev_d");
 }
 
 extern "C" int cms_solver_adjoint_dev_d(cms_solver* s, const double* acoef, const double* ss, const double* sp,

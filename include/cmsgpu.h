@@ -229,6 +229,29 @@ int cms_momentum_coef_dev_d(int ncells, int nmaxfaces, int ndsch, const int* ncf
 int cms_momentum_coef_adjoint_dev_d(int ncells, int nmaxfaces, int ndsch, const int* ncface, const double* visk,
                                     const double* hk, const double* ds, const double* flux, const double* grad_acoef,
                                     double* grad_visk, double* grad_hk, double* grad_flux, void* stream);
+/* Pressure-correction coefficients from the momentum coefficients and their
+ * adjoint (the adjoint has no counterpart in the reference), FP64 device
+ * pointers: cell2cell (1-based) and the face fields in the solve() layout
+ * ([ncellsD][nmaxfaces]), iwet with ncellsD entries, acoef_u / sp_u the
+ * momentum system (solve() layout), area, hk, ds, dn, fintp the cell area and
+ * the face depth, length, centre distance and interpolation weight (fintp on
+ * the two sides of a face adding to 1); on stream (NULL: the legacy default
+ * stream; no wait).  Forward (coefsourcesink_pp, flow_imp.F90:577-794,
+ * without the skewness correction): apu = iwet relax / max(sum acoef_u -
+ * sp_u, 1e-6), ap = apu A, sumu = apu sum acoef_u, and on each face k <
+ * ncface(i) to a wet cell a_pp = hk^2 ds ap_f / (1 - sumu_f) / dn, the face
+ * values interpolated with fintp (the cell's own at a dummy neighbour); 0
+ * across a dry side.  Adjoint: given grad_acoef_pp, writes dL/dacoef_u (the
+ * same value on every face of a row), dL/dsp_u and dL/dhk; outputs may be
+ * NULL. */
+int cms_pp_coef_dev_d(int ncells, int nmaxfaces, const int* cell2cell, const int* ncface, const int* iwet,
+                      double relax, const double* acoef_u, const double* sp_u, const double* area, const double* hk,
+                      const double* ds, const double* dn, const double* fintp, double* acoef_pp, void* stream);
+int cms_pp_coef_adjoint_dev_d(int ncells, int nmaxfaces, const int* cell2cell, const int* ncface, const int* iwet,
+                              double relax, const double* acoef_u, const double* sp_u, const double* area,
+                              const double* hk, const double* ds, const double* dn, const double* fintp,
+                              const double* grad_acoef_pp, double* grad_acoef_u, double* grad_sp_u, double* grad_hk,
+                              void* stream);
 /* Blocks (tiles) of the handle's persistent BiCGStab launch: 0 restores the
  * default (the device's resident capacity, at most one block per 256 rows);
  * returns the count in use, or a negative CMS_* code. */
