@@ -399,6 +399,135 @@ __global__ void __launch_bounds__(TPB) k_pp_coef_adjoint(int n, int nmf, const i
   }
 }
 
+// Right-hand side of the pressure-correction system (coefsourcesink_pp and
+// the Rhie-Chow fluxes of flow_imp_flux_noskew, flow_imp_flux.f90:361-409,
+// as the flow step's kf_pp_face / kf_pp_src evaluate them on wet cells
+// without skewness correction), and its adjoint with respect to the momentum
+// system (through apuareap) and the face depth:
+//   Hu = u + ap dpx h,  Hv = v + ap dpy h,
+//   flux(k,i) = hk ds (nx Hu_f + ny Hv_f - ap_f hk (p_c - p_i) / dn)
+// (outward normal of face k of cell i from its direction 1 N, 2 E, 3 S, 4 W;
+// face values interpolated with fintp, the cell's own at a dummy neighbour;
+// 0 across a dry side), ss_pp(i) = sspp0(i) - sum_k flux(k,i) + p(i) sppp0(i).
+__device__ __forceinline__ double pp_face_flux(int i, int k, int n, int nmf, const int* c2c, const int* idir,
+                                               const int* iwet, const double* u, const double* v, const double* h,
+                                               const double* dpx, const double* dpy, const double* p,
+                                               const double* hk, const double* ds, const double* dn,
+                                               const double* fintp, double api, double apc) {
+  const size_t f = (size_t)i * nmf + k;
+  const int c = c2c[f] - 1;
+  if (iwet[i] * iwet[c] == 0) return 0.0;
+  const double nx = fnxd(idir[f]), ny = fnyd(idir[f]);
+  const double hui = u[i] + api * dpx[i] * h[i], hvi = v[i] + api * dpy[i] * h[i];
+  double huf = hui, hvf = hvi, apf = api;
+  if (c < n) {
+    const double fk = fintp[f];
+    huf = fk * (u[c] + apc * dpx[c] * h[c]) + (1.0 - fk) * hui;
+    hvf = fk * (v[c] + apc * dpy[c] * h[c]) + (1.0 - fk) * hvi;
+    apf = fk * apc + (1.0 - fk) * api;
+  }
+  return hk[f] * ds[f] * (nx * huf + ny * hvf - apf * hk[f] * (p[c] - p[i]) / dn[f]);
+}
+
+__global__ void __launch_bounds__(TPB) k_pp_rhs(int n, int nmf, const int* __restrict__ c2c,
+                                                const int* __restrict__ ncface, const int* __restrict__ idir,
+                                                const int* __restrict__ iwet, double relax,
+                                                const double* __restrict__ acoef_u, const double* __restrict__ sp_u,
+                                                const double* __restrict__ area, const double* __restrict__ u,
+                                                const double* __restrict__ v, const double* __restrict__ h,
+                                                const double* __restrict__ dpx, const double* __restrict__ dpy,
+                                                const double* __restrict__ p, const double* __restrict__ hk,
+                                                const double* __restrict__ ds, const double* __restrict__ dn,
+                                                const double* __restrict__ fintp, const double* __restrict__ sspp0,
+                                                const double* __restrict__ sppp0, double* __restrict__ ss_pp) {
+  for (int i = blockIdx.x * TPB + threadIdx.x; i < n; i += gridDim.x * TPB) {
+    const double api = pp_cell(i, nmf, ncface, iwet, relax, acoef_u, sp_u, area).ap;
+    double sf = 0.0;
+    for (int k = 0; k < ncface[i]; ++k) {
+      const int c = c2c[(size_t)i * nmf + k] - 1;
+      const double apc = c < n ? pp_cell(c, nmf, ncface, iwet, relax, acoef_u, sp_u, area).ap : 0.0;
+      sf += pp_face_flux(i, k, n, nmf, c2c, idir, iwet, u, v, h, dpx, dpy, p, hk, ds, dn, fintp, api, apc);
+    }
+    ss_pp[i] = sspp0[i] - sf + p[i] * sppp0[i];
+  }
+}
+
+// dflux(k,i)/dap(j) for j = i (own side, weight 1 - fintp, 1 at a dummy) or
+// j = c (weight fintp), and dflux/dhk.
+__device__ __forceinline__ void pp_flux_grads(int i, int k, int n, int nmf, const int* c2c, const int* idir,
+                                              const int* iwet, const double* u, const double* v, const double* h,
+                                              const double* dpx, const double* dpy, const double* p,
+                                              const double* hk, const double* ds, const double* dn,
+                                              const double* fintp, double api, double apc, double& d_api,
+                                              double& d_apc, double& d_hk) {
+  const size_t f = (size_t)i * nmf + k;
+  const int c = c2c[f] - 1;
+  d_api = d_apc = d_hk = 0.0;
+  if (iwet[i] * iwet[c] == 0) return;
+  const double nx = fnxd(idir[f]), ny = fnyd(idir[f]);
+  const double K1 = hk[f] * ds[f], dp = (p[c] - p[i]) / dn[f];
+  const double hui = u[i] + api * dpx[i] * h[i], hvi = v[i] + api * dpy[i] * h[i];
+  if (c >= n) {
+    d_api = K1 * (nx * dpx[i] * h[i] + ny * dpy[i] * h[i] - hk[f] * dp);
+    d_hk = ds[f] * (nx * hui + ny * hvi) - 2.0 * hk[f] * ds[f] * api * dp;
+    return;
+  }
+  const double fk = fintp[f], fp = 1.0 - fk;
+  const double huc = u[c] + apc * dpx[c] * h[c], hvc = v[c] + apc * dpy[c] * h[c];
+  const double huf = fk * huc + fp * hui, hvf = fk * hvc + fp * hvi, apf = fk * apc + fp * api;
+  d_api = K1 * fp * (nx * dpx[i] * h[i] + ny * dpy[i] * h[i] - hk[f] * dp);
+  d_apc = K1 * fk * (nx * dpx[c] * h[c] + ny * dpy[c] * h[c] - hk[f] * dp);
+  d_hk = ds[f] * (nx * huf + ny * hvf) - 2.0 * hk[f] * ds[f] * apf * dp;
+}
+
+__global__ void __launch_bounds__(TPB) k_pp_rhs_adjoint(
+    int n, int nmf, const int* __restrict__ c2c, const int* __restrict__ ncface, const int* __restrict__ idir,
+    const int* __restrict__ iwet, double relax, const double* __restrict__ acoef_u, const double* __restrict__ sp_u,
+    const double* __restrict__ area, const double* __restrict__ u, const double* __restrict__ v,
+    const double* __restrict__ h, const double* __restrict__ dpx, const double* __restrict__ dpy,
+    const double* __restrict__ p, const double* __restrict__ hk, const double* __restrict__ ds,
+    const double* __restrict__ dn, const double* __restrict__ fintp, const double* __restrict__ gss,
+    double* __restrict__ gacoef_u, double* __restrict__ gsp_u, double* __restrict__ ghk) {
+  for (int j = blockIdx.x * TPB + threadIdx.x; j < n; j += gridDim.x * TPB) {
+    const PPCell cj = pp_cell(j, nmf, ncface, iwet, relax, acoef_u, sp_u, area);
+    double gap = 0.0;
+    const int nfj = ncface[j];
+    for (int k = 0; k < nmf; ++k) {
+      const size_t f = (size_t)j * nmf + k;
+      double gh = 0.0;
+      if (k < nfj) {
+        const int c = c2c[f] - 1;
+        const double apc = c < n ? pp_cell(c, nmf, ncface, iwet, relax, acoef_u, sp_u, area).ap : 0.0;
+        double da_i, da_c, dh;
+        pp_flux_grads(j, k, n, nmf, c2c, idir, iwet, u, v, h, dpx, dpy, p, hk, ds, dn, fintp, cj.ap, apc, da_i,
+                      da_c, dh);
+        gap += -gss[j] * da_i;  // ss_pp(j) holds -flux(k,j)
+        gh = -gss[j] * dh;
+        if (c < n) {  // the neighbour's faces that point back to j: their flux depends on ap(j) too
+          for (int kb = 0; kb < ncface[c]; ++kb) {
+            if (c2c[(size_t)c * nmf + kb] - 1 != j) continue;
+            double db_c, db_j, dhb;
+            pp_flux_grads(c, kb, n, nmf, c2c, idir, iwet, u, v, h, dpx, dpy, p, hk, ds, dn, fintp, apc, cj.ap,
+                          db_c, db_j, dhb);
+            gap += -gss[c] * db_j;
+          }
+        }
+      }
+      if (ghk) ghk[f] = gh;
+    }
+    const double w = iwet[j] * relax;
+    double gasum = 0.0, gsp = 0.0;
+    if (cj.dn > 1.0e-6) {
+      const double d2 = cj.dn * cj.dn;
+      gasum = gap * (-w * area[j] / d2);
+      gsp = gap * (w * area[j] / d2);
+    }
+    if (gacoef_u)
+      for (int k = 0; k < nmf; ++k) gacoef_u[(size_t)j * nmf + k] = k < nfj ? gasum : 0.0;
+    if (gsp_u) gsp_u[j] = gsp;
+  }
+}
+
 static int fric_launch_check(const char* what) {
   const cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) return CMS_OK;
@@ -479,6 +608,41 @@ extern "C" int cms_pp_coef_adjoint_dev_d(int ncells, int nmaxfaces, const int* c
                                                                         fintp, grad_acoef_pp, grad_acoef_u, grad_sp_u,
                                                                         grad_hk);
   return cms::fric_launch_check("cms_pp_coef_adjoint_dev_d");
+}
+
+extern "C" int cms_pp_rhs_dev_d(int ncells, int nmaxfaces, const int* cell2cell, const int* ncface, const int* idirface,
+                                const int* iwet, double relax, const double* acoef_u, const double* sp_u,
+                                const double* area, const double* u, const double* v, const double* h,
+                                const double* dpx, const double* dpy, const double* p, const double* hk,
+                                const double* ds, const double* dn, const double* fintp, const double* sspp0,
+                                const double* sppp0, double* ss_pp, void* stream) {
+  if (ncells <= 0 || nmaxfaces <= 0 || nmaxfaces > 8 || relax <= 0.0 || !cell2cell || !ncface || !idirface ||
+      !iwet || !acoef_u || !sp_u || !area || !u || !v || !h || !dpx || !dpy || !p || !hk || !ds || !dn || !fintp ||
+      !sspp0 || !sppp0 || !ss_pp)
+    return CMS_BAD_ARGUMENT;
+  const int blocks = std::max(1, std::min((ncells + cms::TPB - 1) / cms::TPB, 148 * 8));
+  cms::k_pp_rhs<<<blocks, cms::TPB, 0, (cudaStream_t)stream>>>(ncells, nmaxfaces, cell2cell, ncface, idirface, iwet,
+                                                               relax, acoef_u, sp_u, area, u, v, h, dpx, dpy, p, hk,
+                                                               ds, dn, fintp, sspp0, sppp0, ss_pp);
+  return cms::fric_launch_check("cms_pp_rhs_dev_d");
+}
+
+extern "C" int cms_pp_rhs_adjoint_dev_d(int ncells, int nmaxfaces, const int* cell2cell, const int* ncface,
+                                        const int* idirface, const int* iwet, double relax, const double* acoef_u,
+                                        const double* sp_u, const double* area, const double* u, const double* v,
+                                        const double* h, const double* dpx, const double* dpy, const double* p,
+                                        const double* hk, const double* ds, const double* dn, const double* fintp,
+                                        const double* grad_ss_pp, double* grad_acoef_u, double* grad_sp_u,
+                                        double* grad_hk, void* stream) {
+  if (ncells <= 0 || nmaxfaces <= 0 || nmaxfaces > 8 || relax <= 0.0 || !cell2cell || !ncface || !idirface ||
+      !iwet || !acoef_u || !sp_u || !area || !u || !v || !h || !dpx || !dpy || !p || !hk || !ds || !dn || !fintp ||
+      !grad_ss_pp)
+    return CMS_BAD_ARGUMENT;
+  const int blocks = std::max(1, std::min((ncells + cms::TPB - 1) / cms::TPB, 148 * 8));
+  cms::k_pp_rhs_adjoint<<<blocks, cms::TPB, 0, (cudaStream_t)stream>>>(
+      ncells, nmaxfaces, cell2cell, ncface, idirface, iwet, relax, acoef_u, sp_u, area, u, v, h, dpx, dpy, p, hk, ds,
+      dn, fintp, grad_ss_pp, grad_acoef_u, grad_sp_u, grad_hk);
+  return cms::fric_launch_check("cms_pp_rhs_adjoint_dev_d");
 }
 
 extern "C" int cms_solver_adjoint_dev_d(cms_solver* s, const double* acoef, const double* ss, const double* sp,

@@ -252,6 +252,29 @@ int cms_pp_coef_adjoint_dev_d(int ncells, int nmaxfaces, const int* cell2cell, c
                               const double* hk, const double* ds, const double* dn, const double* fintp,
                               const double* grad_acoef_pp, double* grad_acoef_u, double* grad_sp_u, double* grad_hk,
                               void* stream);
+/* Right-hand side of the pressure-correction system and its adjoint (the
+ * adjoint has no counterpart in the reference), same conventions as
+ * cms_pp_coef_dev_d, plus idirface (face directions 1 N, 2 E, 3 S, 4 W, the
+ * solve() face layout) and the cell fields u, v, h, dpx, dpy, p (p with
+ * ncellsD entries: dummy values enter the boundary fluxes), sspp0, sppp0.
+ * Forward (coefsourcesink_pp with the Rhie-Chow fluxes of
+ * flow_imp_flux_noskew, flow_imp_flux.f90:361-409, wet cells, no skewness
+ * correction): Hu = u + ap dpx h, Hv = v + ap dpy h, flux(k,i) =
+ * hk ds (nx Hu_f + ny Hv_f - ap_f hk (p_c - p_i) / dn) with the face values
+ * interpolated as in cms_pp_coef_dev_d, ss_pp = sspp0 - sum_k flux + p sppp0.
+ * Adjoint: given grad_ss_pp, writes dL/dacoef_u, dL/dsp_u (through ap) and
+ * dL/dhk; outputs may be NULL. */
+int cms_pp_rhs_dev_d(int ncells, int nmaxfaces, const int* cell2cell, const int* ncface, const int* idirface,
+                     const int* iwet, double relax, const double* acoef_u, const double* sp_u, const double* area,
+                     const double* u, const double* v, const double* h, const double* dpx, const double* dpy,
+                     const double* p, const double* hk, const double* ds, const double* dn, const double* fintp,
+                     const double* sspp0, const double* sppp0, double* ss_pp, void* stream);
+int cms_pp_rhs_adjoint_dev_d(int ncells, int nmaxfaces, const int* cell2cell, const int* ncface, const int* idirface,
+                             const int* iwet, double relax, const double* acoef_u, const double* sp_u,
+                             const double* area, const double* u, const double* v, const double* h, const double* dpx,
+                             const double* dpy, const double* p, const double* hk, const double* ds, const double* dn,
+                             const double* fintp, const double* grad_ss_pp, double* grad_acoef_u, double* grad_sp_u,
+                             double* grad_hk, void* stream);
 /* Blocks (tiles) of the handle's persistent BiCGStab launch: 0 restores the
  * default (the device's resident capacity, at most one block per 256 rows);
  * returns the count in use, or a negative CMS_* code. */

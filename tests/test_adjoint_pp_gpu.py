@@ -17,7 +17,11 @@ Checks: the coefficients against the formula in numpy (1e-13); dL/d(n,
 acoef_u, hk) against an FP64 CPU tangent-linear (the coefficients'
 directional derivative by central differences of the numpy model, scipy
 solves; 1e-6 relative) and against central finite differences of the GPU
-forward model (5e-5).
+forward model (5e-5).  The same again with the right-hand side built too
+(cms_pp_rhs_dev_d: continuity source with the Rhie-Chow fluxes of
+flow_imp_flux_noskew, Hu = u + ap dpx h; adjoint cms_pp_rhs_adjoint_dev_d),
+so that n reaches both sides of the pressure-correction system; face
+directions are opposite on the two sides of a face.
 """
 import numpy as np
 import pytest
@@ -72,8 +76,27 @@ def _case(seed):
     sp_pp[:n] = -rng.uniform(20.0, 60.0, n)
     gauges = np.sort(rng.choice(n, 200, replace=False))
     target = rng.standard_normal(200)
+    # right-hand side inputs: face directions opposite on the two sides of a face
+    idir = np.zeros(shape, np.int32)
+    opp = {1: 3, 3: 1, 2: 4, 4: 2}
+    for i in range(n):
+        for k in range(g.ncface[i]):
+            c = c2c[i, k] - 1
+            if c >= n:
+                idir[i, k] = rng.integers(1, 5)
+            elif c > i:
+                kb = [q for q in range(g.ncface[c]) if c2c[c, q] - 1 == i][0]
+                idir[i, k] = rng.integers(1, 5)
+                idir[c, kb] = opp[int(idir[i, k])]
+    cell = lambda lo, hi: np.concatenate([rng.uniform(lo, hi, n), np.zeros(nD - n)])
+    u, v, dpx, dpy = cell(-1, 1), cell(-1, 1), cell(-0.01, 0.01), cell(-0.01, 0.01)
+    p = rng.uniform(-1.0, 1.0, nD)
+    sspp0 = cell(-5, 5)
+    sppp0 = sp_pp.copy()
+    hcell = np.concatenate([h, np.zeros(nD - n)])
     return dict(g=g, ss=ss, phi=phi, c2c=c2c, mask=mask, hk=hk, ds=ds, dn=dn, fintp=fintp, acoef_u=acoef_u,
-                spuv0=spuv0, nman=nman, h=h, uv=uv, area=area, sp_pp=sp_pp, gauges=gauges, target=target)
+                spuv0=spuv0, nman=nman, h=h, uv=uv, area=area, sp_pp=sp_pp, gauges=gauges, target=target,
+                idir=idir, u=u, v=v, dpx=dpx, dpy=dpy, p=p, sspp0=sspp0, sppp0=sppp0, hcell=hcell)
 
 
 def _pp_numpy(cs, nman, acoef_u, hk):
@@ -94,6 +117,36 @@ def _pp_numpy(cs, nman, acoef_u, hk):
             else:
                 fk = cs["fintp"][i, k]
                 out[i, k] = K * (fk * ap[c] + (1 - fk) * ap[i]) / (1.0 - (fk * sumu[c] + (1 - fk) * sumu[i]))
+    return out
+
+
+def _rhs_numpy(cs, nman, acoef_u, hk):
+    """The pressure-correction right-hand side in numpy."""
+    g, c2c, n = cs["g"], cs["c2c"], cs["g"].ncells
+    sp_u = cs["spuv0"].copy()
+    sp_u[:n] = cs["spuv0"][:n] - _cd(nman, cs["h"]) * cs["uv"] * cs["area"][:n]
+    asum = acoef_u[:n].sum(axis=1)
+    ap = RELAX / np.maximum(asum - sp_u[:n], 1e-6) * cs["area"][:n]
+    hc, u, v, dpx, dpy, p = cs["hcell"], cs["u"], cs["v"], cs["dpx"], cs["dpy"], cs["p"]
+    hu = u[:n] + ap * dpx[:n] * hc[:n]
+    hv = v[:n] + ap * dpy[:n] * hc[:n]
+    nxd = {1: 0.0, 2: 1.0, 3: 0.0, 4: -1.0}
+    nyd = {1: 1.0, 2: 0.0, 3: -1.0, 4: 0.0}
+    out = np.zeros(g.ncellsD)
+    for i in range(n):
+        sf = 0.0
+        for k in range(g.ncface[i]):
+            c = c2c[i, k] - 1
+            d = int(cs["idir"][i, k])
+            if c >= n:
+                huf, hvf, apf = hu[i], hv[i], ap[i]
+            else:
+                fk = cs["fintp"][i, k]
+                huf, hvf = fk * hu[c] + (1 - fk) * hu[i], fk * hv[c] + (1 - fk) * hv[i]
+                apf = fk * ap[c] + (1 - fk) * ap[i]
+            sf += hk[i, k] * cs["ds"][i, k] * (nxd[d] * huf + nyd[d] * hvf
+                                               - apf * hk[i, k] * (p[c] - p[i]) / cs["dn"][i, k])
+        out[i] = cs["sspp0"][i] - sf + p[i] * cs["sppp0"][i]
     return out
 
 
@@ -176,6 +229,76 @@ def test_pp_gradient_matches_finite_differences():
         eps = 1e-4
         lp = _run(s, cs, cs["nman"] + eps * dn_, cs["acoef_u"] + eps * da, cs["hk"] + eps * dh, grad=False)["loss"]
         lm = _run(s, cs, cs["nman"] - eps * dn_, cs["acoef_u"] - eps * da, cs["hk"] - eps * dh, grad=False)["loss"]
+        fd = (lp - lm) / (2 * eps)
+        ad = float(r["gn"] @ dn_ + (r["ga"] * da).sum() + (r["gh"] * dh).sum())
+        assert abs(ad - fd) <= 5e-5 * abs(fd), (ad, fd)
+
+
+def _run_full(s, cs, nman, acoef_u, hk, grad=True):
+    """The whole pressure-correction system (coefficients and right-hand side)
+    from n, the momentum coefficients and the face depth."""
+    from cms2d_b200.adjoint import friction_sink_fn, pp_coef_fn, pp_rhs_fn, solve_fn
+    g = cs["g"]
+    NM, AU, HK = _t(nman, grad), _t(acoef_u, grad), _t(hk, grad)
+    area = _t(cs["area"])
+    sp_u = friction_sink_fn(NM, _t(cs["h"]), _t(cs["uv"]), area, _t(cs["spuv0"]))
+    i32 = lambda a: torch.tensor(np.ascontiguousarray(a, np.int32), device="cuda")
+    c2c, ncf, iwet = i32(cs["c2c"]), i32(g.ncface), i32(np.ones(g.ncellsD))
+    app = pp_coef_fn(c2c, ncf, iwet, g.ncells, RELAX, AU, sp_u, area, HK, _t(cs["ds"]), _t(cs["dn"]),
+                     _t(cs["fintp"]))
+    ssp = pp_rhs_fn(c2c, ncf, i32(cs["idir"]), iwet, g.ncells, RELAX, AU, sp_u, area, HK, _t(cs["ds"]),
+                    _t(cs["dn"]), _t(cs["fintp"]), _t(cs["u"]), _t(cs["v"]), _t(cs["hcell"]), _t(cs["dpx"]),
+                    _t(cs["dpy"]), _t(cs["p"]), _t(cs["sspp0"]), _t(cs["sppp0"]))
+    x = solve_fn(s, app, ssp, _t(cs["sp_pp"]), _t(cs["phi"]), relax=1.0, nswp=4000, tol=1e-9)
+    gi = torch.tensor(cs["gauges"], device="cuda")
+    loss = ((x[gi] - _t(cs["target"])) ** 2).sum()
+    out = {"loss": float(loss.detach()), "ssp": ssp.detach().cpu().numpy(), "x": x.detach().cpu().numpy()}
+    if grad:
+        loss.backward()
+        torch.cuda.synchronize()
+        out.update(gn=NM.grad.cpu().numpy(), ga=AU.grad.cpu().numpy(), gh=HK.grad.cpu().numpy())
+    return out
+
+
+def test_pp_system_gradient_matches_tangent_linear():
+    """Coefficients and right-hand side both from (n, acoef_u, hk)."""
+    cs = _case(101)
+    g, n = cs["g"], cs["g"].ncells
+    s = _solver(g)
+    r = _run_full(s, cs, cs["nman"], cs["acoef_u"], cs["hk"])
+    rhs = _rhs_numpy(cs, cs["nman"], cs["acoef_u"], cs["hk"])
+    assert np.abs(r["ssp"][:n] - rhs[:n]).max() <= 1e-12 * np.abs(rhs[:n]).max()
+    ref = _pp_numpy(cs, cs["nman"], cs["acoef_u"], cs["hk"])
+    A, b = _system(g, ref, rhs, cs["sp_pp"], cs["phi"])
+    xs = spl.spsolve(A, b)
+    assert np.abs(r["x"][:n] - xs).max() <= 1e-8 * np.abs(xs).max()
+    rng = np.random.default_rng(103)
+    for _ in range(3):
+        dn_, da, dh = _directions(cs, rng)
+        e = 1e-6
+        args_p = (cs["nman"] + e * dn_, cs["acoef_u"] + e * da, cs["hk"] + e * dh)
+        args_m = (cs["nman"] - e * dn_, cs["acoef_u"] - e * da, cs["hk"] - e * dh)
+        dapp = (_pp_numpy(cs, *args_p) - _pp_numpy(cs, *args_m)) / (2 * e)
+        drhs = (_rhs_numpy(cs, *args_p) - _rhs_numpy(cs, *args_m)) / (2 * e)
+        A1, b1 = _system(g, ref + dapp, rhs + drhs, cs["sp_pp"], cs["phi"])  # linear in acoef_pp and ss
+        dx = spl.spsolve(A, (b1 - b) - (A1 - A) @ xs)
+        tl = float(2.0 * np.sum((xs[cs["gauges"]] - cs["target"]) * dx[cs["gauges"]]))
+        ad = float(r["gn"] @ dn_ + (r["ga"] * da).sum() + (r["gh"] * dh).sum())
+        assert abs(ad - tl) <= 1e-6 * max(abs(tl), 1e-30), (ad, tl)
+
+
+def test_pp_system_gradient_matches_finite_differences():
+    cs = _case(107)
+    s = _solver(cs["g"])
+    r = _run_full(s, cs, cs["nman"], cs["acoef_u"], cs["hk"])
+    rng = np.random.default_rng(109)
+    for _ in range(2):
+        dn_, da, dh = _directions(cs, rng)
+        eps = 1e-4
+        lp = _run_full(s, cs, cs["nman"] + eps * dn_, cs["acoef_u"] + eps * da, cs["hk"] + eps * dh,
+                       grad=False)["loss"]
+        lm = _run_full(s, cs, cs["nman"] - eps * dn_, cs["acoef_u"] - eps * da, cs["hk"] - eps * dh,
+                       grad=False)["loss"]
         fd = (lp - lm) / (2 * eps)
         ad = float(r["gn"] @ dn_ + (r["ga"] * da).sum() + (r["gh"] * dh).sum())
         assert abs(ad - fd) <= 5e-5 * abs(fd), (ad, fd)
