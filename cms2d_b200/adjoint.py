@@ -50,7 +50,7 @@ def _bind(L):
     L.cms_pp_coef_dev_d.argtypes = [i, i, vp, vp, vp, d] + [vp] * 9
     L.cms_pp_coef_adjoint_dev_d.argtypes = [i, i, vp, vp, vp, d] + [vp] * 12
     L.cms_pp_rhs_dev_d.argtypes = [i, i, vp, vp, vp, vp, d] + [vp] * 17
-    L.cms_pp_rhs_adjoint_dev_d.argtypes = [i, i, vp, vp, vp, vp, d] + [vp] * 18
+    L.cms_pp_rhs_adjoint_dev_d.argtypes = [i, i, vp, vp, vp, vp, d] + [vp] * 20
     L._adj_bound = True
 
 
@@ -244,8 +244,9 @@ def pp_coef_fn(cell2cell, ncface, iwet, ncells: int, relax: float, acoef_u, sp_u
 
 class _PPRhsFn(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, acoef_u, sp_u, hk, geo):
-        c2c, ncface, idir, iwet, relax, area, u, v, h, dpx, dpy, p, ds, dn, fintp, sspp0, sppp0, ncells = geo
+    def forward(ctx, acoef_u, sp_u, hk, u, v, geo):
+        c2c, ncface, idir, iwet, relax, area, h, dpx, dpy, p, ds, dn, fintp, sspp0, sppp0, ncells = geo
+        u, v = u.detach().contiguous(), v.detach().contiguous()
         out = torch.zeros_like(sspp0)
         L = _lib.lib()
         _bind(L)
@@ -255,34 +256,37 @@ class _PPRhsFn(torch.autograd.Function):
                                 _ptr(u), _ptr(v), _ptr(h), _ptr(dpx), _ptr(dpy), _ptr(p), _ptr(hk.detach()),
                                 _ptr(ds), _ptr(dn), _ptr(fintp), _ptr(sspp0), _ptr(sppp0), _ptr(out), stream)
         _lib.check(rc, "cms_pp_rhs_dev_d")
-        ctx.save_for_backward(acoef_u.detach(), sp_u.detach(), hk.detach())
+        ctx.save_for_backward(acoef_u.detach(), sp_u.detach(), hk.detach(), u, v)
         ctx.geo = geo
         return out
 
     @staticmethod
     def backward(ctx, gs):
-        acoef_u, sp_u, hk = ctx.saved_tensors
-        c2c, ncface, idir, iwet, relax, area, u, v, h, dpx, dpy, p, ds, dn, fintp, sspp0, sppp0, ncells = ctx.geo
+        acoef_u, sp_u, hk, u, v = ctx.saved_tensors
+        c2c, ncface, idir, iwet, relax, area, h, dpx, dpy, p, ds, dn, fintp, sspp0, sppp0, ncells = ctx.geo
         g = gs.detach().to(torch.float64).contiguous()
         gac = torch.zeros_like(acoef_u) if ctx.needs_input_grad[0] else None
         gsp = torch.zeros_like(sp_u) if ctx.needs_input_grad[1] else None
         ghk = torch.zeros_like(hk) if ctx.needs_input_grad[2] else None
+        gu = torch.zeros_like(u) if ctx.needs_input_grad[3] else None
+        gv = torch.zeros_like(v) if ctx.needs_input_grad[4] else None
         L = _lib.lib()
         _bind(L)
         stream = C.c_void_p(torch.cuda.current_stream(acoef_u.device).cuda_stream)
         rc = L.cms_pp_rhs_adjoint_dev_d(int(ncells), int(acoef_u.shape[1]), _ptr(c2c), _ptr(ncface), _ptr(idir),
                                         _ptr(iwet), float(relax), _ptr(acoef_u), _ptr(sp_u), _ptr(area), _ptr(u),
                                         _ptr(v), _ptr(h), _ptr(dpx), _ptr(dpy), _ptr(p), _ptr(hk), _ptr(ds), _ptr(dn),
-                                        _ptr(fintp), _ptr(g), _ptr(gac), _ptr(gsp), _ptr(ghk), stream)
+                                        _ptr(fintp), _ptr(g), _ptr(gac), _ptr(gsp), _ptr(ghk), _ptr(gu), _ptr(gv),
+                                        stream)
         _lib.check(rc, "cms_pp_rhs_adjoint_dev_d")
-        return gac, gsp, ghk, None
+        return gac, gsp, ghk, gu, gv, None
 
 
 def pp_rhs_fn(cell2cell, ncface, idirface, iwet, ncells: int, relax: float, acoef_u, sp_u, area, hk, ds, dn, fintp,
               u, v, h, dpx, dpy, p, sspp0, sppp0):
     """Right-hand side [ncellsD] of the pressure-correction system (entries
-    of the active cells; zero beyond), with gradients for acoef_u, sp_u and
-    hk; the cell fields u, v, h, dpx, dpy, p, sspp0, sppp0 are held fixed.
+    of the active cells; zero beyond), with gradients for acoef_u, sp_u, hk,
+    u and v; the cell fields h, dpx, dpy, p, sspp0, sppp0 are held fixed.
     Tensor conventions as pp_coef_fn, idirface int32 of cell2cell's shape."""
     for t in (cell2cell, ncface, idirface, iwet):
         if t.dtype != torch.int32 or not t.is_cuda or not t.is_contiguous():
@@ -290,5 +294,5 @@ def pp_rhs_fn(cell2cell, ncface, idirface, iwet, ncells: int, relax: float, acoe
     for t in (acoef_u, sp_u, area, hk, ds, dn, fintp, u, v, h, dpx, dpy, p, sspp0, sppp0):
         if t.dtype != torch.float64 or not t.is_cuda or not t.is_contiguous():
             raise ValueError("fields: contiguous float64 CUDA tensors")
-    geo = (cell2cell, ncface, idirface, iwet, relax, area, u, v, h, dpx, dpy, p, ds, dn, fintp, sspp0, sppp0, ncells)
-    return _PPRhsFn.apply(acoef_u, sp_u, hk, geo)
+    geo = (cell2cell, ncface, idirface, iwet, relax, area, h, dpx, dpy, p, ds, dn, fintp, sspp0, sppp0, ncells)
+    return _PPRhsFn.apply(acoef_u, sp_u, hk, u, v, geo)

@@ -487,10 +487,11 @@ __global__ void __launch_bounds__(TPB) k_pp_rhs_adjoint(
     const double* __restrict__ h, const double* __restrict__ dpx, const double* __restrict__ dpy,
     const double* __restrict__ p, const double* __restrict__ hk, const double* __restrict__ ds,
     const double* __restrict__ dn, const double* __restrict__ fintp, const double* __restrict__ gss,
-    double* __restrict__ gacoef_u, double* __restrict__ gsp_u, double* __restrict__ ghk) {
+    double* __restrict__ gacoef_u, double* __restrict__ gsp_u, double* __restrict__ ghk, double* __restrict__ gu,
+    double* __restrict__ gv) {
   for (int j = blockIdx.x * TPB + threadIdx.x; j < n; j += gridDim.x * TPB) {
     const PPCell cj = pp_cell(j, nmf, ncface, iwet, relax, acoef_u, sp_u, area);
-    double gap = 0.0;
+    double gap = 0.0, guj = 0.0, gvj = 0.0;
     const int nfj = ncface[j];
     for (int k = 0; k < nmf; ++k) {
       const size_t f = (size_t)j * nmf + k;
@@ -503,13 +504,24 @@ __global__ void __launch_bounds__(TPB) k_pp_rhs_adjoint(
                       da_c, dh);
         gap += -gss[j] * da_i;  // ss_pp(j) holds -flux(k,j)
         gh = -gss[j] * dh;
-        if (c < n) {  // the neighbour's faces that point back to j: their flux depends on ap(j) too
+        if (iwet[j] * iwet[c] != 0) {  // dflux/du(j) = hk ds nx (j's interpolation weight)
+          const double wj = (c < n ? 1.0 - fintp[f] : 1.0) * hk[f] * ds[f];
+          guj += -gss[j] * wj * fnxd(idir[f]);
+          gvj += -gss[j] * wj * fnyd(idir[f]);
+        }
+        if (c < n) {  // the neighbour's faces that point back to j: their flux depends on ap(j), u(j), v(j) too
           for (int kb = 0; kb < ncface[c]; ++kb) {
-            if (c2c[(size_t)c * nmf + kb] - 1 != j) continue;
+            const size_t fb = (size_t)c * nmf + kb;
+            if (c2c[fb] - 1 != j) continue;
             double db_c, db_j, dhb;
             pp_flux_grads(c, kb, n, nmf, c2c, idir, iwet, u, v, h, dpx, dpy, p, hk, ds, dn, fintp, apc, cj.ap,
                           db_c, db_j, dhb);
             gap += -gss[c] * db_j;
+            if (iwet[j] * iwet[c] != 0) {
+              const double wb = fintp[fb] * hk[fb] * ds[fb];
+              guj += -gss[c] * wb * fnxd(idir[fb]);
+              gvj += -gss[c] * wb * fnyd(idir[fb]);
+            }
           }
         }
       }
@@ -525,6 +537,8 @@ __global__ void __launch_bounds__(TPB) k_pp_rhs_adjoint(
     if (gacoef_u)
       for (int k = 0; k < nmf; ++k) gacoef_u[(size_t)j * nmf + k] = k < nfj ? gasum : 0.0;
     if (gsp_u) gsp_u[j] = gsp;
+    if (gu) gu[j] = guj;
+    if (gv) gv[j] = gvj;
   }
 }
 
@@ -633,7 +647,7 @@ extern "C" int cms_pp_rhs_adjoint_dev_d(int ncells, int nmaxfaces, const int* ce
                                         const double* h, const double* dpx, const double* dpy, const double* p,
                                         const double* hk, const double* ds, const double* dn, const double* fintp,
                                         const double* grad_ss_pp, double* grad_acoef_u, double* grad_sp_u,
-                                        double* grad_hk, void* stream) {
+                                        double* grad_hk, double* grad_u, double* grad_v, void* stream) {
   if (ncells <= 0 || nmaxfaces <= 0 || nmaxfaces > 8 || relax <= 0.0 || !cell2cell || !ncface || !idirface ||
       !iwet || !acoef_u || !sp_u || !area || !u || !v || !h || !dpx || !dpy || !p || !hk || !ds || !dn || !fintp ||
       !grad_ss_pp)
@@ -641,7 +655,7 @@ extern "C" int cms_pp_rhs_adjoint_dev_d(int ncells, int nmaxfaces, const int* ce
   const int blocks = std::max(1, std::min((ncells + cms::TPB - 1) / cms::TPB, 148 * 8));
   cms::k_pp_rhs_adjoint<<<blocks, cms::TPB, 0, (cudaStream_t)stream>>>(
       ncells, nmaxfaces, cell2cell, ncface, idirface, iwet, relax, acoef_u, sp_u, area, u, v, h, dpx, dpy, p, hk, ds,
-      dn, fintp, grad_ss_pp, grad_acoef_u, grad_sp_u, grad_hk);
+      dn, fintp, grad_ss_pp, grad_acoef_u, grad_sp_u, grad_hk, grad_u, grad_v);
   return cms::fric_launch_check("cms_pp_rhs_adjoint_dev_d");
 }
 

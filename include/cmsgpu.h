@@ -262,8 +262,8 @@ int cms_pp_coef_adjoint_dev_d(int ncells, int nmaxfaces, const int* cell2cell, c
  * correction): Hu = u + ap dpx h, Hv = v + ap dpy h, flux(k,i) =
  * hk ds (nx Hu_f + ny Hv_f - ap_f hk (p_c - p_i) / dn) with the face values
  * interpolated as in cms_pp_coef_dev_d, ss_pp = sspp0 - sum_k flux + p sppp0.
- * Adjoint: given grad_ss_pp, writes dL/dacoef_u, dL/dsp_u (through ap) and
- * dL/dhk; outputs may be NULL. */
+ * Adjoint: given grad_ss_pp, writes dL/dacoef_u, dL/dsp_u (through ap),
+ * dL/dhk and dL/du, dL/dv (active cells); outputs may be NULL. */
 int cms_pp_rhs_dev_d(int ncells, int nmaxfaces, const int* cell2cell, const int* ncface, const int* idirface,
                      const int* iwet, double relax, const double* acoef_u, const double* sp_u, const double* area,
                      const double* u, const double* v, const double* h, const double* dpx, const double* dpy,
@@ -274,7 +274,7 @@ int cms_pp_rhs_adjoint_dev_d(int ncells, int nmaxfaces, const int* cell2cell, co
                              const double* area, const double* u, const double* v, const double* h, const double* dpx,
                              const double* dpy, const double* p, const double* hk, const double* ds, const double* dn,
                              const double* fintp, const double* grad_ss_pp, double* grad_acoef_u, double* grad_sp_u,
-                             double* grad_hk, void* stream);
+                             double* grad_hk, double* grad_u, double* grad_v, void* stream);
 /* Blocks (tiles) of the handle's persistent BiCGStab launch: 0 restores the
  * default (the device's resident capacity, at most one block per 256 rows);
  * returns the count in use, or a negative CMS_* code. */

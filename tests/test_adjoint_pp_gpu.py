@@ -302,3 +302,106 @@ def test_pp_system_gradient_matches_finite_differences():
         fd = (lp - lm) / (2 * eps)
         ad = float(r["gn"] @ dn_ + (r["ga"] * da).sum() + (r["gh"] * dh).sum())
         assert abs(ad - fd) <= 5e-5 * abs(fd), (ad, fd)
+
+
+# --- the momentum predictor in the chain: u, v = solve(acoef_u, su / sv, sp_u, .),
+# then the pressure-correction system from (n, acoef_u, hk, u, v)
+
+def _momentum_case(cs, seed):
+    rng = np.random.default_rng(seed)
+    g = cs["g"]
+    n, nD = g.ncells, g.ncellsD
+    cs = dict(cs)
+    cs["su"] = np.concatenate([rng.uniform(-2, 2, n), np.zeros(nD - n)])
+    cs["sv"] = np.concatenate([rng.uniform(-2, 2, n), np.zeros(nD - n)])
+    cs["u0"] = rng.uniform(-0.5, 0.5, nD)
+    cs["v0"] = rng.uniform(-0.5, 0.5, nD)
+    return cs
+
+
+def _uv_numpy(cs, nman, acoef_u):
+    g, n = cs["g"], cs["g"].ncells
+    sp_u = cs["spuv0"].copy()
+    sp_u[:n] = cs["spuv0"][:n] - _cd(nman, cs["h"]) * cs["uv"] * cs["area"][:n]
+    out = []
+    for rhs, x0 in ((cs["su"], cs["u0"]), (cs["sv"], cs["v0"])):
+        A, b = _system(g, acoef_u, rhs, sp_u, x0)
+        x = x0.copy()
+        x[:n] = spl.spsolve(A, b)
+        out.append(x)
+    return out
+
+
+def _system_numpy(cs, nman, acoef_u, hk):
+    u, v = _uv_numpy(cs, nman, acoef_u)
+    cs2 = dict(cs, u=u, v=v)
+    return _pp_numpy(cs, nman, acoef_u, hk), _rhs_numpy(cs2, nman, acoef_u, hk)
+
+
+def _run_outer(s, cs, nman, acoef_u, hk, grad=True):
+    from cms2d_b200.adjoint import friction_sink_fn, pp_coef_fn, pp_rhs_fn, solve_fn
+    g = cs["g"]
+    NM, AU, HK = _t(nman, grad), _t(acoef_u, grad), _t(hk, grad)
+    area = _t(cs["area"])
+    sp_u = friction_sink_fn(NM, _t(cs["h"]), _t(cs["uv"]), area, _t(cs["spuv0"]))
+    u = solve_fn(s, AU, _t(cs["su"]), sp_u, _t(cs["u0"]), relax=1.0, nswp=4000, tol=1e-9)
+    v = solve_fn(s, AU, _t(cs["sv"]), sp_u, _t(cs["v0"]), relax=1.0, nswp=4000, tol=1e-9)
+    i32 = lambda a: torch.tensor(np.ascontiguousarray(a, np.int32), device="cuda")
+    c2c, ncf, iwet = i32(cs["c2c"]), i32(g.ncface), i32(np.ones(g.ncellsD))
+    app = pp_coef_fn(c2c, ncf, iwet, g.ncells, RELAX, AU, sp_u, area, HK, _t(cs["ds"]), _t(cs["dn"]),
+                     _t(cs["fintp"]))
+    ssp = pp_rhs_fn(c2c, ncf, i32(cs["idir"]), iwet, g.ncells, RELAX, AU, sp_u, area, HK, _t(cs["ds"]),
+                    _t(cs["dn"]), _t(cs["fintp"]), u, v, _t(cs["hcell"]), _t(cs["dpx"]), _t(cs["dpy"]),
+                    _t(cs["p"]), _t(cs["sspp0"]), _t(cs["sppp0"]))
+    x = solve_fn(s, app, ssp, _t(cs["sp_pp"]), _t(cs["phi"]), relax=1.0, nswp=4000, tol=1e-9)
+    gi = torch.tensor(cs["gauges"], device="cuda")
+    loss = ((x[gi] - _t(cs["target"])) ** 2).sum()
+    out = {"loss": float(loss.detach()), "x": x.detach().cpu().numpy(), "u": u.detach().cpu().numpy()}
+    if grad:
+        loss.backward()
+        torch.cuda.synchronize()
+        out.update(gn=NM.grad.cpu().numpy(), ga=AU.grad.cpu().numpy(), gh=HK.grad.cpu().numpy())
+    return out
+
+
+def test_outer_iteration_gradient_matches_tangent_linear():
+    """n, the momentum coefficients and hk through the momentum predictor
+    (u and v solves) and the whole pressure-correction system."""
+    cs = _momentum_case(_case(111), 113)
+    g, n = cs["g"], cs["g"].ncells
+    s = _solver(g)
+    r = _run_outer(s, cs, cs["nman"], cs["acoef_u"], cs["hk"])
+    u_np, _ = _uv_numpy(cs, cs["nman"], cs["acoef_u"])
+    assert np.abs(r["u"][:n] - u_np[:n]).max() <= 1e-8 * np.abs(u_np[:n]).max()
+    app, rhs = _system_numpy(cs, cs["nman"], cs["acoef_u"], cs["hk"])
+    A, b = _system(g, app, rhs, cs["sp_pp"], cs["phi"])
+    xs = spl.spsolve(A, b)
+    assert np.abs(r["x"][:n] - xs).max() <= 1e-8 * np.abs(xs).max()
+    rng = np.random.default_rng(117)
+    for _ in range(3):
+        dn_, da, dh = _directions(cs, rng)
+        e = 1e-6
+        ap_p, rhs_p = _system_numpy(cs, cs["nman"] + e * dn_, cs["acoef_u"] + e * da, cs["hk"] + e * dh)
+        ap_m, rhs_m = _system_numpy(cs, cs["nman"] - e * dn_, cs["acoef_u"] - e * da, cs["hk"] - e * dh)
+        A1, b1 = _system(g, app + (ap_p - ap_m) / (2 * e), rhs + (rhs_p - rhs_m) / (2 * e), cs["sp_pp"], cs["phi"])
+        dx = spl.spsolve(A, (b1 - b) - (A1 - A) @ xs)
+        tl = float(2.0 * np.sum((xs[cs["gauges"]] - cs["target"]) * dx[cs["gauges"]]))
+        ad = float(r["gn"] @ dn_ + (r["ga"] * da).sum() + (r["gh"] * dh).sum())
+        assert abs(ad - tl) <= 1e-6 * max(abs(tl), 1e-30), (ad, tl)
+
+
+def test_outer_iteration_gradient_matches_finite_differences():
+    cs = _momentum_case(_case(119), 121)
+    s = _solver(cs["g"])
+    r = _run_outer(s, cs, cs["nman"], cs["acoef_u"], cs["hk"])
+    rng = np.random.default_rng(123)
+    for _ in range(2):
+        dn_, da, dh = _directions(cs, rng)
+        eps = 1e-4
+        lp = _run_outer(s, cs, cs["nman"] + eps * dn_, cs["acoef_u"] + eps * da, cs["hk"] + eps * dh,
+                        grad=False)["loss"]
+        lm = _run_outer(s, cs, cs["nman"] - eps * dn_, cs["acoef_u"] - eps * da, cs["hk"] - eps * dh,
+                        grad=False)["loss"]
+        fd = (lp - lm) / (2 * eps)
+        ad = float(r["gn"] @ dn_ + (r["ga"] * da).sum() + (r["gh"] * dh).sum())
+        assert abs(ad - fd) <= 5e-5 * abs(fd), (ad, fd)
