@@ -405,3 +405,49 @@ def test_outer_iteration_gradient_matches_finite_differences():
         fd = (lp - lm) / (2 * eps)
         ad = float(r["gn"] @ dn_ + (r["ga"] * da).sum() + (r["gh"] * dh).sum())
         assert abs(ad - fd) <= 5e-5 * abs(fd), (ad, fd)
+
+
+def test_water_level_misfit_gradient_matches_finite_differences():
+    """The loss config 5 names: gauge water-level misfit after the outer
+    iteration's pressure correction, eta = (p + pp) / g (pvfc with
+    relax_p = 1, flow_imp.F90:797-1072), as a function of per-cell Manning's n
+    through the chain above."""
+    from cms2d_b200.adjoint import friction_sink_fn, pp_coef_fn, pp_rhs_fn, solve_fn
+    cs = _momentum_case(_case(127), 129)
+    g = cs["g"]
+    s = _solver(g)
+    rng = np.random.default_rng(131)
+    eta_obs = rng.standard_normal(200) * 0.1
+
+    def loss(nman, grad):
+        NM = _t(nman, grad)
+        AU, HK, area = _t(cs["acoef_u"]), _t(cs["hk"]), _t(cs["area"])
+        sp_u = friction_sink_fn(NM, _t(cs["h"]), _t(cs["uv"]), area, _t(cs["spuv0"]))
+        u = solve_fn(s, AU, _t(cs["su"]), sp_u, _t(cs["u0"]), relax=1.0, nswp=4000, tol=1e-9)
+        v = solve_fn(s, AU, _t(cs["sv"]), sp_u, _t(cs["v0"]), relax=1.0, nswp=4000, tol=1e-9)
+        i32 = lambda a: torch.tensor(np.ascontiguousarray(a, np.int32), device="cuda")
+        c2c, ncf, iwet = i32(cs["c2c"]), i32(g.ncface), i32(np.ones(g.ncellsD))
+        app = pp_coef_fn(c2c, ncf, iwet, g.ncells, RELAX, AU, sp_u, area, HK, _t(cs["ds"]), _t(cs["dn"]),
+                         _t(cs["fintp"]))
+        ssp = pp_rhs_fn(c2c, ncf, i32(cs["idir"]), iwet, g.ncells, RELAX, AU, sp_u, area, HK, _t(cs["ds"]),
+                        _t(cs["dn"]), _t(cs["fintp"]), u, v, _t(cs["hcell"]), _t(cs["dpx"]), _t(cs["dpy"]),
+                        _t(cs["p"]), _t(cs["sspp0"]), _t(cs["sppp0"]))
+        pp = solve_fn(s, app, ssp, _t(cs["sp_pp"]), torch.zeros(g.ncellsD, dtype=torch.float64, device="cuda"),
+                      relax=1.0, nswp=4000, tol=1e-9)
+        gi = torch.tensor(cs["gauges"], device="cuda")
+        eta = (_t(cs["p"])[gi] + pp[gi]) / GRAV
+        L = ((eta - _t(eta_obs)) ** 2).sum()
+        if grad:
+            L.backward()
+            torch.cuda.synchronize()
+            return float(L.detach()), NM.grad.cpu().numpy()
+        return float(L.detach()), None
+
+    _, gn = loss(cs["nman"], True)
+    assert np.isfinite(gn).all() and np.abs(gn).max() > 0
+    for _ in range(2):
+        dn_ = cs["nman"] * rng.standard_normal(cs["nman"].shape)
+        eps = 1e-4
+        fd = (loss(cs["nman"] + eps * dn_, False)[0] - loss(cs["nman"] - eps * dn_, False)[0]) / (2 * eps)
+        ad = float(gn @ dn_)
+        assert abs(ad - fd) <= 5e-5 * abs(fd), (ad, fd)
